@@ -1,0 +1,330 @@
+"""Seeded procedural scenes for the BNEEPT/BVPT workloads, written out as Photon SDL (.p2) text.
+
+Every workload this library is measured on is generated here, in code, from a seed:
+
+* ``cornell``      -- Cornell box: 5 wall quads of a 555-unit box, two rotated boxes, one ceiling
+                      quad light of radiance (17, 12, 4); Lambertian albedos 0.73 / (0.65, 0.05,
+                      0.05) / (0.12, 0.45, 0.15); pinhole camera, 40 degree FOV.
+* ``ggx_sphere``   -- icosphere subdivided ``level`` times (20 * 4**level triangles), radially
+                      displaced by 3-octave value noise (amplitude 5 % of the radius) on a 2-triangle
+                      ground; GGX conductors in 64 material groups with roughness ~ U[0.05, 0.5]
+                      and F0 ~ U[0.5, 1]; 2 quad lights and a constant environment of 0.1.
+* ``slit_room``    -- 10 x 10 x 4 room filled with seeded boxes, lit only by a 1 x 1 quad behind a
+                      wall with a 0.05-wide slit; 70 % Lambertian / 30 % GGX dielectric groups.
+* ``city``         -- grid city of boxes with lognormal heights and many small emissive quads.
+
+The scene is described once (triangles, materials, emitters, camera) and serialised to SDL in
+the form the reference parser reads (``#version 1.1.0`` command syntax, see the reference's
+Engine/Source/SDL/SdlCommandParser.cpp:84-560 and SdlInlinePacketInterface.cpp:48-200), so the
+same text drives the reference CPU renderer and this library's ``phLoadCommands``/
+``phEnterCommand``.  All geometry is emitted in world space with identity actor transforms:
+the reference then intersects plain ``PTriangle`` primitives (Engine/Source/Actor/AModel.cpp:
+43-81 only wraps them in a transformed intersectable when the actor has a transform).
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+RGB = Tuple[float, float, float]
+
+
+@dataclasses.dataclass
+class Material:
+    """One surface material.
+
+    kind: "matte" (Lambertian, ``albedo``), "conductor" (GGX + Schlick, ``roughness``, ``f0``)
+    or "dielectric" (GGX + exact dielectric Fresnel, ``roughness``, ``ior_outer``,
+    ``ior_inner``).
+    """
+
+    kind: str
+    albedo: RGB = (0.5, 0.5, 0.5)
+    roughness: float = 0.5
+    f0: RGB = (1.0, 1.0, 1.0)
+    ior_outer: float = 1.0
+    ior_inner: float = 1.5
+
+
+@dataclasses.dataclass
+class MeshGroup:
+    """Triangles sharing one material; ``radiance`` set means the group is an area emitter."""
+
+    tris: np.ndarray  # float32 [N, 3, 3]
+    material: Material
+    radiance: Optional[RGB] = None
+
+
+@dataclasses.dataclass
+class Scene:
+    name: str
+    width: int
+    height: int
+    spp: int
+    max_bounces: int
+    cam_pos: RGB
+    cam_dir: RGB
+    cam_up: RGB
+    fov_deg: float
+    groups: List[MeshGroup]
+    estimator: str = "bneept"
+    env_radiance: Optional[RGB] = None
+
+    @property
+    def num_tris(self) -> int:
+        return int(sum(g.tris.shape[0] for g in self.groups))
+
+    @property
+    def num_paths(self) -> int:
+        return self.width * self.height * self.spp
+
+
+# ----------------------------------------------------------------------------------------------
+# geometry helpers
+
+def quad(a, b, c, d) -> np.ndarray:
+    """Two triangles (a, b, c) and (a, c, d); the face normal follows (b - a) x (c - a)."""
+    a, b, c, d = (np.asarray(v, np.float64) for v in (a, b, c, d))
+    return np.array([[a, b, c], [a, c, d]], np.float32)
+
+
+def box(center, size, yaw_deg: float = 0.0) -> np.ndarray:
+    """12 outward-facing triangles of a box rotated about +y by ``yaw_deg``."""
+    cx, cy, cz = center
+    sx, sy, sz = (s * 0.5 for s in size)
+    c, s = math.cos(math.radians(yaw_deg)), math.sin(math.radians(yaw_deg))
+
+    def p(x, y, z):
+        return (cx + c * x + s * z, cy + y, cz - s * x + c * z)
+
+    v = [p(x, y, z) for x in (-sx, sx) for y in (-sy, sy) for z in (-sz, sz)]
+    # v index = 4*ix + 2*iy + iz
+    faces = [
+        (0, 1, 3, 2),  # -x
+        (4, 6, 7, 5),  # +x
+        (0, 4, 5, 1),  # -y
+        (2, 3, 7, 6),  # +y
+        (0, 2, 6, 4),  # -z
+        (1, 5, 7, 3),  # +z
+    ]
+    return np.concatenate([quad(v[f[0]], v[f[1]], v[f[2]], v[f[3]]) for f in faces])
+
+
+def boxes_axis_aligned(mins: np.ndarray, maxs: np.ndarray) -> np.ndarray:
+    """Vectorised outward-facing 12-triangle boxes for arrays of corners [K, 3] -> [12K, 3, 3]."""
+    k = mins.shape[0]
+    corners = np.empty((k, 8, 3), np.float64)
+    for ix in range(2):
+        for iy in range(2):
+            for iz in range(2):
+                corners[:, 4 * ix + 2 * iy + iz] = np.stack(
+                    [(mins, maxs)[ix][:, 0], (mins, maxs)[iy][:, 1], (mins, maxs)[iz][:, 2]], 1)
+    faces = np.array([(0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1),
+                      (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)])
+    tri_idx = np.concatenate([faces[:, [0, 1, 2]], faces[:, [0, 2, 3]]], 0)  # [12, 3]
+    tris = corners[:, tri_idx]  # [K, 12, 3, 3]
+    return tris.reshape(-1, 3, 3).astype(np.float32)
+
+
+def icosphere(level: int) -> np.ndarray:
+    """Unit icosphere subdivided ``level`` times: [20 * 4**level, 3, 3] float64 outward-wound."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    verts = np.array([(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0),
+                      (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+                      (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)], np.float64)
+    verts /= np.linalg.norm(verts, axis=1, keepdims=True)
+    faces = np.array([(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11),
+                      (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6), (7, 1, 8),
+                      (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9),
+                      (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)])
+    tris = verts[faces]
+    for _ in range(level):
+        a, b, c = tris[:, 0], tris[:, 1], tris[:, 2]
+        ab, bc, ca = a + b, b + c, c + a
+        ab /= np.linalg.norm(ab, axis=1, keepdims=True)
+        bc /= np.linalg.norm(bc, axis=1, keepdims=True)
+        ca /= np.linalg.norm(ca, axis=1, keepdims=True)
+        tris = np.stack([np.stack([a, ab, ca], 1), np.stack([ab, b, bc], 1),
+                         np.stack([ca, bc, c], 1), np.stack([ab, bc, ca], 1)], 1).reshape(-1, 3, 3)
+    # make winding outward
+    n = np.cross(tris[:, 1] - tris[:, 0], tris[:, 2] - tris[:, 0])
+    flip = np.einsum("ij,ij->i", n, tris.mean(1)) < 0
+    tris[flip] = tris[flip][:, [0, 2, 1]]
+    return tris
+
+
+def value_noise3(p: np.ndarray, seed: int, octaves: int = 3) -> np.ndarray:
+    """Seeded 3-octave trilinear value noise in [-1, 1] at points p [N, 3]."""
+    rng = np.random.default_rng(seed)
+    table = rng.uniform(-1.0, 1.0, 4096)
+    perm = rng.permutation(4096)
+    total = np.zeros(p.shape[0])
+    amp, freq, norm = 1.0, 2.0, 0.0
+    for _ in range(octaves):
+        q = p * freq
+        i0 = np.floor(q).astype(np.int64)
+        f = q - i0
+        f = f * f * (3 - 2 * f)
+        acc = np.zeros(p.shape[0])
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    h = perm[(perm[(perm[(i0[:, 0] + dx) & 4095] + i0[:, 1] + dy) & 4095]
+                              + i0[:, 2] + dz) & 4095]
+                    w = ((f[:, 0] if dx else 1 - f[:, 0]) * (f[:, 1] if dy else 1 - f[:, 1])
+                         * (f[:, 2] if dz else 1 - f[:, 2]))
+                    acc += w * table[h]
+        total += amp * acc
+        norm += amp
+        amp *= 0.5
+        freq *= 2.0
+    return total / norm
+
+
+# ----------------------------------------------------------------------------------------------
+# workloads
+
+WHITE = Material("matte", albedo=(0.73, 0.73, 0.73))
+RED = Material("matte", albedo=(0.65, 0.05, 0.05))
+GREEN = Material("matte", albedo=(0.12, 0.45, 0.15))
+BLACK = Material("matte", albedo=(0.0, 0.0, 0.0))
+
+
+def cornell(width: int = 256, height: int = 256, spp: int = 64, max_bounces: int = 8,
+            estimator: str = "bneept") -> Scene:
+    """Cornell box (36 triangles) in a 555-unit box, camera looking down +z."""
+    L = 555.0
+    floor = quad((0, 0, 0), (0, 0, L), (L, 0, L), (L, 0, 0))            # normal +y
+    ceiling = quad((0, L, 0), (L, L, 0), (L, L, L), (0, L, L))          # normal -y
+    back = quad((0, 0, L), (0, L, L), (L, L, L), (L, 0, L))             # normal -z
+    left = quad((L, 0, 0), (L, 0, L), (L, L, L), (L, L, 0))             # x = L, normal -x (red)
+    right = quad((0, 0, 0), (0, L, 0), (0, L, L), (0, 0, L))            # x = 0, normal +x (green)
+    short_box = box((185.5, 82.5, 169.0), (165.0, 165.0, 165.0), -18.0)
+    tall_box = box((368.5, 165.0, 351.5), (165.0, 330.0, 165.0), 15.0)
+    light = quad((213, 554, 227), (343, 554, 227), (343, 554, 332), (213, 554, 332))  # normal -y
+    groups = [
+        MeshGroup(np.concatenate([floor, ceiling, back]), WHITE),
+        MeshGroup(left, RED),
+        MeshGroup(right, GREEN),
+        MeshGroup(np.concatenate([short_box, tall_box]), WHITE),
+        MeshGroup(light, BLACK, radiance=(17.0, 12.0, 4.0)),
+    ]
+    return Scene("cornell", width, height, spp, max_bounces,
+                 cam_pos=(278.0, 273.0, -800.0), cam_dir=(0.0, 0.0, 1.0), cam_up=(0.0, 1.0, 0.0),
+                 fov_deg=40.0, groups=groups, estimator=estimator)
+
+
+def ggx_sphere(level: int = 8, width: int = 1024, height: int = 1024, spp: int = 256,
+               max_bounces: int = 10, num_groups: int = 64, seed: int = 1,
+               with_env: bool = True, estimator: str = "bneept") -> Scene:
+    """Displaced GGX icosphere (20 * 4**level triangles) on a ground plane, 2 quad lights."""
+    R = 1.0
+    tris = icosphere(level)
+    flat = tris.reshape(-1, 3)
+    disp = 1.0 + 0.05 * value_noise3(flat, seed)
+    flat = flat * (R * disp)[:, None]
+    tris = flat.reshape(-1, 3, 3)
+    tris[:, :, 1] += R * 1.05  # sit on the ground
+    rng = np.random.default_rng(2)
+    rough = rng.uniform(0.05, 0.5, num_groups)
+    f0 = rng.uniform(0.5, 1.0, (num_groups, 3))
+    gid = np.arange(tris.shape[0]) % num_groups
+    groups = [MeshGroup(tris[gid == g].astype(np.float32),
+                        Material("conductor", roughness=float(rough[g]),
+                                 f0=tuple(float(x) for x in f0[g])))
+              for g in range(num_groups)]
+    G = 20.0
+    groups.append(MeshGroup(quad((-G, 0, -G), (-G, 0, G), (G, 0, G), (G, 0, -G)),
+                            Material("matte", albedo=(0.5, 0.5, 0.5))))
+    groups.append(MeshGroup(quad((-3, 5, -1), (-1, 5, -1), (-1, 5, 1), (-3, 5, 1)), BLACK,
+                            radiance=(8.0, 8.0, 8.0)))
+    groups.append(MeshGroup(quad((2, 4, 1.5), (3.5, 4, 1.5), (3.5, 3, 3.0), (2, 3, 3.0)), BLACK,
+                            radiance=(6.0, 6.0, 6.0)))
+    return Scene(f"ggx_sphere_l{level}", width, height, spp, max_bounces,
+                 cam_pos=(0.0, 1.6, -4.2), cam_dir=(0.0, -0.12, 1.0), cam_up=(0.0, 1.0, 0.0),
+                 fov_deg=45.0, groups=groups, estimator=estimator,
+                 env_radiance=(0.1, 0.1, 0.1) if with_env else None)
+
+
+# ----------------------------------------------------------------------------------------------
+# SDL serialisation
+
+
+def _f(x: float) -> str:
+    """Shortest text that round-trips to the same float32."""
+    return str(np.float32(x))
+
+
+def _v3(v) -> str:
+    return f"{_f(v[0])} {_f(v[1])} {_f(v[2])}"
+
+
+def _vec3_array(points: np.ndarray) -> str:
+    pts = np.asarray(points, np.float32).reshape(-1, 3)
+    return "{" + " ".join('"%s %s %s"' % (str(a), str(b), str(c)) for a, b, c in pts) + "}"
+
+
+def _zeros_array(n: int) -> str:
+    return "{" + " ".join(['"0 0 0"'] * n) + "}"
+
+
+def _material_sdl(name: str, m: Material, lines: List[str]) -> None:
+    if m.kind == "matte":
+        lines.append(f'image(constant) @{name}_albedo = [real-array values "{_v3(m.albedo)}"]'
+                     f"[enum color-space LSRGB];")
+        lines.append(f"material(matte-opaque) @{name} = [image albedo @{name}_albedo];")
+    elif m.kind == "conductor":
+        lines.append(f"material(abraded-opaque) @{name} = [enum microsurface ggx] "
+                     f'[real roughness {_f(m.roughness)}] [spectrum f0 "{_v3(m.f0)}"];')
+    elif m.kind == "dielectric":
+        lines.append(f"material(abraded-translucent) @{name} = [enum microsurface ggx] "
+                     f"[real roughness {_f(m.roughness)}] [real ior-outer {_f(m.ior_outer)}] "
+                     f"[real ior-inner {_f(m.ior_inner)}];")
+    else:
+        raise ValueError(f"unknown material kind {m.kind}")
+
+
+def to_sdl(scene: Scene, env_image_name: str = "env.pfm") -> str:
+    """The whole scene as SDL 1.1 command text."""
+    lines = [
+        "#version 1.1.0;",
+        "option(single-frame-render-session) @session = "
+        f'[vector2 frame-size "{scene.width} {scene.height}"] [string visualizer @visualizer] '
+        "[string observer @observer] [string sample-source @sampler];",
+        f"observer(single-lens) @observer = [real fov-degrees {_f(scene.fov_deg)}] "
+        f'[vector3 pos "{_v3(scene.cam_pos)}"] [vector3 dir "{_v3(scene.cam_dir)}"] '
+        f'[vector3 up-axis "{_v3(scene.cam_up)}"];',
+        f"sample-source(stratified) @sampler = [integer samples {scene.spp}];",
+        "visualizer(path-tracing) @visualizer = [enum sample-filter box] "
+        f"[enum estimator {scene.estimator}];",
+    ]
+    for gi, g in enumerate(scene.groups):
+        mname = f"m{gi}"
+        _material_sdl(mname, g.material, lines)
+        n = g.tris.shape[0] * 3
+        lines.append(f"geometry(triangle-mesh) @g{gi} = "
+                     f"[vector3-array positions {_vec3_array(g.tris)}] "
+                     f"[vector3-array texture-coordinates {_zeros_array(n)}] "
+                     f"[vector3-array normals {_zeros_array(n)}];")
+        if g.radiance is None:
+            lines.append(f"actor(model) @a{gi} = [geometry geometry @g{gi}] [material material @{mname}];")
+        else:
+            lines.append(f'image(constant) @e{gi} = [real-array values "{_v3(g.radiance)}"]'
+                         f"[enum color-space LSRGB];")
+            lines.append(f"actor(model-light) @a{gi} = [geometry geometry @g{gi}] "
+                         f"[material material @{mname}] [image emitted-energy @e{gi}];")
+    if scene.env_radiance is not None:
+        lines.append(f'actor(image-dome) @dome = [resource-identifier? image-file "{env_image_name}"];')
+    return "\n".join(lines) + "\n"
+
+
+def write_pfm(path: str, rgb: np.ndarray) -> None:
+    """Little-endian colour PFM, rows stored bottom to top."""
+    h, w, _ = rgb.shape
+    with open(path, "wb") as f:
+        f.write(f"PF\n{w} {h}\n-1.0\n".encode())
+        f.write(np.ascontiguousarray(rgb[::-1], dtype="<f4").tobytes())
