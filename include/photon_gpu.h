@@ -1,0 +1,86 @@
+/* Low-level C ABI of the B200 path-tracing core (libphoton_gpu.so).
+ *
+ * Plain pointers and sizes only. Every function returns 0 on success or a nonzero status code
+ * (see pg::Status in photon-v2_b200/csrc/pg_common.cuh); pgpu_last_error() returns the message of
+ * the most recent failure on the calling thread. These entry points sit below the Photon C API
+ * (ph_c_core.h, also exported by this library) and expose the hot-path stages one by one so that
+ * each can be checked against the reference and measured on its own.
+ */
+#ifndef PHOTON_GPU_H
+#define PHOTON_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PGPU_API __attribute__((visibility("default")))
+#else
+#define PGPU_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Message of the last failed call on this thread ("" if none). */
+PGPU_API const char* pgpu_last_error(void);
+
+/* Number of CUDA devices visible (0 without a GPU). Never fails. */
+PGPU_API int pgpu_device_count(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Geometry: a triangle soup with its compressed 8-wide BVH resident on the current device.
+ *
+ * Replaces the reference TLAS build over cooked PTriangles:
+ *   TBinaryBvhIntersector<Index>::update/rebuildWithIntersectables
+ *   (Engine/Source/Core/Intersection/BVH/TBinaryBvhIntersector.ipp:20-97), built by
+ *   TBvhBuilder<2> (Engine/Source/Math/Algorithm/BVH/TBvhBuilder.ipp:36).
+ * tris: float32 [num_tris][3][3] host array. max_origin_abs: largest |coordinate| of any ray
+ * origin that will be traced (sizes the conservative box padding; 0 = scene bound only).
+ */
+PGPU_API int pgpu_geometry_create(const float* tris, uint64_t num_tris, float max_origin_abs, uint64_t* out_id);
+PGPU_API int pgpu_geometry_destroy(uint64_t id);
+/* num_nodes, num_tris, wide-tree depth, host build seconds. Any output may be NULL. */
+PGPU_API int pgpu_geometry_stats(uint64_t id, uint64_t* out_num_nodes, uint64_t* out_num_tris,
+                        int32_t* out_max_depth, double* out_build_seconds);
+
+/* Closest hit for host rays [n][8] = origin(3), minT, direction(3), maxT (two float4 per ray).
+ * Replaces TBinaryBvhIntersector::isIntersecting (TBinaryBvhIntersector.ipp:27-50) and
+ * TWatertightTriangle::isIntersecting (Engine/Source/Math/Geometry/TWatertightTriangle.ipp:16-149).
+ * Outputs (host): prim index in input order or -1, hit t, barycentrics [n][3] (any may be NULL). */
+PGPU_API int pgpu_trace_closest(uint64_t id, const float* rays, uint64_t n,
+                       int32_t* out_prim, float* out_t, float* out_bary);
+
+/* Occlusion for host rays [n][8]; out_occluded[i] = 1 if any triangle is hit in [minT, maxT].
+ * Replaces Scene::isOccluding / Intersectable::isOccluding (Engine/Source/World/Scene.cpp:54-69,
+ * Engine/Source/Core/Intersection/Intersectable.cpp:8). */
+PGPU_API int pgpu_trace_any(uint64_t id, const float* rays, uint64_t n, int32_t* out_occluded);
+
+/* Device-resident variants for throughput measurement: d_rays is a device pointer to [n][8]
+ * float32, d_hits a device pointer to [n] x (uint32 leaf triangle or 0xFFFFFFFF, float32 t).
+ * The launch runs on the library's stream; *out_ms (optional) receives the kernel time
+ * measured with CUDA events on that stream. */
+PGPU_API int pgpu_trace_closest_device(uint64_t id, const float* d_rays, uint64_t n, void* d_hits, float* out_ms);
+PGPU_API int pgpu_trace_any_device(uint64_t id, const float* d_rays, uint64_t n, int32_t* d_occluded, float* out_ms);
+
+/* Mean BVH nodes visited and triangles tested per ray over the given host rays (a counting
+ * pass of the same traversal), for the algorithmic-bytes model of the roofline. */
+PGPU_API int pgpu_trace_counts(uint64_t id, const float* rays, uint64_t n, int any_hit,
+                      double* out_nodes_per_ray, double* out_tris_per_ray);
+
+/* ---------------------------------------------------------------------------------------------
+ * BSDF kernels, evaluated one case per thread on the GPU with the same device functions the path
+ * tracer uses. cases: float32 [n][19] (type, p0..p5, N(3), V(3), L(3), u(3)) with
+ *   type 0 Lambertian (p0..p2 albedo)                   LambertianReflector.cpp:39-99
+ *   type 1 GGX conductor (p0 roughness, p1..p3 F0)      OpaqueMicrofacet.cpp:59-155
+ *   type 2 GGX dielectric (p0 roughness, p1 ior outer, p2 ior inner) TranslucentMicrofacet.cpp:62-364
+ * and normals: float32 [n][6] = geometry normal, shading normal.
+ * out: float32 [n][16] = eval_ok, bsdf(3), pdf_ok, pdfW, sample_ok, L(3),
+ *      pdfAppliedBsdfCos(3), relativeIor, cos, 0. Strict sidedness, radiance transport. */
+PGPU_API int pgpu_bsdf_eval(const float* cases, const float* normals, uint64_t n, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHOTON_GPU_H */

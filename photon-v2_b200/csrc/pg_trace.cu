@@ -1,0 +1,404 @@
+// Geometry objects (triangles + compressed 8-wide BVH in HBM) and the ray-query entry points of
+// the C ABI (include/photon_gpu.h): closest hit, occlusion, and the counting pass.
+#include "pg_geometry.h"
+#include "trace.cuh"
+
+#include "../../include/photon_gpu.h"
+
+#include <algorithm>
+#include <vector>
+
+namespace pg
+{
+
+Registry<Geometry>& geometry_registry()
+{
+	static Registry<Geometry> r;
+	return r;
+}
+
+std::unique_ptr<Geometry> make_geometry(const BvhBuildInput& in)
+{
+	require_device();
+	auto g = std::make_unique<Geometry>();
+	WideBvh bvh = build_wide_bvh(in);
+	g->stats = bvh.stats;
+	g->nodes.resize(bvh.nodes.size());
+	g->tris.resize(bvh.tris.size());
+	cudaStream_t s = library_stream();
+	PG_CUDA_CHECK(cudaMemcpyAsync(g->nodes.get(), bvh.nodes.data(), g->nodes.bytes(), cudaMemcpyHostToDevice, s));
+	PG_CUDA_CHECK(cudaMemcpyAsync(g->tris.get(), bvh.tris.data(), g->tris.bytes(), cudaMemcpyHostToDevice, s));
+	g->error.resize(1);
+	PG_CUDA_CHECK(cudaMemsetAsync(g->error.get(), 0, sizeof(uint32_t), s));
+	PG_CUDA_CHECK(cudaStreamSynchronize(s));
+	return g;
+}
+
+namespace
+{
+
+constexpr int kTraceBlock = 128;
+
+struct HitRecord
+{
+	uint32_t tri;
+	float    t;
+};
+
+__global__ void __launch_bounds__(kTraceBlock)
+trace_closest_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
+                     const float4* __restrict__ rays, uint64_t n,
+                     HitRecord* __restrict__ hits, uint32_t* __restrict__ error)
+{
+	uint32_t err = 0;
+	for(uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+	    i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+	{
+		const float4 a = __ldg(rays + 2 * i);
+		const float4 b = __ldg(rays + 2 * i + 1);
+		const RayTraits r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
+		float t;
+		uint32_t tri;
+		const bool hit = traverse<false>(r, nodes, tris, a.w, b.w, &t, &tri, &err);
+		hits[i] = HitRecord{hit ? tri : 0xFFFFFFFFu, hit ? t : 0.0f};
+	}
+	if(err)
+	{
+		atomicOr(error, err);
+	}
+}
+
+__global__ void __launch_bounds__(kTraceBlock)
+trace_any_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
+                 const float4* __restrict__ rays, uint64_t n,
+                 int32_t* __restrict__ occluded, uint32_t* __restrict__ error)
+{
+	uint32_t err = 0;
+	for(uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+	    i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+	{
+		const float4 a = __ldg(rays + 2 * i);
+		const float4 b = __ldg(rays + 2 * i + 1);
+		const RayTraits r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
+		float t;
+		uint32_t tri;
+		occluded[i] = traverse<true>(r, nodes, tris, a.w, b.w, &t, &tri, &err) ? 1 : 0;
+	}
+	if(err)
+	{
+		atomicOr(error, err);
+	}
+}
+
+// Re-runs the winning triangle's test to report the reference-facing results: primitive index in
+// input order and the barycentrics (identical arithmetic, so identical bits).
+__global__ void resolve_hits_kernel(const LeafTri* __restrict__ tris, const float4* __restrict__ rays,
+                                    const HitRecord* __restrict__ hits, uint64_t n,
+                                    int32_t* __restrict__ prim, float* __restrict__ t_out,
+                                    float* __restrict__ bary)
+{
+	const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+	if(i >= n)
+	{
+		return;
+	}
+	const HitRecord h = hits[i];
+	if(h.tri == 0xFFFFFFFFu)
+	{
+		prim[i] = -1;
+		t_out[i] = 0.0f;
+		bary[3 * i + 0] = bary[3 * i + 1] = bary[3 * i + 2] = 0.0f;
+		return;
+	}
+	const float4 a = rays[2 * i];
+	const float4 b = rays[2 * i + 1];
+	const RayTraits r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
+	float t, b0, b1, b2;
+	// The winning triangle passed with some maxT >= its t, so it passes again with the ray's own
+	// range and yields the same bits.
+	watertight_hit_tri(r, tris, h.tri, a.w, b.w, &t, &b0, &b1, &b2);
+	prim[i] = static_cast<int32_t>(tris[h.tri].prim);
+	t_out[i] = h.t;
+	bary[3 * i + 0] = b0;
+	bary[3 * i + 1] = b1;
+	bary[3 * i + 2] = b2;
+}
+
+__global__ void count_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
+                             const float4* __restrict__ rays, uint64_t n, int any_hit,
+                             unsigned long long* __restrict__ sums, uint32_t* __restrict__ error)
+{
+	const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+	uint32_t nodes_visited = 0, tris_tested = 0, err = 0;
+	if(i < n)
+	{
+		const float4 a = rays[2 * i];
+		const float4 b = rays[2 * i + 1];
+		const RayTraits r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
+		float t;
+		uint32_t tri;
+		if(any_hit)
+		{
+			traverse<true, true>(r, nodes, tris, a.w, b.w, &t, &tri, &err, &nodes_visited, &tris_tested);
+		}
+		else
+		{
+			traverse<false, true>(r, nodes, tris, a.w, b.w, &t, &tri, &err, &nodes_visited, &tris_tested);
+		}
+	}
+	atomicAdd(&sums[0], static_cast<unsigned long long>(nodes_visited));
+	atomicAdd(&sums[1], static_cast<unsigned long long>(tris_tested));
+	if(err)
+	{
+		atomicOr(error, err);
+	}
+}
+
+int grid_for(uint64_t n, int block)
+{
+	const uint64_t blocks = (n + block - 1) / block;
+	const uint64_t cap = static_cast<uint64_t>(sm_count()) * 16;
+	return static_cast<int>(std::max<uint64_t>(1, std::min(blocks, cap)));
+}
+
+std::shared_ptr<Geometry> get_geometry(uint64_t id)
+{
+	auto g = geometry_registry().get(id);
+	if(!g)
+	{
+		throw Error(PG_ERR_NOT_FOUND, "unknown geometry id " + std::to_string(id));
+	}
+	return g;
+}
+
+void check_device_error(Geometry& g, cudaStream_t s)
+{
+	uint32_t flags = 0;
+	PG_CUDA_CHECK(cudaMemcpyAsync(&flags, g.error.get(), sizeof(flags), cudaMemcpyDeviceToHost, s));
+	PG_CUDA_CHECK(cudaStreamSynchronize(s));
+	if(flags & PG_DEV_ERR_STACK)
+	{
+		PG_CUDA_CHECK(cudaMemsetAsync(g.error.get(), 0, sizeof(uint32_t), s));
+		throw Error(PG_ERR_STACK_OVERFLOW, "BVH traversal stack overflow");
+	}
+}
+
+}// end anonymous namespace
+
+void launch_trace_closest(const Geometry& g, const float* d_rays, uint64_t n, void* d_hits, cudaStream_t s)
+{
+	if(n == 0)
+	{
+		return;
+	}
+	trace_closest_kernel<<<grid_for(n, kTraceBlock), kTraceBlock, 0, s>>>(
+		g.nodes.get(), g.tris.get(), reinterpret_cast<const float4*>(d_rays), n,
+		reinterpret_cast<HitRecord*>(d_hits), g.error.get());
+	PG_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_trace_any(const Geometry& g, const float* d_rays, uint64_t n, int32_t* d_occluded, cudaStream_t s)
+{
+	if(n == 0)
+	{
+		return;
+	}
+	trace_any_kernel<<<grid_for(n, kTraceBlock), kTraceBlock, 0, s>>>(
+		g.nodes.get(), g.tris.get(), reinterpret_cast<const float4*>(d_rays), n, d_occluded, g.error.get());
+	PG_CUDA_CHECK(cudaGetLastError());
+}
+
+}// end namespace pg
+
+using namespace pg;
+
+extern "C" {
+
+const char* pgpu_last_error(void)
+{
+	return pg::last_error();
+}
+
+int pgpu_device_count(void)
+{
+	int n = 0;
+	if(cudaGetDeviceCount(&n) != cudaSuccess)
+	{
+		cudaGetLastError();
+		return 0;
+	}
+	return n;
+}
+
+int pgpu_geometry_create(const float* tris, uint64_t num_tris, float max_origin_abs, uint64_t* out_id)
+{
+	return guarded([&]
+	{
+		if(!tris || num_tris == 0 || !out_id)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_geometry_create: empty input");
+		}
+		BvhBuildInput in{tris, nullptr, nullptr, static_cast<std::size_t>(num_tris), max_origin_abs};
+		*out_id = geometry_registry().add(make_geometry(in));
+	});
+}
+
+int pgpu_geometry_destroy(uint64_t id)
+{
+	return guarded([&]
+	{
+		if(!geometry_registry().remove(id))
+		{
+			throw Error(PG_ERR_NOT_FOUND, "unknown geometry id " + std::to_string(id));
+		}
+	});
+}
+
+int pgpu_geometry_stats(uint64_t id, uint64_t* out_num_nodes, uint64_t* out_num_tris,
+                        int32_t* out_max_depth, double* out_build_seconds)
+{
+	return guarded([&]
+	{
+		auto g = get_geometry(id);
+		if(out_num_nodes) { *out_num_nodes = g->stats.num_nodes; }
+		if(out_num_tris) { *out_num_tris = g->stats.num_leaf_tris; }
+		if(out_max_depth) { *out_max_depth = g->stats.max_depth; }
+		if(out_build_seconds) { *out_build_seconds = g->stats.build_seconds; }
+	});
+}
+
+int pgpu_trace_closest(uint64_t id, const float* rays, uint64_t n,
+                       int32_t* out_prim, float* out_t, float* out_bary)
+{
+	return guarded([&]
+	{
+		if(!rays && n > 0)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_trace_closest: null rays");
+		}
+		auto g = get_geometry(id);
+		if(n == 0)
+		{
+			return;
+		}
+		cudaStream_t s = library_stream();
+		DeviceBuffer<float> d_rays(n * 8);
+		DeviceBuffer<HitRecord> d_hits(n);
+		DeviceBuffer<int32_t> d_prim(n);
+		DeviceBuffer<float> d_t(n), d_bary(3 * n);
+		PG_CUDA_CHECK(cudaMemcpyAsync(d_rays.get(), rays, d_rays.bytes(), cudaMemcpyHostToDevice, s));
+		launch_trace_closest(*g, d_rays.get(), n, d_hits.get(), s);
+		resolve_hits_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(
+			g->tris.get(), reinterpret_cast<const float4*>(d_rays.get()), d_hits.get(), n,
+			d_prim.get(), d_t.get(), d_bary.get());
+		PG_CUDA_CHECK(cudaGetLastError());
+		std::vector<int32_t> prim(n);
+		std::vector<float> t(n), bary(3 * n);
+		PG_CUDA_CHECK(cudaMemcpyAsync(prim.data(), d_prim.get(), d_prim.bytes(), cudaMemcpyDeviceToHost, s));
+		PG_CUDA_CHECK(cudaMemcpyAsync(t.data(), d_t.get(), d_t.bytes(), cudaMemcpyDeviceToHost, s));
+		PG_CUDA_CHECK(cudaMemcpyAsync(bary.data(), d_bary.get(), d_bary.bytes(), cudaMemcpyDeviceToHost, s));
+		PG_CUDA_CHECK(cudaStreamSynchronize(s));
+		check_device_error(*g, s);
+		if(out_prim) { std::copy(prim.begin(), prim.end(), out_prim); }
+		if(out_t) { std::copy(t.begin(), t.end(), out_t); }
+		if(out_bary) { std::copy(bary.begin(), bary.end(), out_bary); }
+	});
+}
+
+int pgpu_trace_any(uint64_t id, const float* rays, uint64_t n, int32_t* out_occluded)
+{
+	return guarded([&]
+	{
+		if((!rays || !out_occluded) && n > 0)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_trace_any: null pointer");
+		}
+		auto g = get_geometry(id);
+		if(n == 0)
+		{
+			return;
+		}
+		cudaStream_t s = library_stream();
+		DeviceBuffer<float> d_rays(n * 8);
+		DeviceBuffer<int32_t> d_occ(n);
+		PG_CUDA_CHECK(cudaMemcpyAsync(d_rays.get(), rays, d_rays.bytes(), cudaMemcpyHostToDevice, s));
+		launch_trace_any(*g, d_rays.get(), n, d_occ.get(), s);
+		PG_CUDA_CHECK(cudaMemcpyAsync(out_occluded, d_occ.get(), d_occ.bytes(), cudaMemcpyDeviceToHost, s));
+		PG_CUDA_CHECK(cudaStreamSynchronize(s));
+		check_device_error(*g, s);
+	});
+}
+
+int pgpu_trace_closest_device(uint64_t id, const float* d_rays, uint64_t n, void* d_hits, float* out_ms)
+{
+	return guarded([&]
+	{
+		auto g = get_geometry(id);
+		cudaStream_t s = library_stream();
+		cudaEvent_t e0, e1;
+		PG_CUDA_CHECK(cudaEventCreate(&e0));
+		PG_CUDA_CHECK(cudaEventCreate(&e1));
+		PG_CUDA_CHECK(cudaEventRecord(e0, s));
+		launch_trace_closest(*g, d_rays, n, d_hits, s);
+		PG_CUDA_CHECK(cudaEventRecord(e1, s));
+		PG_CUDA_CHECK(cudaEventSynchronize(e1));
+		float ms = 0.0f;
+		PG_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+		cudaEventDestroy(e0);
+		cudaEventDestroy(e1);
+		check_device_error(*g, s);
+		if(out_ms) { *out_ms = ms; }
+	});
+}
+
+int pgpu_trace_any_device(uint64_t id, const float* d_rays, uint64_t n, int32_t* d_occluded, float* out_ms)
+{
+	return guarded([&]
+	{
+		auto g = get_geometry(id);
+		cudaStream_t s = library_stream();
+		cudaEvent_t e0, e1;
+		PG_CUDA_CHECK(cudaEventCreate(&e0));
+		PG_CUDA_CHECK(cudaEventCreate(&e1));
+		PG_CUDA_CHECK(cudaEventRecord(e0, s));
+		launch_trace_any(*g, d_rays, n, d_occluded, s);
+		PG_CUDA_CHECK(cudaEventRecord(e1, s));
+		PG_CUDA_CHECK(cudaEventSynchronize(e1));
+		float ms = 0.0f;
+		PG_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+		cudaEventDestroy(e0);
+		cudaEventDestroy(e1);
+		check_device_error(*g, s);
+		if(out_ms) { *out_ms = ms; }
+	});
+}
+
+int pgpu_trace_counts(uint64_t id, const float* rays, uint64_t n, int any_hit,
+                      double* out_nodes_per_ray, double* out_tris_per_ray)
+{
+	return guarded([&]
+	{
+		auto g = get_geometry(id);
+		if(n == 0 || !rays)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_trace_counts: no rays");
+		}
+		cudaStream_t s = library_stream();
+		DeviceBuffer<float> d_rays(n * 8);
+		DeviceBuffer<unsigned long long> d_sums(2);
+		PG_CUDA_CHECK(cudaMemcpyAsync(d_rays.get(), rays, d_rays.bytes(), cudaMemcpyHostToDevice, s));
+		PG_CUDA_CHECK(cudaMemsetAsync(d_sums.get(), 0, d_sums.bytes(), s));
+		count_kernel<<<static_cast<unsigned>((n + 127) / 128), 128, 0, s>>>(
+			g->nodes.get(), g->tris.get(), reinterpret_cast<const float4*>(d_rays.get()), n, any_hit,
+			d_sums.get(), g->error.get());
+		PG_CUDA_CHECK(cudaGetLastError());
+		unsigned long long sums[2] = {0, 0};
+		PG_CUDA_CHECK(cudaMemcpyAsync(sums, d_sums.get(), sizeof(sums), cudaMemcpyDeviceToHost, s));
+		PG_CUDA_CHECK(cudaStreamSynchronize(s));
+		check_device_error(*g, s);
+		if(out_nodes_per_ray) { *out_nodes_per_ray = static_cast<double>(sums[0]) / n; }
+		if(out_tris_per_ray) { *out_tris_per_ray = static_cast<double>(sums[1]) / n; }
+	});
+}
+
+}// extern "C"

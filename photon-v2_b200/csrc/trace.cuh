@@ -1,0 +1,335 @@
+// Ray traversal of the compressed 8-wide BVH with watertight FP32 triangle tests.
+//
+// Closest hit replaces the reference's TLAS query
+//   TBinaryBvhIntersector::isIntersecting (Engine/Source/Core/Intersection/BVH/
+//   TBinaryBvhIntersector.ipp:27-50) -> TLinearDepthFirstBinaryBvh::nearestTraversal
+//   (Engine/Source/Math/Algorithm/BVH/TLinearDepthFirstBinaryBvh.ipp:45-138)
+//   -> PTriangle::isIntersecting (Engine/Source/Core/Intersection/PTriangle.cpp:37-49)
+//   -> TWatertightTriangle::isIntersecting (Engine/Source/Math/Geometry/TWatertightTriangle.ipp:16-149)
+// and any hit replaces Scene::isOccluding (Engine/Source/World/Scene.cpp:54-69), which in the
+// reference runs the same nearest traversal without an early exit; the boolean is identical.
+#pragma once
+
+#include "pg_common.cuh"
+
+namespace pg
+{
+
+// Per-ray constants of the watertight test (axis permutation and shear) and of the slab test.
+struct RayTraits
+{
+	float ox, oy, oz;
+	float dx, dy, dz;
+	int   kx, ky, kz;
+	float sx, sy, sz;
+	float rdx, rdy, rdz;     // reciprocal direction for the slab test (zero components nudged)
+	float obx, oby, obz;     // origin * reciprocal direction
+	uint32_t oct;            // bit a set <=> direction component a is negative
+};
+
+__device__ __forceinline__ float pick3(float a, float b, float c, int k)
+{
+	return k == 0 ? a : (k == 1 ? b : c);
+}
+
+__device__ __forceinline__ RayTraits make_ray_traits(float ox, float oy, float oz, float dx, float dy, float dz)
+{
+	RayTraits r;
+	r.ox = ox; r.oy = oy; r.oz = oz;
+	r.dx = dx; r.dy = dy; r.dz = dz;
+
+	// Dominant axis becomes z; the others keep the reference's cyclic order
+	// (TWatertightTriangle.ipp:31-62).
+	const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
+	if(ax > ay)
+	{
+		if(ax > az) { r.kx = 1; r.ky = 2; r.kz = 0; }
+		else        { r.kx = 0; r.ky = 1; r.kz = 2; }
+	}
+	else
+	{
+		if(ay > az) { r.kx = 2; r.ky = 0; r.kz = 1; }
+		else        { r.kx = 0; r.ky = 1; r.kz = 2; }
+	}
+	const float dkx = pick3(dx, dy, dz, r.kx);
+	const float dky = pick3(dx, dy, dz, r.ky);
+	const float dkz = pick3(dx, dy, dz, r.kz);
+	const float rcp_z = __fdiv_rn(1.0f, dkz);
+	r.sx = __fmul_rn(-dkx, rcp_z);
+	r.sy = __fmul_rn(-dky, rcp_z);
+	r.sz = rcp_z;
+
+	const float tiny = 1e-20f;
+	r.rdx = 1.0f / (fabsf(dx) > tiny ? dx : copysignf(tiny, dx));
+	r.rdy = 1.0f / (fabsf(dy) > tiny ? dy : copysignf(tiny, dy));
+	r.rdz = 1.0f / (fabsf(dz) > tiny ? dz : copysignf(tiny, dz));
+	r.obx = ox * r.rdx;
+	r.oby = oy * r.rdy;
+	r.obz = oz * r.rdz;
+	r.oct = (dx < 0.0f ? 1u : 0u) | (dy < 0.0f ? 2u : 0u) | (dz < 0.0f ? 4u : 0u);
+	return r;
+}
+
+// Watertight ray/triangle test, arithmetic identical to TWatertightTriangle::isIntersecting
+// (TWatertightTriangle.ipp:16-149) including operand order, the FP64 recomputation of zero edge
+// functions (:85-100) and the inclusive [minT, maxT] range in scaled form (:119-133). Every
+// FP32 operation is an explicitly rounded intrinsic so that no FMA contraction changes bits.
+__device__ __forceinline__ bool watertight_hit(
+	const RayTraits& r,
+	float ax, float ay, float az,
+	float bx, float by, float bz,
+	float cx, float cy, float cz,
+	float min_t, float max_t,
+	float* out_t, float* out_b0, float* out_b1, float* out_b2)
+{
+	const float Ax = __fsub_rn(ax, r.ox), Ay = __fsub_rn(ay, r.oy), Az = __fsub_rn(az, r.oz);
+	const float Bx = __fsub_rn(bx, r.ox), By = __fsub_rn(by, r.oy), Bz = __fsub_rn(bz, r.oz);
+	const float Cx = __fsub_rn(cx, r.ox), Cy = __fsub_rn(cy, r.oy), Cz = __fsub_rn(cz, r.oz);
+
+	float atx = pick3(Ax, Ay, Az, r.kx), aty = pick3(Ax, Ay, Az, r.ky), atz = pick3(Ax, Ay, Az, r.kz);
+	float btx = pick3(Bx, By, Bz, r.kx), bty = pick3(Bx, By, Bz, r.ky), btz = pick3(Bx, By, Bz, r.kz);
+	float ctx = pick3(Cx, Cy, Cz, r.kx), cty = pick3(Cx, Cy, Cz, r.ky), ctz = pick3(Cx, Cy, Cz, r.kz);
+
+	atx = __fadd_rn(atx, __fmul_rn(r.sx, atz));
+	aty = __fadd_rn(aty, __fmul_rn(r.sy, atz));
+	btx = __fadd_rn(btx, __fmul_rn(r.sx, btz));
+	bty = __fadd_rn(bty, __fmul_rn(r.sy, btz));
+	ctx = __fadd_rn(ctx, __fmul_rn(r.sx, ctz));
+	cty = __fadd_rn(cty, __fmul_rn(r.sy, ctz));
+
+	float ea = __fsub_rn(__fmul_rn(btx, cty), __fmul_rn(bty, ctx));
+	float eb = __fsub_rn(__fmul_rn(ctx, aty), __fmul_rn(cty, atx));
+	float ec = __fsub_rn(__fmul_rn(atx, bty), __fmul_rn(aty, btx));
+
+	if(ea == 0.0f || eb == 0.0f || ec == 0.0f)
+	{
+		const double ea64 = __dsub_rn(__dmul_rn((double)btx, (double)cty), __dmul_rn((double)bty, (double)ctx));
+		const double eb64 = __dsub_rn(__dmul_rn((double)ctx, (double)aty), __dmul_rn((double)cty, (double)atx));
+		const double ec64 = __dsub_rn(__dmul_rn((double)atx, (double)bty), __dmul_rn((double)aty, (double)btx));
+		ea = __double2float_rn(ea64);
+		eb = __double2float_rn(eb64);
+		ec = __double2float_rn(ec64);
+	}
+
+	if((ea < 0.0f || eb < 0.0f || ec < 0.0f) && (ea > 0.0f || eb > 0.0f || ec > 0.0f))
+	{
+		return false;
+	}
+
+	const float det = __fadd_rn(__fadd_rn(ea, eb), ec);
+	if(det == 0.0f || !isfinite(det))
+	{
+		return false;
+	}
+
+	atz = __fmul_rn(atz, r.sz);
+	btz = __fmul_rn(btz, r.sz);
+	ctz = __fmul_rn(ctz, r.sz);
+	const float t_scaled = __fadd_rn(__fadd_rn(__fmul_rn(ea, atz), __fmul_rn(eb, btz)), __fmul_rn(ec, ctz));
+	if(det > 0.0f)
+	{
+		if(t_scaled < __fmul_rn(min_t, det) || t_scaled > __fmul_rn(max_t, det))
+		{
+			return false;
+		}
+	}
+	else
+	{
+		if(t_scaled > __fmul_rn(min_t, det) || t_scaled < __fmul_rn(max_t, det))
+		{
+			return false;
+		}
+	}
+
+	const float rcp_det = __fdiv_rn(1.0f, det);
+	*out_b0 = __fmul_rn(ea, rcp_det);
+	*out_b1 = __fmul_rn(eb, rcp_det);
+	*out_b2 = __fmul_rn(ec, rcp_det);
+	*out_t  = __fmul_rn(t_scaled, rcp_det);
+	return true;
+}
+
+__device__ __forceinline__ bool watertight_hit_tri(
+	const RayTraits& r, const LeafTri* __restrict__ tris, uint32_t k,
+	float min_t, float max_t, float* t, float* b0, float* b1, float* b2)
+{
+	const float4* p = reinterpret_cast<const float4*>(tris + k);
+	const float4 a = __ldg(p + 0);
+	const float4 b = __ldg(p + 1);
+	const float4 c = __ldg(p + 2);
+	return watertight_hit(r, a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, min_t, max_t, t, b0, b1, b2);
+}
+
+__device__ __forceinline__ uint32_t byte_of(uint32_t word, int i)
+{
+	return (word >> (8 * i)) & 0xFFu;
+}
+
+// Intersects the 8 child boxes of a wide node. Returns the hit mask: bits 24..31 are internal
+// children at key (slot ^ oct), bits 0..23 are leaf triangles relative to tri_base.
+__device__ __forceinline__ uint32_t intersect_children(
+	const RayTraits& r, const WideNode* __restrict__ nodes, uint32_t node_index,
+	float t_min, float t_max,
+	uint32_t* out_child_base, uint32_t* out_tri_base, uint32_t* out_imask)
+{
+	const uint4* np = reinterpret_cast<const uint4*>(nodes + node_index);
+	const uint4 w0 = __ldg(np + 0);
+	const uint4 w1 = __ldg(np + 1);
+	const uint4 w2 = __ldg(np + 2);
+	const uint4 w3 = __ldg(np + 3);
+	const uint4 w4 = __ldg(np + 4);
+
+	const float px = __uint_as_float(w0.x);
+	const float py = __uint_as_float(w0.y);
+	const float pz = __uint_as_float(w0.z);
+	const uint32_t ex = byte_of(w0.w, 0), ey = byte_of(w0.w, 1), ez = byte_of(w0.w, 2);
+	const uint32_t imask = byte_of(w0.w, 3);
+	*out_child_base = w1.x;
+	*out_tri_base = w1.y;
+	*out_imask = imask;
+
+	const float scx = __uint_as_float(ex << 23) * r.rdx;
+	const float scy = __uint_as_float(ey << 23) * r.rdy;
+	const float scz = __uint_as_float(ez << 23) * r.rdz;
+	const float bx = px * r.rdx - r.obx;
+	const float by = py * r.rdy - r.oby;
+	const float bz = pz * r.rdz - r.obz;
+
+	// Near/far plane bytes per axis depend on the direction sign.
+	const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
+	const uint32_t qlox[2] = {w2.x, w2.y}, qloy[2] = {w2.z, w2.w}, qloz[2] = {w3.x, w3.y};
+	const uint32_t qhix[2] = {w3.z, w3.w}, qhiy[2] = {w4.x, w4.y}, qhiz[2] = {w4.z, w4.w};
+	const uint32_t meta[2] = {w1.z, w1.w};
+
+	uint32_t hits = 0;
+#pragma unroll
+	for(int half = 0; half < 2; ++half)
+	{
+		const uint32_t nearx = nx ? qhix[half] : qlox[half], farx = nx ? qlox[half] : qhix[half];
+		const uint32_t neary = ny ? qhiy[half] : qloy[half], fary = ny ? qloy[half] : qhiy[half];
+		const uint32_t nearz = nz ? qhiz[half] : qloz[half], farz = nz ? qloz[half] : qhiz[half];
+#pragma unroll
+		for(int j = 0; j < 4; ++j)
+		{
+			const uint32_t m = byte_of(meta[half], j);
+			if(m == 0u)
+			{
+				continue;
+			}
+			const float tnx = fmaf(static_cast<float>(byte_of(nearx, j)), scx, bx);
+			const float tny = fmaf(static_cast<float>(byte_of(neary, j)), scy, by);
+			const float tnz = fmaf(static_cast<float>(byte_of(nearz, j)), scz, bz);
+			const float tfx = fmaf(static_cast<float>(byte_of(farx, j)), scx, bx);
+			const float tfy = fmaf(static_cast<float>(byte_of(fary, j)), scy, by);
+			const float tfz = fmaf(static_cast<float>(byte_of(farz, j)), scz, bz);
+			const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, t_min));
+			const float tf = fminf(fminf(tfx, tfy), fminf(tfz, t_max));
+			if(tn <= tf)
+			{
+				const int s = half * 4 + j;
+				if((imask >> s) & 1u)
+				{
+					hits |= 1u << (24u + (static_cast<uint32_t>(s) ^ r.oct));
+				}
+				else
+				{
+					const uint32_t unary = m >> 5;
+					hits |= unary << (m & 31u);
+				}
+			}
+		}
+	}
+	return hits;
+}
+
+// Closest-hit (ANY_HIT = false) or first-hit (ANY_HIT = true) traversal. COUNT adds the
+// visited-node and tested-triangle counters used by the algorithmic-bytes model.
+template<bool ANY_HIT, bool COUNT = false>
+__device__ __forceinline__ bool traverse(
+	const RayTraits& r,
+	const WideNode* __restrict__ nodes,
+	const LeafTri* __restrict__ tris,
+	float t_min, float t_max,
+	float* out_t, uint32_t* out_tri, uint32_t* out_error,
+	uint32_t* node_count = nullptr, uint32_t* tri_count = nullptr)
+{
+	uint2 stack[kTraversalStackSize];
+	int sp = 0;
+
+	float best_t = t_max;
+	uint32_t best_tri = 0xFFFFFFFFu;
+	uint32_t best_prim = 0xFFFFFFFFu;
+
+	uint32_t child_base, tri_base, imask;
+	uint32_t hits = intersect_children(r, nodes, 0, t_min, best_t, &child_base, &tri_base, &imask);
+	if(COUNT) { ++*node_count; }
+	uint32_t node_hits = hits >> 24;
+	uint32_t tri_hits = hits & 0x00FFFFFFu;
+
+	while(true)
+	{
+		while(tri_hits)
+		{
+			const uint32_t bit = __ffs(tri_hits) - 1u;
+			tri_hits &= tri_hits - 1u;
+			const uint32_t k = tri_base + bit;
+			if(COUNT) { ++*tri_count; }
+			float t, b0, b1, b2;
+			if(watertight_hit_tri(r, tris, k, t_min, best_t, &t, &b0, &b1, &b2))
+			{
+				if(ANY_HIT)
+				{
+					*out_t = t;
+					*out_tri = k;
+					return true;
+				}
+				const uint32_t prim = __ldg(&tris[k].prim);
+				if(t < best_t || prim < best_prim)
+				{
+					best_t = t;
+					best_tri = k;
+					best_prim = prim;
+				}
+			}
+		}
+
+		if(node_hits == 0u)
+		{
+			if(sp == 0)
+			{
+				break;
+			}
+			--sp;
+			child_base = stack[sp].x;
+			imask = stack[sp].y >> 8;
+			node_hits = stack[sp].y & 0xFFu;
+			continue;
+		}
+
+		const uint32_t key = 31u - __clz(node_hits);
+		node_hits &= ~(1u << key);
+		const uint32_t slot = key ^ r.oct;
+		const uint32_t child = child_base + __popc(imask & ((1u << slot) - 1u));
+		if(node_hits)
+		{
+			if(sp < kTraversalStackSize)
+			{
+				stack[sp++] = make_uint2(child_base, (imask << 8) | node_hits);
+			}
+			else
+			{
+				*out_error |= PG_DEV_ERR_STACK;
+			}
+		}
+		hits = intersect_children(r, nodes, child, t_min, best_t, &child_base, &tri_base, &imask);
+		if(COUNT) { ++*node_count; }
+		node_hits = hits >> 24;
+		tri_hits = hits & 0x00FFFFFFu;
+	}
+
+	*out_t = best_t;
+	*out_tri = best_tri;
+	return best_tri != 0xFFFFFFFFu;
+}
+
+}// end namespace pg

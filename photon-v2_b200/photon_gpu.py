@@ -1,0 +1,157 @@
+"""ctypes binding of libphoton_gpu.so: the low-level C ABI (include/photon_gpu.h) and the Photon C
+API (include/ph_c_core.h) exported by the same library.
+
+The library is built in-tree (``make -C photon-v2_b200``). Loading fails loudly when it is missing:
+there is no CPU fallback for any entry point.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libphoton_gpu.so")
+
+_lib: Optional[ctypes.CDLL] = None
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_dblp = ctypes.POINTER(ctypes.c_double)
+
+# (name, restype, argtypes) of every exported entry point.
+PGPU_SIGNATURES = [
+    ("pgpu_last_error", ctypes.c_char_p, []),
+    ("pgpu_device_count", ctypes.c_int, []),
+    ("pgpu_geometry_create", ctypes.c_int, [_f32p, ctypes.c_uint64, ctypes.c_float, _u64p]),
+    ("pgpu_geometry_destroy", ctypes.c_int, [ctypes.c_uint64]),
+    ("pgpu_geometry_stats", ctypes.c_int, [ctypes.c_uint64, _u64p, _u64p, _i32p, _dblp]),
+    ("pgpu_trace_closest", ctypes.c_int, [ctypes.c_uint64, _f32p, ctypes.c_uint64, _i32p, _f32p, _f32p]),
+    ("pgpu_trace_any", ctypes.c_int, [ctypes.c_uint64, _f32p, ctypes.c_uint64, _i32p]),
+    ("pgpu_trace_closest_device", ctypes.c_int,
+     [ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, _f32p]),
+    ("pgpu_trace_any_device", ctypes.c_int,
+     [ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, _f32p]),
+    ("pgpu_trace_counts", ctypes.c_int,
+     [ctypes.c_uint64, _f32p, ctypes.c_uint64, ctypes.c_int, _dblp, _dblp]),
+    ("pgpu_bsdf_eval", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
+]
+
+
+class PhotonGpuError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[status {status}] {message}")
+        self.status = status
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads the library (once) and declares all signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `make -C photon-v2_b200` (there is no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    for name, res, args in PGPU_SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _declare_ph_api(lib)
+    _lib = lib
+    return lib
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        msg = load().pgpu_last_error().decode(errors="replace")
+        raise PhotonGpuError(status, msg)
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def device_count() -> int:
+    return int(load().pgpu_device_count())
+
+
+class Geometry:
+    """Triangles [N, 3, 3] with their 8-wide BVH resident on the GPU."""
+
+    def __init__(self, tris: np.ndarray, max_origin_abs: float = 0.0):
+        lib = load()
+        t = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+        self.num_tris = t.shape[0]
+        gid = ctypes.c_uint64(0)
+        _check(lib.pgpu_geometry_create(_ptr(t, ctypes.c_float), t.shape[0], float(max_origin_abs),
+                                        ctypes.byref(gid)))
+        self.id = gid.value
+
+    def close(self) -> None:
+        if self.id:
+            _check(load().pgpu_geometry_destroy(self.id))
+            self.id = 0
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def stats(self) -> dict:
+        nn, nt = ctypes.c_uint64(), ctypes.c_uint64()
+        depth, secs = ctypes.c_int32(), ctypes.c_double()
+        _check(load().pgpu_geometry_stats(self.id, ctypes.byref(nn), ctypes.byref(nt),
+                                          ctypes.byref(depth), ctypes.byref(secs)))
+        return {"num_nodes": nn.value, "num_tris": nt.value, "max_depth": depth.value,
+                "build_seconds": secs.value}
+
+    def closest(self, rays: np.ndarray) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = r.shape[0]
+        prim = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        bary = np.empty((n, 3), np.float32)
+        _check(load().pgpu_trace_closest(self.id, _ptr(r, ctypes.c_float), n, _ptr(prim, ctypes.c_int32),
+                                         _ptr(t, ctypes.c_float), _ptr(bary, ctypes.c_float)))
+        return prim, t, bary
+
+    def occluded(self, rays: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        out = np.empty(r.shape[0], np.int32)
+        _check(load().pgpu_trace_any(self.id, _ptr(r, ctypes.c_float), r.shape[0], _ptr(out, ctypes.c_int32)))
+        return out
+
+    def counts(self, rays: np.ndarray, any_hit: bool = False) -> Tuple[float, float]:
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        nodes, tris = ctypes.c_double(), ctypes.c_double()
+        _check(load().pgpu_trace_counts(self.id, _ptr(r, ctypes.c_float), r.shape[0], int(any_hit),
+                                        ctypes.byref(nodes), ctypes.byref(tris)))
+        return nodes.value, tris.value
+
+
+def bsdf_eval(cases: np.ndarray, normals: np.ndarray) -> np.ndarray:
+    c = np.ascontiguousarray(cases, np.float32).reshape(-1, 19)
+    nrm = np.ascontiguousarray(normals, np.float32).reshape(-1, 6)
+    out = np.empty((c.shape[0], 16), np.float32)
+    _check(load().pgpu_bsdf_eval(_ptr(c, ctypes.c_float), _ptr(nrm, ctypes.c_float), c.shape[0],
+                                 _ptr(out, ctypes.c_float)))
+    return out
+
+
+# ----------------------------------------------------------------------------------------------
+# Photon C API (ph_c_core.h) declared on the same library.
+
+PH_SIGNATURES = []
+
+
+def _declare_ph_api(lib: ctypes.CDLL) -> None:
+    for name, res, args in PH_SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
