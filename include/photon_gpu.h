@@ -79,6 +79,40 @@ PGPU_API int pgpu_trace_counts(uint64_t id, const float* rays, uint64_t n, int a
  *      pdfAppliedBsdfCos(3), relativeIor, cos, 0. Strict sidedness, radiance transport. */
 PGPU_API int pgpu_bsdf_eval(const float* cases, const float* normals, uint64_t n, float* out);
 
+/* ---------------------------------------------------------------------------------------------
+ * Render scenes: the full BNEEPT / BVPT estimator on the GPU.
+ *
+ * Replaces EqualSamplingRenderer::doRender (Engine/Source/Core/Renderer/Sampling/
+ * EqualSamplingRenderer.cpp:119-203) driving BNEEPTEstimator::estimate
+ * (Engine/Source/Core/Estimator/BNEEPTEstimator.cpp:38-262) or BVPTEstimator::estimate
+ * (Engine/Source/Core/Estimator/BVPTEstimator.cpp:25-160) into an HdrRgbFilm with a box filter.
+ *
+ * tris: float32 [n][3][3]; tri_material: uint32 [n]; tri_emitter: uint32 [n] = emitter index + 1
+ *   (0 = not emissive; may be NULL).
+ * materials: float32 [m][8] = type (0 matte, 1 GGX conductor, 2 GGX dielectric), c0, c1, c2,
+ *   roughness, ior_outer, ior_inner, 0 -- c = albedo (matte) or F0 (conductor).
+ * emitters: float32 [e][4] = radiance r, g, b, type (0 triangle group, 1 constant environment).
+ * camera: float32 [12] = position(3), direction(3), up(3), horizontal fov (degrees), width, height.
+ */
+PGPU_API int pgpu_scene_create(const float* tris, const uint32_t* tri_material, const uint32_t* tri_emitter,
+                               uint64_t num_tris, const float* materials, uint32_t num_materials,
+                               const float* emitters, uint32_t num_emitters, const float* camera,
+                               uint64_t* out_id);
+PGPU_API int pgpu_scene_destroy(uint64_t id);
+
+/* Renders spp samples per pixel (estimator 0 = BNEEPT, 1 = BVPT; max_bounces = the reference's
+ * MAX_RAY_BOUNCES) and adds them to the scene's FP64 film. Samples are numbered from first_sample
+ * so that separate calls draw independent random numbers. Optional outputs: device time of the
+ * render (CUDA events), closest-hit rays and shadow rays traced. */
+PGPU_API int pgpu_scene_render(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator,
+                               uint64_t seed, uint64_t first_sample, float* out_ms,
+                               uint64_t* out_rays, uint64_t* out_shadow_rays);
+
+/* Developed frame (host float32 [h][w][3], row 0 = bottom, the reference's frame layout), the raw
+ * FP64 sums (host double [h][w][3]) and the samples per pixel accumulated; any may be NULL. */
+PGPU_API int pgpu_scene_film(uint64_t id, float* out_rgb, double* out_sum, uint64_t* out_spp);
+PGPU_API int pgpu_scene_clear(uint64_t id);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,226 @@
+// Render-scene entry points of the low-level C ABI (include/photon_gpu.h): a flat scene
+// description in, FP64 film sums and developed frames out.
+#include "pg_render.h"
+#include "scene_build.h"
+
+#include "../../include/photon_gpu.h"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace pg
+{
+
+struct RenderObject
+{
+	std::unique_ptr<RenderScene> scene;
+	DeviceBuffer<double> film;
+	uint32_t width = 0, height = 0;
+	uint64_t samples = 0;     // samples per pixel accumulated in the film
+	float last_ms = 0.0f;
+};
+
+Registry<RenderObject>& render_registry()
+{
+	static Registry<RenderObject> r;
+	return r;
+}
+
+namespace
+{
+
+std::shared_ptr<RenderObject> get_render(uint64_t id)
+{
+	auto r = render_registry().get(id);
+	if(!r)
+	{
+		throw Error(PG_ERR_NOT_FOUND, "unknown scene id " + std::to_string(id));
+	}
+	return r;
+}
+
+}// end anonymous namespace
+
+// Builds a RenderObject from flat arrays (shared with the Photon C API engine).
+std::unique_ptr<RenderObject> make_render_object(SceneDesc&& desc)
+{
+	float max_abs = 1.0f;
+	for(float v : desc.tris)
+	{
+		if(std::isfinite(v))
+		{
+			max_abs = std::max(max_abs, std::fabs(v));
+		}
+	}
+	for(float v : desc.camera.pos)
+	{
+		max_abs = std::max(max_abs, std::fabs(v));
+	}
+	if(desc.has_env && desc.env_area <= 0.0)
+	{
+		const float origin[3] = {0.0f, 0.0f, 0.0f};
+		desc.env_area = dome_area(desc.tris, origin);
+	}
+	auto obj = std::make_unique<RenderObject>();
+	obj->scene = std::make_unique<RenderScene>(desc, max_abs);
+	obj->width = desc.camera.width;
+	obj->height = desc.camera.height;
+	obj->film.resize(static_cast<std::size_t>(obj->width) * obj->height * 3);
+	PG_CUDA_CHECK(cudaMemsetAsync(obj->film.get(), 0, obj->film.bytes(), library_stream()));
+	PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
+	return obj;
+}
+
+}// end namespace pg
+
+using namespace pg;
+
+extern "C" {
+
+int pgpu_scene_create(const float* tris, const uint32_t* tri_material, const uint32_t* tri_emitter,
+                      uint64_t num_tris, const float* materials, uint32_t num_materials,
+                      const float* emitters, uint32_t num_emitters, const float* camera, uint64_t* out_id)
+{
+	return guarded([&]
+	{
+		if(!tris || num_tris == 0 || !tri_material || !materials || num_materials == 0 || !camera || !out_id)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create: missing input");
+		}
+		SceneDesc d;
+		d.tris.assign(tris, tris + 9 * num_tris);
+		d.tri_material.assign(tri_material, tri_material + num_tris);
+		d.tri_emitter.assign(num_tris, 0u);
+		if(tri_emitter)
+		{
+			d.tri_emitter.assign(tri_emitter, tri_emitter + num_tris);
+		}
+		for(uint64_t i = 0; i < num_tris; ++i)
+		{
+			if(d.tri_material[i] >= num_materials)
+			{
+				throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create: material index out of range");
+			}
+			if(d.tri_emitter[i] > num_emitters)
+			{
+				throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create: emitter index out of range");
+			}
+		}
+		for(uint32_t m = 0; m < num_materials; ++m)
+		{
+			const float* p = materials + 8 * m;
+			const int type = static_cast<int>(p[0]);
+			if(type == 0)      { d.materials.push_back(make_matte(p[1], p[2], p[3])); }
+			else if(type == 1) { d.materials.push_back(make_conductor(p[4], p[1], p[2], p[3])); }
+			else if(type == 2) { d.materials.push_back(make_dielectric(p[4], p[5], p[6])); }
+			else
+			{
+				throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create: unknown material type");
+			}
+		}
+		for(uint32_t e = 0; e < num_emitters; ++e)
+		{
+			const float* p = emitters + 4 * e;
+			EmitterRec rec{};
+			rec.r = p[0]; rec.g = p[1]; rec.b = p[2];
+			rec.type = static_cast<uint32_t>(p[3]);
+			if(rec.type == PG_EMITTER_ENV)
+			{
+				if(d.has_env)
+				{
+					throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create: more than one environment");
+				}
+				d.has_env = true;
+				d.env_rgb[0] = p[0]; d.env_rgb[1] = p[1]; d.env_rgb[2] = p[2];
+			}
+			d.emitters.push_back(rec);
+		}
+		const uint32_t w = static_cast<uint32_t>(camera[10]);
+		const uint32_t h = static_cast<uint32_t>(camera[11]);
+		if(w == 0 || h == 0)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create: zero resolution");
+		}
+		d.camera = make_camera(camera, camera + 3, camera + 6, camera[9], w, h);
+		*out_id = render_registry().add(make_render_object(std::move(d)));
+	});
+}
+
+int pgpu_scene_destroy(uint64_t id)
+{
+	return guarded([&]
+	{
+		if(!render_registry().remove(id))
+		{
+			throw Error(PG_ERR_NOT_FOUND, "unknown scene id " + std::to_string(id));
+		}
+	});
+}
+
+int pgpu_scene_render(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator, uint64_t seed,
+                      uint64_t first_sample, float* out_ms, uint64_t* out_rays, uint64_t* out_shadow_rays)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		if(estimator > PG_EST_BVPT)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_render: unknown estimator");
+		}
+		RenderParams p;
+		p.width = r->width;
+		p.height = r->height;
+		p.spp = spp;
+		p.max_bounces = max_bounces;
+		p.estimator = estimator;
+		p.seed = seed;
+		p.first_sample = first_sample;
+		const float ms = r->scene->render(p, r->film.get());
+		r->samples += spp;
+		r->last_ms = ms;
+		if(out_ms) { *out_ms = ms; }
+		if(out_rays) { *out_rays = r->scene->last_rays(); }
+		if(out_shadow_rays) { *out_shadow_rays = r->scene->last_shadow_rays(); }
+	});
+}
+
+int pgpu_scene_film(uint64_t id, float* out_rgb, double* out_sum, uint64_t* out_spp)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		const std::size_t n = static_cast<std::size_t>(r->width) * r->height * 3;
+		std::vector<double> sum(n);
+		PG_CUDA_CHECK(cudaMemcpyAsync(sum.data(), r->film.get(), n * sizeof(double), cudaMemcpyDeviceToHost, library_stream()));
+		PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
+		if(out_sum)
+		{
+			std::copy(sum.begin(), sum.end(), out_sum);
+		}
+		if(out_rgb)
+		{
+			// develop: per-pixel weighted mean; the box filter gives every sample weight 1
+			// (HdrRgbFilm::developRegion, Engine/Source/Core/Filmic/HdrRgbFilm.cpp:167-205)
+			const double rcp = r->samples > 0 ? 1.0 / static_cast<double>(r->samples) : 0.0;
+			for(std::size_t i = 0; i < n; ++i)
+			{
+				out_rgb[i] = static_cast<float>(sum[i] * rcp);
+			}
+		}
+		if(out_spp) { *out_spp = r->samples; }
+	});
+}
+
+int pgpu_scene_clear(uint64_t id)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		PG_CUDA_CHECK(cudaMemsetAsync(r->film.get(), 0, r->film.bytes(), library_stream()));
+		PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
+		r->samples = 0;
+	});
+}
+
+}// extern "C"

@@ -1,0 +1,804 @@
+// Wavefront BNEEPT / BVPT kernels (camera rays, shading, bookkeeping) and the render driver.
+//
+// Compiled without FMA contraction (see the Makefile) so that the FP32 shading arithmetic rounds
+// like the reference's x86 build. The estimator logic follows
+//   BNEEPTEstimator::estimate  Engine/Source/Core/Estimator/BNEEPTEstimator.cpp:38-262
+//   BVPTEstimator::estimate    Engine/Source/Core/Estimator/BVPTEstimator.cpp:25-160
+// with the per-bounce loop unrolled across kernel launches: one shade invocation is one loop
+// iteration of one path.
+#include "pg_render.h"
+#include "refinery.cuh"
+
+#include "../../include/photon_gpu.h"
+
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace cg = cooperative_groups;
+
+namespace pg
+{
+namespace
+{
+
+constexpr int kShadeBlock = 128;
+constexpr float kClampMax = 1e9f;
+
+// ---------------------------------------------------------------------------------------------
+// Counter-based random numbers: every (path, bounce, dimension) has its own independent uniform,
+// so results do not depend on scheduling (the reference draws from per-thread PCG32 streams and
+// is not reproducible run to run; parity with it is statistical).
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+	z += 0x9E3779B97F4A7C15ull;
+	z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+	z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+	return z ^ (z >> 31);
+}
+
+struct PathRng
+{
+	uint64_t base;
+
+	__device__ __forceinline__ float u01(uint32_t bounce, uint32_t dim) const
+	{
+		const uint64_t h = mix64(base + ((static_cast<uint64_t>(bounce) << 4) | dim) * 0xD1B54A32D192ED03ull);
+		return static_cast<float>(h >> 40) * (1.0f / 16777216.0f);
+	}
+};
+
+__device__ __forceinline__ PathRng make_rng(uint64_t seed, uint64_t global_path)
+{
+	return PathRng{mix64(global_path ^ mix64(seed))};
+}
+
+// Dimensions per vertex.
+enum : uint32_t
+{
+	DIM_CAM_X = 0, DIM_CAM_Y = 1,
+	DIM_NEE_PICK = 2, DIM_NEE_TRI = 3, DIM_NEE_U = 4, DIM_NEE_V = 5,
+	DIM_BSDF_0 = 6, DIM_BSDF_1 = 7, DIM_BSDF_2 = 8,
+	DIM_RR = 9,
+};
+
+// Relative luminance of linear sRGB (CIE Y), used by Russian roulette
+// (RussianRoulette.h:30-55 -> TSpectrumBase::relativeLuminance).
+__device__ __forceinline__ float luminance(RGB c)
+{
+	return 0.2126729f * c.r + 0.7151522f * c.g + 0.0721750f * c.b;
+}
+
+__device__ __forceinline__ float4 ld4(const float4* p) { return *p; }
+
+__device__ __forceinline__ V3 xyz(float4 v) { return v3(v.x, v.y, v.z); }
+
+// Face normal as PTriangle stores it: (B-A) x (C-A), normalised, (0,1,0) for degenerate
+// triangles (PTriangle.cpp:19-35, TBasicTriangle::safeGetFaceNormal).
+__device__ __forceinline__ V3 face_normal(const TriVerts& t)
+{
+	const V3 n = cross(t.b - t.a, t.c - t.a);
+	const float len2 = length_sq(n);
+	if(!(len2 > 0.0f) || isinf(len2))
+	{
+		return v3(0.0f, 1.0f, 0.0f);
+	}
+	const V3 u = normalize(n);
+	return is_finite(u) ? u : v3(0.0f, 1.0f, 0.0f);
+}
+
+__device__ __forceinline__ float tri_area(const TriVerts& t)
+{
+	return length(cross(t.b - t.a, t.c - t.a)) * 0.5f;
+}
+
+__device__ __forceinline__ TriVerts load_tri(const LeafTri* tris, uint32_t k, uint32_t* material, uint32_t* emitter)
+{
+	const float4* p = reinterpret_cast<const float4*>(tris + k);
+	const float4 a = p[0], b = p[1], c = p[2];
+	if(material) { *material = __float_as_uint(b.w); }
+	if(emitter) { *emitter = __float_as_uint(c.w); }
+	return TriVerts{v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z)};
+}
+
+// Area pdf -> solid angle pdf (Engine/Source/Core/LTA/lta.h:17-25).
+__device__ __forceinline__ float pdfa_to_pdfw(float pdf_a, V3 da_to_target, V3 da_normal)
+{
+	const float dist2 = length_sq(da_to_target);
+	const float w = pdf_a / dot(normalize(da_to_target), da_normal) * dist2;
+	return isfinite(w) ? fabsf(w) : 0.0f;
+}
+
+__device__ __forceinline__ RGB emitter_radiance(const EmitterRec& e) { return RGB{e.r, e.g, e.b}; }
+
+__device__ __forceinline__ uint32_t alias_pick(const float2* alias, uint32_t n, float u)
+{
+	const float scaled = u * static_cast<float>(n);
+	uint32_t i = min(static_cast<uint32_t>(scaled), n - 1u);
+	const float frac = scaled - static_cast<float>(i);
+	const float2 a = alias[i];
+	return frac < a.x ? i : __float_as_uint(a.y);
+}
+
+__device__ __forceinline__ void splat(double* film, uint32_t pixel, RGB c)
+{
+	if(c.r != 0.0f) { atomicAdd(&film[3 * pixel + 0], static_cast<double>(c.r)); }
+	if(c.g != 0.0f) { atomicAdd(&film[3 * pixel + 1], static_cast<double>(c.g)); }
+	if(c.b != 0.0f) { atomicAdd(&film[3 * pixel + 2], static_cast<double>(c.b)); }
+}
+
+// Warp-aggregated slot allocation on a queue counter.
+__device__ __forceinline__ uint32_t alloc_slot(uint32_t* counter)
+{
+	cg::coalesced_group g = cg::coalesced_threads();
+	uint32_t base = 0;
+	if(g.thread_rank() == 0)
+	{
+		base = atomicAdd(counter, g.size());
+	}
+	base = g.shfl(base, 0);
+	return base + g.thread_rank();
+}
+
+// ---------------------------------------------------------------------------------------------
+
+__global__ void prepare_kernel(RenderCounters* c, uint32_t capacity)
+{
+	if(threadIdx.x != 0 || blockIdx.x != 0)
+	{
+		return;
+	}
+	const uint32_t active = c->n_next;
+	const unsigned long long remaining = c->total_paths - c->next_path;
+	const unsigned long long room = static_cast<unsigned long long>(capacity - active);
+	const uint32_t n_new = static_cast<uint32_t>(remaining < room ? remaining : room);
+	c->n_active = active;
+	c->n_total = active + n_new;
+	c->gen_base = c->next_path;
+	c->next_path += n_new;
+	c->n_next = 0;
+	c->n_shadow = 0;
+	c->rays_traced += c->n_total;
+}
+
+// Camera rays of new paths into the tail of the current queue
+// (PinholeCamera::receiveRay, then BNEEPTEstimator.cpp:63-64: reversed, range [0, max]).
+__global__ void __launch_bounds__(kShadeBlock)
+regen_kernel(const RenderCounters* __restrict__ c, Camera cam, uint64_t seed, uint64_t first_global,
+             PathBuffers cur)
+{
+	const uint32_t active = c->n_active;
+	const uint32_t total = c->n_total;
+	const unsigned long long base = c->gen_base;
+	const uint32_t wh = cam.width * cam.height;
+	for(uint32_t i = active + blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+	{
+		const uint32_t p = static_cast<uint32_t>(base + (i - active));
+		const uint32_t pixel = p % wh;
+		const uint32_t x = pixel % cam.width;
+		const uint32_t y = pixel / cam.width;
+		const PathRng rng = make_rng(seed, first_global + p);
+		const float rx = static_cast<float>(x) + rng.u01(0, DIM_CAM_X);
+		const float ry = static_cast<float>(y) + rng.u01(0, DIM_CAM_Y);
+
+		// raster -> sensor (SingleLensObserver::makeRasterToSensor)
+		const float sx = -cam.sensor_w / static_cast<float>(cam.width) * rx + cam.sensor_w * 0.5f;
+		const float sy = -cam.sensor_h / static_cast<float>(cam.height) * ry + cam.sensor_h * 0.5f;
+		const float sz = cam.sensor_offset;
+		const V3 recv = normalize(v3(cam.axis_x[0], cam.axis_x[1], cam.axis_x[2]) * sx +
+		                          v3(cam.axis_y[0], cam.axis_y[1], cam.axis_y[2]) * sy +
+		                          v3(cam.axis_z[0], cam.axis_z[1], cam.axis_z[2]) * sz);
+		const V3 d = -recv;
+
+		cur.path[i] = p;
+		cur.meta[i] = 0u;
+		cur.thr[i] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+		cur.rad[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+		cur.prev[i] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+		cur.ray_o[i] = make_float4(cam.pos[0], cam.pos[1], cam.pos[2], 0.0f);
+		cur.ray_d[i] = make_float4(d.x, d.y, d.z, kFloatMax);
+	}
+}
+
+struct ShadeArgs
+{
+	DeviceScene   scene;
+	PathBuffers   cur;
+	PathBuffers   next;
+	const uint2*  hits;
+	ShadowQueue   shadow;
+	RenderCounters* counters;
+	double*       film;
+	uint64_t      seed;
+	uint64_t      first_global;
+	uint32_t      max_bounces;
+	uint32_t      estimator;
+	uint32_t      width_height;
+};
+
+__global__ void __launch_bounds__(kShadeBlock)
+shade_kernel(ShadeArgs a)
+{
+	const uint32_t total = a.counters->n_total;
+	const DeviceScene& s = a.scene;
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+	{
+		const uint32_t p = a.cur.path[i];
+		const uint32_t meta = a.cur.meta[i];
+		const uint32_t bounce = meta & kMetaBounceMask;
+		const float4 thr4 = ld4(a.cur.thr + i);
+		const float4 rad4 = ld4(a.cur.rad + i);
+		const float4 prev4 = ld4(a.cur.prev + i);
+		const float4 ro = ld4(a.cur.ray_o + i);
+		const float4 rd = ld4(a.cur.ray_d + i);
+		const uint2 hit = a.hits[i];
+		const uint32_t pixel = p % a.width_height;
+		const PathRng rng = make_rng(a.seed, a.first_global + p);
+
+		const RGB thr_emit = RGB{thr4.x, thr4.y, thr4.z};
+		const float cont = thr4.w;
+		RGB radiance = RGB{rad4.x, rad4.y, rad4.z};
+		const float prev_bsdf_pdf = rad4.w;
+		const V3 prev_pos = xyz(prev4);
+		float rr_scale = prev4.w;
+		const V3 d = xyz(rd);
+		const bool bvpt = a.estimator == PG_EST_BVPT;
+
+		// ---- miss: environment (the dome primitive is hit after every triangle missed)
+		if(hit.x == 0xFFFFFFFFu)
+		{
+			if(s.env_emitter >= 0)
+			{
+				const RGB le = RGB{s.env_r, s.env_g, s.env_b};
+				if(bvpt)
+				{
+					radiance = radiance + le * safe_clamp(thr_emit * cont, 0.0f, kClampMax);
+				}
+				else if(bounce == 0)
+				{
+					radiance = radiance + le;
+				}
+				else if(meta & kMetaPrevNee)
+				{
+					if(prev_bsdf_pdf > 0.0f)
+					{
+						const EmitterRec e = s.emitters[s.env_emitter];
+						const float light_pdf = e.pmf * (1.0f / (4.0f * kPi));
+						const float mis = prev_bsdf_pdf * prev_bsdf_pdf /
+						                  (prev_bsdf_pdf * prev_bsdf_pdf + light_pdf * light_pdf);
+						radiance = radiance + le * safe_clamp(thr_emit * mis, 0.0f, kClampMax);
+					}
+				}
+				else
+				{
+					radiance = radiance + le * safe_clamp(thr_emit, 0.0f, kClampMax);
+				}
+			}
+			splat(a.film, pixel, radiance);
+			continue;
+		}
+
+		// ---- surface hit: recover barycentrics, position and normals
+		uint32_t mat_index, emitter_plus_one;
+		const TriVerts tri = load_tri(s.tris, hit.x, &mat_index, &emitter_plus_one);
+		const RayTraits rt = make_ray_traits(ro.x, ro.y, ro.z, d.x, d.y, d.z);
+		float t_hit, b0, b1, b2;
+		watertight_hit(rt, tri.a.x, tri.a.y, tri.a.z, tri.b.x, tri.b.y, tri.b.z, tri.c.x, tri.c.y, tri.c.z,
+		               ro.w, rd.w, &t_hit, &b0, &b1, &b2);
+		const V3 pos = tri.a * b0 + tri.b * b1 + tri.c * b2;
+		const V3 ng = face_normal(tri);
+		const Frame frame = make_frame(ng, ng);
+
+		// traceNextSurface rejects hits whose sidedness disagrees (SurfaceTracer.h:126-141).
+		if(!(dot(ng, d) * dot(frame.ns, d) > 0.0f))
+		{
+			splat(a.film, pixel, radiance);
+			continue;
+		}
+
+		// ---- emission arriving at this vertex
+		if(emitter_plus_one != 0u)
+		{
+			const EmitterRec e = s.emitters[emitter_plus_one - 1u];
+			// one-sided emission: canEmit(-d, Ns) (SurfaceEmitter.cpp:20-25)
+			const RGB le = dot(-d, frame.ns) > 0.0f ? emitter_radiance(e) : RGB{0.0f, 0.0f, 0.0f};
+			if(bvpt)
+			{
+				radiance = radiance + le * safe_clamp(thr_emit * cont, 0.0f, kClampMax);
+			}
+			else if(bounce == 0)
+			{
+				radiance = radiance + le;   // zero-bounce emission (BNEEPTEstimator.cpp:74-82)
+			}
+			else if((meta & kMetaPrevNee) && !is_zero(le))
+			{
+				// MIS of the BSDF-sampled hit against NEE (BNEEPTEstimator.cpp:178-213)
+				if(prev_bsdf_pdf > 0.0f)
+				{
+					float light_pdf = 0.0f;
+					const V3 to_target = prev_pos - pos;
+					if(dot(to_target, frame.ns) > 0.0f)
+					{
+						light_pdf = pdfa_to_pdfw(1.0f / tri_area(tri), to_target, frame.ns) * e.rcp_count * e.pmf;
+					}
+					const float mis = prev_bsdf_pdf * prev_bsdf_pdf /
+					                  (prev_bsdf_pdf * prev_bsdf_pdf + light_pdf * light_pdf);
+					radiance = radiance + le * safe_clamp(thr_emit * mis, 0.0f, kClampMax);
+				}
+			}
+			else
+			{
+				radiance = radiance + le * safe_clamp(thr_emit, 0.0f, kClampMax);
+			}
+		}
+
+		// ---- does the path continue past this vertex?
+		if((meta & kMetaStopAfter) || bounce >= a.max_bounces)
+		{
+			splat(a.film, pixel, radiance);
+			continue;
+		}
+		const RGB throughput = thr_emit * cont;
+		const Material mat = s.materials[mat_index];
+		const V3 v = -d;
+
+		// ---- next-event estimation (TDirectLightEstimator::neeSampleEmission,
+		//      TDirectLightEstimator.ipp:71-102; BNEEPTEstimator.cpp:103-149)
+		bool has_shadow = false;
+		V3 sh_o{}, sh_d{};
+		float sh_tmax = 0.0f;
+		RGB sh_c{};
+		// Every material here is non-delta, so NEE applies at every vertex of BNEEPT
+		// (TDirectLightEstimator::isNeeSamplable); a black Lambertian surface can gain nothing
+		// from it, so its shadow ray is skipped (its contribution would be exactly zero).
+		const bool black_matte = mat.type == PG_MAT_MATTE && mat.cr == 0.0f && mat.cg == 0.0f && mat.cb == 0.0f;
+		const bool nee_samplable = !bvpt;
+		const bool use_nee = nee_samplable && s.num_emitters > 0 && !black_matte;
+		if(use_nee)
+		{
+			const uint32_t ei = alias_pick(s.alias, s.num_emitters, rng.u01(bounce, DIM_NEE_PICK));
+			const EmitterRec e = s.emitters[ei];
+			bool ok = false;
+			V3 to_light{};
+			float pdf_w = 0.0f;
+			RGB le{};
+			if(e.type == PG_EMITTER_ENV)
+			{
+				// uniform sphere direction
+				const float u = rng.u01(bounce, DIM_NEE_U), w = rng.u01(bounce, DIM_NEE_V);
+				const float z = 1.0f - 2.0f * u;
+				const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+				float sp, cp;
+				sincosf(kTwoPi * w, &sp, &cp);
+				to_light = v3(r * cp, r * sp, z);
+				pdf_w = e.pmf * (1.0f / (4.0f * kPi));
+				le = emitter_radiance(e);
+				if(sidedness_agreed(frame, to_light))
+				{
+					const OffsetResult off = iterative_offset(pos, ng, tri, to_light);
+					sh_o = pos + off.offset;
+					sh_d = off.unit_dir;
+					sh_tmax = kFloatMax;
+					ok = true;
+				}
+			}
+			else if(e.count > 0u)
+			{
+				const uint32_t j = e.first + min(static_cast<uint32_t>(rng.u01(bounce, DIM_NEE_TRI) * e.count), e.count - 1u);
+				const TriVerts lt = load_tri(s.tris, s.emitter_tris ? s.emitter_tris[j] : 0u, nullptr, nullptr);
+				// Osada uniform triangle sampling (TBasicTriangle::sampleToBarycentricOsada)
+				const float su = sqrtf(rng.u01(bounce, DIM_NEE_U));
+				const float sv = rng.u01(bounce, DIM_NEE_V);
+				const float lb0 = 1.0f - su, lb1 = su * (1.0f - sv), lb2 = sv * su;
+				const V3 xe = lt.a * lb0 + lt.b * lb1 + lt.c * lb2;
+				const V3 ne = face_normal(lt);
+				const V3 emitter_to_target = pos - xe;
+				if(dot(emitter_to_target, ne) > 0.0f)
+				{
+					pdf_w = pdfa_to_pdfw(1.0f / tri_area(lt), emitter_to_target, ne) * e.rcp_count * e.pmf;
+					le = emitter_radiance(e);
+					const V3 target_to_emit = xe - pos;
+					if(pdf_w > 0.0f && isfinite(pdf_w) && sidedness_agreed(frame, target_to_emit))
+					{
+						const OffsetResult off = iterative_mutual_offset(pos, ng, tri, xe, lt);
+						if(off.max_distance > 0.0f && isfinite(off.max_distance))
+						{
+							sh_o = pos + off.offset;
+							sh_d = off.unit_dir;
+							sh_tmax = off.max_distance;
+							to_light = target_to_emit;
+							ok = true;
+						}
+					}
+				}
+			}
+			if(ok && pdf_w > 0.0f)
+			{
+				const V3 l = normalize(to_light);
+				RGB f;
+				if(bsdf_eval(mat, frame, l, v, &f))
+				{
+					const float pdf_bsdf = bsdf_pdf(mat, frame, l, v);
+					const float mis = pdf_w * pdf_w / (pdf_w * pdf_w + pdf_bsdf * pdf_bsdf);
+					RGB w = f * fabsf(dot(frame.ns, l));
+					w = w * throughput;
+					w = w * (mis / pdf_w);
+					w = safe_clamp(w, 0.0f, kClampMax);
+					sh_c = le * w;
+					has_shadow = !is_zero(sh_c);
+				}
+			}
+		}
+
+		// ---- BSDF sampling and extension (BNEEPTEstimator.cpp:155-247, BVPTEstimator.cpp:80-110)
+		const BsdfSample bs = bsdf_sample(mat, frame, v, rng.u01(bounce, DIM_BSDF_0),
+		                                  rng.u01(bounce, DIM_BSDF_1), rng.u01(bounce, DIM_BSDF_2));
+		bool continues = bs.ok;
+		RGB next_thr_emit{};
+		float next_cont = 1.0f;
+		float next_pdf = 0.0f;
+		uint32_t next_meta = 0u;
+		if(continues)
+		{
+			next_thr_emit = throughput * bs.weight;
+			rr_scale /= bs.rel_ior * bs.rel_ior;
+			if(!bvpt)
+			{
+				next_pdf = bsdf_pdf(mat, frame, bs.l, v);
+			}
+			bool stop_after = false;
+			if(bounce >= 3)
+			{
+				const float survival = safe_clamp(luminance(next_thr_emit * rr_scale), 0.0f, 0.95f);
+				if(rng.u01(bounce, DIM_RR) < survival)
+				{
+					next_cont = 1.0f / survival;
+				}
+				else
+				{
+					stop_after = true;
+				}
+			}
+			if(is_zero(next_thr_emit) || (bvpt && stop_after))
+			{
+				// zero throughput: nothing more can be gathered (the emission at the next hit
+				// is weighted by it); BVPT gathers emission only with the post-roulette
+				// throughput, so a killed BVPT path ends here
+				continues = false;
+			}
+			next_meta = (bounce + 1u) | (nee_samplable ? kMetaPrevNee : 0u) | (stop_after ? kMetaStopAfter : 0u);
+		}
+
+		uint32_t slot = 0;
+		if(continues)
+		{
+			slot = alloc_slot(&a.counters->n_next);
+			const OffsetResult off = iterative_offset(pos, ng, tri, bs.l);
+			const V3 o = pos + off.offset;
+			a.next.path[slot] = p;
+			a.next.meta[slot] = next_meta;
+			a.next.thr[slot] = make_float4(next_thr_emit.r, next_thr_emit.g, next_thr_emit.b, next_cont);
+			a.next.rad[slot] = make_float4(radiance.r, radiance.g, radiance.b, next_pdf);
+			a.next.prev[slot] = make_float4(pos.x, pos.y, pos.z, rr_scale);
+			a.next.ray_o[slot] = make_float4(o.x, o.y, o.z, 0.0f);
+			a.next.ray_d[slot] = make_float4(off.unit_dir.x, off.unit_dir.y, off.unit_dir.z, kFloatMax);
+		}
+		else
+		{
+			splat(a.film, pixel, radiance);
+		}
+
+		if(has_shadow)
+		{
+			const uint32_t k = alloc_slot(&a.counters->n_shadow);
+			const uint32_t target = continues ? slot : (kTargetFinal | pixel);
+			a.shadow.o[k] = make_float4(sh_o.x, sh_o.y, sh_o.z, 0.0f);
+			a.shadow.d[k] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
+			a.shadow.c[k] = make_float4(sh_c.r, sh_c.g, sh_c.b, __uint_as_float(target));
+		}
+	}
+}
+
+}// end anonymous namespace
+
+// ---------------------------------------------------------------------------------------------
+// RenderScene
+
+namespace
+{
+
+void build_alias(const std::vector<double>& weights, std::vector<float2>& out_alias, std::vector<double>& out_pmf)
+{
+	const std::size_t n = weights.size();
+	out_alias.assign(n, make_float2(1.0f, 0.0f));
+	out_pmf.assign(n, 0.0);
+	double sum = 0.0;
+	for(double w : weights)
+	{
+		sum += w;
+	}
+	if(n == 0 || !(sum > 0.0))
+	{
+		return;
+	}
+	std::vector<double> scaled(n);
+	std::vector<std::size_t> small, large;
+	for(std::size_t i = 0; i < n; ++i)
+	{
+		out_pmf[i] = weights[i] / sum;
+		scaled[i] = out_pmf[i] * static_cast<double>(n);
+		(scaled[i] < 1.0 ? small : large).push_back(i);
+	}
+	std::vector<double> prob(n, 1.0);
+	std::vector<uint32_t> alias(n);
+	for(std::size_t i = 0; i < n; ++i)
+	{
+		alias[i] = static_cast<uint32_t>(i);
+	}
+	while(!small.empty() && !large.empty())
+	{
+		const std::size_t s = small.back(); small.pop_back();
+		const std::size_t l = large.back(); large.pop_back();
+		prob[s] = scaled[s];
+		alias[s] = static_cast<uint32_t>(l);
+		scaled[l] = (scaled[l] + scaled[s]) - 1.0;
+		(scaled[l] < 1.0 ? small : large).push_back(l);
+	}
+	for(std::size_t i = 0; i < n; ++i)
+	{
+		uint32_t bits;
+		std::memcpy(&bits, &alias[i], 4);
+		float fbits;
+		std::memcpy(&fbits, &bits, 4);
+		out_alias[i] = make_float2(static_cast<float>(prob[i]), fbits);
+	}
+}
+
+}// end anonymous namespace
+
+RenderScene::RenderScene(const SceneDesc& desc, float max_origin_abs)
+{
+	require_device();
+	const std::size_t n = desc.tris.size() / 9;
+	if(n == 0)
+	{
+		throw Error(PG_ERR_SCENE, "scene has no triangles");
+	}
+	BvhBuildInput in{desc.tris.data(), desc.tri_material.data(), desc.tri_emitter.data(), n, max_origin_abs};
+	m_geometry = make_geometry(in);
+
+	// Map original triangle index -> leaf slot to build the per-emitter triangle lists.
+	std::vector<LeafTri> leaf(m_geometry->tris.size());
+	cudaStream_t st = library_stream();
+	PG_CUDA_CHECK(cudaMemcpyAsync(leaf.data(), m_geometry->tris.get(), m_geometry->tris.bytes(), cudaMemcpyDeviceToHost, st));
+	PG_CUDA_CHECK(cudaStreamSynchronize(st));
+
+	std::vector<EmitterRec> emitters = desc.emitters;
+	std::vector<std::vector<uint32_t>> per_emitter(emitters.size());
+	std::vector<double> area(emitters.size(), 0.0);
+	for(uint32_t k = 0; k < leaf.size(); ++k)
+	{
+		const uint32_t e = leaf[k].emitter_plus_one;
+		if(e == 0u)
+		{
+			continue;
+		}
+		if(e > emitters.size())
+		{
+			throw Error(PG_ERR_SCENE, "triangle refers to a missing emitter");
+		}
+		per_emitter[e - 1].push_back(k);
+		const float* v = &desc.tris[9 * static_cast<std::size_t>(leaf[k].prim)];
+		const double ax = v[3] - v[0], ay = v[4] - v[1], az = v[5] - v[2];
+		const double bx = v[6] - v[0], by = v[7] - v[1], bz = v[8] - v[2];
+		const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+		area[e - 1] += 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+	}
+	// The reference keeps emitter triangles in cooked order; sort each list by original index.
+	std::vector<uint32_t> emitter_tris;
+	std::vector<double> weights(emitters.size(), 0.0);
+	int32_t env_index = -1;
+	for(std::size_t e = 0; e < emitters.size(); ++e)
+	{
+		auto& list = per_emitter[e];
+		std::sort(list.begin(), list.end(), [&](uint32_t x, uint32_t y) { return leaf[x].prim < leaf[y].prim; });
+		emitters[e].first = static_cast<uint32_t>(emitter_tris.size());
+		emitters[e].count = static_cast<uint32_t>(list.size());
+		emitters[e].rcp_count = list.empty() ? 0.0f : 1.0f / static_cast<float>(list.size());
+		emitter_tris.insert(emitter_tris.end(), list.begin(), list.end());
+		const double lum = 0.2126729 * emitters[e].r + 0.7151522 * emitters[e].g + 0.0721750 * emitters[e].b;
+		if(emitters[e].type == PG_EMITTER_ENV)
+		{
+			env_index = static_cast<int32_t>(e);
+			weights[e] = std::max(lum, 1e-6) * desc.env_area;
+		}
+		else
+		{
+			// radiant flux approximation: radiance * area * pi (DiffuseSurfaceEmitter.cpp:55-86)
+			weights[e] = list.empty() ? 0.0 : std::max(lum, 0.0) * area[e] * 3.14159265358979323846;
+		}
+	}
+	std::vector<float2> alias;
+	std::vector<double> pmf;
+	build_alias(weights, alias, pmf);
+	for(std::size_t e = 0; e < emitters.size(); ++e)
+	{
+		emitters[e].pmf = static_cast<float>(pmf[e]);
+	}
+
+	m_materials.resize(std::max<std::size_t>(1, desc.materials.size()));
+	if(!desc.materials.empty())
+	{
+		PG_CUDA_CHECK(cudaMemcpyAsync(m_materials.get(), desc.materials.data(), desc.materials.size() * sizeof(Material), cudaMemcpyHostToDevice, st));
+	}
+	m_emitters.resize(std::max<std::size_t>(1, emitters.size()));
+	if(!emitters.empty())
+	{
+		PG_CUDA_CHECK(cudaMemcpyAsync(m_emitters.get(), emitters.data(), emitters.size() * sizeof(EmitterRec), cudaMemcpyHostToDevice, st));
+	}
+	m_emitter_tris.resize(std::max<std::size_t>(1, emitter_tris.size()));
+	if(!emitter_tris.empty())
+	{
+		PG_CUDA_CHECK(cudaMemcpyAsync(m_emitter_tris.get(), emitter_tris.data(), emitter_tris.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+	}
+	m_alias.resize(std::max<std::size_t>(1, alias.size()));
+	if(!alias.empty())
+	{
+		PG_CUDA_CHECK(cudaMemcpyAsync(m_alias.get(), alias.data(), alias.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
+	}
+	m_counters.resize(1);
+	PG_CUDA_CHECK(cudaStreamSynchronize(st));
+
+	m_dev.nodes = m_geometry->nodes.get();
+	m_dev.tris = m_geometry->tris.get();
+	m_dev.materials = m_materials.get();
+	m_dev.emitters = m_emitters.get();
+	m_dev.emitter_tris = m_emitter_tris.get();
+	m_dev.alias = m_alias.get();
+	m_dev.num_emitters = static_cast<uint32_t>(emitters.size());
+	m_dev.env_emitter = env_index;
+	m_dev.env_r = desc.env_rgb[0];
+	m_dev.env_g = desc.env_rgb[1];
+	m_dev.env_b = desc.env_rgb[2];
+	m_dev.cam = desc.camera;
+}
+
+RenderScene::~RenderScene() = default;
+
+void RenderScene::ensure_capacity(uint32_t capacity)
+{
+	if(capacity <= m_capacity)
+	{
+		return;
+	}
+	for(int b = 0; b < 2; ++b)
+	{
+		m_path[b].resize(capacity);
+		m_meta[b].resize(capacity);
+		m_thr[b].resize(capacity);
+		m_rad[b].resize(capacity);
+		m_prev[b].resize(capacity);
+		m_ro[b].resize(capacity);
+		m_rd[b].resize(capacity);
+	}
+	m_hits.resize(capacity);
+	m_so.resize(capacity);
+	m_sd.resize(capacity);
+	m_sc.resize(capacity);
+	m_capacity = capacity;
+}
+
+float RenderScene::render(const RenderParams& params, double* film)
+{
+	if(params.width == 0 || params.height == 0 || params.spp == 0)
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, "render: empty image or zero samples");
+	}
+	if(params.width != m_dev.cam.width || params.height != m_dev.cam.height)
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, "render: resolution differs from the camera's");
+	}
+	const unsigned long long wh = static_cast<unsigned long long>(params.width) * params.height;
+	const unsigned long long total = wh * params.spp;
+	if(total > 0xFFFFFFFFull)
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, "render: more than 2^32 paths in one call; split the samples");
+	}
+	const uint32_t capacity = static_cast<uint32_t>(std::min<unsigned long long>(params.capacity, total));
+	ensure_capacity(std::max<uint32_t>(capacity, 1024u));
+
+	cudaStream_t st = library_stream();
+	RenderCounters init{};
+	init.total_paths = total;
+	PG_CUDA_CHECK(cudaMemcpyAsync(m_counters.get(), &init, sizeof(init), cudaMemcpyHostToDevice, st));
+
+	const int sms = sm_count();
+	const int grid = sms * 8;   // grid-stride kernels: 8 blocks of 128 threads per SM
+	PathBuffers buf[2];
+	for(int b = 0; b < 2; ++b)
+	{
+		buf[b] = PathBuffers{m_path[b].get(), m_meta[b].get(), m_thr[b].get(), m_rad[b].get(),
+		                     m_prev[b].get(), m_ro[b].get(), m_rd[b].get()};
+	}
+	ShadowQueue sq{m_so.get(), m_sd.get(), m_sc.get()};
+	const uint64_t first_global = params.first_sample * wh;
+
+	// One graph = two iterations (ping -> pong -> ping).
+	cudaGraph_t graph;
+	cudaGraphExec_t exec;
+	PG_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+	for(int b = 0; b < 2; ++b)
+	{
+		const PathBuffers& cur = buf[b];
+		const PathBuffers& nxt = buf[1 - b];
+		prepare_kernel<<<1, 32, 0, st>>>(m_counters.get(), m_capacity < capacity ? m_capacity : capacity);
+		regen_kernel<<<grid, kShadeBlock, 0, st>>>(m_counters.get(), m_dev.cam, params.seed, first_global, cur);
+		launch_extend(m_dev, m_counters.get(), cur.ray_o, cur.ray_d, m_hits.get(), grid, 128, st);
+		ShadeArgs sa{m_dev, cur, nxt, m_hits.get(), sq, m_counters.get(), film, params.seed, first_global,
+		             params.max_bounces, params.estimator, static_cast<uint32_t>(wh)};
+		shade_kernel<<<grid, kShadeBlock, 0, st>>>(sa);
+		launch_shadow(m_dev, m_counters.get(), sq, nxt.rad, film, grid, 128, st);
+	}
+	PG_CUDA_CHECK(cudaStreamEndCapture(st, &graph));
+	PG_CUDA_CHECK(cudaGraphInstantiate(&exec, graph, 0));
+
+	RenderCounters* host_counters = nullptr;
+	PG_CUDA_CHECK(cudaMallocHost(&host_counters, sizeof(RenderCounters)));
+
+	cudaEvent_t e0, e1;
+	PG_CUDA_CHECK(cudaEventCreate(&e0));
+	PG_CUDA_CHECK(cudaEventCreate(&e1));
+	PG_CUDA_CHECK(cudaEventRecord(e0, st));
+	unsigned long long launches = 0;
+	const unsigned long long max_launches = 1ull << 24;
+	int batch = 4;
+	bool done = false;
+	while(!done)
+	{
+		for(int k = 0; k < batch; ++k)
+		{
+			PG_CUDA_CHECK(cudaGraphLaunch(exec, st));
+		}
+		launches += batch;
+		PG_CUDA_CHECK(cudaMemcpyAsync(host_counters, m_counters.get(), sizeof(RenderCounters), cudaMemcpyDeviceToHost, st));
+		PG_CUDA_CHECK(cudaStreamSynchronize(st));
+		done = host_counters->next_path >= host_counters->total_paths && host_counters->n_next == 0;
+		if(host_counters->error)
+		{
+			break;
+		}
+		if(launches > max_launches)
+		{
+			break;
+		}
+		batch = std::min(batch * 2, 64);
+	}
+	PG_CUDA_CHECK(cudaEventRecord(e1, st));
+	PG_CUDA_CHECK(cudaEventSynchronize(e1));
+	float ms = 0.0f;
+	PG_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	const RenderCounters final_counters = *host_counters;
+	cudaFreeHost(host_counters);
+	cudaGraphExecDestroy(exec);
+	cudaGraphDestroy(graph);
+
+	m_last_rays = final_counters.rays_traced;
+	m_last_shadow = final_counters.shadow_rays;
+	m_last_iterations = launches * 2;
+	if(final_counters.error & PG_DEV_ERR_STACK)
+	{
+		throw Error(PG_ERR_STACK_OVERFLOW, "render: BVH traversal stack overflow");
+	}
+	if(!done)
+	{
+		throw Error(PG_ERR_ITERATION_LIMIT, "render: iteration limit reached before all paths finished");
+	}
+	return ms;
+}
+
+}// end namespace pg

@@ -1,0 +1,190 @@
+// Wavefront path tracer: scene records, per-path state in HBM, and the render driver.
+//
+// One render = W x H x spp independent paths of the BNEEPT (or BVPT) estimator. Paths live in a
+// fixed-capacity pool of slots; every iteration
+//   prepare  -> compacts bookkeeping and decides how many new camera paths join,
+//   regen    -> writes the new camera rays into the free tail of the ray queue,
+//   extend   -> closest hit for every queued ray (pg_trace.cu),
+//   shade    -> emission / NEE / BSDF sampling / Russian roulette per hit, writing continuing
+//               paths compacted (warp-aggregated) into the other buffer and shadow rays into the
+//               shadow queue,
+//   shadow   -> any hit for the shadow queue; unoccluded contributions are added to the path
+//               (or straight to the film for paths that ended at that vertex),
+// and the buffers swap. Two iterations (ping and pong) are captured in one CUDA graph.
+#pragma once
+
+#include "bsdf.cuh"
+#include "pg_common.cuh"
+#include "pg_geometry.h"
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+namespace pg
+{
+
+enum EmitterType : uint32_t
+{
+	PG_EMITTER_TRIANGLES = 0,   // a group of triangles with one constant radiance
+	PG_EMITTER_ENV = 1,         // constant environment radiance (the dome)
+};
+
+// 32-byte emitter record.
+struct alignas(16) EmitterRec
+{
+	float    r, g, b;        // emitted radiance
+	uint32_t type;
+	uint32_t first;          // first entry in the emitter-triangle list
+	uint32_t count;          // number of triangles
+	float    pmf;            // pick probability (power-proportional)
+	float    rcp_count;
+};
+
+// Pinhole camera: raster -> sensor -> world, as SingleLensObserver builds it
+// (Engine/Source/EngineEnv/Observer/SingleLensObserver.cpp:30-80,
+//  Engine/Source/EngineEnv/Observer/OrientedRasterObserver.cpp:48-100) and as
+// PinholeCamera::receiveRay uses it (Engine/Source/Core/Receiver/PinholeCamera.cpp:26-62).
+struct Camera
+{
+	float pos[3];
+	float axis_x[3], axis_y[3], axis_z[3];   // camera-to-world rotation columns
+	float sensor_w, sensor_h, sensor_offset; // metres
+	uint32_t width, height;
+};
+
+enum Estimator : uint32_t
+{
+	PG_EST_BNEEPT = 0,
+	PG_EST_BVPT = 1,
+};
+
+struct RenderParams
+{
+	uint32_t width = 0, height = 0;
+	uint32_t spp = 1;
+	uint32_t max_bounces = 10000;       // MAX_RAY_BOUNCES of the reference estimators
+	uint32_t estimator = PG_EST_BNEEPT;
+	uint64_t seed = 42;
+	uint64_t first_sample = 0;          // sample index offset (resume / replicas)
+	uint32_t capacity = 1u << 21;       // path slots in flight
+};
+
+// Host-side scene description handed to the renderer.
+struct SceneDesc
+{
+	std::vector<float>    tris;           // [n][3][3]
+	std::vector<uint32_t> tri_material;   // [n]
+	std::vector<uint32_t> tri_emitter;    // [n] emitter index + 1 (0 = none)
+	std::vector<Material> materials;
+	std::vector<EmitterRec> emitters;     // pmf / first / count filled by the scene builder
+	float env_rgb[3] = {0.0f, 0.0f, 0.0f};
+	bool  has_env = false;
+	// Surface area of the dome sphere (4 pi r^2, r = 1.01 x the farthest scene-bound corner from
+	// the dome centre, ADome.cpp:45-60); the environment's flux approximation is its luminance
+	// times this area (LatLongEnvEmitter.cpp:36-68), which sets its share of NEE samples.
+	double env_area = 0.0;
+	Camera camera{};
+};
+
+// Device view of a scene (all pointers are device memory).
+struct DeviceScene
+{
+	const WideNode*   nodes;
+	const LeafTri*    tris;
+	const Material*   materials;
+	const EmitterRec* emitters;
+	const uint32_t*   emitter_tris;     // leaf triangle indices, grouped per emitter
+	const float2*     alias;            // per emitter: (accept probability, alias index bits)
+	uint32_t          num_emitters;
+	int32_t           env_emitter;      // index of the environment emitter or -1
+	float             env_r, env_g, env_b;
+	Camera            cam;
+};
+
+// Counters shared by the kernels of one render (device memory).
+struct alignas(16) RenderCounters
+{
+	uint32_t n_active;      // continuing paths at the head of the current queue
+	uint32_t n_total;       // n_active + newly generated paths this iteration
+	uint32_t n_next;        // compaction counter of the next queue
+	uint32_t n_shadow;      // shadow queue length
+	unsigned long long next_path;   // next path index to generate
+	unsigned long long total_paths;
+	unsigned long long gen_base;    // first path index generated this iteration
+	unsigned long long rays_traced; // closest-hit rays (extension + camera)
+	unsigned long long shadow_rays;
+	uint32_t error;
+	uint32_t pad;
+};
+
+// Per-path state, one buffer of the ping-pong pair (structure of arrays).
+struct PathBuffers
+{
+	uint32_t* path;     // global path index
+	uint32_t* meta;     // bounce (bits 0-7) | flags
+	float4*   thr;      // throughput used for emission at this vertex (rgb), continuation factor (w)
+	float4*   rad;      // accumulated radiance (rgb), BSDF pdf of the ray that led here (w)
+	float4*   prev;     // previous vertex position (xyz), Russian-roulette scale (w)
+	float4*   ray_o;    // origin, tmin
+	float4*   ray_d;    // direction, tmax
+};
+
+struct ShadowQueue
+{
+	float4* o;          // origin, tmin
+	float4* d;          // direction, tmax
+	float4* c;          // contribution rgb, target (slot in next buffer, or 0x80000000|pixel)
+};
+
+constexpr uint32_t kMetaBounceMask = 0xFFu;
+constexpr uint32_t kMetaPrevNee = 1u << 8;      // the previous vertex used NEE (MIS applies)
+constexpr uint32_t kMetaStopAfter = 1u << 9;    // Russian roulette ended the path after this hit
+constexpr uint32_t kTargetFinal = 0x80000000u;
+
+// Launchers implemented in pg_trace.cu (FMA-enabled traversal kernels).
+void launch_extend(const DeviceScene& s, const RenderCounters* counters, const float4* ray_o,
+                   const float4* ray_d, uint2* hits, int grid, int block, cudaStream_t st);
+void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
+                   float4* rad_next, double* film, int grid, int block, cudaStream_t st);
+
+// A scene resident on the GPU together with its render buffers.
+class RenderScene
+{
+public:
+	explicit RenderScene(const SceneDesc& desc, float max_origin_abs);
+	~RenderScene();
+
+	// Renders `params` and accumulates into the FP64 film (sum of RGB per pixel). Returns the
+	// device time of the render in milliseconds (CUDA events on the library stream).
+	float render(const RenderParams& params, double* film_device);
+
+	const DeviceScene& device() const { return m_dev; }
+	const Geometry& geometry() const { return *m_geometry; }
+	unsigned long long last_rays() const { return m_last_rays; }
+	unsigned long long last_shadow_rays() const { return m_last_shadow; }
+	unsigned long long last_iterations() const { return m_last_iterations; }
+	float last_extend_ms() const { return m_last_extend_ms; }
+
+private:
+	void ensure_capacity(uint32_t capacity);
+
+	std::unique_ptr<Geometry> m_geometry;
+	DeviceBuffer<Material>    m_materials;
+	DeviceBuffer<EmitterRec>  m_emitters;
+	DeviceBuffer<uint32_t>    m_emitter_tris;
+	DeviceBuffer<float2>      m_alias;
+	DeviceScene               m_dev{};
+
+	uint32_t m_capacity = 0;
+	DeviceBuffer<uint32_t> m_path[2], m_meta[2];
+	DeviceBuffer<float4>   m_thr[2], m_rad[2], m_prev[2], m_ro[2], m_rd[2];
+	DeviceBuffer<uint2>    m_hits;
+	DeviceBuffer<float4>   m_so, m_sd, m_sc;
+	DeviceBuffer<RenderCounters> m_counters;
+
+	unsigned long long m_last_rays = 0, m_last_shadow = 0, m_last_iterations = 0;
+	float m_last_extend_ms = 0.0f;
+};
+
+}// end namespace pg

@@ -1,6 +1,7 @@
 // Geometry objects (triangles + compressed 8-wide BVH in HBM) and the ray-query entry points of
 // the C ABI (include/photon_gpu.h): closest hit, occlusion, and the counting pass.
 #include "pg_geometry.h"
+#include "pg_render.h"
 #include "trace.cuh"
 
 #include "../../include/photon_gpu.h"
@@ -183,7 +184,97 @@ void check_device_error(Geometry& g, cudaStream_t s)
 	}
 }
 
+// Closest hit for the render's ray queue; the queue length is read on the device.
+__global__ void __launch_bounds__(kTraceBlock)
+extend_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
+              const RenderCounters* __restrict__ counters,
+              const float4* __restrict__ ray_o, const float4* __restrict__ ray_d,
+              uint2* __restrict__ hits, uint32_t* __restrict__ error)
+{
+	const uint32_t n = counters->n_total;
+	uint32_t err = 0;
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		const float4 a = __ldg(ray_o + i);
+		const float4 b = __ldg(ray_d + i);
+		const RayTraits r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
+		float t;
+		uint32_t tri;
+		const bool hit = traverse<false>(r, nodes, tris, a.w, b.w, &t, &tri, &err);
+		hits[i] = make_uint2(hit ? tri : 0xFFFFFFFFu, __float_as_uint(t));
+	}
+	if(err)
+	{
+		atomicOr(error, err);
+	}
+}
+
+// Visibility of the NEE segments; unoccluded contributions go to the owning path (slot in the
+// next state buffer) or, for paths that ended at that vertex, straight to the FP64 film.
+__global__ void __launch_bounds__(kTraceBlock)
+shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
+              RenderCounters* __restrict__ counters,
+              const float4* __restrict__ so, const float4* __restrict__ sd, const float4* __restrict__ sc,
+              float4* __restrict__ rad_next, double* __restrict__ film, uint32_t* __restrict__ error)
+{
+	const uint32_t n = counters->n_shadow;
+	if(blockIdx.x == 0 && threadIdx.x == 0)
+	{
+		counters->shadow_rays += n;
+	}
+	uint32_t err = 0;
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		const float4 a = __ldg(so + i);
+		const float4 b = __ldg(sd + i);
+		const RayTraits r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
+		float t;
+		uint32_t tri;
+		if(traverse<true>(r, nodes, tris, a.w, b.w, &t, &tri, &err))
+		{
+			continue;
+		}
+		const float4 c = __ldg(sc + i);
+		const uint32_t target = __float_as_uint(c.w);
+		if(target & kTargetFinal)
+		{
+			const uint32_t pixel = target & ~kTargetFinal;
+			if(c.x != 0.0f) { atomicAdd(&film[3 * pixel + 0], static_cast<double>(c.x)); }
+			if(c.y != 0.0f) { atomicAdd(&film[3 * pixel + 1], static_cast<double>(c.y)); }
+			if(c.z != 0.0f) { atomicAdd(&film[3 * pixel + 2], static_cast<double>(c.z)); }
+		}
+		else
+		{
+			float4 rv = rad_next[target];
+			rv.x += c.x;
+			rv.y += c.y;
+			rv.z += c.z;
+			rad_next[target] = rv;
+		}
+	}
+	if(err)
+	{
+		atomicOr(error, err);
+	}
+}
+
 }// end anonymous namespace
+
+void launch_extend(const DeviceScene& s, const RenderCounters* counters, const float4* ray_o,
+                   const float4* ray_d, uint2* hits, int grid, int block, cudaStream_t st)
+{
+	extend_kernel<<<grid, block, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
+		const_cast<uint32_t*>(&counters->error));
+	PG_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
+                   float4* rad_next, double* film, int grid, int block, cudaStream_t st)
+{
+	shadow_kernel<<<grid, block, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, rad_next, film,
+		&counters->error);
+	PG_CUDA_CHECK(cudaGetLastError());
+}
 
 void launch_trace_closest(const Geometry& g, const float* d_rays, uint64_t n, void* d_hits, cudaStream_t s)
 {

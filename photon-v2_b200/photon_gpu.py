@@ -21,6 +21,7 @@ _lib: Optional[ctypes.CDLL] = None
 _f32p = ctypes.POINTER(ctypes.c_float)
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
 _dblp = ctypes.POINTER(ctypes.c_double)
 
 # (name, restype, argtypes) of every exported entry point.
@@ -39,6 +40,14 @@ PGPU_SIGNATURES = [
     ("pgpu_trace_counts", ctypes.c_int,
      [ctypes.c_uint64, _f32p, ctypes.c_uint64, ctypes.c_int, _dblp, _dblp]),
     ("pgpu_bsdf_eval", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
+    ("pgpu_scene_create", ctypes.c_int,
+     [_f32p, _u32p, _u32p, ctypes.c_uint64, _f32p, ctypes.c_uint32, _f32p, ctypes.c_uint32, _f32p, _u64p]),
+    ("pgpu_scene_destroy", ctypes.c_int, [ctypes.c_uint64]),
+    ("pgpu_scene_render", ctypes.c_int,
+     [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64,
+      _f32p, _u64p, _u64p]),
+    ("pgpu_scene_film", ctypes.c_int, [ctypes.c_uint64, _f32p, _dblp, _u64p]),
+    ("pgpu_scene_clear", ctypes.c_int, [ctypes.c_uint64]),
 ]
 
 
@@ -142,6 +151,80 @@ def bsdf_eval(cases: np.ndarray, normals: np.ndarray) -> np.ndarray:
     _check(load().pgpu_bsdf_eval(_ptr(c, ctypes.c_float), _ptr(nrm, ctypes.c_float), c.shape[0],
                                  _ptr(out, ctypes.c_float)))
     return out
+
+
+MATTE, CONDUCTOR, DIELECTRIC = 0, 1, 2
+BNEEPT, BVPT = 0, 1
+
+
+def flatten_scene(scene):
+    """Flat arrays of a ``scenes.Scene`` in the layout pgpu_scene_create expects."""
+    tris, tri_mat, tri_em, mats, ems = [], [], [], [], []
+    for g in scene.groups:
+        m = g.material
+        kind = {"matte": MATTE, "conductor": CONDUCTOR, "dielectric": DIELECTRIC}[m.kind]
+        c = m.albedo if m.kind == "matte" else m.f0
+        mats.append([kind, c[0], c[1], c[2], m.roughness, m.ior_outer, m.ior_inner, 0.0])
+        n = g.tris.shape[0]
+        tris.append(np.asarray(g.tris, np.float32).reshape(n, 9))
+        tri_mat.append(np.full(n, len(mats) - 1, np.uint32))
+        if g.radiance is not None:
+            ems.append([g.radiance[0], g.radiance[1], g.radiance[2], 0.0])
+            tri_em.append(np.full(n, len(ems), np.uint32))
+        else:
+            tri_em.append(np.zeros(n, np.uint32))
+    if scene.env_radiance is not None:
+        ems.append([scene.env_radiance[0], scene.env_radiance[1], scene.env_radiance[2], 1.0])
+    cam = np.array(list(scene.cam_pos) + list(scene.cam_dir) + list(scene.cam_up)
+                   + [scene.fov_deg, scene.width, scene.height], np.float32)
+    return (np.ascontiguousarray(np.concatenate(tris)), np.concatenate(tri_mat), np.concatenate(tri_em),
+            np.asarray(mats, np.float32).reshape(-1, 8), np.asarray(ems, np.float32).reshape(-1, 4), cam)
+
+
+class RenderScene:
+    """A scene resident on the GPU with its FP64 film (pgpu_scene_*)."""
+
+    def __init__(self, scene):
+        lib = load()
+        tris, tri_mat, tri_em, mats, ems, cam = flatten_scene(scene)
+        self.width, self.height = scene.width, scene.height
+        sid = ctypes.c_uint64(0)
+        em_ptr = _ptr(ems, ctypes.c_float) if ems.size else None
+        _check(lib.pgpu_scene_create(_ptr(tris, ctypes.c_float), _ptr(tri_mat, ctypes.c_uint32),
+                                     _ptr(tri_em, ctypes.c_uint32), tris.shape[0],
+                                     _ptr(mats, ctypes.c_float), mats.shape[0], em_ptr, ems.shape[0],
+                                     _ptr(cam, ctypes.c_float), ctypes.byref(sid)))
+        self.id = sid.value
+
+    def close(self):
+        if self.id:
+            _check(load().pgpu_scene_destroy(self.id))
+            self.id = 0
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def render(self, spp, max_bounces=10000, estimator=BNEEPT, seed=42, first_sample=0):
+        ms = ctypes.c_float()
+        rays, shadow = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(load().pgpu_scene_render(self.id, spp, max_bounces, estimator, seed, first_sample,
+                                        ctypes.byref(ms), ctypes.byref(rays), ctypes.byref(shadow)))
+        return {"ms": ms.value, "rays": rays.value, "shadow_rays": shadow.value}
+
+    def film(self):
+        """(developed float32 [H, W, 3], FP64 sums [H, W, 3], spp)."""
+        rgb = np.empty((self.height, self.width, 3), np.float32)
+        sums = np.empty((self.height, self.width, 3), np.float64)
+        spp = ctypes.c_uint64()
+        _check(load().pgpu_scene_film(self.id, _ptr(rgb, ctypes.c_float), _ptr(sums, ctypes.c_double),
+                                      ctypes.byref(spp)))
+        return rgb, sums, spp.value
+
+    def clear(self):
+        _check(load().pgpu_scene_clear(self.id))
 
 
 # ----------------------------------------------------------------------------------------------
