@@ -1,0 +1,367 @@
+"""Throughput benchmark of the GPU BNEEPT path tracer (and of the reference CPU renderer).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Default workload: the 1M-triangle GGX scene -- an icosphere subdivided 8 times (1,310,720
+triangles) with seeded 3-octave value-noise radial displacement (5 % of the radius) on a
+2-triangle ground, GGX conductors in 64 groups (roughness U[0.05, 0.5], F0 U[0.5, 1]), 2 quad
+lights + constant environment 0.1, 1024 x 1024, 256 spp, 10 bounces, FP32 shading with FP64 film.
+A step is one full render of that image through the Photon C API (phRender). The scene is
+generated in code from fixed seeds (synthetic data, no files).
+
+One JSON line is printed by rank 0. `value` is Mpaths/s (paths = W x H x spp rendered to
+completion) over all ranks, timed with CUDA events on the library's stream (max over ranks);
+`e2e` is the same metric through phRender + phAquireFrameRaw + phGetFrameRgbData with the
+frame copied to host memory, timed on the host clock. Multi-GPU runs are weak-scaled replicas:
+every rank renders the full image with its own sample numbering (paths are independent, no
+data-path collective).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "photon-v2_b200")
+sys.path.insert(0, PKG)
+
+import scenes  # noqa: E402
+
+METRIC = "Mpaths/s and equal-time relMSE: guided vs plain GPU BNEEPT on 1 B200"
+REF_RENDER = os.path.join(ROOT, "oracle", "_ref", "ph_ref_render")
+PORT_RENDER = os.path.join(ROOT, "oracle", "_build", "ph_port_render")
+
+
+def workload(name: str) -> scenes.Scene:
+    if name == "ggx_1m":
+        return scenes.ggx_sphere(level=8, width=1024, height=1024, spp=256, max_bounces=10)
+    if name == "cornell":
+        return scenes.cornell(256, 256, 64, 8)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def write_scene(scene: scenes.Scene, directory: str) -> str:
+    path = os.path.join(directory, "scene.p2")
+    with open(path, "w") as f:
+        f.write(scenes.to_sdl(scene))
+    if scene.env_radiance is not None:
+        scenes.write_pfm(os.path.join(directory, "env.pfm"),
+                         np.array(scene.env_radiance, np.float32).reshape(1, 1, 3))
+    return path
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu_index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+# Reference CPU cost per path on this workload family, measured on the build container's cores
+# (1.0 Mpaths/s with 8 threads on the 1M-triangle GGX scene); only used to size the bounded CPU
+# sample so that it runs for about `target_seconds` -- the reported number is always measured.
+EST_CPU_PATHS_PER_CORE_S = 0.13e6
+
+
+def cpu_sample(scene: scenes.Scene, tmp: str, target_seconds: float = 12.0, repeats: int = 1) -> list:
+    """Times the reference CPU renderer (or, without it, the oracle port) on a bounded sample of
+    the same workload -- the same scene with fewer samples per pixel -- on all host threads.
+    Returns one record per repeat (phUpdate untimed, phRender timed)."""
+    threads = os.cpu_count() or 1
+    tool, kind = (REF_RENDER, "reference") if os.path.exists(REF_RENDER) else (PORT_RENDER, "port")
+    if not os.path.exists(tool):
+        return [{"value": None, "unit": "Mpaths/s", "cores": threads, "kind": kind,
+                 "sample": "unavailable: neither oracle/_ref/ph_ref_render nor the port is built"}]
+    per_spp_paths = scene.width * scene.height
+    spp = int(max(1, min(scene.spp, round(target_seconds * EST_CPU_PATHS_PER_CORE_S * threads / per_spp_paths))))
+    s = scenes.Scene(**{**scene.__dict__, "spp": spp})
+    d = tempfile.mkdtemp(dir=tmp)
+    p2 = write_scene(s, d)
+    out = subprocess.run([tool, p2, str(threads), str(scene.max_bounces), os.path.join(d, "out.rgbf32"),
+                          str(repeats)], cwd=d, capture_output=True, text=True, check=True)
+    records = []
+    for line in out.stdout.splitlines():
+        if not line.startswith("{"):
+            continue
+        r = json.loads(line)
+        paths = per_spp_paths * spp
+        records.append({
+            "value": paths / r["render_s"] / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": kind,
+            "sample": f"{scene.width}x{scene.height} x {spp} spp of the same scene ({paths} paths), phRender "
+                      f"only ({r['render_s']:.2f} s); scene load {r['load_s']:.1f} s and update "
+                      f"{r['update_s']:.1f} s excluded"})
+    return records
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    scene = workload(args.workload)
+    with tempfile.TemporaryDirectory() as tmp:
+        samples = cpu_sample(scene, tmp, target_seconds=args.cpu_seconds, repeats=args.warmup + args.steps)
+        timed = samples[args.warmup:] if len(samples) > args.warmup else samples
+        vals = [s["value"] for s in timed if s["value"]]
+        value = statistics.median(vals) if vals else None
+        base = timed[-1]
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpaths/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": (scene.width * scene.height * scene.spp / (value * 1e6) * 1e3) if value else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": args.workload, "width": scene.width, "height": scene.height,
+                       "spp": scene.spp, "max_bounces": scene.max_bounces, "triangles": scene.num_tris},
+            "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": base["cores"], "kind": base["kind"],
+                             "sample": base["sample"]},
+            "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+
+
+def run_ours(args) -> None:
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local_rank))
+        dist = dist_mod
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    import photon_gpu
+
+    photon_gpu.load()
+    scene = workload(args.workload)
+    if args.spp:
+        scene.spp = args.spp
+    paths_per_step = scene.width * scene.height * scene.spp
+    l2_flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > 126 MB L2
+
+    with tempfile.TemporaryDirectory() as tmp:
+        p2 = write_scene(scene, tmp)
+        eng = photon_gpu.PhotonEngine()
+        eng.set_working_directory(tmp)
+        t0 = time.time()
+        assert eng.load_file(p2), eng.errors()
+        load_s = time.time() - t0
+        eng.set_max_bounces(scene.max_bounces)
+        eng.set_seed(1000003 * rank + 7)
+        eng.update()
+        update_s = eng.info()["update_seconds"]
+
+        for _ in range(args.warmup):
+            eng.clear_film()
+            eng.render()
+
+        # Traversal counts (untimed): nodes / triangles per ray for the algorithmic-bytes model.
+        counts = eng.profile(2, 4)
+        # Per-kernel device times with CUDA events around each launch (untimed pass).
+        kprof = eng.profile(1, scene.spp)
+
+        # ---- timed region: device time of K full renders
+        barrier()
+        with ClockSampler(local_rank) as clocks:
+            device_ms = 0.0
+            launches = 0
+            wall0 = time.time()
+            for _ in range(args.steps):
+                l2_flush.fill_(1.0)
+                torch.cuda.synchronize()
+                eng.clear_film()
+                eng.render()
+                info = eng.info()
+                assert info["paths"] == paths_per_step
+                device_ms += info["device_ms"]
+                launches += eng.launch_count()
+            wall = time.time() - wall0
+        barrier()
+        device_ms = max_over_ranks(device_ms)
+        value = world * paths_per_step * args.steps / (device_ms / 1e3) / 1e6
+
+        # ---- end to end through the public C API, frame copied to host every step
+        barrier()
+        e2e_s = 0.0
+        for _ in range(args.steps):
+            eng.clear_film()
+            t = time.time()
+            eng.render()
+            frame = eng.frame()
+            e2e_s += time.time() - t
+        barrier()
+        e2e_s = max_over_ranks(e2e_s)
+        e2e_value = world * paths_per_step * args.steps / e2e_s / 1e6
+        d2h = int(scene.width * scene.height * 3 * 8)   # FP64 film sums read back to develop the frame
+        mean_rgb = frame.reshape(-1, 3).mean(0).tolist()
+        eng.close()
+
+        # ---- roofline of the dominant kernel
+        peaks = measured_peaks()
+        kernel_ms = {k: kprof[k] for k in ("prepare_ms", "regen_ms", "extend_ms", "shade_ms", "shadow_ms")}
+        total_k = sum(kernel_ms.values())
+        rays = kprof["rays"]
+        shadow_rays = kprof["shadow_rays"]
+        nodes_per_ray = counts["nodes_closest"] / max(1.0, counts["rays"])
+        tris_per_ray = counts["tris_closest"] / max(1.0, counts["rays"])
+        s_nodes = counts["nodes_any"] / max(1.0, counts["shadow_rays"])
+        s_tris = counts["tris_any"] / max(1.0, counts["shadow_rays"])
+        # bytes per closest-hit ray: 32 ray in + 8 hit out + 80 per node + 48 per triangle
+        bytes_closest = 40.0 + 80.0 * nodes_per_ray + 48.0 * tris_per_ray
+        bytes_shadow = 48.0 + 80.0 * s_nodes + 48.0 * s_tris
+        dominant = max(("extend_ms", "shadow_ms", "shade_ms"), key=lambda k: kernel_ms[k])
+        if dominant == "shadow_ms":
+            alg_bytes, launches_k, kname = bytes_shadow * shadow_rays, kprof["iterations"], "shadow (any hit)"
+        elif dominant == "extend_ms":
+            alg_bytes, launches_k, kname = bytes_closest * rays, kprof["iterations"], "extend (closest hit)"
+        else:
+            # shade: ray + hit + state in/out + triangle + shadow record per queued ray
+            alg_bytes = (32 + 8 + 80 + 48 + 112 + 48) * rays
+            launches_k, kname = kprof["iterations"], "shade"
+        achieved = alg_bytes / (kernel_ms[dominant] / 1e3) / 1e9
+        traffic = None
+        prof_path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+        if os.path.exists(prof_path):
+            with open(prof_path) as f:
+                traffic = json.load(f).get(dominant)
+
+    clock = clocks.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": device_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": args.workload, "width": scene.width, "height": scene.height, "spp": scene.spp,
+                   "max_bounces": scene.max_bounces, "triangles": scene.num_tris, "estimator": "bneept",
+                   "l2": "256 MiB write between timed steps", "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
+                "path": "phRender + phAquireFrameRaw + phGetFrameRgbData (scene resident after phUpdate)"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "peak_source": peaks["source"],
+                     "model": {"bytes_per_closest_ray": bytes_closest, "nodes_per_closest_ray": nodes_per_ray,
+                               "tris_per_closest_ray": tris_per_ray, "bytes_per_shadow_ray": bytes_shadow,
+                               "nodes_per_shadow_ray": s_nodes, "tris_per_shadow_ray": s_tris}},
+        "kernel_ms_per_step": {k: v for k, v in kernel_ms.items()},
+        "kernel_share": {k: v / total_k for k, v in kernel_ms.items()},
+        "rays_per_step": {"closest": rays, "shadow": shadow_rays},
+        "mrays_per_s": (rays + shadow_rays) / (device_ms / args.steps / 1e3) / 1e6,
+        "clocks": {"sm_mhz": clock["sm_mhz"], "sm_max_mhz": clock["sm_max_mhz"], "reasons": clock["reasons"]},
+        "host": {"scene_load_s": load_s, "update_s": update_s, "wall_s_timed": wall, "image_mean_rgb": mean_rgb},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as tmp:
+            line["cpu_baseline"] = cpu_sample(scene, tmp, target_seconds=args.cpu_seconds)[-1]
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ggx_1m")
+    ap.add_argument("--spp", type=int, default=0, help="override samples per pixel")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

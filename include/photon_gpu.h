@@ -113,6 +113,18 @@ PGPU_API int pgpu_scene_render(uint64_t id, uint32_t spp, uint32_t max_bounces, 
 PGPU_API int pgpu_scene_film(uint64_t id, float* out_rgb, double* out_sum, uint64_t* out_spp);
 PGPU_API int pgpu_scene_clear(uint64_t id);
 
+/* ---------------------------------------------------------------------------------------------
+ * Scene cooking without a GPU: parses SDL text (the grammar of the reference's SdlCommandParser,
+ * Engine/Source/SDL/SdlCommandParser.cpp:84-560) and cooks it the way phUpdate does (actors to
+ * world-space triangles, materials, emitters, camera). Call once with NULL arrays to get the
+ * counts, then again with arrays of those sizes. out_dims: uint32 [4] = width, height, spp,
+ * estimator. out_emitters: float32 [e][4] = radiance rgb, type. out_camera: float32 [16] =
+ * position, camera x/y/z axes, sensor width, height, offset (metres), dome area. */
+PGPU_API int pgpu_sdl_cook(const char* sdl_text, const char* working_dir, uint64_t* out_num_tris,
+                           uint32_t* out_num_materials, uint32_t* out_num_emitters, uint32_t* out_dims,
+                           float* out_tris, uint32_t* out_tri_material, uint32_t* out_tri_emitter,
+                           float* out_emitters, float* out_camera);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,6 +8,8 @@
 //     tris: float32 [N][3][3]; rays: float32 [M][8] = origin(3), minT, direction(3), maxT.
 //     out:  per ray int32 prim (-1 = miss), float32 t, b0, b1, b2, int32 occluded.
 //
+// energy <r> <g> <b> <watts>   (see run_energy)
+//
 // bsdf  <cases.f32> <out.f32>
 //     Evaluates LambertianReflector, OpaqueMicrofacet (IsoTrowbridgeReitzConstant + Schlick) and
 //     TranslucentMicrofacet (IsoTrowbridgeReitzConstant + exact dielectric Fresnel) through the
@@ -266,8 +268,23 @@ int run_bsdf(const char* casesPath, const char* outPath)
 
 }// end anonymous namespace
 
+// energy <r> <g> <b> <watts>: the radiance colour an area light of that colour and power gets,
+// Spectrum(color).putEnergy(watts) (Engine/Source/Actor/Light/AAreaLight.cpp:57-58), and the
+// relative luminance of the colour.
+int run_energy(float r, float g, float b, float watts)
+{
+	const math::Spectrum c(std::array<real, 3>{r, g, b});
+	const auto e = math::Spectrum(c).putEnergy(watts);
+	std::printf("%.9g %.9g %.9g %.9g\n", e[0], e[1], e[2], c.relativeLuminance());
+	return 0;
+}
+
 int main(int argc, char** argv)
 {
+	if(argc >= 6 && std::string(argv[1]) == "energy")
+	{
+		return run_energy(std::stof(argv[2]), std::stof(argv[3]), std::stof(argv[4]), std::stof(argv[5]));
+	}
 	if(argc >= 5 && std::string(argv[1]) == "hits")
 	{
 		return run_hits(argv[2], argv[3], argv[4]);

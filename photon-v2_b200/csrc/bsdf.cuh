@@ -31,6 +31,7 @@ enum MaterialType : uint32_t
 	PG_MAT_MATTE = 0,
 	PG_MAT_CONDUCTOR = 1,
 	PG_MAT_DIELECTRIC = 2,
+	PG_MAT_ABSORBER = 3,     // IdealAbsorber: never measurable (the surface of an area light)
 };
 
 // 32-byte material record. For matte: c = albedo. Conductor: c = F0, alpha. Dielectric:
@@ -191,8 +192,10 @@ __device__ __forceinline__ bool half_vector_same_hemisphere(V3 l, V3 v, V3 n, V3
 
 __device__ __forceinline__ RGB schlick(RGB f0, float cos_i)
 {
-	const float c = fabsf(cos_i);
-	const float m = powf(1.0f - c, 5.0f);
+	// std::pow(float, int) promotes to double in the reference; x^5 in double then to float.
+	const double x = static_cast<double>(1.0f - fabsf(cos_i));
+	const double x2 = x * x;
+	const float m = static_cast<float>(x2 * x2 * x);
 	return RGB{(1.0f - f0.r) * m + f0.r, (1.0f - f0.g) * m + f0.g, (1.0f - f0.b) * m + f0.b};
 }
 
@@ -251,7 +254,7 @@ struct BsdfSample
 // calcBsdf: returns false when not measurable.
 __device__ __forceinline__ bool bsdf_eval(const Material& mat, const Frame& f, V3 l, V3 v, RGB* out)
 {
-	if(!sidedness_agreed(f, l) || !sidedness_agreed(f, v))
+	if(!sidedness_agreed(f, l) || !sidedness_agreed(f, v) || mat.type == PG_MAT_ABSORBER)
 	{
 		return false;
 	}
@@ -345,7 +348,7 @@ __device__ __forceinline__ bool bsdf_eval(const Material& mat, const Frame& f, V
 // `operator bool` on lta::PDF requires a finite positive value).
 __device__ __forceinline__ float bsdf_pdf(const Material& mat, const Frame& f, V3 l, V3 v)
 {
-	if(!sidedness_agreed(f, l) || !sidedness_agreed(f, v))
+	if(!sidedness_agreed(f, l) || !sidedness_agreed(f, v) || mat.type == PG_MAT_ABSORBER)
 	{
 		return 0.0f;
 	}
@@ -429,7 +432,7 @@ __device__ __forceinline__ BsdfSample bsdf_sample(const Material& mat, const Fra
 	s.cos = 0.0f;
 	s.weight = RGB{0.0f, 0.0f, 0.0f};
 	s.l = v3(0.0f, 0.0f, 0.0f);
-	if(!sidedness_agreed(f, v))
+	if(!sidedness_agreed(f, v) || mat.type == PG_MAT_ABSORBER)
 	{
 		return s;
 	}

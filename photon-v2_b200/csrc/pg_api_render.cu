@@ -1,6 +1,6 @@
 // Render-scene entry points of the low-level C ABI (include/photon_gpu.h): a flat scene
 // description in, FP64 film sums and developed frames out.
-#include "pg_render.h"
+#include "pg_render_object.h"
 #include "scene_build.h"
 
 #include "../../include/photon_gpu.h"
@@ -11,15 +11,6 @@
 
 namespace pg
 {
-
-struct RenderObject
-{
-	std::unique_ptr<RenderScene> scene;
-	DeviceBuffer<double> film;
-	uint32_t width = 0, height = 0;
-	uint64_t samples = 0;     // samples per pixel accumulated in the film
-	float last_ms = 0.0f;
-};
 
 Registry<RenderObject>& render_registry()
 {
@@ -70,6 +61,13 @@ std::unique_ptr<RenderObject> make_render_object(SceneDesc&& desc)
 	PG_CUDA_CHECK(cudaMemsetAsync(obj->film.get(), 0, obj->film.bytes(), library_stream()));
 	PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
 	return obj;
+}
+
+void download_film(const RenderObject& r, double* out_sum)
+{
+	const std::size_t n = static_cast<std::size_t>(r.width) * r.height * 3;
+	PG_CUDA_CHECK(cudaMemcpyAsync(out_sum, r.film.get(), n * sizeof(double), cudaMemcpyDeviceToHost, library_stream()));
+	PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
 }
 
 }// end namespace pg

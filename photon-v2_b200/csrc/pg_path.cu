@@ -8,6 +8,7 @@
 // iteration of one path.
 #include "pg_render.h"
 #include "refinery.cuh"
+#include "scene_build.h"
 
 #include "../../include/photon_gpu.h"
 
@@ -69,7 +70,7 @@ enum : uint32_t
 // (RussianRoulette.h:30-55 -> TSpectrumBase::relativeLuminance).
 __device__ __forceinline__ float luminance(RGB c)
 {
-	return 0.2126729f * c.r + 0.7151522f * c.g + 0.0721750f * c.b;
+	return static_cast<float>(kLumR) * c.r + static_cast<float>(kLumG) * c.g + static_cast<float>(kLumB) * c.b;
 }
 
 __device__ __forceinline__ float4 ld4(const float4* p) { return *p; }
@@ -354,7 +355,8 @@ shade_kernel(ShadeArgs a)
 		// Every material here is non-delta, so NEE applies at every vertex of BNEEPT
 		// (TDirectLightEstimator::isNeeSamplable); a black Lambertian surface can gain nothing
 		// from it, so its shadow ray is skipped (its contribution would be exactly zero).
-		const bool black_matte = mat.type == PG_MAT_MATTE && mat.cr == 0.0f && mat.cg == 0.0f && mat.cb == 0.0f;
+		const bool black_matte = (mat.type == PG_MAT_MATTE && mat.cr == 0.0f && mat.cg == 0.0f && mat.cb == 0.0f) ||
+		                         mat.type == PG_MAT_ABSORBER;
 		const bool nee_samplable = !bvpt;
 		const bool use_nee = nee_samplable && s.num_emitters > 0 && !black_matte;
 		if(use_nee)
@@ -609,16 +611,20 @@ RenderScene::RenderScene(const SceneDesc& desc, float max_origin_abs)
 		emitters[e].count = static_cast<uint32_t>(list.size());
 		emitters[e].rcp_count = list.empty() ? 0.0f : 1.0f / static_cast<float>(list.size());
 		emitter_tris.insert(emitter_tris.end(), list.begin(), list.end());
-		const double lum = 0.2126729 * emitters[e].r + 0.7151522 * emitters[e].g + 0.0721750 * emitters[e].b;
 		if(emitters[e].type == PG_EMITTER_ENV)
 		{
+			// luminance x sin(theta) summed over the 1x1 image, times the dome area
+			// (LatLongEnvEmitter.cpp:36-68)
 			env_index = static_cast<int32_t>(e);
+			const double lum = kLumR * emitters[e].r + kLumG * emitters[e].g + kLumB * emitters[e].b;
 			weights[e] = std::max(lum, 1e-6) * desc.env_area;
 		}
 		else
 		{
-			// radiant flux approximation: radiance * area * pi (DiffuseSurfaceEmitter.cpp:55-86)
-			weights[e] = list.empty() ? 0.0 : std::max(lum, 0.0) * area[e] * 3.14159265358979323846;
+			// radiant flux approximation: energy(radiance) * area * pi, summed over the group
+			// (DiffuseSurfaceEmitter.cpp:55-86, GroupedDiffuseSurfaceEmitter.cpp:110-120)
+			weights[e] = list.empty() ? 0.0
+				: color_energy(emitters[e].r, emitters[e].g, emitters[e].b) * area[e] * 3.14159265358979323846;
 		}
 	}
 	std::vector<float2> alias;
@@ -725,71 +731,122 @@ float RenderScene::render(const RenderParams& params, double* film)
 	}
 	ShadowQueue sq{m_so.get(), m_sd.get(), m_sc.get()};
 	const uint64_t first_global = params.first_sample * wh;
+	const bool counting = params.mode == PG_RENDER_COUNT;
 
-	// One graph = two iterations (ping -> pong -> ping).
-	cudaGraph_t graph;
-	cudaGraphExec_t exec;
-	PG_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-	for(int b = 0; b < 2; ++b)
+	// The five launches of one iteration; `ev` (optional) brackets each with events.
+	auto iteration = [&](int b, cudaEvent_t* ev)
 	{
 		const PathBuffers& cur = buf[b];
 		const PathBuffers& nxt = buf[1 - b];
-		prepare_kernel<<<1, 32, 0, st>>>(m_counters.get(), m_capacity < capacity ? m_capacity : capacity);
+		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[0], st)); }
+		prepare_kernel<<<1, 32, 0, st>>>(m_counters.get(), capacity);
+		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[1], st)); }
 		regen_kernel<<<grid, kShadeBlock, 0, st>>>(m_counters.get(), m_dev.cam, params.seed, first_global, cur);
-		launch_extend(m_dev, m_counters.get(), cur.ray_o, cur.ray_d, m_hits.get(), grid, 128, st);
+		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[2], st)); }
+		launch_extend(m_dev, m_counters.get(), cur.ray_o, cur.ray_d, m_hits.get(), grid, 128, st, counting);
+		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[3], st)); }
 		ShadeArgs sa{m_dev, cur, nxt, m_hits.get(), sq, m_counters.get(), film, params.seed, first_global,
 		             params.max_bounces, params.estimator, static_cast<uint32_t>(wh)};
 		shade_kernel<<<grid, kShadeBlock, 0, st>>>(sa);
-		launch_shadow(m_dev, m_counters.get(), sq, nxt.rad, film, grid, 128, st);
-	}
-	PG_CUDA_CHECK(cudaStreamEndCapture(st, &graph));
-	PG_CUDA_CHECK(cudaGraphInstantiate(&exec, graph, 0));
+		PG_CUDA_CHECK(cudaGetLastError());
+		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[4], st)); }
+		launch_shadow(m_dev, m_counters.get(), sq, nxt.rad, film, grid, 128, st, counting);
+		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[5], st)); }
+	};
 
 	RenderCounters* host_counters = nullptr;
 	PG_CUDA_CHECK(cudaMallocHost(&host_counters, sizeof(RenderCounters)));
-
 	cudaEvent_t e0, e1;
 	PG_CUDA_CHECK(cudaEventCreate(&e0));
 	PG_CUDA_CHECK(cudaEventCreate(&e1));
-	PG_CUDA_CHECK(cudaEventRecord(e0, st));
-	unsigned long long launches = 0;
-	const unsigned long long max_launches = 1ull << 24;
-	int batch = 4;
+	unsigned long long iterations = 0;
+	const unsigned long long max_iterations = 1ull << 25;
 	bool done = false;
-	while(!done)
+	for(double& k : m_kernel_ms) { k = 0.0; }
+
+	if(params.mode == PG_RENDER_GRAPH)
 	{
-		for(int k = 0; k < batch; ++k)
+		// One graph = two iterations (ping -> pong -> ping).
+		cudaGraph_t graph;
+		cudaGraphExec_t exec;
+		PG_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+		iteration(0, nullptr);
+		iteration(1, nullptr);
+		PG_CUDA_CHECK(cudaStreamEndCapture(st, &graph));
+		PG_CUDA_CHECK(cudaGraphInstantiate(&exec, graph, 0));
+		PG_CUDA_CHECK(cudaEventRecord(e0, st));
+		int batch = 4;
+		while(!done && iterations < max_iterations)
 		{
-			PG_CUDA_CHECK(cudaGraphLaunch(exec, st));
+			for(int k = 0; k < batch; ++k)
+			{
+				PG_CUDA_CHECK(cudaGraphLaunch(exec, st));
+			}
+			iterations += 2ull * batch;
+			PG_CUDA_CHECK(cudaMemcpyAsync(host_counters, m_counters.get(), sizeof(RenderCounters), cudaMemcpyDeviceToHost, st));
+			PG_CUDA_CHECK(cudaStreamSynchronize(st));
+			done = host_counters->next_path >= host_counters->total_paths && host_counters->n_next == 0;
+			if(host_counters->error)
+			{
+				break;
+			}
+			batch = std::min(batch * 2, 64);
 		}
-		launches += batch;
-		PG_CUDA_CHECK(cudaMemcpyAsync(host_counters, m_counters.get(), sizeof(RenderCounters), cudaMemcpyDeviceToHost, st));
-		PG_CUDA_CHECK(cudaStreamSynchronize(st));
-		done = host_counters->next_path >= host_counters->total_paths && host_counters->n_next == 0;
-		if(host_counters->error)
-		{
-			break;
-		}
-		if(launches > max_launches)
-		{
-			break;
-		}
-		batch = std::min(batch * 2, 64);
+		PG_CUDA_CHECK(cudaEventRecord(e1, st));
+		PG_CUDA_CHECK(cudaEventSynchronize(e1));
+		cudaGraphExecDestroy(exec);
+		cudaGraphDestroy(graph);
 	}
-	PG_CUDA_CHECK(cudaEventRecord(e1, st));
-	PG_CUDA_CHECK(cudaEventSynchronize(e1));
+	else
+	{
+		// Plain launches, one iteration at a time; in timing mode every kernel is bracketed by
+		// events on the launching stream and the durations are summed per kernel.
+		cudaEvent_t ev[6];
+		const bool timing = params.mode == PG_RENDER_TIMING;
+		for(cudaEvent_t& e : ev) { PG_CUDA_CHECK(cudaEventCreate(&e)); }
+		PG_CUDA_CHECK(cudaEventRecord(e0, st));
+		int b = 0;
+		while(!done && iterations < max_iterations)
+		{
+			iteration(b, timing ? ev : nullptr);
+			b = 1 - b;
+			++iterations;
+			PG_CUDA_CHECK(cudaMemcpyAsync(host_counters, m_counters.get(), sizeof(RenderCounters), cudaMemcpyDeviceToHost, st));
+			PG_CUDA_CHECK(cudaStreamSynchronize(st));
+			if(timing)
+			{
+				for(int k = 0; k < 5; ++k)
+				{
+					float ms = 0.0f;
+					PG_CUDA_CHECK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+					m_kernel_ms[k] += ms;
+				}
+			}
+			done = host_counters->next_path >= host_counters->total_paths && host_counters->n_next == 0;
+			if(host_counters->error)
+			{
+				break;
+			}
+		}
+		PG_CUDA_CHECK(cudaEventRecord(e1, st));
+		PG_CUDA_CHECK(cudaEventSynchronize(e1));
+		for(cudaEvent_t& e : ev) { cudaEventDestroy(e); }
+	}
+
 	float ms = 0.0f;
 	PG_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	const RenderCounters final_counters = *host_counters;
 	cudaFreeHost(host_counters);
-	cudaGraphExecDestroy(exec);
-	cudaGraphDestroy(graph);
 
 	m_last_rays = final_counters.rays_traced;
 	m_last_shadow = final_counters.shadow_rays;
-	m_last_iterations = launches * 2;
+	m_last_iterations = iterations;
+	m_last_counts[0] = final_counters.nodes_closest;
+	m_last_counts[1] = final_counters.tris_closest;
+	m_last_counts[2] = final_counters.nodes_any;
+	m_last_counts[3] = final_counters.tris_any;
 	if(final_counters.error & PG_DEV_ERR_STACK)
 	{
 		throw Error(PG_ERR_STACK_OVERFLOW, "render: BVH traversal stack overflow");

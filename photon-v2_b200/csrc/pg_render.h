@@ -59,6 +59,13 @@ enum Estimator : uint32_t
 	PG_EST_BVPT = 1,
 };
 
+enum RenderMode : uint32_t
+{
+	PG_RENDER_GRAPH = 0,    // iterations captured in a CUDA graph (the production path)
+	PG_RENDER_TIMING = 1,   // plain launches with per-kernel CUDA events (profiling)
+	PG_RENDER_COUNT = 2,    // plain launches, traversal kernels count nodes and triangles
+};
+
 struct RenderParams
 {
 	uint32_t width = 0, height = 0;
@@ -68,6 +75,7 @@ struct RenderParams
 	uint64_t seed = 42;
 	uint64_t first_sample = 0;          // sample index offset (resume / replicas)
 	uint32_t capacity = 1u << 21;       // path slots in flight
+	uint32_t mode = PG_RENDER_GRAPH;
 };
 
 // Host-side scene description handed to the renderer.
@@ -114,6 +122,8 @@ struct alignas(16) RenderCounters
 	unsigned long long gen_base;    // first path index generated this iteration
 	unsigned long long rays_traced; // closest-hit rays (extension + camera)
 	unsigned long long shadow_rays;
+	unsigned long long nodes_closest, tris_closest;   // counting mode only
+	unsigned long long nodes_any, tris_any;
 	uint32_t error;
 	uint32_t pad;
 };
@@ -143,10 +153,10 @@ constexpr uint32_t kMetaStopAfter = 1u << 9;    // Russian roulette ended the pa
 constexpr uint32_t kTargetFinal = 0x80000000u;
 
 // Launchers implemented in pg_trace.cu (FMA-enabled traversal kernels).
-void launch_extend(const DeviceScene& s, const RenderCounters* counters, const float4* ray_o,
-                   const float4* ray_d, uint2* hits, int grid, int block, cudaStream_t st);
+void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4* ray_o,
+                   const float4* ray_d, uint2* hits, int grid, int block, cudaStream_t st, bool count);
 void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
-                   float4* rad_next, double* film, int grid, int block, cudaStream_t st);
+                   float4* rad_next, double* film, int grid, int block, cudaStream_t st, bool count);
 
 // A scene resident on the GPU together with its render buffers.
 class RenderScene
@@ -164,7 +174,11 @@ public:
 	unsigned long long last_rays() const { return m_last_rays; }
 	unsigned long long last_shadow_rays() const { return m_last_shadow; }
 	unsigned long long last_iterations() const { return m_last_iterations; }
-	float last_extend_ms() const { return m_last_extend_ms; }
+	// Per-kernel device milliseconds of the last timing-mode render: prepare, regen, extend,
+	// shade, shadow.
+	const double* last_kernel_ms() const { return m_kernel_ms; }
+	// Nodes / triangles visited by closest-hit and any-hit queries in the last counting render.
+	const unsigned long long* last_counts() const { return m_last_counts; }
 
 private:
 	void ensure_capacity(uint32_t capacity);
@@ -184,7 +198,8 @@ private:
 	DeviceBuffer<RenderCounters> m_counters;
 
 	unsigned long long m_last_rays = 0, m_last_shadow = 0, m_last_iterations = 0;
-	float m_last_extend_ms = 0.0f;
+	unsigned long long m_last_counts[4] = {0, 0, 0, 0};
+	double m_kernel_ms[5] = {0, 0, 0, 0, 0};
 };
 
 }// end namespace pg

@@ -184,15 +184,17 @@ void check_device_error(Geometry& g, cudaStream_t s)
 	}
 }
 
-// Closest hit for the render's ray queue; the queue length is read on the device.
+// Closest hit for the render's ray queue; the queue length is read on the device. COUNT adds
+// the visited-node / tested-triangle tallies of the counting render.
+template<bool COUNT>
 __global__ void __launch_bounds__(kTraceBlock)
 extend_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
-              const RenderCounters* __restrict__ counters,
+              RenderCounters* __restrict__ counters,
               const float4* __restrict__ ray_o, const float4* __restrict__ ray_d,
-              uint2* __restrict__ hits, uint32_t* __restrict__ error)
+              uint2* __restrict__ hits)
 {
 	const uint32_t n = counters->n_total;
-	uint32_t err = 0;
+	uint32_t err = 0, node_count = 0, tri_count = 0;
 	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		const float4 a = __ldg(ray_o + i);
@@ -200,29 +202,35 @@ extend_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tr
 		const RayTraits r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
 		float t;
 		uint32_t tri;
-		const bool hit = traverse<false>(r, nodes, tris, a.w, b.w, &t, &tri, &err);
+		const bool hit = traverse<false, COUNT>(r, nodes, tris, a.w, b.w, &t, &tri, &err, &node_count, &tri_count);
 		hits[i] = make_uint2(hit ? tri : 0xFFFFFFFFu, __float_as_uint(t));
+	}
+	if(COUNT)
+	{
+		atomicAdd(&counters->nodes_closest, static_cast<unsigned long long>(node_count));
+		atomicAdd(&counters->tris_closest, static_cast<unsigned long long>(tri_count));
 	}
 	if(err)
 	{
-		atomicOr(error, err);
+		atomicOr(&counters->error, err);
 	}
 }
 
 // Visibility of the NEE segments; unoccluded contributions go to the owning path (slot in the
 // next state buffer) or, for paths that ended at that vertex, straight to the FP64 film.
+template<bool COUNT>
 __global__ void __launch_bounds__(kTraceBlock)
 shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
               RenderCounters* __restrict__ counters,
               const float4* __restrict__ so, const float4* __restrict__ sd, const float4* __restrict__ sc,
-              float4* __restrict__ rad_next, double* __restrict__ film, uint32_t* __restrict__ error)
+              float4* __restrict__ rad_next, double* __restrict__ film)
 {
 	const uint32_t n = counters->n_shadow;
 	if(blockIdx.x == 0 && threadIdx.x == 0)
 	{
 		counters->shadow_rays += n;
 	}
-	uint32_t err = 0;
+	uint32_t err = 0, node_count = 0, tri_count = 0;
 	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		const float4 a = __ldg(so + i);
@@ -230,7 +238,7 @@ shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tr
 		const RayTraits r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
 		float t;
 		uint32_t tri;
-		if(traverse<true>(r, nodes, tris, a.w, b.w, &t, &tri, &err))
+		if(traverse<true, COUNT>(r, nodes, tris, a.w, b.w, &t, &tri, &err, &node_count, &tri_count))
 		{
 			continue;
 		}
@@ -252,27 +260,44 @@ shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tr
 			rad_next[target] = rv;
 		}
 	}
+	if(COUNT)
+	{
+		atomicAdd(&counters->nodes_any, static_cast<unsigned long long>(node_count));
+		atomicAdd(&counters->tris_any, static_cast<unsigned long long>(tri_count));
+	}
 	if(err)
 	{
-		atomicOr(error, err);
+		atomicOr(&counters->error, err);
 	}
 }
 
 }// end anonymous namespace
 
-void launch_extend(const DeviceScene& s, const RenderCounters* counters, const float4* ray_o,
-                   const float4* ray_d, uint2* hits, int grid, int block, cudaStream_t st)
+void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4* ray_o,
+                   const float4* ray_d, uint2* hits, int grid, int block, cudaStream_t st, bool count)
 {
-	extend_kernel<<<grid, block, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
-		const_cast<uint32_t*>(&counters->error));
+	if(count)
+	{
+		extend_kernel<true><<<grid, block, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits);
+	}
+	else
+	{
+		extend_kernel<false><<<grid, block, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits);
+	}
 	PG_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
-                   float4* rad_next, double* film, int grid, int block, cudaStream_t st)
+                   float4* rad_next, double* film, int grid, int block, cudaStream_t st, bool count)
 {
-	shadow_kernel<<<grid, block, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, rad_next, film,
-		&counters->error);
+	if(count)
+	{
+		shadow_kernel<true><<<grid, block, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, rad_next, film);
+	}
+	else
+	{
+		shadow_kernel<false><<<grid, block, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, rad_next, film);
+	}
 	PG_CUDA_CHECK(cudaGetLastError());
 }
 

@@ -109,6 +109,36 @@ Material make_dielectric(float roughness, float ior_outer, float ior_inner)
 	return m;
 }
 
+namespace
+{
+// Energy of the seven Smits basis spectra (white, cyan, magenta, yellow, red, green, blue) as the
+// reference's upsampling sums them, obtained by running its estimate_color_energy on the seven
+// basis colours. With Smits' decomposition (min * white + (mid - min) * secondary +
+// (max - mid) * primary) they give the energy of any colour.
+constexpr double kSmitsEnergy[7] = {
+	0.999678004, 0.539849638, 0.734938899, 0.704456255, 0.454419964, 0.258257833, 0.302870461};
+}
+
+double color_energy(double r, double g, double b)
+{
+	const double W = kSmitsEnergy[0], C = kSmitsEnergy[1], M = kSmitsEnergy[2], Y = kSmitsEnergy[3];
+	const double R = kSmitsEnergy[4], G = kSmitsEnergy[5], B = kSmitsEnergy[6];
+	double e;
+	if(r <= g && r <= b)
+	{
+		e = r * W + (g <= b ? (g - r) * C + (b - g) * B : (b - r) * C + (g - b) * G);
+	}
+	else if(g <= r && g <= b)
+	{
+		e = g * W + (r <= b ? (r - g) * M + (b - r) * B : (b - g) * M + (r - b) * R);
+	}
+	else
+	{
+		e = b * W + (r <= g ? (r - b) * Y + (g - r) * G : (g - b) * Y + (r - g) * R);
+	}
+	return e > 0.0 ? e : 0.0;
+}
+
 double dome_area(const std::vector<float>& tris, const float center[3])
 {
 	double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};

@@ -21,6 +21,16 @@ Material make_matte(float r, float g, float b);
 Material make_conductor(float roughness, float f0r, float f0g, float f0b);
 Material make_dielectric(float roughness, float ior_outer, float ior_inner);
 
+// Energy of a linear-sRGB colour as the reference estimates it (estimate_color_energy,
+// Engine/Source/Math/Color/color_spaces.ipp:744-764: Smits' RGB -> spectrum upsampling, then the
+// sum of the spectral samples). Drives area-light radiance from watts and the power-proportional
+// light pick.
+double color_energy(double r, double g, double b);
+
+// Relative luminance (CIE Y) of linear sRGB with the coefficients of the reference's colour
+// transform (TSpectrumBase::relativeLuminance).
+constexpr double kLumR = 0.212639004, kLumG = 0.715168655, kLumB = 0.0721923187;
+
 // Surface area of the dome sphere around the scene (ADome::cook, Engine/Source/Actor/ADome.cpp:
 // 45-60: radius = 1.01 x the farthest bound corner from the dome centre, at least 1).
 double dome_area(const std::vector<float>& tris, const float center[3]);

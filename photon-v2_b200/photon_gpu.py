@@ -48,6 +48,8 @@ PGPU_SIGNATURES = [
       _f32p, _u64p, _u64p]),
     ("pgpu_scene_film", ctypes.c_int, [ctypes.c_uint64, _f32p, _dblp, _u64p]),
     ("pgpu_scene_clear", ctypes.c_int, [ctypes.c_uint64]),
+    ("pgpu_sdl_cook", ctypes.c_int,
+     [ctypes.c_char_p, ctypes.c_char_p, _u64p, _u32p, _u32p, _u32p, _f32p, _u32p, _u32p, _f32p, _f32p]),
 ]
 
 
@@ -230,7 +232,189 @@ class RenderScene:
 # ----------------------------------------------------------------------------------------------
 # Photon C API (ph_c_core.h) declared on the same library.
 
-PH_SIGNATURES = []
+_u8pp = ctypes.POINTER(ctypes.POINTER(ctypes.c_ubyte))
+_f32pp = ctypes.POINTER(_f32p)
+_charpp = ctypes.POINTER(ctypes.c_char_p)
+
+PH_SIGNATURES = [
+    ("phConfigRendererResourceDirectory", None, [ctypes.c_char_p]),
+    ("phInit", ctypes.c_int, []),
+    ("phExit", ctypes.c_int, []),
+    ("phCreateEngine", None, [_u64p, ctypes.c_uint32]),
+    ("phSetNumRenderThreads", None, [ctypes.c_uint64, ctypes.c_uint32]),
+    ("phEnterCommand", None, [ctypes.c_uint64, ctypes.c_char_p]),
+    ("phLoadCommands", ctypes.c_int, [ctypes.c_uint64, ctypes.c_char_p]),
+    ("phRender", None, [ctypes.c_uint64]),
+    ("phUpdate", None, [ctypes.c_uint64]),
+    ("phGetRenderDimension", None, [ctypes.c_uint64, _u32p, _u32p]),
+    ("phGetObservableRenderData", None, [ctypes.c_uint64, ctypes.c_void_p]),
+    ("phDeleteEngine", None, [ctypes.c_uint64]),
+    ("phSetWorkingDirectory", None, [ctypes.c_uint64, ctypes.c_char_p]),
+    ("phAquireFrame", None, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
+    ("phAquireFrameRaw", None, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
+    ("phCreateFrame", None, [_u64p, ctypes.c_uint32, ctypes.c_uint32]),
+    ("phGetFrameDimension", None, [ctypes.c_uint64, _u32p, _u32p]),
+    ("phGetFrameRgbData", None, [ctypes.c_uint64, _f32pp]),
+    ("phDeleteFrame", None, [ctypes.c_uint64]),
+    ("phLoadFrame", ctypes.c_int, [ctypes.c_uint64, ctypes.c_char_p]),
+    ("phSaveFrame", ctypes.c_int, [ctypes.c_uint64, ctypes.c_char_p, ctypes.c_void_p]),
+    ("phSaveFrameToBuffer", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),
+    ("phFrameOpAbsDifference", None, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
+    ("phFrameOpMSE", ctypes.c_float, [ctypes.c_uint64, ctypes.c_uint64]),
+    ("phCreateBuffer", None, [_u64p]),
+    ("phGetBufferBytes", None, [ctypes.c_uint64, _u8pp, ctypes.POINTER(ctypes.c_size_t)]),
+    ("phDeleteBuffer", None, [ctypes.c_uint64]),
+    ("phAsyncGetRenderProgress", None, [ctypes.c_uint64, ctypes.c_void_p]),
+    ("phAsyncGetRenderStatistics", None, [ctypes.c_uint64, _f32p, _f32p]),
+    ("phAsyncGetRenderState", None, [ctypes.c_uint64, ctypes.c_void_p]),
+    ("phAsyncPollUpdatedFrameRegion", ctypes.c_int, [ctypes.c_uint64, ctypes.c_void_p]),
+    ("phAsyncPollUpdatedFrameRegions", ctypes.c_size_t,
+     [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_size_t]),
+    ("phAsyncPollMergedUpdatedFrameRegions", ctypes.c_size_t,
+     [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t]),
+    ("phAsyncPeekFrame", None,
+     [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+      ctypes.c_uint64]),
+    ("phAsyncPeekFrameRaw", None,
+     [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+      ctypes.c_uint64]),
+    ("phGpuGetErrors", ctypes.c_int, [ctypes.c_uint64, _charpp]),
+    ("phGpuSetMaxRayBounces", None, [ctypes.c_uint64, ctypes.c_uint32]),
+    ("phGpuSetSeed", None, [ctypes.c_uint64, ctypes.c_uint64]),
+    ("phGpuClearFilm", None, [ctypes.c_uint64]),
+    ("phGpuGetRenderInfo", None, [ctypes.c_uint64, _dblp, _u64p, _u64p, _u64p, _dblp]),
+    ("phGpuGetLaunchCount", ctypes.c_uint64, [ctypes.c_uint64]),
+    ("phGpuProfileRender", None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, _dblp]),
+]
+
+
+class CookedScene:
+    """Result of pgpu_sdl_cook: what phUpdate would upload, computed on the host."""
+
+    def __init__(self, sdl_text: str, working_dir: str = "."):
+        lib = load()
+        txt = sdl_text.encode()
+        wd = working_dir.encode()
+        n = ctypes.c_uint64()
+        nm, ne = ctypes.c_uint32(), ctypes.c_uint32()
+        dims = np.zeros(4, np.uint32)
+        _check(lib.pgpu_sdl_cook(txt, wd, ctypes.byref(n), ctypes.byref(nm), ctypes.byref(ne),
+                                 _ptr(dims, ctypes.c_uint32), None, None, None, None, None))
+        self.tris = np.empty((n.value, 3, 3), np.float32)
+        self.tri_material = np.empty(n.value, np.uint32)
+        self.tri_emitter = np.empty(n.value, np.uint32)
+        self.emitters = np.empty((ne.value, 4), np.float32)
+        self.camera = np.empty(16, np.float32)
+        _check(lib.pgpu_sdl_cook(txt, wd, ctypes.byref(n), ctypes.byref(nm), ctypes.byref(ne),
+                                 _ptr(dims, ctypes.c_uint32), _ptr(self.tris, ctypes.c_float),
+                                 _ptr(self.tri_material, ctypes.c_uint32), _ptr(self.tri_emitter, ctypes.c_uint32),
+                                 _ptr(self.emitters, ctypes.c_float) if ne.value else None,
+                                 _ptr(self.camera, ctypes.c_float)))
+        self.num_materials = nm.value
+        self.width, self.height, self.spp, self.estimator = (int(x) for x in dims)
+
+
+class PhotonEngine:
+    """The Photon C API (phCreateEngine ... phAquireFrameRaw) on this library."""
+
+    def __init__(self, threads: int = 1):
+        lib = load()
+        if not lib.phInit():
+            raise PhotonGpuError(PG_ERR_NO_DEVICE, "phInit failed (no CUDA device?)")
+        eid = ctypes.c_uint64()
+        lib.phCreateEngine(ctypes.byref(eid), threads)
+        self.id = eid.value
+
+    def enter(self, text: str) -> None:
+        load().phEnterCommand(self.id, text.encode())
+
+    def load_file(self, path: str) -> bool:
+        return bool(load().phLoadCommands(self.id, path.encode()))
+
+    def set_working_directory(self, path: str) -> None:
+        load().phSetWorkingDirectory(self.id, path.encode())
+
+    def set_max_bounces(self, n: int) -> None:
+        load().phGpuSetMaxRayBounces(self.id, n)
+
+    def set_seed(self, seed: int) -> None:
+        load().phGpuSetSeed(self.id, seed)
+
+    def update(self) -> None:
+        load().phUpdate(self.id)
+        self._raise_errors()
+
+    def render(self) -> None:
+        load().phRender(self.id)
+        self._raise_errors()
+
+    def clear_film(self) -> None:
+        load().phGpuClearFilm(self.id)
+
+    def errors(self) -> str:
+        msg = ctypes.c_char_p()
+        load().phGpuGetErrors(self.id, ctypes.byref(msg))
+        return (msg.value or b"").decode(errors="replace")
+
+    def _raise_errors(self) -> None:
+        err = self.errors()
+        fatal = [line for line in err.splitlines() if "failed" in line]
+        if fatal:
+            raise PhotonGpuError(PG_ERR_SCENE, "\n".join(fatal))
+
+    def dimension(self):
+        w, h = ctypes.c_uint32(), ctypes.c_uint32()
+        load().phGetRenderDimension(self.id, ctypes.byref(w), ctypes.byref(h))
+        return w.value, h.value
+
+    def info(self) -> dict:
+        ms, upd = ctypes.c_double(), ctypes.c_double()
+        paths, rays, shadow = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        load().phGpuGetRenderInfo(self.id, ctypes.byref(ms), ctypes.byref(paths), ctypes.byref(rays),
+                                  ctypes.byref(shadow), ctypes.byref(upd))
+        return {"device_ms": ms.value, "paths": paths.value, "rays": rays.value,
+                "shadow_rays": shadow.value, "update_seconds": upd.value}
+
+    def launch_count(self) -> int:
+        return int(load().phGpuGetLaunchCount(self.id))
+
+    def profile(self, mode: int, spp: int) -> dict:
+        """phGpuProfileRender: mode 1 per-kernel timing, mode 2 traversal counting."""
+        stats = np.zeros(14, np.float64)
+        load().phGpuProfileRender(self.id, mode, spp, _ptr(stats, ctypes.c_double))
+        self._raise_errors()
+        keys = ["prepare_ms", "regen_ms", "extend_ms", "shade_ms", "shadow_ms", "total_ms", "paths",
+                "rays", "shadow_rays", "iterations", "nodes_closest", "tris_closest", "nodes_any", "tris_any"]
+        return dict(zip(keys, stats.tolist()))
+
+    def frame(self) -> np.ndarray:
+        """phCreateFrame + phAquireFrameRaw + phGetFrameRgbData: float32 [H, W, 3], row 0 bottom."""
+        lib = load()
+        w, h = self.dimension()
+        fid = ctypes.c_uint64()
+        lib.phCreateFrame(ctypes.byref(fid), w, h)
+        try:
+            lib.phAquireFrameRaw(self.id, 0, fid.value)
+            data = _f32p()
+            lib.phGetFrameRgbData(fid.value, ctypes.byref(data))
+            return np.ctypeslib.as_array(data, shape=(h, w, 3)).copy()
+        finally:
+            lib.phDeleteFrame(fid.value)
+
+    def close(self) -> None:
+        if self.id:
+            load().phDeleteEngine(self.id)
+            self.id = 0
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+PG_ERR_SCENE = 6
+PG_ERR_NO_DEVICE = 7
 
 
 def _declare_ph_api(lib: ctypes.CDLL) -> None:

@@ -218,6 +218,24 @@ def cornell(width: int = 256, height: int = 256, spp: int = 64, max_bounces: int
                  fov_deg=40.0, groups=groups, estimator=estimator)
 
 
+def cornell_glossy(width: int = 64, height: int = 64, spp: int = 64, max_bounces: int = 8,
+                   estimator: str = "bneept") -> Scene:
+    """Cornell box whose tall box is a rough GGX dielectric (IOR 1.5, roughness 0.1) and whose
+    short box is a GGX conductor (roughness 0.3, gold-like F0): exercises every BSDF."""
+    sc = cornell(width, height, spp, max_bounces, estimator)
+    L = 555.0
+    floor = quad((0, 0, 0), (0, 0, L), (L, 0, L), (L, 0, 0))
+    ceiling = quad((0, L, 0), (L, L, 0), (L, L, L), (0, L, L))
+    back = quad((0, 0, L), (0, L, L), (L, L, L), (L, 0, L))
+    short_box = box((185.5, 82.5, 169.0), (165.0, 165.0, 165.0), -18.0)
+    tall_box = box((368.5, 165.0, 351.5), (165.0, 330.0, 165.0), 15.0)
+    sc.groups[0] = MeshGroup(np.concatenate([floor, ceiling, back]), WHITE)
+    sc.groups[3] = MeshGroup(short_box, Material("conductor", roughness=0.3, f0=(1.0, 0.77, 0.34)))
+    sc.groups.insert(4, MeshGroup(tall_box, Material("dielectric", roughness=0.1, ior_outer=1.0, ior_inner=1.5)))
+    sc.name = "cornell_glossy"
+    return sc
+
+
 def ggx_sphere(level: int = 8, width: int = 1024, height: int = 1024, spp: int = 256,
                max_bounces: int = 10, num_groups: int = 64, seed: int = 1,
                with_env: bool = True, estimator: str = "bneept") -> Scene:
@@ -318,7 +336,7 @@ def to_sdl(scene: Scene, env_image_name: str = "env.pfm") -> str:
             lines.append(f"actor(model-light) @a{gi} = [geometry geometry @g{gi}] "
                          f"[material material @{mname}] [image emitted-energy @e{gi}];")
     if scene.env_radiance is not None:
-        lines.append(f'actor(image-dome) @dome = [resource-identifier? image-file "{env_image_name}"];')
+        lines.append(f'actor(image-dome) @dome = [PRI image-file ":{env_image_name}"];')
     return "\n".join(lines) + "\n"
 
 

@@ -1,0 +1,68 @@
+"""Reference renders for the image-parity tests, made by the reference CPU renderer itself.
+
+Run in the build container after building the oracle (``make -f oracle/Makefile.ref -j8``):
+
+    python tests/golden/make_golden_images.py
+
+For each workload below the scene is generated by photon-v2_b200/scenes.py, written as SDL, and
+rendered with oracle/_ref/ph_ref_render (phLoadCommands -> phUpdate -> phRender ->
+phAquireFrameRaw). The developed frames go to images.npz (float32 [H, W, 3], row 0 = bottom)
+together with the spp and bounce cap used. Every workload is small (64 x 64) and rendered with
+many samples so that its own noise stays well below the parity bar.
+"""
+
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "photon-v2_b200"))
+
+import scenes  # noqa: E402
+
+RENDER_TOOL = os.path.join(ROOT, "oracle", "_ref", "ph_ref_render")
+
+# name -> (scene factory, spp, max bounces)
+WORKLOADS = {
+    "cornell_bneept": (lambda spp: scenes.cornell(64, 64, spp, 8, "bneept"), 8192, 8),
+    "cornell_bvpt": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvpt"), 8192, 8),
+    "cornell_glossy_bneept": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 8192, 8),
+    "ggx_sphere_env_bneept": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
+                                                            max_bounces=10), 4096, 10),
+}
+
+
+def render(scene: scenes.Scene, max_bounces: int, threads: int) -> np.ndarray:
+    with tempfile.TemporaryDirectory() as tmp:
+        p2 = os.path.join(tmp, "scene.p2")
+        with open(p2, "w") as f:
+            f.write(scenes.to_sdl(scene))
+        if scene.env_radiance is not None:
+            scenes.write_pfm(os.path.join(tmp, "env.pfm"),
+                             np.array(scene.env_radiance, np.float32).reshape(1, 1, 3))
+        out = os.path.join(tmp, "out.rgbf32")
+        subprocess.run([RENDER_TOOL, p2, str(threads), str(max_bounces), out], check=True, cwd=tmp,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        return np.fromfile(out, np.float32).reshape(scene.height, scene.width, 3)
+
+
+def main() -> None:
+    if not os.path.exists(RENDER_TOOL):
+        raise SystemExit(f"{RENDER_TOOL} missing: run `make -f oracle/Makefile.ref -j8` first")
+    threads = os.cpu_count() or 1
+    arrays = {}
+    for name, (factory, spp, bounces) in WORKLOADS.items():
+        img = render(factory(spp), bounces, threads)
+        arrays[name] = img
+        arrays[name + "__spp"] = np.array(spp)
+        arrays[name + "__bounces"] = np.array(bounces)
+        print(f"{name}: mean {img.mean(axis=(0, 1))}")
+    np.savez_compressed(os.path.join(HERE, "images.npz"), **arrays)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,128 @@
+"""Host-side scene cooking through the library's SDL parser (no GPU needed).
+
+The parser follows the reference grammar (Engine/Source/SDL/SdlCommandParser.cpp:84-560,
+SdlInlinePacketInterface.cpp:48-245); cooking follows the actors it supports (AModel,
+AModelLight, ARectangleLight, AImageDome) and bakes actor transforms (TDecomposedTransform:
+T * R * S) into world-space triangles.
+"""
+
+import math
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import photon_gpu
+import scenes
+
+
+def _cook(text, wd="."):
+    return photon_gpu.CookedScene(text, wd)
+
+
+def test_cornell_cooks_to_generator_triangles():
+    s = scenes.cornell()
+    c = _cook(scenes.to_sdl(s))
+    ref = np.concatenate([g.tris for g in s.groups])
+    assert np.array_equal(c.tris.view(np.uint32), ref.view(np.uint32))
+    assert (c.width, c.height, c.spp, c.estimator) == (256, 256, 64, 0)
+    assert c.emitters.shape == (1, 4) and np.allclose(c.emitters[0], [17, 12, 4, 0])
+    # light triangles are the last group
+    assert np.all(c.tri_emitter[-2:] == 1) and np.all(c.tri_emitter[:-2] == 0)
+    # camera looking down +z with +y up: camera x = -x (world), y = +y, z = -z
+    cam = c.camera
+    assert np.allclose(cam[0:3], [278, 273, -800])
+    assert np.allclose(cam[3:6], [-1, 0, 0]) and np.allclose(cam[6:9], [0, 1, 0]) and np.allclose(cam[9:12], [0, 0, -1])
+    # 40 degree horizontal field of view on a 36 mm sensor
+    assert abs(cam[14] - (0.018 / math.tan(math.radians(20.0)))) < 1e-6
+
+
+def test_bvpt_and_materials():
+    s = scenes.cornell_glossy(estimator="bvpt")
+    c = _cook(scenes.to_sdl(s))
+    assert c.estimator == 1
+    assert c.num_materials == len(s.groups)
+
+
+def test_streamed_fragments_equal_whole_text():
+    text = scenes.to_sdl(scenes.cornell(32, 32, 4))
+    whole = _cook(text)
+    # split the text at arbitrary points, including inside comments and tokens
+    pieces = [text[i:i + 97] for i in range(0, len(text), 97)]
+    eng_text = "// leading comment\n" + "".join(pieces)
+    again = _cook(eng_text)
+    assert np.array_equal(whole.tris, again.tris)
+
+
+def test_reference_style_scene_with_transforms_and_area_light():
+    text = """#version 1.1.0;
+option(single-frame-render-session) @session = [vector2 frame-size "40 30"] [string visualizer @visualizer]
+    [string observer @observer] [string sample-source @sampler];
+observer(single-lens) @observer = [real fov-degrees 50] [vector3 pos "0 0 16"] [vector3 dir "0 0 -1"] [vector3 up-axis "0 1 0"];
+sample-source(stratified) @sampler = [integer samples 40];
+visualizer(path-tracing) @visualizer = [enum sample-filter box] [enum estimator bneept];
+geometry(rectangle) @boxWall = [real width 1] [real height 1];
+image(constant) @white = [real-array values "0.7 0.7 0.7"][enum color-space LSRGB];
+// top light
+actor(rectangle-light) @topLight = [spectrum color "1 1 1"][real watts 500][real width 3][real height 3];
+translate(@topLight) = [vector3 amount "0 4.75 0"];
+rotate(@topLight)    = [vector3 axis "1 0 0"] [real degrees 90];
+material(matte-opaque) @wallMat = [image albedo @white];
+actor(model) @bottomWall = [geometry geometry @boxWall] [material material @wallMat];
+actor(model).translate(@bottomWall) = [vector3 amount "0 -5 0"];
+actor(model).rotate(@bottomWall)    = [vector3 axis "1 0 0"] [real degrees -90];
+actor(model).scale(@bottomWall)     = [vector3 amount "10 10 10"];
+"""
+    c = _cook(text)
+    assert (c.width, c.height, c.spp) == (40, 30, 40)
+    assert c.tris.shape[0] == 4
+    light = c.tris[c.tri_emitter == 1]
+    floor = c.tris[c.tri_emitter == 0]
+    # the light lies in the plane y = 4.75 (rectangle in XY rotated +90 deg about x), facing -y
+    assert np.allclose(light[:, :, 1], 4.75, atol=1e-5)
+    n = np.cross(light[:, 1] - light[:, 0], light[:, 2] - light[:, 0])
+    assert np.all(n[:, 1] < 0)
+    # the floor is the 10 x 10 square at y = -5 facing +y
+    assert np.allclose(floor[:, :, 1], -5.0, atol=1e-5)
+    assert np.isclose(np.abs(floor[:, :, 0]).max(), 5.0, atol=1e-5)
+    n = np.cross(floor[:, 1] - floor[:, 0], floor[:, 2] - floor[:, 0])
+    assert np.all(n[:, 1] > 0)
+    # radiance = watts / (area * pi * energy(white)), the reference's putEnergy normalisation
+    expected = 500.0 / (9.0 * math.pi * 0.999678004)
+    assert np.allclose(c.emitters[0, :3], expected, rtol=1e-5)
+
+
+def test_environment_dome(tmp_path):
+    s = scenes.ggx_sphere(level=2, width=16, height=16, spp=1)
+    scenes.write_pfm(str(tmp_path / "env.pfm"), np.full((1, 1, 3), 0.1, np.float32))
+    c = _cook(scenes.to_sdl(s), str(tmp_path))
+    env = c.emitters[c.emitters[:, 3] == 1]
+    assert env.shape[0] == 1 and np.allclose(env[0, :3], 0.1)
+    # dome radius: 1.01 x the farthest bound corner from the origin
+    tris = c.tris.reshape(-1, 3)
+    lo, hi = tris.min(0), tris.max(0)
+    corners = np.array([[x, y, z] for x in (lo[0], hi[0]) for y in (lo[1], hi[1]) for z in (lo[2], hi[2])])
+    r = max(1.0, np.linalg.norm(corners, axis=1).max() * 1.01)
+    assert np.isclose(c.camera[15], 4 * math.pi * r * r, rtol=1e-5)
+
+
+@pytest.mark.parametrize("snippet, message", [
+    ("geometry(sphere) @g = [real radius 1];\nactor(model) @a = [geometry geometry @g] [material material @m];\n"
+     "material(matte-opaque) @m = ;", "not supported"),
+    ("actor(model) @a = [geometry geometry @g] [material material @m] [bad", "clause"),
+])
+def test_errors_are_reported(snippet, message):
+    base = scenes.to_sdl(scenes.cornell(8, 8, 1))
+    with pytest.raises(photon_gpu.PhotonGpuError) as err:
+        _cook(base + snippet)
+    assert message in str(err.value)
+
+
+def test_degenerate_triangles_are_dropped():
+    s = scenes.cornell(8, 8, 1)
+    g = s.groups[0]
+    bad = np.zeros((1, 3, 3), np.float32)
+    g.tris = np.concatenate([g.tris, bad])
+    c = _cook(scenes.to_sdl(s))
+    assert c.tris.shape[0] == 36
