@@ -145,8 +145,16 @@ def cpu_sample(scene: scenes.Scene, tmp: str, target_seconds: float = 12.0, repe
     spp = int(max(1, min(scene.spp, round(target_seconds * EST_CPU_PATHS_PER_CORE_S * threads / per_spp_paths))))
     s = scenes.Scene(**{**scene.__dict__, "spp": spp})
     d = tempfile.mkdtemp(dir=tmp)
-    p2 = write_scene(s, d)
-    out = subprocess.run([tool, p2, str(threads), str(scene.max_bounces), os.path.join(d, "out.rgbf32"),
+    if kind == "reference":
+        scene_file = write_scene(s, d)   # SDL, loaded through phLoadCommands
+    else:
+        import photon_gpu
+        from oracle.port import port as oracle_port
+
+        scene_file = os.path.join(d, "scene.bin")
+        oracle_port.write_scene_bin(scene_file, photon_gpu.flatten_scene(s), spp,
+                                    0 if s.estimator == "bneept" else 1)
+    out = subprocess.run([tool, scene_file, str(threads), str(scene.max_bounces), os.path.join(d, "out.rgbf32"),
                           str(repeats)], cwd=d, capture_output=True, text=True, check=True)
     records = []
     for line in out.stdout.splitlines():
@@ -156,8 +164,9 @@ def cpu_sample(scene: scenes.Scene, tmp: str, target_seconds: float = 12.0, repe
         paths = per_spp_paths * spp
         records.append({
             "value": paths / r["render_s"] / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": kind,
-            "sample": f"{scene.width}x{scene.height} x {spp} spp of the same scene ({paths} paths), phRender "
-                      f"only ({r['render_s']:.2f} s); scene load {r['load_s']:.1f} s and update "
+            "sample": f"{scene.width}x{scene.height} x {spp} spp of the same scene ({paths} paths), "
+                      f"{'phRender' if kind == 'reference' else 'oracle port render'} only "
+                      f"({r['render_s']:.2f} s); scene load {r['load_s']:.1f} s and update "
                       f"{r['update_s']:.1f} s excluded"})
     return records
 

@@ -221,14 +221,20 @@ def cornell(width: int = 256, height: int = 256, spp: int = 64, max_bounces: int
 def cornell_glossy(width: int = 64, height: int = 64, spp: int = 64, max_bounces: int = 8,
                    estimator: str = "bneept") -> Scene:
     """Cornell box whose tall box is a rough GGX dielectric (IOR 1.5, roughness 0.1) and whose
-    short box is a GGX conductor (roughness 0.3, gold-like F0): exercises every BSDF."""
+    short box is a GGX conductor (roughness 0.3, gold-like F0): exercises every BSDF.
+
+    The glass box floats one unit above the floor. Resting on it, its bottom face would be
+    coplanar with the floor, and a ray leaving the glass downwards would hit both at (nearly) the
+    same t: which one the reference reports depends on its BVH traversal order and last-ulp
+    rounding, and the two answers (refract out of the glass vs. a diffuse bounce) carry different
+    energy, so such a scene has no well-defined expected image."""
     sc = cornell(width, height, spp, max_bounces, estimator)
     L = 555.0
     floor = quad((0, 0, 0), (0, 0, L), (L, 0, L), (L, 0, 0))
     ceiling = quad((0, L, 0), (L, L, 0), (L, L, L), (0, L, L))
     back = quad((0, 0, L), (0, L, L), (L, L, L), (L, 0, L))
     short_box = box((185.5, 82.5, 169.0), (165.0, 165.0, 165.0), -18.0)
-    tall_box = box((368.5, 165.0, 351.5), (165.0, 330.0, 165.0), 15.0)
+    tall_box = box((368.5, 166.0, 351.5), (165.0, 330.0, 165.0), 15.0)
     sc.groups[0] = MeshGroup(np.concatenate([floor, ceiling, back]), WHITE)
     sc.groups[3] = MeshGroup(short_box, Material("conductor", roughness=0.3, f0=(1.0, 0.77, 0.34)))
     sc.groups.insert(4, MeshGroup(tall_box, Material("dielectric", roughness=0.1, ior_outer=1.0, ior_inner=1.5)))

@@ -2,7 +2,9 @@
 
 Run in the build container after building the oracle (``make -f oracle/Makefile.ref -j8``):
 
-    python tests/golden/make_golden_images.py
+    python tests/golden/make_golden_images.py [workload ...]
+
+With workload names given, only those are re-rendered and the rest of images.npz is kept.
 
 For each workload below the scene is generated by photon-v2_b200/scenes.py, written as SDL, and
 rendered with oracle/_ref/ph_ref_render (phLoadCommands -> phUpdate -> phRender ->
@@ -54,14 +56,18 @@ def main() -> None:
     if not os.path.exists(RENDER_TOOL):
         raise SystemExit(f"{RENDER_TOOL} missing: run `make -f oracle/Makefile.ref -j8` first")
     threads = os.cpu_count() or 1
-    arrays = {}
+    path = os.path.join(HERE, "images.npz")
+    only = sys.argv[1:]
+    arrays = dict(np.load(path)) if only and os.path.exists(path) else {}
     for name, (factory, spp, bounces) in WORKLOADS.items():
+        if only and name not in only:
+            continue
         img = render(factory(spp), bounces, threads)
         arrays[name] = img
         arrays[name + "__spp"] = np.array(spp)
         arrays[name + "__bounces"] = np.array(bounces)
         print(f"{name}: mean {img.mean(axis=(0, 1))}")
-    np.savez_compressed(os.path.join(HERE, "images.npz"), **arrays)
+    np.savez_compressed(path, **arrays)
 
 
 if __name__ == "__main__":
