@@ -251,8 +251,12 @@ struct BsdfSample
 	bool  ok;
 };
 
+// bsdf_eval / bsdf_pdf / bsdf_sample are kept out of line: each holds all three surface optics,
+// and the shade kernel calls pdf twice. Inlined copies made that kernel large enough to stall
+// on instruction fetch.
+//
 // calcBsdf: returns false when not measurable.
-__device__ __forceinline__ bool bsdf_eval(const Material& mat, const Frame& f, V3 l, V3 v, RGB* out)
+static __device__ __noinline__ bool bsdf_eval(const Material& mat, const Frame& f, V3 l, V3 v, RGB* out)
 {
 	if(!sidedness_agreed(f, l) || !sidedness_agreed(f, v) || mat.type == PG_MAT_ABSORBER)
 	{
@@ -346,7 +350,7 @@ __device__ __forceinline__ bool bsdf_eval(const Material& mat, const Frame& f, V
 
 // calcBsdfPdf: returns the solid-angle pdf, or 0 for an empty/invalid pdf (the reference's
 // `operator bool` on lta::PDF requires a finite positive value).
-__device__ __forceinline__ float bsdf_pdf(const Material& mat, const Frame& f, V3 l, V3 v)
+static __device__ __noinline__ float bsdf_pdf(const Material& mat, const Frame& f, V3 l, V3 v)
 {
 	if(!sidedness_agreed(f, l) || !sidedness_agreed(f, v) || mat.type == PG_MAT_ABSORBER)
 	{
@@ -424,7 +428,7 @@ __device__ __forceinline__ float bsdf_pdf(const Material& mat, const Frame& f, V
 
 // genBsdfSample with three uniform numbers (u0, u1 for the direction, u2 for the dielectric
 // reflect/transmit pick, which the reference draws with `unflowedPick`).
-__device__ __forceinline__ BsdfSample bsdf_sample(const Material& mat, const Frame& f, V3 v, float u0, float u1, float u2)
+static __device__ __noinline__ BsdfSample bsdf_sample(const Material& mat, const Frame& f, V3 v, float u0, float u1, float u2)
 {
 	BsdfSample s;
 	s.ok = false;

@@ -26,7 +26,9 @@ constexpr float kFloatMin = 1.17549435e-38f;   // std::numeric_limits<float>::mi
 constexpr float kFloatMax = 3.40282347e+38f;
 constexpr int   kMaxEscapeIterations = 64;
 
-__device__ __forceinline__ bool reintersect(const TriVerts& tri, V3 o, V3 d, float min_t, float max_t, float* out_t)
+// Out of line (as is iterative_offset): the shade kernel runs up to three offsets per vertex, and
+// inlined copies of the watertight test with its FP64 fallback bloated its instruction footprint.
+static __device__ __noinline__ bool reintersect(const TriVerts& tri, V3 o, V3 d, float min_t, float max_t, float* out_t)
 {
 	const RayTraits r = make_ray_traits(o.x, o.y, o.z, d.x, d.y, d.z);
 	float b0, b1, b2;
@@ -43,7 +45,7 @@ struct OffsetResult
 
 // iterativeOffset (SurfaceHitRefinery.cpp:62-153). Triangles always pass canVerifyOffset
 // (planar, triangular face topology), so the empirical fallback never applies.
-__device__ __forceinline__ OffsetResult iterative_offset(V3 pos, V3 ng, const TriVerts& tri, V3 dir)
+static __device__ __noinline__ OffsetResult iterative_offset(V3 pos, V3 ng, const TriVerts& tri, V3 dir)
 {
 	const V3 offset_dir = dot(ng, dir) > 0.0f ? ng : -ng;
 	const V3 escape_dir = normalize(dir);

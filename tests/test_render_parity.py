@@ -9,8 +9,11 @@ phRender -> phAquireFrameRaw), exactly as a reference user would drive it. Refer
   and channels of (x - ref)^2 / (ref^2 + 1e-2). Both images carry Monte Carlo noise, which the
   bound includes. BNEEPT images meet it at full resolution; BVPT (no light sampling, a small
   light) is noise-dominated at these sample counts, so it is held to the bar on 4 x 4 block means
-  (16 x fewer noise, same expectation) and to a looser full-resolution bound. Per-channel image
-  means must agree within 1 % everywhere.
+  (16 x fewer noise, same expectation) and to a looser full-resolution bound. The glossy scene's
+  caustics through the glass box are noisy at any spp, so its GPU side renders 16384 spp: the
+  relMSE of two independent renders is the sum of their variances, and this keeps the GPU's
+  share below the reference image's own. Per-channel image means must agree within 1 %
+  everywhere.
 * the furnace known answer (the reference's Main/RenderTest/tests/test_gray_furnace_box.py:
   |mean - 0.5| < 1e-3): a convex Lambertian object of albedo 0.5 under a uniform environment of
   radiance 1 reflects exactly 0.5;
@@ -33,7 +36,7 @@ IMAGES = os.path.join(GOLDEN, "images.npz")
 WORKLOADS = {
     "cornell_bneept": (lambda spp: scenes.cornell(64, 64, spp, 8, "bneept"), 4096),
     "cornell_bvpt": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvpt"), 4096),
-    "cornell_glossy_bneept": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 4096),
+    "cornell_glossy_bneept": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 16384),
     "ggx_sphere_env_bneept": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
                                                             max_bounces=10), 4096),
 }
