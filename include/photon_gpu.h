@@ -63,6 +63,22 @@ PGPU_API int pgpu_trace_any(uint64_t id, const float* rays, uint64_t n, int32_t*
 PGPU_API int pgpu_trace_closest_device(uint64_t id, const float* d_rays, uint64_t n, void* d_hits, float* out_ms);
 PGPU_API int pgpu_trace_any_device(uint64_t id, const float* d_rays, uint64_t n, int32_t* d_occluded, float* out_ms);
 
+/* Closest hit like pgpu_trace_closest (same kernels, same results), but the call allocates
+ * nothing -- no device or host buffers -- for callers that cannot allocate at query time (a
+ * device-memory budget already spent, or a thread that must not wait on cudaFree, which stalls
+ * behind all work queued on the device). No counterpart in the reference: its CPU intersector
+ * needs no staging memory.
+ * Staging lives in one static device array per device, 3.75 MiB, holding at most 65536 rays per
+ * call; larger n is rejected with PG_ERR_INVALID_ARGUMENT before any work. The array needs no
+ * zero-initialisation (every slot a call reads is written earlier in that call).
+ * Setup: the first call on a device (with that device current) looks up the array's device
+ * address once; a call with n = 0 does only that. Make that first call before beginning any
+ * stream capture on the device.
+ * Calls that overlap in time on the same device (several host threads) race on the one array:
+ * the caller serialises them. */
+PGPU_API int pgpu_trace_closest_noalloc(uint64_t id, const float* rays, uint64_t n,
+                       int32_t* out_prim, float* out_t, float* out_bary);
+
 /* Mean BVH nodes visited and triangles tested per ray over the given host rays (a counting
  * pass of the same traversal), for the algorithmic-bytes model of the roofline. */
 PGPU_API int pgpu_trace_counts(uint64_t id, const float* rays, uint64_t n, int any_hit,

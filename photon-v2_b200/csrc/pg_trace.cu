@@ -7,6 +7,8 @@
 #include "../../include/photon_gpu.h"
 
 #include <algorithm>
+#include <mutex>
+#include <string>
 #include <vector>
 
 namespace pg
@@ -514,6 +516,125 @@ int pgpu_trace_counts(uint64_t id, const float* rays, uint64_t n, int any_hit,
 		check_device_error(*g, s);
 		if(out_nodes_per_ray) { *out_nodes_per_ray = static_cast<double>(sums[0]) / n; }
 		if(out_tris_per_ray) { *out_tris_per_ray = static_cast<double>(sums[1]) / n; }
+	});
+}
+
+}// extern "C"
+
+/* ---------------------------------------------------------------------------------------------
+ * Closest hit that allocates nothing: pgpu_trace_closest_noalloc.
+ *
+ * pgpu_trace_closest stages rays and results in device buffers it allocates and frees per call.
+ * Some callers cannot afford that at the moment they query a few hits: a host thread working under
+ * a fixed device-memory budget that is already spent (a renderer that has sized its path state to
+ * fill HBM), or one that must not stall -- cudaFree waits for all work queued on the device, so a
+ * per-call free serialises the query behind whatever else the device is running. This variant
+ * runs the same two kernels (traversal, then the resolve pass that reports prim / t /
+ * barycentrics) on staging space carved from one statically sized device array per device.
+ *
+ * Scratch layout (kNoAllocMaxRays slots each, offsets multiples of 256 bytes): rays float4[2 n],
+ * hit records {u32, f32}[n], prim i32[n], t f32[n], barycentrics f32[3 n]. Nothing in it has to
+ * start at zero: every slot a call reads (i < n) is written earlier in the same call -- rays by the
+ * host-to-device copy, hit records by the traversal kernel, results by the resolve kernel.
+ * ------------------------------------------------------------------------------------------- */
+
+namespace
+{
+
+constexpr uint64_t kNoAllocMaxRays = uint64_t(1) << 16;
+constexpr size_t kNoAllocRaysOffset = 0;
+constexpr size_t kNoAllocHitsOffset = kNoAllocRaysOffset + kNoAllocMaxRays * 32;
+constexpr size_t kNoAllocPrimOffset = kNoAllocHitsOffset + kNoAllocMaxRays * sizeof(HitRecord);
+constexpr size_t kNoAllocTOffset = kNoAllocPrimOffset + kNoAllocMaxRays * 4;
+constexpr size_t kNoAllocBaryOffset = kNoAllocTOffset + kNoAllocMaxRays * 4;
+constexpr size_t kNoAllocScratchBytes = kNoAllocBaryOffset + kNoAllocMaxRays * 12;   // 3.75 MiB
+static_assert(sizeof(HitRecord) == 8, "scratch layout assumes 8-byte hit records");
+static_assert(kNoAllocHitsOffset % 256 == 0 && kNoAllocPrimOffset % 256 == 0 &&
+              kNoAllocTOffset % 256 == 0 && kNoAllocBaryOffset % 256 == 0, "scratch offsets");
+
+constexpr int kNoAllocMaxDevices = 64;
+
+}// end anonymous namespace
+
+// One copy per device, part of the module image: it exists once the module is loaded on a device
+// and is never freed.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace
+{
+
+std::mutex g_noalloc_setup_mutex;
+unsigned char* g_noalloc_scratch_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the current device's scratch, looked up once per device (with that device
+// current) on the first call that runs there.
+unsigned char* noalloc_scratch_of_current_device()
+{
+	int dev = -1;
+	PG_CUDA_CHECK(cudaGetDevice(&dev));
+	if(dev < 0 || dev >= kNoAllocMaxDevices)
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_trace_closest_noalloc: device index out of range");
+	}
+	std::lock_guard<std::mutex> lock(g_noalloc_setup_mutex);
+	if(!g_noalloc_scratch_ptr[dev])
+	{
+		void* p = nullptr;
+		const cudaError_t status = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+		if(status != cudaSuccess || !p)
+		{
+			cudaGetLastError();
+			throw Error(PG_ERR_CUDA, std::string("pgpu_trace_closest_noalloc: cudaGetSymbolAddress of the "
+			                                     "static scratch failed: ") + cudaGetErrorString(status));
+		}
+		g_noalloc_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+	}
+	return g_noalloc_scratch_ptr[dev];
+}
+
+}// end anonymous namespace
+
+extern "C" {
+
+int pgpu_trace_closest_noalloc(uint64_t id, const float* rays, uint64_t n,
+                               int32_t* out_prim, float* out_t, float* out_bary)
+{
+	return guarded([&]
+	{
+		if(n > kNoAllocMaxRays)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT,
+				"pgpu_trace_closest_noalloc: " + std::to_string(n) + " rays exceed the static scratch "
+				"capacity of " + std::to_string(kNoAllocMaxRays) + " rays per call; split the batch");
+		}
+		if(!rays && n > 0)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_trace_closest_noalloc: null rays");
+		}
+		auto g = get_geometry(id);
+		unsigned char* scratch = noalloc_scratch_of_current_device();
+		if(n == 0)
+		{
+			return;
+		}
+		float* d_rays = reinterpret_cast<float*>(scratch + kNoAllocRaysOffset);
+		HitRecord* d_hits = reinterpret_cast<HitRecord*>(scratch + kNoAllocHitsOffset);
+		int32_t* d_prim = reinterpret_cast<int32_t*>(scratch + kNoAllocPrimOffset);
+		float* d_t = reinterpret_cast<float*>(scratch + kNoAllocTOffset);
+		float* d_bary = reinterpret_cast<float*>(scratch + kNoAllocBaryOffset);
+
+		cudaStream_t s = library_stream();
+		PG_CUDA_CHECK(cudaMemcpyAsync(d_rays, rays, n * 8 * sizeof(float), cudaMemcpyHostToDevice, s));
+		launch_trace_closest(*g, d_rays, n, d_hits, s);
+		resolve_hits_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(
+			g->tris.get(), reinterpret_cast<const float4*>(d_rays), d_hits, n, d_prim, d_t, d_bary);
+		PG_CUDA_CHECK(cudaGetLastError());
+		// straight into the caller's arrays: no host staging either
+		if(out_prim) { PG_CUDA_CHECK(cudaMemcpyAsync(out_prim, d_prim, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s)); }
+		if(out_t) { PG_CUDA_CHECK(cudaMemcpyAsync(out_t, d_t, n * sizeof(float), cudaMemcpyDeviceToHost, s)); }
+		if(out_bary) { PG_CUDA_CHECK(cudaMemcpyAsync(out_bary, d_bary, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s)); }
+		PG_CUDA_CHECK(cudaStreamSynchronize(s));
+		check_device_error(*g, s);
 	});
 }
 

@@ -33,6 +33,8 @@ PGPU_SIGNATURES = [
     ("pgpu_geometry_stats", ctypes.c_int, [ctypes.c_uint64, _u64p, _u64p, _i32p, _dblp]),
     ("pgpu_trace_closest", ctypes.c_int, [ctypes.c_uint64, _f32p, ctypes.c_uint64, _i32p, _f32p, _f32p]),
     ("pgpu_trace_any", ctypes.c_int, [ctypes.c_uint64, _f32p, ctypes.c_uint64, _i32p]),
+    ("pgpu_trace_closest_noalloc", ctypes.c_int,
+     [ctypes.c_uint64, _f32p, ctypes.c_uint64, _i32p, _f32p, _f32p]),
     ("pgpu_trace_closest_device", ctypes.c_int,
      [ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, _f32p]),
     ("pgpu_trace_any_device", ctypes.c_int,
