@@ -12,6 +12,7 @@ struct Geometry
 	DeviceBuffer<WideNode> nodes;
 	DeviceBuffer<LeafTri>  tris;
 	DeviceBuffer<uint32_t> error;     // device error flags (PG_DEV_ERR_*)
+	DeviceBuffer<uint32_t> fetch;     // dynamic-fetch cursor of the trace kernels, zeroed per launch
 	BvhBuildStats          stats;
 };
 

@@ -162,6 +162,8 @@ __global__ void prepare_kernel(RenderCounters* c, uint32_t capacity)
 	c->next_path += n_new;
 	c->n_next = 0;
 	c->n_shadow = 0;
+	c->fetch_extend = 0;
+	c->fetch_shadow = 0;
 	c->rays_traced += c->n_total;
 }
 

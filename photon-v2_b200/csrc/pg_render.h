@@ -126,6 +126,8 @@ struct alignas(16) RenderCounters
 	unsigned long long nodes_any, tris_any;
 	uint32_t error;
 	uint32_t pad;
+	uint32_t fetch_extend;   // dynamic-fetch cursors of the persistent traversal kernels,
+	uint32_t fetch_shadow;   // zeroed by prepare_kernel at the start of every iteration
 };
 
 // Per-path state, one buffer of the ping-pong pair (structure of arrays).

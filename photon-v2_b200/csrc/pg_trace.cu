@@ -33,6 +33,7 @@ std::unique_ptr<Geometry> make_geometry(const BvhBuildInput& in)
 	PG_CUDA_CHECK(cudaMemcpyAsync(g->tris.get(), bvh.tris.data(), g->tris.bytes(), cudaMemcpyHostToDevice, s));
 	g->error.resize(1);
 	PG_CUDA_CHECK(cudaMemsetAsync(g->error.get(), 0, sizeof(uint32_t), s));
+	g->fetch.resize(1);
 	PG_CUDA_CHECK(cudaStreamSynchronize(s));
 	return g;
 }
@@ -50,21 +51,14 @@ struct HitRecord
 
 __global__ void __launch_bounds__(kTraceBlock)
 trace_closest_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
-                     const float4* __restrict__ rays, uint64_t n,
+                     const float4* __restrict__ rays, uint32_t n, uint32_t* __restrict__ next_ray,
                      HitRecord* __restrict__ hits, uint32_t* __restrict__ error)
 {
 	uint32_t err = 0;
-	for(uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
-	    i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-	{
-		const float4 a = __ldg(rays + 2 * i);
-		const float4 b = __ldg(rays + 2 * i + 1);
-		const RayTraits r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
-		float t;
-		uint32_t tri;
-		const bool hit = traverse<false>(r, nodes, tris, a.w, b.w, &t, &tri, &err);
-		hits[i] = HitRecord{hit ? tri : 0xFFFFFFFFu, hit ? t : 0.0f};
-	}
+	traverse_persistent<false, false>(nodes, tris, n, next_ray,
+		[&](uint32_t i, float4* a, float4* b) { *a = __ldg(rays + 2 * i); *b = __ldg(rays + 2 * i + 1); },
+		[&](uint32_t i, bool hit, uint32_t tri, float t) { hits[i] = HitRecord{hit ? tri : 0xFFFFFFFFu, hit ? t : 0.0f}; },
+		&err);
 	if(err)
 	{
 		atomicOr(error, err);
@@ -73,20 +67,14 @@ trace_closest_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restri
 
 __global__ void __launch_bounds__(kTraceBlock)
 trace_any_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
-                 const float4* __restrict__ rays, uint64_t n,
+                 const float4* __restrict__ rays, uint32_t n, uint32_t* __restrict__ next_ray,
                  int32_t* __restrict__ occluded, uint32_t* __restrict__ error)
 {
 	uint32_t err = 0;
-	for(uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
-	    i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-	{
-		const float4 a = __ldg(rays + 2 * i);
-		const float4 b = __ldg(rays + 2 * i + 1);
-		const RayTraits r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
-		float t;
-		uint32_t tri;
-		occluded[i] = traverse<true>(r, nodes, tris, a.w, b.w, &t, &tri, &err) ? 1 : 0;
-	}
+	traverse_persistent<true, false>(nodes, tris, n, next_ray,
+		[&](uint32_t i, float4* a, float4* b) { *a = __ldg(rays + 2 * i); *b = __ldg(rays + 2 * i + 1); },
+		[&](uint32_t i, bool hit, uint32_t, float) { occluded[i] = hit ? 1 : 0; },
+		&err);
 	if(err)
 	{
 		atomicOr(error, err);
@@ -157,11 +145,22 @@ __global__ void count_kernel(const WideNode* __restrict__ nodes, const LeafTri* 
 	}
 }
 
-int grid_for(uint64_t n, int block)
+// Persistent grid: as many blocks as stay resident on the device at once.
+template<class Kernel>
+int persistent_grid(Kernel kernel)
 {
-	const uint64_t blocks = (n + block - 1) / block;
-	const uint64_t cap = static_cast<uint64_t>(sm_count()) * 16;
-	return static_cast<int>(std::max<uint64_t>(1, std::min(blocks, cap)));
+	int per_sm = 0;
+	PG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTraceBlock, 0));
+	return std::max(1, per_sm) * sm_count();
+}
+
+uint32_t checked_ray_count(uint64_t n)
+{
+	if(n > 0xFFF00000ull)
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, "too many rays in one call: " + std::to_string(n));
+	}
+	return static_cast<uint32_t>(n);
 }
 
 std::shared_ptr<Geometry> get_geometry(uint64_t id)
@@ -197,16 +196,10 @@ extend_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tr
 {
 	const uint32_t n = counters->n_total;
 	uint32_t err = 0, node_count = 0, tri_count = 0;
-	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-	{
-		const float4 a = __ldg(ray_o + i);
-		const float4 b = __ldg(ray_d + i);
-		const RayTraits r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
-		float t;
-		uint32_t tri;
-		const bool hit = traverse<false, COUNT>(r, nodes, tris, a.w, b.w, &t, &tri, &err, &node_count, &tri_count);
-		hits[i] = make_uint2(hit ? tri : 0xFFFFFFFFu, __float_as_uint(t));
-	}
+	traverse_persistent<false, COUNT>(nodes, tris, n, &counters->fetch_extend,
+		[&](uint32_t i, float4* a, float4* b) { *a = __ldg(ray_o + i); *b = __ldg(ray_d + i); },
+		[&](uint32_t i, bool hit, uint32_t tri, float t) { hits[i] = make_uint2(hit ? tri : 0xFFFFFFFFu, __float_as_uint(t)); },
+		&err, &node_count, &tri_count);
 	if(COUNT)
 	{
 		atomicAdd(&counters->nodes_closest, static_cast<unsigned long long>(node_count));
@@ -233,35 +226,33 @@ shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tr
 		counters->shadow_rays += n;
 	}
 	uint32_t err = 0, node_count = 0, tri_count = 0;
-	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-	{
-		const float4 a = __ldg(so + i);
-		const float4 b = __ldg(sd + i);
-		const RayTraits r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
-		float t;
-		uint32_t tri;
-		if(traverse<true, COUNT>(r, nodes, tris, a.w, b.w, &t, &tri, &err, &node_count, &tri_count))
+	traverse_persistent<true, COUNT>(nodes, tris, n, &counters->fetch_shadow,
+		[&](uint32_t i, float4* a, float4* b) { *a = __ldg(so + i); *b = __ldg(sd + i); },
+		[&](uint32_t i, bool occluded, uint32_t, float)
 		{
-			continue;
-		}
-		const float4 c = __ldg(sc + i);
-		const uint32_t target = __float_as_uint(c.w);
-		if(target & kTargetFinal)
-		{
-			const uint32_t pixel = target & ~kTargetFinal;
-			if(c.x != 0.0f) { atomicAdd(&film[3 * pixel + 0], static_cast<double>(c.x)); }
-			if(c.y != 0.0f) { atomicAdd(&film[3 * pixel + 1], static_cast<double>(c.y)); }
-			if(c.z != 0.0f) { atomicAdd(&film[3 * pixel + 2], static_cast<double>(c.z)); }
-		}
-		else
-		{
-			float4 rv = rad_next[target];
-			rv.x += c.x;
-			rv.y += c.y;
-			rv.z += c.z;
-			rad_next[target] = rv;
-		}
-	}
+			if(occluded)
+			{
+				return;
+			}
+			const float4 c = __ldg(sc + i);
+			const uint32_t target = __float_as_uint(c.w);
+			if(target & kTargetFinal)
+			{
+				const uint32_t pixel = target & ~kTargetFinal;
+				if(c.x != 0.0f) { atomicAdd(&film[3 * pixel + 0], static_cast<double>(c.x)); }
+				if(c.y != 0.0f) { atomicAdd(&film[3 * pixel + 1], static_cast<double>(c.y)); }
+				if(c.z != 0.0f) { atomicAdd(&film[3 * pixel + 2], static_cast<double>(c.z)); }
+			}
+			else
+			{
+				float4 rv = rad_next[target];
+				rv.x += c.x;
+				rv.y += c.y;
+				rv.z += c.z;
+				rad_next[target] = rv;
+			}
+		},
+		&err, &node_count, &tri_count);
 	if(COUNT)
 	{
 		atomicAdd(&counters->nodes_any, static_cast<unsigned long long>(node_count));
@@ -276,29 +267,33 @@ shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tr
 }// end anonymous namespace
 
 void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4* ray_o,
-                   const float4* ray_d, uint2* hits, int grid, int block, cudaStream_t st, bool count)
+                   const float4* ray_d, uint2* hits, int, int, cudaStream_t st, bool count)
 {
 	if(count)
 	{
-		extend_kernel<true><<<grid, block, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits);
+		static const int grid = persistent_grid(extend_kernel<true>);
+		extend_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits);
 	}
 	else
 	{
-		extend_kernel<false><<<grid, block, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits);
+		static const int grid = persistent_grid(extend_kernel<false>);
+		extend_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits);
 	}
 	PG_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
-                   float4* rad_next, double* film, int grid, int block, cudaStream_t st, bool count)
+                   float4* rad_next, double* film, int, int, cudaStream_t st, bool count)
 {
 	if(count)
 	{
-		shadow_kernel<true><<<grid, block, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, rad_next, film);
+		static const int grid = persistent_grid(shadow_kernel<true>);
+		shadow_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, rad_next, film);
 	}
 	else
 	{
-		shadow_kernel<false><<<grid, block, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, rad_next, film);
+		static const int grid = persistent_grid(shadow_kernel<false>);
+		shadow_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, rad_next, film);
 	}
 	PG_CUDA_CHECK(cudaGetLastError());
 }
@@ -309,9 +304,11 @@ void launch_trace_closest(const Geometry& g, const float* d_rays, uint64_t n, vo
 	{
 		return;
 	}
-	trace_closest_kernel<<<grid_for(n, kTraceBlock), kTraceBlock, 0, s>>>(
-		g.nodes.get(), g.tris.get(), reinterpret_cast<const float4*>(d_rays), n,
-		reinterpret_cast<HitRecord*>(d_hits), g.error.get());
+	static const int grid = persistent_grid(trace_closest_kernel);
+	PG_CUDA_CHECK(cudaMemsetAsync(g.fetch.get(), 0, sizeof(uint32_t), s));
+	trace_closest_kernel<<<grid, kTraceBlock, 0, s>>>(
+		g.nodes.get(), g.tris.get(), reinterpret_cast<const float4*>(d_rays), checked_ray_count(n),
+		g.fetch.get(), reinterpret_cast<HitRecord*>(d_hits), g.error.get());
 	PG_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -321,8 +318,11 @@ void launch_trace_any(const Geometry& g, const float* d_rays, uint64_t n, int32_
 	{
 		return;
 	}
-	trace_any_kernel<<<grid_for(n, kTraceBlock), kTraceBlock, 0, s>>>(
-		g.nodes.get(), g.tris.get(), reinterpret_cast<const float4*>(d_rays), n, d_occluded, g.error.get());
+	static const int grid = persistent_grid(trace_any_kernel);
+	PG_CUDA_CHECK(cudaMemsetAsync(g.fetch.get(), 0, sizeof(uint32_t), s));
+	trace_any_kernel<<<grid, kTraceBlock, 0, s>>>(
+		g.nodes.get(), g.tris.get(), reinterpret_cast<const float4*>(d_rays), checked_ray_count(n),
+		g.fetch.get(), d_occluded, g.error.get());
 	PG_CUDA_CHECK(cudaGetLastError());
 }
 

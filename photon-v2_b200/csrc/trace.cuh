@@ -332,4 +332,162 @@ __device__ __forceinline__ bool traverse(
 	return best_tri != 0xFFFFFFFFu;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Persistent traversal with dynamic ray fetch.
+//
+// Rays differ widely in the work they need (nodes visited, triangles tested), and a warp that
+// traverses 32 rays to completion runs at the pace of its longest ray while finished lanes idle.
+// Here every lane keeps its own traversal state and the warp advances all lanes one step per
+// loop turn (one wide-node intersection, or one triangle test); lanes whose ray has finished are
+// refilled from a global ray counter as soon as kRefillMinIdle of them are idle. The visit order
+// of a single ray is exactly that of traverse() above (same node order, same triangle order,
+// same tie rule), so results are identical; only the scheduling of rays onto lanes changes.
+//
+// Fetch(uint32_t i, float4* origin_tmin, float4* dir_tmax) loads ray i; Finish(uint32_t i,
+// bool hit, uint32_t leaf_tri, float t) consumes its result. n rays are taken from *next_ray,
+// which must be zero when the launch starts. Every lane of the warp must call this function.
+
+constexpr uint32_t kFullWarp = 0xFFFFFFFFu;
+constexpr int kRefillMinIdle = 8;
+
+template<bool ANY_HIT, bool COUNT, class Fetch, class Finish>
+__device__ __forceinline__ void traverse_persistent(
+	const WideNode* __restrict__ nodes,
+	const LeafTri* __restrict__ tris,
+	uint32_t n, uint32_t* __restrict__ next_ray,
+	Fetch fetch, Finish finish,
+	uint32_t* out_error, uint32_t* node_count = nullptr, uint32_t* tri_count = nullptr)
+{
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t lanes_below = (1u << lane) - 1u;
+
+	uint2 stack[kTraversalStackSize];
+	int sp = 0;
+	RayTraits r{};
+	float t_min = 0.0f;
+	float best_t = 0.0f;
+	uint32_t best_tri = 0xFFFFFFFFu, best_prim = 0xFFFFFFFFu;
+	uint32_t child_base = 0, imask = 0, node_hits = 0;
+	uint32_t tri_base = 0, tri_hits = 0;
+	uint32_t ray = 0;
+	bool has_ray = false;
+	bool exhausted = false;   // warp-uniform: the counter has passed n
+
+	while(true)
+	{
+		// ---- refill idle lanes (warp-uniform branch)
+		const uint32_t idle = __ballot_sync(kFullWarp, !has_ray);
+		const int num_idle = __popc(idle);
+		if(!exhausted && num_idle >= kRefillMinIdle)
+		{
+			uint32_t base = 0;
+			if(lane == 0)
+			{
+				base = atomicAdd(next_ray, static_cast<uint32_t>(num_idle));
+			}
+			base = __shfl_sync(kFullWarp, base, 0);
+			exhausted = base >= n || n - base <= static_cast<uint32_t>(num_idle);
+			if(!has_ray)
+			{
+				const uint32_t i = base + __popc(idle & lanes_below);
+				if(i < n && i >= base)
+				{
+					float4 a, b;
+					fetch(i, &a, &b);
+					r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
+					t_min = a.w;
+					best_t = b.w;
+					best_tri = 0xFFFFFFFFu;
+					best_prim = 0xFFFFFFFFu;
+					// the root as the only internal child of a virtual parent: slot 0, key = oct
+					child_base = 0;
+					imask = 1u;
+					node_hits = 1u << r.oct;
+					tri_hits = 0;
+					sp = 0;
+					ray = i;
+					has_ray = true;
+				}
+			}
+		}
+		if(!__any_sync(kFullWarp, has_ray))
+		{
+			break;   // no lane holds a ray, so the last refill found the counter past n
+		}
+		if(!has_ray)
+		{
+			continue;
+		}
+
+		// ---- one traversal step
+		if(tri_hits)
+		{
+			const uint32_t bit = __ffs(tri_hits) - 1u;
+			tri_hits &= tri_hits - 1u;
+			const uint32_t k = tri_base + bit;
+			if(COUNT) { ++*tri_count; }
+			float t, b0, b1, b2;
+			if(watertight_hit_tri(r, tris, k, t_min, best_t, &t, &b0, &b1, &b2))
+			{
+				if(ANY_HIT)
+				{
+					best_t = t;
+					best_tri = k;
+					tri_hits = 0;
+					node_hits = 0;
+					sp = 0;
+				}
+				else
+				{
+					const uint32_t prim = __ldg(&tris[k].prim);
+					if(t < best_t || prim < best_prim)
+					{
+						best_t = t;
+						best_tri = k;
+						best_prim = prim;
+					}
+				}
+			}
+		}
+		else
+		{
+			if(node_hits == 0u && sp > 0)
+			{
+				--sp;
+				child_base = stack[sp].x;
+				imask = stack[sp].y >> 8;
+				node_hits = stack[sp].y & 0xFFu;
+			}
+			if(node_hits)
+			{
+				const uint32_t key = 31u - __clz(node_hits);
+				node_hits &= ~(1u << key);
+				const uint32_t slot = key ^ r.oct;
+				const uint32_t child = child_base + __popc(imask & ((1u << slot) - 1u));
+				if(node_hits)
+				{
+					if(sp < kTraversalStackSize)
+					{
+						stack[sp++] = make_uint2(child_base, (imask << 8) | node_hits);
+					}
+					else
+					{
+						*out_error |= PG_DEV_ERR_STACK;
+					}
+				}
+				const uint32_t hits = intersect_children(r, nodes, child, t_min, best_t, &child_base, &tri_base, &imask);
+				if(COUNT) { ++*node_count; }
+				node_hits = hits >> 24;
+				tri_hits = hits & 0x00FFFFFFu;
+			}
+		}
+
+		if(tri_hits == 0u && node_hits == 0u && sp == 0)
+		{
+			finish(ray, best_tri != 0xFFFFFFFFu, best_tri, best_t);
+			has_ray = false;
+		}
+	}
+}
+
 }// end namespace pg
