@@ -316,11 +316,17 @@ def run_ours(args) -> None:
             alg_bytes = (32 + 8 + 80 + 48 + 112 + 48) * rays
             launches_k, kname = kprof["iterations"], "shade"
         achieved = alg_bytes / (kernel_ms[dominant] / 1e3) / 1e9
+        # DRAM bytes per launch from an ncu capture of a full-queue launch, scaled by queue
+        # entries to this workload's average launch (rays / iterations)
         traffic = None
         prof_path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
         if os.path.exists(prof_path):
             with open(prof_path) as f:
-                traffic = json.load(f).get(dominant)
+                rec = json.load(f).get(dominant) or {}
+            if rec.get("dram_bytes_per_entry"):
+                entries = (shadow_rays if dominant == "shadow_ms" else rays) / max(1, kprof["iterations"])
+                traffic = rec["dram_bytes_per_entry"] * entries
+        achieved_per_launch = alg_bytes / max(1, launches_k)
 
     clock = clocks.summary()
     line = {
@@ -335,6 +341,7 @@ def run_ours(args) -> None:
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "algorithmic_bytes_per_launch": achieved_per_launch,
                      "peak_source": peaks["source"],
                      "model": {"bytes_per_closest_ray": bytes_closest, "nodes_per_closest_ray": nodes_per_ray,
                                "tris_per_closest_ray": tris_per_ray, "bytes_per_shadow_ray": bytes_shadow,
