@@ -85,6 +85,15 @@ PGPU_API int pgpu_trace_counts(uint64_t id, const float* rays, uint64_t n, int a
                       double* out_nodes_per_ray, double* out_tris_per_ray);
 
 /* ---------------------------------------------------------------------------------------------
+ * Learned path guiding (no reference counterpart: the reference has no guiding). The network maps
+ * a surface query -- 7 scalars in [0, 1]: position (3), normal (2), outgoing direction (2) -- to
+ * 40 raw outputs, 8 von Mises-Fisher lobes x (weight logit, mean xyz, log concentration).
+ * params: the 29,480 FP32 parameters in the packed order W0[224][64], b0, W1[64][64], b1, W2, b2,
+ * W3, b3, W4[64][40], b4 (W[in][out]). The forward pass runs on the tensor cores (tcgen05, BF16
+ * operands, FP32 accumulation). features: host [n][7]; out_raw: host [n][40]. */
+PGPU_API int pgpu_guide_forward(const float* params, const float* features, uint64_t n, float* out_raw);
+
+/* ---------------------------------------------------------------------------------------------
  * BSDF kernels, evaluated one case per thread on the GPU with the same device functions the path
  * tracer uses. cases: float32 [n][19] (type, p0..p5, N(3), V(3), L(3), u(3)) with
  *   type 0 Lambertian (p0..p2 albedo)                   LambertianReflector.cpp:39-99

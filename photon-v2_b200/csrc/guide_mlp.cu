@@ -1,0 +1,485 @@
+// Guiding network on the 5th-generation tensor cores: fused forward pass of the whole MLP with
+// tcgen05.mma (BF16 operands in shared memory, FP32 accumulators in tensor memory).
+//
+// One CTA of 128 threads per SM walks 128-row tiles of queries. Per tile:
+//   1. every thread one-blob encodes its query row into the A operand buffer (BF16, 224 columns);
+//   2. per layer, one elected thread issues the K/16 MMAs (M = 128, N = 64 or 48, K = 16 each)
+//      into tensor memory and commits them to an mbarrier;
+//   3. after the barrier completes, thread t reads row t of the accumulator (tcgen05.ld, TMEM lane
+//      t), adds the bias, applies ReLU, rounds to BF16 and writes the row as the next layer's A
+//      operand (or, after the last layer, the 40 raw outputs to global memory).
+// All weights (BF16, 59 KB) stay resident in shared memory for the kernel's lifetime.
+//
+// Operand layout: K-major, no swizzle. A core matrix is 8 rows x 16 bytes (8 BF16 along K); for a
+// matrix of R rows, element (r, k) lives at
+//   (k / 8) * (R * 16) + (r / 8) * 128 + (r % 8) * 16 + (k % 8) * 2,
+// so the descriptor's leading byte offset (between K chunks) is R * 16 and its stride byte offset
+// (between 8-row groups) is 128. Weights are stored transposed (W^T, [out][in]) so that both
+// operands are K-major: D[M x N] = A[M x K] * B[N x K]^T.
+#include "guide_mlp.h"
+
+#include "pg_runtime.h"
+#include "../../include/photon_gpu.h"
+
+#include <cuda_bf16.h>
+
+#include <cstring>
+#include <vector>
+
+namespace pg
+{
+namespace guide
+{
+
+namespace
+{
+
+constexpr int kThreads = 128;
+constexpr uint32_t kTmemCols = 128;   // power of two >= 64 accumulator columns
+
+// ---- shared-memory image of the weights (also the device-side packed format)
+constexpr int kW0Bytes = kHidden * kIn * 2;         // 28,672
+constexpr int kWhBytes = kHidden * kHidden * 2;     //  8,192
+constexpr int kW4Bytes = kOutPad * kHidden * 2;     //  6,144
+constexpr int kOffImgW0 = 0;
+constexpr int kOffImgW1 = kOffImgW0 + kW0Bytes;
+constexpr int kOffImgW2 = kOffImgW1 + kWhBytes;
+constexpr int kOffImgW3 = kOffImgW2 + kWhBytes;
+constexpr int kOffImgW4 = kOffImgW3 + kWhBytes;
+constexpr int kOffImgBias = kOffImgW4 + kW4Bytes;   // FP32 biases: 4 x 64 + 48
+constexpr int kBiasCount = kHiddenLayers * kHidden + kOutPad;
+constexpr int kImageBytes = kOffImgBias + kBiasCount * 4;   // 60,576
+
+// ---- activation buffers
+constexpr int kActInBytes = kTile * kIn * 2;        // 57,344: input, later hidden ping
+constexpr int kActHBytes = kTile * kHidden * 2;     // 16,384: hidden pong
+constexpr int kOffSmemImage = 0;
+constexpr int kOffSmemActIn = (kImageBytes + 1023) / 1024 * 1024;
+constexpr int kOffSmemActH = kOffSmemActIn + kActInBytes;
+constexpr int kOffSmemBar = kOffSmemActH + kActHBytes;         // 8-byte aligned
+constexpr int kOffSmemTmem = kOffSmemBar + 8;
+constexpr int kSmemBytes = kOffSmemTmem + 8;
+static_assert(kImageBytes % 16 == 0 && kOffSmemActH % 16 == 0 && kOffSmemBar % 8 == 0, "alignment");
+static_assert(kSmemBytes <= 227 * 1024, "shared memory");
+
+constexpr uint32_t kWaitLimit = 1u << 22;   // bounded mbarrier wait: error flag instead of a hang
+
+PG_HD uint32_t core_offset(uint32_t r, uint32_t k, uint32_t rows)
+{
+	return (k >> 3) * (rows * 16u) + (r >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+}
+
+// ---- PTX wrappers (tcgen05 / mbarrier), sm_100a
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+	return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+	uint64_t d = 0;
+	d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+	d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
+	d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
+	d |= static_cast<uint64_t>(1u) << 46;   // descriptor version 1 (sm_100); no swizzle, base offset 0
+	return d;
+}
+
+// kind::f16 instruction descriptor: BF16 A and B (K-major), FP32 D, shape M x N.
+constexpr uint32_t instr_desc(uint32_t m, uint32_t n)
+{
+	return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate)
+{
+	asm volatile(
+		"{\n\t.reg .pred p;\n\t"
+		"setp.ne.b32 p, %4, 0;\n\t"
+		"tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+		:
+		: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate),
+		  "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+		: "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar)
+{
+	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+	for(uint32_t i = 0; i < kWaitLimit; ++i)
+	{
+		uint32_t done;
+		asm volatile(
+			"{\n\t.reg .pred P;\n\t"
+			"mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+			"selp.u32 %0, 1, 0, P;\n\t}\n"
+			: "=r"(done) : "r"(bar), "r"(parity) : "memory");
+		if(done)
+		{
+			return true;
+		}
+	}
+	return false;
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
+{
+	uint32_t r[16];
+	asm volatile(
+		"tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+		"{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+		: "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+		  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+		: "r"(taddr));
+	#pragma unroll
+	for(int i = 0; i < 16; ++i)
+	{
+		v[i] = __uint_as_float(r[i]);
+	}
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b)
+{
+	const __nv_bfloat16 lo = __float2bfloat16_rn(a);
+	const __nv_bfloat16 hi = __float2bfloat16_rn(b);
+	return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) | (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
+}
+
+// Writes 8 consecutive K values of row r (k0 multiple of 8) of an A-layout buffer.
+__device__ __forceinline__ void store_row8(unsigned char* buf, uint32_t r, uint32_t k0, const float* v)
+{
+	uint4 q;
+	q.x = pack_bf16x2(v[0], v[1]);
+	q.y = pack_bf16x2(v[2], v[3]);
+	q.z = pack_bf16x2(v[4], v[5]);
+	q.w = pack_bf16x2(v[6], v[7]);
+	*reinterpret_cast<uint4*>(buf + core_offset(r, k0, kTile)) = q;
+}
+
+// ---- the fused forward kernel
+
+__global__ void __launch_bounds__(kThreads, 1)
+mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restrict__ features,
+                   uint32_t n, float* __restrict__ out_raw, __nv_bfloat16* __restrict__ out_acts,
+                   uint32_t* __restrict__ error)
+{
+	extern __shared__ __align__(128) unsigned char smem[];
+	const uint32_t tid = threadIdx.x;
+	const uint32_t warp = tid >> 5;
+
+	// weights + biases into shared memory
+	{
+		const uint4* src = reinterpret_cast<const uint4*>(image);
+		uint4* dst = reinterpret_cast<uint4*>(smem + kOffSmemImage);
+		for(uint32_t i = tid; i < kImageBytes / 16; i += kThreads)
+		{
+			dst[i] = __ldg(src + i);
+		}
+	}
+	const uint32_t bar = smem_u32(smem + kOffSmemBar);
+	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kOffSmemTmem);
+	if(tid == 0)
+	{
+		mbar_init(bar, 1);
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	if(warp == 0)
+	{
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+		             :: "r"(smem_u32(tmem_slot)), "r"(kTmemCols) : "memory");
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+	}
+	fence_before_sync();
+	__syncthreads();
+	fence_after_sync();
+	const uint32_t tmem = *tmem_slot;
+	const uint32_t tmem_row = tmem + ((warp * 32u) << 16);   // this warp's 32 lanes, column 0
+
+	const float* bias = reinterpret_cast<const float*>(smem + kOffImgBias);
+	unsigned char* act_in = smem + kOffSmemActIn;
+	unsigned char* act_h = smem + kOffSmemActH;
+	const uint32_t w_addr[5] = {smem_u32(smem + kOffImgW0), smem_u32(smem + kOffImgW1), smem_u32(smem + kOffImgW2),
+	                            smem_u32(smem + kOffImgW3), smem_u32(smem + kOffImgW4)};
+
+	uint32_t phase = 0;
+	bool failed = false;
+	const uint32_t num_tiles = (n + kTile - 1) / kTile;
+	for(uint32_t tile = blockIdx.x; tile < num_tiles && !failed; tile += gridDim.x)
+	{
+		const uint32_t row = tile * kTile + tid;
+		const bool valid = row < n;
+
+		// 1. one-blob encoding of this thread's query into the input buffer
+		float f[kInputs];
+		#pragma unroll
+		for(int i = 0; i < kInputs; ++i)
+		{
+			f[i] = valid ? __ldg(features + static_cast<size_t>(row) * 8 + i) : -1.0f;
+		}
+		#pragma unroll
+		for(int i = 0; i < kInputs; ++i)
+		{
+			#pragma unroll
+			for(int c = 0; c < kBins / 8; ++c)
+			{
+				float v[8];
+				#pragma unroll
+				for(int j = 0; j < 8; ++j)
+				{
+					v[j] = valid ? one_blob(f[i], c * 8 + j) : 0.0f;
+				}
+				store_row8(act_in, tid, static_cast<uint32_t>(i * kBins + c * 8), v);
+			}
+		}
+		fence_async_smem();
+		fence_before_sync();
+		__syncthreads();
+
+		// 2./3. five layers: input -> H1 (act_h) -> H2 (act_in) -> H3 (act_h) -> H4 (act_in) -> out
+		#pragma unroll 1
+		for(int layer = 0; layer < 5; ++layer)
+		{
+			const bool last = layer == 4;
+			const uint32_t k_dim = layer == 0 ? kIn : kHidden;
+			const uint32_t n_dim = last ? kOutPad : kHidden;
+			const unsigned char* a_buf = (layer & 1) ? act_h : act_in;
+			unsigned char* o_buf = (layer & 1) ? act_in : act_h;
+			if(tid == 0)
+			{
+				fence_after_sync();
+				const uint32_t a_base = smem_u32(a_buf);
+				const uint32_t idesc = instr_desc(kTile, n_dim);
+				for(uint32_t ks = 0; ks < k_dim / 16; ++ks)
+				{
+					const uint64_t ad = smem_desc(a_base + ks * 2u * (kTile * 16u), kTile * 16u, 128u);
+					const uint64_t bd = smem_desc(w_addr[layer] + ks * 2u * (n_dim * 16u), n_dim * 16u, 128u);
+					mma_bf16(tmem, ad, bd, idesc, ks > 0 ? 1u : 0u);
+				}
+				mma_commit(bar);
+			}
+			const bool ok = mbar_wait(bar, phase);
+			if(__syncthreads_or(ok ? 0 : 1))
+			{
+				// the tensor cores did not report back: stop, after one more bounded wait for the
+				// MMAs of this phase so that the accumulator is not freed under them
+				failed = true;
+				if(!ok)
+				{
+					mbar_wait(bar, phase);
+				}
+				break;
+			}
+			phase ^= 1u;
+			fence_after_sync();
+
+			float acc[64];
+			#pragma unroll
+			for(int c = 0; c < 4; ++c)
+			{
+				if(c * 16 < static_cast<int>(n_dim))
+				{
+					tmem_ld16(tmem_row + c * 16, acc + c * 16);
+				}
+			}
+			tmem_wait_ld();
+
+			if(!last)
+			{
+				const float* b = bias + layer * kHidden;
+				#pragma unroll
+				for(int j = 0; j < kHidden; ++j)
+				{
+					acc[j] = fmaxf(acc[j] + b[j], 0.0f);
+				}
+				#pragma unroll
+				for(int c = 0; c < kHidden / 8; ++c)
+				{
+					store_row8(o_buf, tid, c * 8, acc + c * 8);
+				}
+				if(out_acts && valid)
+				{
+					uint4* dst = reinterpret_cast<uint4*>(out_acts + (static_cast<size_t>(row) * kHiddenLayers + layer) * kHidden);
+					#pragma unroll
+					for(int c = 0; c < kHidden / 8; ++c)
+					{
+						dst[c] = make_uint4(pack_bf16x2(acc[c * 8 + 0], acc[c * 8 + 1]), pack_bf16x2(acc[c * 8 + 2], acc[c * 8 + 3]),
+						                    pack_bf16x2(acc[c * 8 + 4], acc[c * 8 + 5]), pack_bf16x2(acc[c * 8 + 6], acc[c * 8 + 7]));
+					}
+				}
+			}
+			else if(valid)
+			{
+				const float* b = bias + kHiddenLayers * kHidden;
+				float4* dst = reinterpret_cast<float4*>(out_raw + static_cast<size_t>(row) * kOut);
+				#pragma unroll
+				for(int c = 0; c < kOut / 4; ++c)
+				{
+					dst[c] = make_float4(acc[4 * c + 0] + b[4 * c + 0], acc[4 * c + 1] + b[4 * c + 1],
+					                     acc[4 * c + 2] + b[4 * c + 2], acc[4 * c + 3] + b[4 * c + 3]);
+				}
+			}
+			fence_async_smem();
+			fence_before_sync();
+			__syncthreads();
+			fence_after_sync();
+		}
+	}
+
+	if(failed && tid == 0)
+	{
+		atomicOr(error, PG_DEV_ERR_GUIDE_WAIT);
+	}
+	fence_before_sync();
+	__syncthreads();
+	if(warp == 0)
+	{
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTmemCols) : "memory");
+	}
+}
+
+// FP32 parameters -> BF16 shared-memory image (W^T in the K-major core-matrix layout) + biases.
+__global__ void pack_image_kernel(const float* __restrict__ params, unsigned char* __restrict__ image)
+{
+	const uint32_t total = kHidden * kIn + 3 * kHidden * kHidden + kOutPad * kHidden + kBiasCount;
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+	{
+		uint32_t j = i;
+		if(j < kHidden * kIn)
+		{
+			const uint32_t o = j / kIn, k = j % kIn;   // W0^T[o][k] = W0[k][o]
+			*reinterpret_cast<__nv_bfloat16*>(image + kOffImgW0 + core_offset(o, k, kHidden)) =
+				__float2bfloat16_rn(params[kOffW0 + k * kHidden + o]);
+			continue;
+		}
+		j -= kHidden * kIn;
+		if(j < 3u * kHidden * kHidden)
+		{
+			const uint32_t l = j / (kHidden * kHidden), e = j % (kHidden * kHidden);
+			const uint32_t o = e / kHidden, k = e % kHidden;
+			const int src = (l == 0 ? kOffW1 : (l == 1 ? kOffW2 : kOffW3)) + k * kHidden + o;
+			*reinterpret_cast<__nv_bfloat16*>(image + kOffImgW1 + l * kWhBytes + core_offset(o, k, kHidden)) =
+				__float2bfloat16_rn(params[src]);
+			continue;
+		}
+		j -= 3u * kHidden * kHidden;
+		if(j < static_cast<uint32_t>(kOutPad * kHidden))
+		{
+			const uint32_t o = j / kHidden, k = j % kHidden;
+			const float w = o < static_cast<uint32_t>(kOut) ? params[kOffW4 + k * kOut + o] : 0.0f;
+			*reinterpret_cast<__nv_bfloat16*>(image + kOffImgW4 + core_offset(o, k, kOutPad)) = __float2bfloat16_rn(w);
+			continue;
+		}
+		j -= kOutPad * kHidden;
+		float b = 0.0f;
+		if(j < static_cast<uint32_t>(kHiddenLayers * kHidden))
+		{
+			const uint32_t l = j / kHidden, o = j % kHidden;
+			const int off[4] = {kOffB0, kOffB1, kOffB2, kOffB3};
+			b = params[off[l] + o];
+		}
+		else if(j - kHiddenLayers * kHidden < static_cast<uint32_t>(kOut))
+		{
+			b = params[kOffB4 + (j - kHiddenLayers * kHidden)];
+		}
+		reinterpret_cast<float*>(image + kOffImgBias)[j] = b;
+	}
+}
+
+}// end anonymous namespace
+
+int image_bytes() { return kImageBytes; }
+
+void pack_image(const float* d_params, unsigned char* d_image, cudaStream_t s)
+{
+	pack_image_kernel<<<64, 256, 0, s>>>(d_params, d_image);
+	PG_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_forward(const unsigned char* d_image, const float* d_features, uint32_t n, float* d_out_raw,
+                    __nv_bfloat16* d_out_acts, uint32_t* d_error, cudaStream_t s)
+{
+	if(n == 0)
+	{
+		return;
+	}
+	static const bool configured = []
+	{
+		PG_CUDA_CHECK(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+		return true;
+	}();
+	(void)configured;
+	const uint32_t tiles = (n + kTile - 1) / kTile;
+	const uint32_t grid = std::min<uint32_t>(tiles, static_cast<uint32_t>(sm_count()));
+	mlp_forward_kernel<<<grid, kThreads, kSmemBytes, s>>>(d_image, d_features, n, d_out_raw, d_out_acts, d_error);
+	PG_CUDA_CHECK(cudaGetLastError());
+}
+
+}// end namespace guide
+}// end namespace pg
+
+using namespace pg;
+
+extern "C" {
+
+int pgpu_guide_forward(const float* params, const float* features, uint64_t n, float* out_raw)
+{
+	return guarded([&]
+	{
+		if(!params || (n > 0 && (!features || !out_raw)))
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_guide_forward: null pointer");
+		}
+		if(n > (1u << 30))
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_guide_forward: too many queries");
+		}
+		require_device();
+		if(n == 0)
+		{
+			return;
+		}
+		cudaStream_t s = library_stream();
+		DeviceBuffer<float> d_params(guide::kNumParams);
+		DeviceBuffer<unsigned char> d_image(guide::image_bytes());
+		DeviceBuffer<float> d_feat(n * 8);
+		DeviceBuffer<float> d_out(n * guide::kOut);
+		DeviceBuffer<uint32_t> d_err(1);
+		PG_CUDA_CHECK(cudaMemsetAsync(d_err.get(), 0, sizeof(uint32_t), s));
+		PG_CUDA_CHECK(cudaMemcpyAsync(d_params.get(), params, d_params.bytes(), cudaMemcpyHostToDevice, s));
+		// features: host [n][7] -> device [n][8]
+		std::vector<float> feat(n * 8, 0.0f);
+		for(uint64_t i = 0; i < n; ++i)
+		{
+			std::memcpy(&feat[i * 8], features + i * guide::kInputs, sizeof(float) * guide::kInputs);
+		}
+		PG_CUDA_CHECK(cudaMemcpyAsync(d_feat.get(), feat.data(), d_feat.bytes(), cudaMemcpyHostToDevice, s));
+		guide::pack_image(d_params.get(), d_image.get(), s);
+		guide::launch_forward(d_image.get(), d_feat.get(), static_cast<uint32_t>(n), d_out.get(), nullptr, d_err.get(), s);
+		uint32_t err = 0;
+		PG_CUDA_CHECK(cudaMemcpyAsync(out_raw, d_out.get(), d_out.bytes(), cudaMemcpyDeviceToHost, s));
+		PG_CUDA_CHECK(cudaMemcpyAsync(&err, d_err.get(), sizeof(err), cudaMemcpyDeviceToHost, s));
+		PG_CUDA_CHECK(cudaStreamSynchronize(s));
+		if(err)
+		{
+			throw Error(PG_ERR_CUDA, "guiding network: tensor-core wait timed out");
+		}
+	});
+}
+
+}// extern "C"

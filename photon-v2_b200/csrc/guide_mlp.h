@@ -1,0 +1,27 @@
+// Guiding network kernels (tcgen05 BF16 forward pass; training in guide_train.cu).
+#pragma once
+
+#include "guide.cuh"
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace pg
+{
+namespace guide
+{
+
+// Bytes of the packed BF16 weight image the forward kernel copies into shared memory.
+int image_bytes();
+
+// FP32 parameters (kNumParams, packed order of guide.cuh) -> weight image.
+void pack_image(const float* d_params, unsigned char* d_image, cudaStream_t s);
+
+// Forward pass of n queries. d_features: [n][8] FP32 (7 used). d_out_raw: [n][40] FP32 raw
+// outputs (decode() turns them into a mixture). d_out_acts (optional): [n][4][64] BF16 post-ReLU
+// hidden activations, for training. Errors are OR-ed into *d_error (PG_DEV_ERR_GUIDE_WAIT).
+void launch_forward(const unsigned char* d_image, const float* d_features, uint32_t n, float* d_out_raw,
+                    __nv_bfloat16* d_out_acts, uint32_t* d_error, cudaStream_t s);
+
+}// end namespace guide
+}// end namespace pg

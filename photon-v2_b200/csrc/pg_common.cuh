@@ -117,6 +117,7 @@ enum DeviceErrorFlag : uint32_t
 	PG_DEV_ERR_STACK = 1u << 0,
 	PG_DEV_ERR_QUEUE = 1u << 1,
 	PG_DEV_ERR_NAN = 1u << 2,
+	PG_DEV_ERR_GUIDE_WAIT = 1u << 3,   // a guiding-network kernel gave up waiting on its tensor cores
 };
 
 // Traversal stack depth (node groups). The builder checks the tree depth against it.

@@ -42,6 +42,7 @@ PGPU_SIGNATURES = [
     ("pgpu_trace_counts", ctypes.c_int,
      [ctypes.c_uint64, _f32p, ctypes.c_uint64, ctypes.c_int, _dblp, _dblp]),
     ("pgpu_bsdf_eval", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
+    ("pgpu_guide_forward", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
     ("pgpu_scene_create", ctypes.c_int,
      [_f32p, _u32p, _u32p, ctypes.c_uint64, _f32p, ctypes.c_uint32, _f32p, ctypes.c_uint32, _f32p, _u64p]),
     ("pgpu_scene_destroy", ctypes.c_int, [ctypes.c_uint64]),
@@ -154,6 +155,16 @@ def bsdf_eval(cases: np.ndarray, normals: np.ndarray) -> np.ndarray:
     out = np.empty((c.shape[0], 16), np.float32)
     _check(load().pgpu_bsdf_eval(_ptr(c, ctypes.c_float), _ptr(nrm, ctypes.c_float), c.shape[0],
                                  _ptr(out, ctypes.c_float)))
+    return out
+
+
+def guide_forward(params: np.ndarray, features: np.ndarray) -> np.ndarray:
+    """Raw outputs [n, 40] of the guiding network (tensor-core forward pass) for features [n, 7]."""
+    p = np.ascontiguousarray(params, np.float32).reshape(-1)
+    f = np.ascontiguousarray(features, np.float32).reshape(-1, 7)
+    out = np.empty((f.shape[0], 40), np.float32)
+    _check(load().pgpu_guide_forward(_ptr(p, ctypes.c_float), _ptr(f, ctypes.c_float), f.shape[0],
+                                     _ptr(out, ctypes.c_float)))
     return out
 
 

@@ -1,0 +1,73 @@
+"""Learned path guiding: the tensor-core network against the NumPy oracle (oracle/guide_ref.py).
+
+The reference renderer has no guiding, so the oracle is our own FP64/FP32 restatement of the
+network, its loss and its gradients; the oracle's gradients are themselves pinned by central
+finite differences here. GPU tolerances: the forward pass mirrors the GPU's BF16 rounding points,
+so outputs agree to FP32 accumulation-order noise, except where a hidden activation lands on the
+other side of a BF16 rounding boundary; the bound is 2 % of the output RMS per element and 0.2 %
+on average.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import guide_ref as ref
+
+
+def _batch(n, seed):
+    rng = np.random.default_rng(seed)
+    f = rng.random((n, 7)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    w = rng.random(n) + 0.1
+    return f, d, w
+
+
+def test_oracle_gradients_match_finite_differences():
+    rng = np.random.default_rng(1)
+    p = ref.init_params(3, out_scale=1.0).astype(np.float64)
+    p[ref.NUM_PARAMS - ref.OUT:] = rng.normal(0.0, 0.5, ref.OUT)
+    f, d, w = _batch(48, 2)
+    _, g = ref.gradients(p, f, d, w, exact=True)
+    for _ in range(3):
+        v = rng.normal(size=p.size)
+        eps = 1e-6
+        lp = ref.loss_and_output_grad(ref.forward(p + eps * v, f, exact=True), d, w)[0]
+        lm = ref.loss_and_output_grad(ref.forward(p - eps * v, f, exact=True), d, w)[0]
+        assert abs((lp - lm) / (2 * eps) - g @ v) <= 1e-6 * max(1.0, abs(g @ v))
+
+
+def test_mixture_density_integrates_to_one():
+    rng = np.random.default_rng(4)
+    raw = rng.normal(size=(1, ref.OUT))
+    raw[0, 4::5] = np.log([0.5, 2.0, 10.0, 40.0, 1.0, 3.0, 100.0, 7.0])
+    # stratified Monte Carlo over the sphere
+    u = (np.arange(200000) + rng.random(200000)) / 200000
+    z = 1 - 2 * u
+    phi = 2 * np.pi * rng.random(200000)
+    r = np.sqrt(1 - z * z)
+    dirs = np.stack([r * np.cos(phi), r * np.sin(phi), z], axis=1)
+    q = ref.mixture_pdf(np.repeat(raw, len(dirs), axis=0), dirs)
+    assert abs(q.mean() * 4 * np.pi - 1.0) < 0.02
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 127, 128, 4099])
+def test_tensor_core_forward_matches_oracle(gpu_lib, n):
+    import photon_gpu
+
+    params = ref.init_params(7, out_scale=1.0)
+    rng = np.random.default_rng(8)
+    params[ref.NUM_PARAMS - 4 * 64 - 64 * 40 - 40:] += 0.0
+    b = ref.unpack(params)
+    for name in ("b0", "b1", "b2", "b3", "b4"):
+        b[name] = rng.normal(0.0, 0.1, b[name].shape).astype(np.float32)
+    params = ref.pack(b)
+    f, _, _ = _batch(n, 9)
+    got = photon_gpu.guide_forward(params, f)
+    want = ref.forward(params, f)
+    rms = float(np.sqrt(np.mean(want ** 2)))
+    err = np.abs(got - want)
+    assert np.all(np.isfinite(got))
+    assert err.max() <= 0.02 * rms, (err.max(), rms)
+    assert err.mean() <= 0.002 * rms, (err.mean(), rms)
