@@ -93,6 +93,17 @@ PGPU_API int pgpu_trace_counts(uint64_t id, const float* rays, uint64_t n, int a
  * operands, FP32 accumulation). features: host [n][7]; out_raw: host [n][40]. */
 PGPU_API int pgpu_guide_forward(const float* params, const float* features, uint64_t n, float* out_raw);
 
+/* Training loss -sum_i w_i log q(d_i | x_i) / sum_i w_i of a batch (features [n][7], unit
+ * directions [n][3], weights [n]) and its gradient with respect to all parameters
+ * (out_grads[29480]); forward pass on the tensor cores, backward in FP32. */
+PGPU_API int pgpu_guide_gradients(const float* params, const float* features, const float* dirs,
+                       const float* weights, uint64_t n, float* out_loss, float* out_grads);
+
+/* `steps` Adam steps (learning rate lr) over consecutive batches of `batch` samples of the data
+ * set (cycled); params is updated in place, out_losses[steps] (optional) receives each step's loss. */
+PGPU_API int pgpu_guide_train(float* params, const float* features, const float* dirs, const float* weights,
+                       uint64_t n, uint32_t steps, uint32_t batch, float lr, float* out_losses);
+
 /* ---------------------------------------------------------------------------------------------
  * BSDF kernels, evaluated one case per thread on the GPU with the same device functions the path
  * tracer uses. cases: float32 [n][19] (type, p0..p5, N(3), V(3), L(3), u(3)) with

@@ -23,5 +23,15 @@ void pack_image(const float* d_params, unsigned char* d_image, cudaStream_t s);
 void launch_forward(const unsigned char* d_image, const float* d_features, uint32_t n, float* d_out_raw,
                     __nv_bfloat16* d_out_acts, uint32_t* d_error, cudaStream_t s);
 
+// Loss and gradient of a batch (forward pass included): d_grads += d loss / d params, *d_loss +=
+// loss; d_total receives sum of weights. d_dirw: [n] (direction xyz, weight). d_raw: [n][40] and
+// d_acts: [n][4][64] scratch.
+void launch_gradients(const float* d_params, const unsigned char* d_image, const float* d_features,
+                      const float4* d_dirw, uint32_t n, float* d_raw, __nv_bfloat16* d_acts,
+                      float* d_grads, float* d_loss, float* d_total, uint32_t* d_error, cudaStream_t s);
+
+// One Adam step (beta 0.9 / 0.999, eps 1e-8) on the FP32 parameters; zeroes d_grads.
+void launch_adam(float* d_params, float* d_grads, float* d_m, float* d_v, uint32_t step, float lr, cudaStream_t s);
+
 }// end namespace guide
 }// end namespace pg

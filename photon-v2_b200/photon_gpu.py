@@ -43,6 +43,9 @@ PGPU_SIGNATURES = [
      [ctypes.c_uint64, _f32p, ctypes.c_uint64, ctypes.c_int, _dblp, _dblp]),
     ("pgpu_bsdf_eval", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
     ("pgpu_guide_forward", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
+    ("pgpu_guide_gradients", ctypes.c_int, [_f32p, _f32p, _f32p, _f32p, ctypes.c_uint64, _f32p, _f32p]),
+    ("pgpu_guide_train", ctypes.c_int,
+     [_f32p, _f32p, _f32p, _f32p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _f32p]),
     ("pgpu_scene_create", ctypes.c_int,
      [_f32p, _u32p, _u32p, ctypes.c_uint64, _f32p, ctypes.c_uint32, _f32p, ctypes.c_uint32, _f32p, _u64p]),
     ("pgpu_scene_destroy", ctypes.c_int, [ctypes.c_uint64]),
@@ -166,6 +169,31 @@ def guide_forward(params: np.ndarray, features: np.ndarray) -> np.ndarray:
     _check(load().pgpu_guide_forward(_ptr(p, ctypes.c_float), _ptr(f, ctypes.c_float), f.shape[0],
                                      _ptr(out, ctypes.c_float)))
     return out
+
+
+def guide_gradients(params, features, dirs, weights):
+    """(loss, gradient [29480]) of the guiding loss on one batch (GPU)."""
+    p = np.ascontiguousarray(params, np.float32).reshape(-1)
+    f = np.ascontiguousarray(features, np.float32).reshape(-1, 7)
+    d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+    w = np.ascontiguousarray(weights, np.float32).reshape(-1)
+    g = np.empty_like(p)
+    loss = ctypes.c_float()
+    _check(load().pgpu_guide_gradients(_ptr(p, ctypes.c_float), _ptr(f, ctypes.c_float), _ptr(d, ctypes.c_float),
+                                       _ptr(w, ctypes.c_float), f.shape[0], ctypes.byref(loss), _ptr(g, ctypes.c_float)))
+    return loss.value, g
+
+
+def guide_train(params, features, dirs, weights, steps, batch, lr=1e-2):
+    """Adam-trains a copy of params on the data set; returns (params, per-step losses)."""
+    p = np.array(params, np.float32).reshape(-1)
+    f = np.ascontiguousarray(features, np.float32).reshape(-1, 7)
+    d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+    w = np.ascontiguousarray(weights, np.float32).reshape(-1)
+    losses = np.empty(steps, np.float32)
+    _check(load().pgpu_guide_train(_ptr(p, ctypes.c_float), _ptr(f, ctypes.c_float), _ptr(d, ctypes.c_float),
+                                   _ptr(w, ctypes.c_float), f.shape[0], steps, batch, lr, _ptr(losses, ctypes.c_float)))
+    return p, losses
 
 
 MATTE, CONDUCTOR, DIELECTRIC = 0, 1, 2
