@@ -108,6 +108,10 @@ extern PH_API PhBool phGpuGetErrors(PhUInt64 engineId, const PhChar** out_messag
 extern PH_API void phGpuSetMaxRayBounces(PhUInt64 engineId, PhUInt32 maxRayBounces);
 /* Seed of the counter-based random numbers (default 42). */
 extern PH_API void phGpuSetSeed(PhUInt64 engineId, PhUInt64 seed);
+/* Learned path guiding for the BNEEPT estimator: a small MLP proposes incident directions at
+ * Lambertian vertices (mixed with BSDF sampling by one-sample MIS, so results stay unbiased) and
+ * is trained online on the render's own radiance samples. Off by default. */
+extern PH_API void phGpuSetGuiding(PhUInt64 engineId, PhBool enabled);
 /* Clears the film; the next phRender starts a fresh image. */
 extern PH_API void phGpuClearFilm(PhUInt64 engineId);
 /* Device milliseconds, paths, closest-hit rays and shadow rays of the last phRender, and the

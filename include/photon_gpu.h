@@ -149,6 +149,20 @@ PGPU_API int pgpu_scene_render(uint64_t id, uint32_t spp, uint32_t max_bounces, 
 PGPU_API int pgpu_scene_film(uint64_t id, float* out_rgb, double* out_sum, uint64_t* out_spp);
 PGPU_API int pgpu_scene_clear(uint64_t id);
 
+/* Learned path guiding for the scene's subsequent BNEEPT renders (no reference counterpart). At
+ * Lambertian vertices the next direction comes from the network's vMF mixture with probability
+ * alpha, else from the BSDF, weighted by the one-sample MIS density, so renders stay unbiased;
+ * NEE's MIS uses the same density. With train != 0 every render iteration records up to `batch`
+ * (vertex, direction, incident radiance) samples and takes one Adam step (learning rate lr).
+ * The network persists across renders until pgpu_scene_guide_reset. */
+PGPU_API int pgpu_scene_set_guiding(uint64_t id, int enabled, int train, float alpha, float lr, uint32_t batch);
+PGPU_API int pgpu_scene_guide_reset(uint64_t id);
+/* Last render's mean training loss, guided vertices, per-kernel milliseconds of a profiled render
+ * (prepare, regen, extend, shade, shadow, guide inference, guide training; 7 doubles) and the FP32
+ * network parameters (29,480 floats). Any output may be NULL. */
+PGPU_API int pgpu_scene_guide_info(uint64_t id, float* out_loss, uint64_t* out_guided_vertices,
+                        double* out_kernel_ms, float* out_params);
+
 /* ---------------------------------------------------------------------------------------------
  * Scene cooking without a GPU: parses SDL text (the grammar of the reference's SdlCommandParser,
  * Engine/Source/SDL/SdlCommandParser.cpp:84-560) and cooks it the way phUpdate does (actors to

@@ -443,6 +443,14 @@ void phGpuSetSeed(PhUInt64 engineId, PhUInt64 seed)
 	}
 }
 
+void phGpuSetGuiding(PhUInt64 engineId, PhBool enabled)
+{
+	if(auto e = engines().get(engineId))
+	{
+		e->engine.set_guiding(enabled == PH_TRUE);
+	}
+}
+
 void phGpuClearFilm(PhUInt64 engineId)
 {
 	if(auto e = engines().get(engineId))

@@ -757,6 +757,11 @@ void Engine::render()
 		if(chunk > max_chunk_spp) { chunk = static_cast<uint32_t>(max_chunk_spp); }
 		m_work_total = m_spp;
 		m_work_done = 0;
+		{
+			GuideParams g = m_render->scene->guiding();
+			g.enabled = m_guiding;
+			m_render->scene->set_guiding(g);
+		}
 		m_info = RenderInfo{0.0, 0, 0, 0, m_info.update_seconds, m_info.num_triangles};
 		m_launches = 0;
 		uint32_t done = 0;

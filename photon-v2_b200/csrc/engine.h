@@ -74,6 +74,8 @@ public:
 	void set_max_ray_bounces(uint32_t n) { m_max_bounces = n; }
 	void set_seed(uint64_t seed) { m_seed = seed; }
 	void set_sample_offset(uint64_t first_sample) { m_first_sample = first_sample; }
+	// Learned path guiding of the BNEEPT estimator (network trained online during rendering).
+	void set_guiding(bool enabled) { m_guiding = enabled; }
 	const RenderInfo& info() const { return m_info; }
 	uint64_t launch_count() const { return m_launches; }
 	// Renders into a scratch film with the given render mode and returns the statistics of
@@ -104,6 +106,7 @@ private:
 	uint32_t m_max_bounces = 10000;
 	uint64_t m_seed = 42;
 	uint64_t m_first_sample = 0;
+	bool m_guiding = false;
 
 	std::shared_ptr<RenderObject> m_render;
 	uint32_t m_width = 0, m_height = 0;

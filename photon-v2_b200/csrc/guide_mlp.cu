@@ -176,9 +176,10 @@ __device__ __forceinline__ void store_row8(unsigned char* buf, uint32_t r, uint3
 
 __global__ void __launch_bounds__(kThreads, 1)
 mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restrict__ features,
-                   uint32_t n, float* __restrict__ out_raw, __nv_bfloat16* __restrict__ out_acts,
-                   uint32_t* __restrict__ error)
+                   uint32_t n_max, const uint32_t* __restrict__ d_n, float* __restrict__ out_raw,
+                   __nv_bfloat16* __restrict__ out_acts, uint32_t* __restrict__ error)
 {
+	const uint32_t n = d_n ? min(*d_n, n_max) : n_max;
 	extern __shared__ __align__(128) unsigned char smem[];
 	const uint32_t tid = threadIdx.x;
 	const uint32_t warp = tid >> 5;
@@ -412,7 +413,7 @@ void pack_image(const float* d_params, unsigned char* d_image, cudaStream_t s)
 }
 
 void launch_forward(const unsigned char* d_image, const float* d_features, uint32_t n, float* d_out_raw,
-                    __nv_bfloat16* d_out_acts, uint32_t* d_error, cudaStream_t s)
+                    __nv_bfloat16* d_out_acts, uint32_t* d_error, cudaStream_t s, const uint32_t* d_n)
 {
 	if(n == 0)
 	{
@@ -426,7 +427,7 @@ void launch_forward(const unsigned char* d_image, const float* d_features, uint3
 	(void)configured;
 	const uint32_t tiles = (n + kTile - 1) / kTile;
 	const uint32_t grid = std::min<uint32_t>(tiles, static_cast<uint32_t>(sm_count()));
-	mlp_forward_kernel<<<grid, kThreads, kSmemBytes, s>>>(d_image, d_features, n, d_out_raw, d_out_acts, d_error);
+	mlp_forward_kernel<<<grid, kThreads, kSmemBytes, s>>>(d_image, d_features, n, d_n, d_out_raw, d_out_acts, d_error);
 	PG_CUDA_CHECK(cudaGetLastError());
 }
 

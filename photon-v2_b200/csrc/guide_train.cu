@@ -38,8 +38,10 @@ __device__ __forceinline__ float bf16r(float x)
 	return __bfloat162float(__float2bfloat16_rn(x));
 }
 
-__global__ void weight_sum_kernel(const float4* __restrict__ dirw, uint32_t n, float* __restrict__ total)
+__global__ void weight_sum_kernel(const float4* __restrict__ dirw, uint32_t n_max, const uint32_t* __restrict__ d_n,
+                                  float* __restrict__ total)
 {
+	const uint32_t n = d_n ? min(*d_n, n_max) : n_max;
 	float s = 0.0f;
 	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
@@ -52,6 +54,22 @@ __global__ void weight_sum_kernel(const float4* __restrict__ dirw, uint32_t n, f
 	if((threadIdx.x & 31) == 0)
 	{
 		atomicAdd(total, s);
+	}
+}
+
+// Caps every sample weight at factor x the batch's mean weight (the sum in *total), in place.
+__global__ void clamp_weights_kernel(float4* __restrict__ dirw, uint32_t n_max, const uint32_t* __restrict__ d_n,
+                                     const float* __restrict__ total, float factor)
+{
+	const uint32_t n = d_n ? min(*d_n, n_max) : n_max;
+	if(n == 0u)
+	{
+		return;
+	}
+	const float cap = factor * *total / static_cast<float>(n);
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		dirw[i].w = fminf(dirw[i].w, cap);
 	}
 }
 
@@ -127,9 +145,14 @@ __device__ void reduce_bias_grad(const float* sd, int out_dim, float* grad)
 __global__ void __launch_bounds__(kBlock)
 backward_kernel(const float* __restrict__ params, const float* __restrict__ features,
                 const float4* __restrict__ dirw, const float* __restrict__ raw_out,
-                const __nv_bfloat16* __restrict__ acts, uint32_t n, const float* __restrict__ total_weight,
-                float* __restrict__ grads, float* __restrict__ loss)
+                const __nv_bfloat16* __restrict__ acts, uint32_t n_max, const uint32_t* __restrict__ d_n,
+                const float* __restrict__ total_weight, float* __restrict__ grads, float* __restrict__ loss)
 {
+	const uint32_t n = d_n ? min(*d_n, n_max) : n_max;
+	if(blockIdx.x * kBlock >= n)
+	{
+		return;   // whole block past the live samples (uniform exit before any barrier)
+	}
 	extern __shared__ float smem_f[];   // sx, sd: [kBlock][kPitch] each (dynamic, 66 KB)
 	float* sx = smem_f;
 	float* sd = smem_f + kBlock * kPitch;
@@ -277,8 +300,11 @@ backward_kernel(const float* __restrict__ params, const float* __restrict__ feat
 
 __global__ void adam_kernel(float* __restrict__ params, float* __restrict__ grads, float* __restrict__ m,
                             float* __restrict__ v, uint32_t count, float lr, float beta1, float beta2,
-                            float eps, float bias1, float bias2)
+                            float eps, const uint32_t* __restrict__ step)
 {
+	const float t = static_cast<float>(*step + 1u);
+	const float bias1 = 1.0f - powf(beta1, t);
+	const float bias2 = 1.0f - powf(beta2, t);
 	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
 	{
 		const float g = grads[i];
@@ -291,20 +317,34 @@ __global__ void adam_kernel(float* __restrict__ params, float* __restrict__ grad
 	}
 }
 
+__global__ void step_kernel(uint32_t* step)
+{
+	++*step;
+}
+
 }// end anonymous namespace
 
 void launch_gradients(const float* d_params, const unsigned char* d_image, const float* d_features,
                       const float4* d_dirw, uint32_t n, float* d_raw, __nv_bfloat16* d_acts,
-                      float* d_grads, float* d_loss, float* d_total, uint32_t* d_error, cudaStream_t s)
+                      float* d_grads, float* d_loss, float* d_total, uint32_t* d_error, cudaStream_t s,
+                      const uint32_t* d_n, float clamp_factor)
 {
 	if(n == 0)
 	{
 		return;
 	}
 	PG_CUDA_CHECK(cudaMemsetAsync(d_total, 0, sizeof(float), s));
-	weight_sum_kernel<<<64, 256, 0, s>>>(d_dirw, n, d_total);
+	weight_sum_kernel<<<64, 256, 0, s>>>(d_dirw, n, d_n, d_total);
 	PG_CUDA_CHECK(cudaGetLastError());
-	launch_forward(d_image, d_features, n, d_raw, d_acts, d_error, s);
+	if(clamp_factor > 0.0f)
+	{
+		// rare, very bright samples would otherwise dominate single steps
+		clamp_weights_kernel<<<64, 256, 0, s>>>(const_cast<float4*>(d_dirw), n, d_n, d_total, clamp_factor);
+		PG_CUDA_CHECK(cudaMemsetAsync(d_total, 0, sizeof(float), s));
+		weight_sum_kernel<<<64, 256, 0, s>>>(d_dirw, n, d_n, d_total);
+		PG_CUDA_CHECK(cudaGetLastError());
+	}
+	launch_forward(d_image, d_features, n, d_raw, d_acts, d_error, s, d_n);
 	constexpr int smem_bytes = 2 * kBlock * kPitch * sizeof(float);
 	static const bool configured = []
 	{
@@ -313,16 +353,15 @@ void launch_gradients(const float* d_params, const unsigned char* d_image, const
 	}();
 	(void)configured;
 	backward_kernel<<<(n + kBlock - 1) / kBlock, kBlock, smem_bytes, s>>>(d_params, d_features, d_dirw, d_raw, d_acts,
-	                                                                     n, d_total, d_grads, d_loss);
+	                                                                     n, d_n, d_total, d_grads, d_loss);
 	PG_CUDA_CHECK(cudaGetLastError());
 }
 
-void launch_adam(float* d_params, float* d_grads, float* d_m, float* d_v, uint32_t step, float lr, cudaStream_t s)
+void launch_adam(float* d_params, float* d_grads, float* d_m, float* d_v, uint32_t* d_step, float lr, cudaStream_t s)
 {
-	const float beta1 = 0.9f, beta2 = 0.999f;
-	const float bias1 = 1.0f - powf(beta1, static_cast<float>(step));
-	const float bias2 = 1.0f - powf(beta2, static_cast<float>(step));
-	adam_kernel<<<64, 256, 0, s>>>(d_params, d_grads, d_m, d_v, kNumParams, lr, beta1, beta2, 1e-8f, bias1, bias2);
+	adam_kernel<<<64, 256, 0, s>>>(d_params, d_grads, d_m, d_v, kNumParams, lr, 0.9f, 0.999f, 1e-8f, d_step);
+	PG_CUDA_CHECK(cudaGetLastError());
+	step_kernel<<<1, 1, 0, s>>>(d_step);
 	PG_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -419,8 +458,9 @@ int pgpu_guide_train(float* params, const float* features, const float* dirs, co
 		DeviceBuffer<float> d_feat(n * 8), d_raw(b * guide::kOut), d_scalars(2 * steps);
 		DeviceBuffer<float4> d_dirw(n);
 		DeviceBuffer<__nv_bfloat16> d_acts(static_cast<size_t>(b) * guide::kHiddenLayers * guide::kHidden);
-		DeviceBuffer<uint32_t> d_err(1);
+		DeviceBuffer<uint32_t> d_err(1), d_step(1);
 		PG_CUDA_CHECK(cudaMemsetAsync(d_err.get(), 0, sizeof(uint32_t), s));
+		PG_CUDA_CHECK(cudaMemsetAsync(d_step.get(), 0, sizeof(uint32_t), s));
 		PG_CUDA_CHECK(cudaMemsetAsync(d_grads.get(), 0, d_grads.bytes(), s));
 		PG_CUDA_CHECK(cudaMemsetAsync(d_m.get(), 0, d_m.bytes(), s));
 		PG_CUDA_CHECK(cudaMemsetAsync(d_v.get(), 0, d_v.bytes(), s));
@@ -435,7 +475,7 @@ int pgpu_guide_train(float* params, const float* features, const float* dirs, co
 			guide::launch_gradients(d_params.get(), d_image.get(), d_feat.get() + static_cast<size_t>(first) * 8,
 			                        d_dirw.get() + first, count, d_raw.get(), d_acts.get(), d_grads.get(),
 			                        d_scalars.get() + 2 * step, d_scalars.get() + 2 * step + 1, d_err.get(), s);
-			guide::launch_adam(d_params.get(), d_grads.get(), d_m.get(), d_v.get(), step + 1, lr, s);
+			guide::launch_adam(d_params.get(), d_grads.get(), d_m.get(), d_v.get(), d_step.get(), lr, s);
 		}
 		std::vector<float> scalars(2 * steps);
 		uint32_t err = 0;

@@ -221,4 +221,52 @@ int pgpu_scene_clear(uint64_t id)
 	});
 }
 
+int pgpu_scene_set_guiding(uint64_t id, int enabled, int train, float alpha, float lr, uint32_t batch)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		if(!(alpha > 0.0f && alpha < 1.0f) || !(lr > 0.0f) || batch == 0 || batch > (1u << 22))
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_set_guiding: alpha must lie in (0, 1), lr > 0, "
+			                                     "0 < batch <= 2^22");
+		}
+		GuideParams g;
+		g.enabled = enabled != 0;
+		g.train = train != 0;
+		g.alpha = alpha;
+		g.lr = lr;
+		g.batch = batch;
+		r->scene->set_guiding(g);
+	});
+}
+
+int pgpu_scene_guide_reset(uint64_t id)
+{
+	return guarded([&]
+	{
+		get_render(id)->scene->reset_guiding();
+	});
+}
+
+int pgpu_scene_guide_info(uint64_t id, float* out_loss, uint64_t* out_guided_vertices, double* out_kernel_ms,
+                          float* out_params)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		const RenderScene& rs = *r->scene;
+		if(out_loss) { *out_loss = rs.last_guide_loss(); }
+		if(out_guided_vertices) { *out_guided_vertices = rs.last_guided_vertices(); }
+		if(out_kernel_ms)
+		{
+			for(int k = 0; k < 7; ++k)
+			{
+				out_kernel_ms[k] = rs.last_kernel_ms()[k];
+			}
+		}
+		if(out_params) { rs.guide_params(out_params); }
+	});
+}
+
 }// extern "C"

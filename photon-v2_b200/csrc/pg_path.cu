@@ -6,6 +6,7 @@
 //   BVPTEstimator::estimate    Engine/Source/Core/Estimator/BVPTEstimator.cpp:25-160
 // with the per-bounce loop unrolled across kernel launches: one shade invocation is one loop
 // iteration of one path.
+#include "guide_mlp.h"
 #include "pg_render.h"
 #include "refinery.cuh"
 #include "scene_build.h"
@@ -64,6 +65,7 @@ enum : uint32_t
 	DIM_NEE_PICK = 2, DIM_NEE_TRI = 3, DIM_NEE_U = 4, DIM_NEE_V = 5,
 	DIM_BSDF_0 = 6, DIM_BSDF_1 = 7, DIM_BSDF_2 = 8,
 	DIM_RR = 9,
+	DIM_GUIDE_SEL = 10, DIM_GUIDE_0 = 11, DIM_GUIDE_1 = 12, DIM_GUIDE_2 = 13,
 };
 
 // Relative luminance of linear sRGB (CIE Y), used by Russian roulette
@@ -164,6 +166,9 @@ __global__ void prepare_kernel(RenderCounters* c, uint32_t capacity)
 	c->n_shadow = 0;
 	c->fetch_extend = 0;
 	c->fetch_shadow = 0;
+	c->guided_total += c->n_guided;
+	c->n_guided = 0;
+	c->n_train = 0;
 	c->rays_traced += c->n_total;
 }
 
@@ -206,6 +211,90 @@ regen_kernel(const RenderCounters* __restrict__ c, Camera cam, uint64_t seed, ui
 	}
 }
 
+// ---------------------------------------------------------------------------------------------
+// Learned guiding at Lambertian vertices.
+
+__device__ __forceinline__ void load_raw(const float* __restrict__ raw, float* r)
+{
+	const float4* q = reinterpret_cast<const float4*>(raw);
+	#pragma unroll
+	for(int i = 0; i < guide::kOut / 4; ++i)
+	{
+		const float4 v = __ldg(q + i);
+		r[4 * i + 0] = v.x; r[4 * i + 1] = v.y; r[4 * i + 2] = v.z; r[4 * i + 3] = v.w;
+	}
+}
+
+// Mixture density of network row `raw` at unit direction w.
+__device__ __noinline__ float guide_pdf(const float* __restrict__ raw, V3 w)
+{
+	float r[guide::kOut];
+	load_raw(raw, r);
+	return guide::mixture_pdf(guide::decode(r), w);
+}
+
+__device__ __noinline__ V3 guide_sample(const float* __restrict__ raw, float u0, float u1, float u2)
+{
+	float r[guide::kOut];
+	load_raw(raw, r);
+	return guide::mixture_sample(guide::decode(r), u0, u1, u2);
+}
+
+__device__ __forceinline__ bool guidable(const Material& m)
+{
+	return m.type == PG_MAT_MATTE && (m.cr > 0.0f || m.cg > 0.0f || m.cb > 0.0f);
+}
+
+// Network inputs for every queue entry that will be shaded at a guidable vertex; entries are
+// compacted into rows (map: entry -> row).
+__global__ void __launch_bounds__(kShadeBlock)
+guide_query_kernel(DeviceScene s, RenderCounters* __restrict__ c, PathBuffers cur, const uint2* __restrict__ hits,
+                   GuideArgs g, uint32_t max_bounces)
+{
+	const uint32_t total = c->n_total;
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+	{
+		const uint2 hit = hits[i];
+		const uint32_t meta = cur.meta[i];
+		uint32_t row = 0xFFFFFFFFu;
+		if(hit.x != 0xFFFFFFFFu && !(meta & kMetaStopAfter) && (meta & kMetaBounceMask) < max_bounces)
+		{
+			const LeafTri& lt = s.tris[hit.x];
+			if(guidable(s.materials[lt.material]))
+			{
+				const float4 o = cur.ray_o[i];
+				const float4 d4 = cur.ray_d[i];
+				const V3 d = v3(d4.x, d4.y, d4.z);
+				const float t = __uint_as_float(hit.y);
+				const V3 pos = v3(o.x, o.y, o.z) + d * t;
+				const V3 a = v3(lt.v0x, lt.v0y, lt.v0z), b = v3(lt.v1x, lt.v1y, lt.v1z), cc = v3(lt.v2x, lt.v2y, lt.v2z);
+				V3 n = normalize(cross(b - a, cc - a));
+				if(dot(n, d) > 0.0f)
+				{
+					n = -n;   // the side the path arrives on
+				}
+				const guide::Features f = guide::make_features(pos, v3(g.lo[0], g.lo[1], g.lo[2]),
+				                                               v3(g.rcp[0], g.rcp[1], g.rcp[2]), n, -d);
+				row = alloc_slot(&c->n_guided);
+				float4* dst = reinterpret_cast<float4*>(g.feat + static_cast<size_t>(row) * 8);
+				dst[0] = make_float4(f.v[0], f.v[1], f.v[2], f.v[3]);
+				dst[1] = make_float4(f.v[4], f.v[5], f.v[6], 0.0f);
+			}
+		}
+		g.map[i] = row;
+	}
+}
+
+// Running mean of the per-step training loss over a render (steps that had samples).
+__global__ void guide_loss_kernel(float* scalars, const uint32_t* n_train)
+{
+	if(*n_train > 0u)
+	{
+		scalars[2] += scalars[0];
+		scalars[3] += 1.0f;
+	}
+}
+
 struct ShadeArgs
 {
 	DeviceScene   scene;
@@ -220,8 +309,14 @@ struct ShadeArgs
 	uint32_t      max_bounces;
 	uint32_t      estimator;
 	uint32_t      width_height;
+	GuideArgs     guide;
 };
 
+__device__ __forceinline__ float4 cur_gf0(const ShadeArgs& a, uint32_t i) { return a.cur.gf0[i]; }
+__device__ __forceinline__ float4 cur_gf1(const ShadeArgs& a, uint32_t i) { return a.cur.gf1[i]; }
+
+// GUIDED instantiates the learned-guiding paths; the plain estimator compiles without them.
+template<bool GUIDED>
 __global__ void __launch_bounds__(kShadeBlock)
 shade_kernel(ShadeArgs a)
 {
@@ -250,9 +345,34 @@ shade_kernel(ShadeArgs a)
 		const V3 d = xyz(rd);
 		const bool bvpt = a.estimator == PG_EST_BVPT;
 
+		// ---- training sample for the guided vertex this ray left from: its incident radiance
+		//      is estimated by the emission found here plus the unoccluded NEE at this vertex
+		//      (added by the shadow kernel)
+		uint32_t train_row = 0xFFFFFFFFu;
+		float train_wfac = 0.0f;
+		if(GUIDED && (meta & kMetaGuideRec) && a.guide.train_cap)
+		{
+			const uint32_t k = alloc_slot(&a.counters->n_train);
+			if(k < a.guide.train_cap)
+			{
+				const float4 g0 = cur_gf0(a, i);
+				const float4 g1 = cur_gf1(a, i);
+				float4* dst = reinterpret_cast<float4*>(a.guide.train_feat + static_cast<size_t>(k) * 8);
+				dst[0] = g0;
+				dst[1] = g1;
+				train_row = k;
+				train_wfac = g1.w;
+				a.guide.train_dirw[k] = make_float4(d.x, d.y, d.z, 0.0f);
+			}
+		}
+
 		// ---- miss: environment (the dome primitive is hit after every triangle missed)
 		if(hit.x == 0xFFFFFFFFu)
 		{
+			if(train_row != 0xFFFFFFFFu && s.env_emitter >= 0)
+			{
+				a.guide.train_dirw[train_row].w = luminance(RGB{s.env_r, s.env_g, s.env_b}) * train_wfac;
+			}
 			if(s.env_emitter >= 0)
 			{
 				const RGB le = RGB{s.env_r, s.env_g, s.env_b};
@@ -308,6 +428,10 @@ shade_kernel(ShadeArgs a)
 			const EmitterRec e = s.emitters[emitter_plus_one - 1u];
 			// one-sided emission: canEmit(-d, Ns) (SurfaceEmitter.cpp:20-25)
 			const RGB le = dot(-d, frame.ns) > 0.0f ? emitter_radiance(e) : RGB{0.0f, 0.0f, 0.0f};
+			if(train_row != 0xFFFFFFFFu)
+			{
+				a.guide.train_dirw[train_row].w = luminance(le) * train_wfac;
+			}
 			if(bvpt)
 			{
 				radiance = radiance + le * safe_clamp(thr_emit * cont, 0.0f, kClampMax);
@@ -354,6 +478,11 @@ shade_kernel(ShadeArgs a)
 		V3 sh_o{}, sh_d{};
 		float sh_tmax = 0.0f;
 		RGB sh_c{};
+		float sh_train = 0.0f;   // unweighted direct-light estimate (luminance) for the training sample
+		const uint32_t grow = GUIDED ? a.guide.map[i] : 0xFFFFFFFFu;
+		const bool guided = GUIDED && grow != 0xFFFFFFFFu;
+		const float* graw = guided ? a.guide.raw + static_cast<size_t>(grow) * guide::kOut : nullptr;
+		const float alpha = a.guide.alpha;
 		// Every material here is non-delta, so NEE applies at every vertex of BNEEPT
 		// (TDirectLightEstimator::isNeeSamplable); a black Lambertian surface can gain nothing
 		// from it, so its shadow ray is skipped (its contribution would be exactly zero).
@@ -425,7 +554,16 @@ shade_kernel(ShadeArgs a)
 				RGB f;
 				if(bsdf_eval(mat, frame, l, v, &f))
 				{
-					const float pdf_bsdf = bsdf_pdf(mat, frame, l, v);
+					float pdf_bsdf = bsdf_pdf(mat, frame, l, v);
+					if(guided)
+					{
+						// the direction-sampling technique at a guided vertex is the one-sample mixture
+						pdf_bsdf = alpha * guide_pdf(graw, l) + (1.0f - alpha) * pdf_bsdf;
+					}
+					if(GUIDED && train_row != 0xFFFFFFFFu)
+					{
+						sh_train = luminance(le * (f * (fabsf(dot(frame.ns, l)) / pdf_w))) * train_wfac;
+					}
 					const float mis = pdf_w * pdf_w / (pdf_w * pdf_w + pdf_bsdf * pdf_bsdf);
 					RGB w = f * fabsf(dot(frame.ns, l));
 					w = w * throughput;
@@ -438,8 +576,48 @@ shade_kernel(ShadeArgs a)
 		}
 
 		// ---- BSDF sampling and extension (BNEEPTEstimator.cpp:155-247, BVPTEstimator.cpp:80-110)
-		const BsdfSample bs = bsdf_sample(mat, frame, v, rng.u01(bounce, DIM_BSDF_0),
-		                                  rng.u01(bounce, DIM_BSDF_1), rng.u01(bounce, DIM_BSDF_2));
+		BsdfSample bs;
+		float guided_pdf = 0.0f;
+		if(guided)
+		{
+			// one-sample MIS of the learned mixture (probability alpha) and the BSDF
+			V3 l;
+			bool have;
+			if(rng.u01(bounce, DIM_GUIDE_SEL) < alpha)
+			{
+				l = guide_sample(graw, rng.u01(bounce, DIM_GUIDE_0), rng.u01(bounce, DIM_GUIDE_1),
+				                 rng.u01(bounce, DIM_GUIDE_2));
+				have = true;
+			}
+			else
+			{
+				const BsdfSample b0 = bsdf_sample(mat, frame, v, rng.u01(bounce, DIM_BSDF_0),
+				                                  rng.u01(bounce, DIM_BSDF_1), rng.u01(bounce, DIM_BSDF_2));
+				l = b0.l;
+				have = b0.ok;
+			}
+			bs.ok = false;
+			RGB f;
+			if(have && bsdf_eval(mat, frame, l, v, &f))
+			{
+				const float pdf = alpha * guide_pdf(graw, l) + (1.0f - alpha) * bsdf_pdf(mat, frame, l, v);
+				const float c = fabsf(dot(frame.ns, l));
+				if(pdf > 0.0f && isfinite(pdf))
+				{
+					bs.l = l;
+					bs.weight = f * (c / pdf);
+					bs.rel_ior = 1.0f;
+					bs.cos = c;
+					bs.ok = is_finite(bs.weight) && c > 0.0f;
+					guided_pdf = pdf;
+				}
+			}
+		}
+		else
+		{
+			bs = bsdf_sample(mat, frame, v, rng.u01(bounce, DIM_BSDF_0),
+			                 rng.u01(bounce, DIM_BSDF_1), rng.u01(bounce, DIM_BSDF_2));
+		}
 		bool continues = bs.ok;
 		RGB next_thr_emit{};
 		float next_cont = 1.0f;
@@ -451,7 +629,7 @@ shade_kernel(ShadeArgs a)
 			rr_scale /= bs.rel_ior * bs.rel_ior;
 			if(!bvpt)
 			{
-				next_pdf = bsdf_pdf(mat, frame, bs.l, v);
+				next_pdf = guided ? guided_pdf : bsdf_pdf(mat, frame, bs.l, v);
 			}
 			bool stop_after = false;
 			if(bounce >= 3)
@@ -473,7 +651,8 @@ shade_kernel(ShadeArgs a)
 				// throughput, so a killed BVPT path ends here
 				continues = false;
 			}
-			next_meta = (bounce + 1u) | (nee_samplable ? kMetaPrevNee : 0u) | (stop_after ? kMetaStopAfter : 0u);
+			next_meta = (bounce + 1u) | (nee_samplable ? kMetaPrevNee : 0u) | (stop_after ? kMetaStopAfter : 0u) |
+			            (guided && a.guide.train_cap ? kMetaGuideRec : 0u);
 		}
 
 		uint32_t slot = 0;
@@ -489,6 +668,13 @@ shade_kernel(ShadeArgs a)
 			a.next.prev[slot] = make_float4(pos.x, pos.y, pos.z, rr_scale);
 			a.next.ray_o[slot] = make_float4(o.x, o.y, o.z, 0.0f);
 			a.next.ray_d[slot] = make_float4(off.unit_dir.x, off.unit_dir.y, off.unit_dir.z, kFloatMax);
+			if(GUIDED && (next_meta & kMetaGuideRec))
+			{
+				const float4* fr = reinterpret_cast<const float4*>(a.guide.feat + static_cast<size_t>(grow) * 8);
+				const float4 f1 = fr[1];
+				a.next.gf0[slot] = fr[0];
+				a.next.gf1[slot] = make_float4(f1.x, f1.y, f1.z, bs.cos / guided_pdf);
+			}
 		}
 		else
 		{
@@ -502,6 +688,10 @@ shade_kernel(ShadeArgs a)
 			a.shadow.o[k] = make_float4(sh_o.x, sh_o.y, sh_o.z, 0.0f);
 			a.shadow.d[k] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
 			a.shadow.c[k] = make_float4(sh_c.r, sh_c.g, sh_c.b, __uint_as_float(target));
+			if(GUIDED && a.shadow.t)
+			{
+				a.shadow.t[k] = make_float2(__uint_as_float(train_row), sh_train);
+			}
 		}
 	}
 }
@@ -573,6 +763,21 @@ RenderScene::RenderScene(const SceneDesc& desc, float max_origin_abs)
 	}
 	BvhBuildInput in{desc.tris.data(), desc.tri_material.data(), desc.tri_emitter.data(), n, max_origin_abs};
 	m_geometry = make_geometry(in);
+
+	// scene bound, normalising the guiding network's position inputs
+	{
+		float lo[3] = {desc.tris[0], desc.tris[1], desc.tris[2]}, hi[3] = {lo[0], lo[1], lo[2]};
+		for(std::size_t k = 0; k < desc.tris.size(); ++k)
+		{
+			lo[k % 3] = std::min(lo[k % 3], desc.tris[k]);
+			hi[k % 3] = std::max(hi[k % 3], desc.tris[k]);
+		}
+		for(int a = 0; a < 3; ++a)
+		{
+			m_bound_lo[a] = lo[a];
+			m_bound_rcp[a] = hi[a] > lo[a] ? 1.0f / (hi[a] - lo[a]) : 1.0f;
+		}
+	}
 
 	// Map original triangle index -> leaf slot to build the per-emitter triangle lists.
 	std::vector<LeafTri> leaf(m_geometry->tris.size());
@@ -699,6 +904,94 @@ void RenderScene::ensure_capacity(uint32_t capacity)
 	m_capacity = capacity;
 }
 
+void RenderScene::ensure_guiding(uint32_t capacity)
+{
+	cudaStream_t st = library_stream();
+	if(capacity > m_guide_capacity)
+	{
+		for(int b = 0; b < 2; ++b)
+		{
+			m_gf0[b].resize(capacity);
+			m_gf1[b].resize(capacity);
+		}
+		m_st.resize(capacity);
+		m_gmap.resize(capacity);
+		m_gfeat.resize(static_cast<std::size_t>(capacity) * 8);
+		m_graw.resize(static_cast<std::size_t>(capacity) * guide::kOut);
+		m_guide_capacity = capacity;
+	}
+	const uint32_t batch = std::max<uint32_t>(m_guide_params.batch, guide::kTile);
+	if(m_tdirw.size() < batch)
+	{
+		m_tfeat.resize(static_cast<std::size_t>(batch) * 8);
+		m_traw.resize(static_cast<std::size_t>(batch) * guide::kOut);
+		m_tdirw.resize(batch);
+		m_tacts.resize(static_cast<std::size_t>(batch) * guide::kHiddenLayers * guide::kHidden);
+	}
+	if(!m_guide_ready)
+	{
+		// He-initialised weights (fixed seed), zero biases, output layer scaled down so that the
+		// first mixtures are broad
+		std::vector<float> p(guide::kNumParams, 0.0f);
+		uint64_t state = 0x853C49E6748FEA9Bull;
+		auto gauss = [&]()
+		{
+			auto u = [&]()
+			{
+				state = state * 6364136223846793005ull + 1442695040888963407ull;
+				return (static_cast<double>(state >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+			};
+			const double a = u(), b = u();
+			return std::sqrt(-2.0 * std::log(a)) * std::cos(6.283185307179586 * b);
+		};
+		auto fill = [&](int off, int fan_in, int count, double scale)
+		{
+			for(int k = 0; k < count; ++k)
+			{
+				p[off + k] = static_cast<float>(gauss() * std::sqrt(2.0 / fan_in) * scale);
+			}
+		};
+		fill(guide::kOffW0, guide::kIn, guide::kIn * guide::kHidden, 1.0);
+		fill(guide::kOffW1, guide::kHidden, guide::kHidden * guide::kHidden, 1.0);
+		fill(guide::kOffW2, guide::kHidden, guide::kHidden * guide::kHidden, 1.0);
+		fill(guide::kOffW3, guide::kHidden, guide::kHidden * guide::kHidden, 1.0);
+		fill(guide::kOffW4, guide::kHidden, guide::kHidden * guide::kOut, 0.1);
+		m_gparams.resize(guide::kNumParams);
+		m_gm.resize(guide::kNumParams);
+		m_gv.resize(guide::kNumParams);
+		m_ggrads.resize(guide::kNumParams);
+		m_gscalars.resize(4);   // step loss, weight total, loss sum over the render, steps with samples
+		m_gimage.resize(guide::image_bytes());
+		m_gstep.resize(1);
+		m_gerr.resize(1);
+		PG_CUDA_CHECK(cudaMemcpyAsync(m_gparams.get(), p.data(), m_gparams.bytes(), cudaMemcpyHostToDevice, st));
+		PG_CUDA_CHECK(cudaMemsetAsync(m_gm.get(), 0, m_gm.bytes(), st));
+		PG_CUDA_CHECK(cudaMemsetAsync(m_gv.get(), 0, m_gv.bytes(), st));
+		PG_CUDA_CHECK(cudaMemsetAsync(m_ggrads.get(), 0, m_ggrads.bytes(), st));
+		PG_CUDA_CHECK(cudaMemsetAsync(m_gscalars.get(), 0, m_gscalars.bytes(), st));
+		PG_CUDA_CHECK(cudaMemsetAsync(m_gstep.get(), 0, m_gstep.bytes(), st));
+		PG_CUDA_CHECK(cudaMemsetAsync(m_gerr.get(), 0, m_gerr.bytes(), st));
+		guide::pack_image(m_gparams.get(), m_gimage.get(), st);
+		PG_CUDA_CHECK(cudaStreamSynchronize(st));
+		m_guide_ready = true;
+	}
+}
+
+void RenderScene::reset_guiding()
+{
+	m_guide_ready = false;
+}
+
+void RenderScene::guide_params(float* out) const
+{
+	if(!m_guide_ready)
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, "guiding network not created yet");
+	}
+	PG_CUDA_CHECK(cudaMemcpyAsync(out, m_gparams.get(), m_gparams.bytes(), cudaMemcpyDeviceToHost, library_stream()));
+	PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
+}
+
 float RenderScene::render(const RenderParams& params, double* film)
 {
 	if(params.width == 0 || params.height == 0 || params.spp == 0)
@@ -735,6 +1028,38 @@ float RenderScene::render(const RenderParams& params, double* film)
 	const uint64_t first_global = params.first_sample * wh;
 	const bool counting = params.mode == PG_RENDER_COUNT;
 
+	// learned guiding (BNEEPT only)
+	const bool guided = m_guide_params.enabled && params.estimator == PG_EST_BNEEPT;
+	const bool training = guided && m_guide_params.train;
+	GuideArgs gargs;
+	uint32_t train_cap = 0;
+	if(guided)
+	{
+		ensure_guiding(m_capacity);
+		train_cap = training ? std::max<uint32_t>(m_guide_params.batch, guide::kTile) : 0u;
+		for(int b = 0; b < 2; ++b)
+		{
+			buf[b].gf0 = m_gf0[b].get();
+			buf[b].gf1 = m_gf1[b].get();
+		}
+		sq.t = m_st.get();
+		gargs.map = m_gmap.get();
+		gargs.feat = m_gfeat.get();
+		gargs.raw = m_graw.get();
+		gargs.train_feat = m_tfeat.get();
+		gargs.train_dirw = m_tdirw.get();
+		gargs.train_cap = train_cap;
+		gargs.alpha = m_guide_params.alpha;
+		for(int a = 0; a < 3; ++a)
+		{
+			gargs.lo[a] = m_bound_lo[a];
+			gargs.rcp[a] = m_bound_rcp[a];
+		}
+		PG_CUDA_CHECK(cudaMemsetAsync(m_gerr.get(), 0, sizeof(uint32_t), st));
+		PG_CUDA_CHECK(cudaMemsetAsync(m_gscalars.get(), 0, 4 * sizeof(float), st));
+	}
+	RenderCounters* const d_counters = m_counters.get();
+
 	// The five launches of one iteration; `ev` (optional) brackets each with events.
 	auto iteration = [&](int b, cudaEvent_t* ev)
 	{
@@ -747,13 +1072,46 @@ float RenderScene::render(const RenderParams& params, double* film)
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[2], st)); }
 		launch_extend(m_dev, m_counters.get(), cur.ray_o, cur.ray_d, m_hits.get(), grid, 128, st, counting);
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[3], st)); }
+		if(guided)
+		{
+			// network inputs of this iteration's guidable vertices, then the tensor-core forward pass
+			guide_query_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, cur, m_hits.get(), gargs, params.max_bounces);
+			PG_CUDA_CHECK(cudaGetLastError());
+			guide::launch_forward(m_gimage.get(), m_gfeat.get(), capacity, m_graw.get(), nullptr, m_gerr.get(), st,
+			                      &d_counters->n_guided);
+		}
+		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[4], st)); }
 		ShadeArgs sa{m_dev, cur, nxt, m_hits.get(), sq, m_counters.get(), film, params.seed, first_global,
 		             params.max_bounces, params.estimator, static_cast<uint32_t>(wh)};
-		shade_kernel<<<grid, kShadeBlock, 0, st>>>(sa);
+		sa.guide = gargs;
+		if(guided)
+		{
+			shade_kernel<true><<<grid, kShadeBlock, 0, st>>>(sa);
+		}
+		else
+		{
+			shade_kernel<false><<<grid, kShadeBlock, 0, st>>>(sa);
+		}
 		PG_CUDA_CHECK(cudaGetLastError());
-		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[4], st)); }
-		launch_shadow(m_dev, m_counters.get(), sq, nxt.rad, film, grid, 128, st, counting);
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[5], st)); }
+		launch_shadow(m_dev, m_counters.get(), sq, nxt.rad, film, grid, 128, st, counting,
+		              training ? m_tdirw.get() : nullptr);
+		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[6], st)); }
+		if(training)
+		{
+			// one Adam step on this iteration's samples; the new weights serve the next iteration
+			PG_CUDA_CHECK(cudaMemsetAsync(m_gscalars.get(), 0, sizeof(float), st));
+			guide::launch_gradients(m_gparams.get(), m_gimage.get(), m_tfeat.get(), m_tdirw.get(), train_cap,
+			                        m_traw.get(), reinterpret_cast<__nv_bfloat16*>(m_tacts.get()), m_ggrads.get(),
+			                        m_gscalars.get(), m_gscalars.get() + 1, m_gerr.get(), st, &d_counters->n_train,
+			                        m_guide_params.clamp);
+			guide::launch_adam(m_gparams.get(), m_ggrads.get(), m_gm.get(), m_gv.get(), m_gstep.get(),
+			                   m_guide_params.lr, st);
+			guide::pack_image(m_gparams.get(), m_gimage.get(), st);
+			guide_loss_kernel<<<1, 1, 0, st>>>(m_gscalars.get(), &d_counters->n_train);
+			PG_CUDA_CHECK(cudaGetLastError());
+		}
+		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[7], st)); }
 	};
 
 	RenderCounters* host_counters = nullptr;
@@ -803,7 +1161,7 @@ float RenderScene::render(const RenderParams& params, double* film)
 	{
 		// Plain launches, one iteration at a time; in timing mode every kernel is bracketed by
 		// events on the launching stream and the durations are summed per kernel.
-		cudaEvent_t ev[6];
+		cudaEvent_t ev[8];
 		const bool timing = params.mode == PG_RENDER_TIMING;
 		for(cudaEvent_t& e : ev) { PG_CUDA_CHECK(cudaEventCreate(&e)); }
 		PG_CUDA_CHECK(cudaEventRecord(e0, st));
@@ -817,11 +1175,13 @@ float RenderScene::render(const RenderParams& params, double* film)
 			PG_CUDA_CHECK(cudaStreamSynchronize(st));
 			if(timing)
 			{
-				for(int k = 0; k < 5; ++k)
+				// event pairs: prepare, regen, extend, guide inference, shade, shadow, guide training
+				static const int slot[7] = {0, 1, 2, 5, 3, 4, 6};
+				for(int k = 0; k < 7; ++k)
 				{
 					float ms = 0.0f;
 					PG_CUDA_CHECK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
-					m_kernel_ms[k] += ms;
+					m_kernel_ms[slot[k]] += ms;
 				}
 			}
 			done = host_counters->next_path >= host_counters->total_paths && host_counters->n_next == 0;
@@ -849,6 +1209,20 @@ float RenderScene::render(const RenderParams& params, double* film)
 	m_last_counts[1] = final_counters.tris_closest;
 	m_last_counts[2] = final_counters.nodes_any;
 	m_last_counts[3] = final_counters.tris_any;
+	m_last_guided = final_counters.guided_total + final_counters.n_guided;
+	if(guided)
+	{
+		uint32_t gerr = 0;
+		float sc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+		PG_CUDA_CHECK(cudaMemcpyAsync(sc, m_gscalars.get(), sizeof(sc), cudaMemcpyDeviceToHost, st));
+		PG_CUDA_CHECK(cudaMemcpyAsync(&gerr, m_gerr.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+		PG_CUDA_CHECK(cudaStreamSynchronize(st));
+		m_last_guide_loss = sc[3] > 0.0f ? sc[2] / sc[3] : 0.0f;
+		if(gerr)
+		{
+			throw Error(PG_ERR_CUDA, "render: guiding network kernel timed out waiting on its tensor cores");
+		}
+	}
 	if(final_counters.error & PG_DEV_ERR_STACK)
 	{
 		throw Error(PG_ERR_STACK_OVERFLOW, "render: BVH traversal stack overflow");

@@ -78,6 +78,21 @@ struct RenderParams
 	uint32_t mode = PG_RENDER_GRAPH;
 };
 
+// Learned path guiding (BNEEPT only). At Lambertian vertices the direction is drawn from the
+// network's vMF mixture with probability alpha, else from the BSDF, and weighted by the one-sample
+// MIS density alpha q + (1 - alpha) p_bsdf, which keeps the estimator unbiased. With training on,
+// every iteration records up to `batch` (vertex, direction, incident radiance) samples and takes
+// one Adam step on them, so the network keeps learning across renders of the scene.
+struct GuideParams
+{
+	bool     enabled = false;
+	bool     train = true;
+	float    alpha = 0.5f;
+	float    lr = 1e-2f;
+	uint32_t batch = 16384;
+	float    clamp = 10.0f;     // training weights capped at clamp x the batch mean (0 = off)
+};
+
 // Host-side scene description handed to the renderer.
 struct SceneDesc
 {
@@ -124,10 +139,13 @@ struct alignas(16) RenderCounters
 	unsigned long long shadow_rays;
 	unsigned long long nodes_closest, tris_closest;   // counting mode only
 	unsigned long long nodes_any, tris_any;
+	unsigned long long guided_total;   // guided vertices over the whole render
 	uint32_t error;
 	uint32_t pad;
 	uint32_t fetch_extend;   // dynamic-fetch cursors of the persistent traversal kernels,
 	uint32_t fetch_shadow;   // zeroed by prepare_kernel at the start of every iteration
+	uint32_t n_guided;       // guided vertices this iteration (network rows)
+	uint32_t n_train;        // training samples recorded this iteration (may exceed the batch)
 };
 
 // Per-path state, one buffer of the ping-pong pair (structure of arrays).
@@ -140,6 +158,8 @@ struct PathBuffers
 	float4*   prev;     // previous vertex position (xyz), Russian-roulette scale (w)
 	float4*   ray_o;    // origin, tmin
 	float4*   ray_d;    // direction, tmax
+	float4*   gf0;      // guiding record of the previous vertex: features 0-3
+	float4*   gf1;      // features 4-6, |cos| / pdf of the sampled direction (guided renders only)
 };
 
 struct ShadowQueue
@@ -147,18 +167,35 @@ struct ShadowQueue
 	float4* o;          // origin, tmin
 	float4* d;          // direction, tmax
 	float4* c;          // contribution rgb, target (slot in next buffer, or 0x80000000|pixel)
+	float2* t;          // guided renders: training sample index (bits, or ~0), weight added if unoccluded
+};
+
+// Device view of the guiding buffers for one render iteration.
+struct GuideArgs
+{
+	uint32_t*       map = nullptr;        // queue entry -> network row, 0xFFFFFFFF = not guided
+	float*          feat = nullptr;       // [capacity][8] network input rows
+	const float*    raw = nullptr;        // [capacity][40] network outputs
+	float*          train_feat = nullptr; // [batch][8]: features 0-6, |cos| / pdf
+	float4*         train_dirw = nullptr; // [batch]: direction, weight
+	uint32_t        train_cap = 0;        // 0: no training samples recorded
+	float           alpha = 0.0f;         // 0: guiding off
+	float           lo[3] = {0, 0, 0};    // scene bound, for the position features
+	float           rcp[3] = {1, 1, 1};
 };
 
 constexpr uint32_t kMetaBounceMask = 0xFFu;
 constexpr uint32_t kMetaPrevNee = 1u << 8;      // the previous vertex used NEE (MIS applies)
 constexpr uint32_t kMetaStopAfter = 1u << 9;    // Russian roulette ended the path after this hit
+constexpr uint32_t kMetaGuideRec = 1u << 10;    // gf0/gf1 hold a guided vertex awaiting its training sample
 constexpr uint32_t kTargetFinal = 0x80000000u;
 
 // Launchers implemented in pg_trace.cu (FMA-enabled traversal kernels).
 void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4* ray_o,
                    const float4* ray_d, uint2* hits, int grid, int block, cudaStream_t st, bool count);
 void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
-                   float4* rad_next, double* film, int grid, int block, cudaStream_t st, bool count);
+                   float4* rad_next, double* film, int grid, int block, cudaStream_t st, bool count,
+                   float4* train_dirw = nullptr);
 
 // A scene resident on the GPU together with its render buffers.
 class RenderScene
@@ -177,13 +214,26 @@ public:
 	unsigned long long last_shadow_rays() const { return m_last_shadow; }
 	unsigned long long last_iterations() const { return m_last_iterations; }
 	// Per-kernel device milliseconds of the last timing-mode render: prepare, regen, extend,
-	// shade, shadow.
+	// shade, shadow, guiding inference (query + network), guiding training.
 	const double* last_kernel_ms() const { return m_kernel_ms; }
 	// Nodes / triangles visited by closest-hit and any-hit queries in the last counting render.
 	const unsigned long long* last_counts() const { return m_last_counts; }
 
+	// Learned guiding for subsequent renders; the network is created (He-initialised, fixed seed)
+	// on first use and keeps its training state until reset_guiding().
+	void set_guiding(const GuideParams& g) { m_guide_params = g; }
+	const GuideParams& guiding() const { return m_guide_params; }
+	void reset_guiding();
+	// Mean training loss over the training steps of the last guided render, and its number of
+	// guided vertices.
+	float last_guide_loss() const { return m_last_guide_loss; }
+	unsigned long long last_guided_vertices() const { return m_last_guided; }
+	// The FP32 network parameters (kNumParams) to the host.
+	void guide_params(float* out) const;
+
 private:
 	void ensure_capacity(uint32_t capacity);
+	void ensure_guiding(uint32_t capacity);
 
 	std::unique_ptr<Geometry> m_geometry;
 	DeviceBuffer<Material>    m_materials;
@@ -199,9 +249,27 @@ private:
 	DeviceBuffer<float4>   m_so, m_sd, m_sc;
 	DeviceBuffer<RenderCounters> m_counters;
 
+	// learned guiding
+	GuideParams m_guide_params;
+	uint32_t m_guide_capacity = 0;
+	bool m_guide_ready = false;
+	float m_bound_lo[3] = {0, 0, 0}, m_bound_rcp[3] = {1, 1, 1};
+	DeviceBuffer<float4>   m_gf0[2], m_gf1[2];
+	DeviceBuffer<float2>   m_st;
+	DeviceBuffer<uint32_t> m_gmap;
+	DeviceBuffer<float>    m_gfeat, m_graw;
+	DeviceBuffer<float>    m_tfeat, m_traw;
+	DeviceBuffer<float4>   m_tdirw;
+	DeviceBuffer<uint16_t> m_tacts;
+	DeviceBuffer<float>    m_gparams, m_gm, m_gv, m_ggrads, m_gscalars;
+	DeviceBuffer<unsigned char> m_gimage;
+	DeviceBuffer<uint32_t> m_gstep, m_gerr;
+	float m_last_guide_loss = 0.0f;
+	unsigned long long m_last_guided = 0;
+
 	unsigned long long m_last_rays = 0, m_last_shadow = 0, m_last_iterations = 0;
 	unsigned long long m_last_counts[4] = {0, 0, 0, 0};
-	double m_kernel_ms[5] = {0, 0, 0, 0, 0};
+	double m_kernel_ms[7] = {0, 0, 0, 0, 0, 0, 0};
 };
 
 }// end namespace pg

@@ -218,7 +218,8 @@ __global__ void __launch_bounds__(kTraceBlock)
 shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
               RenderCounters* __restrict__ counters,
               const float4* __restrict__ so, const float4* __restrict__ sd, const float4* __restrict__ sc,
-              float4* __restrict__ rad_next, double* __restrict__ film)
+              const float2* __restrict__ st, float4* __restrict__ rad_next, double* __restrict__ film,
+              float4* __restrict__ train_dirw)
 {
 	const uint32_t n = counters->n_shadow;
 	if(blockIdx.x == 0 && threadIdx.x == 0)
@@ -233,6 +234,16 @@ shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tr
 			if(occluded)
 			{
 				return;
+			}
+			if(train_dirw)
+			{
+				// guided renders: the unoccluded direct light joins the training sample it belongs to
+				const float2 tr = __ldg(st + i);
+				const uint32_t row = __float_as_uint(tr.x);
+				if(row != 0xFFFFFFFFu && tr.y != 0.0f)
+				{
+					atomicAdd(&train_dirw[row].w, tr.y);
+				}
 			}
 			const float4 c = __ldg(sc + i);
 			const uint32_t target = __float_as_uint(c.w);
@@ -283,17 +294,19 @@ void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4*
 }
 
 void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
-                   float4* rad_next, double* film, int, int, cudaStream_t st, bool count)
+                   float4* rad_next, double* film, int, int, cudaStream_t st, bool count, float4* train_dirw)
 {
 	if(count)
 	{
 		static const int grid = persistent_grid(shadow_kernel<true>);
-		shadow_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, rad_next, film);
+		shadow_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, q.t, rad_next,
+		                                                  film, train_dirw);
 	}
 	else
 	{
 		static const int grid = persistent_grid(shadow_kernel<false>);
-		shadow_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, rad_next, film);
+		shadow_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, q.t, rad_next,
+		                                                   film, train_dirw);
 	}
 	PG_CUDA_CHECK(cudaGetLastError());
 }

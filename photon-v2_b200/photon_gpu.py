@@ -54,6 +54,10 @@ PGPU_SIGNATURES = [
       _f32p, _u64p, _u64p]),
     ("pgpu_scene_film", ctypes.c_int, [ctypes.c_uint64, _f32p, _dblp, _u64p]),
     ("pgpu_scene_clear", ctypes.c_int, [ctypes.c_uint64]),
+    ("pgpu_scene_set_guiding", ctypes.c_int,
+     [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_uint32]),
+    ("pgpu_scene_guide_reset", ctypes.c_int, [ctypes.c_uint64]),
+    ("pgpu_scene_guide_info", ctypes.c_int, [ctypes.c_uint64, _f32p, _u64p, _dblp, _f32p]),
     ("pgpu_sdl_cook", ctypes.c_int,
      [ctypes.c_char_p, ctypes.c_char_p, _u64p, _u32p, _u32p, _u32p, _f32p, _u32p, _u32p, _f32p, _f32p]),
 ]
@@ -269,6 +273,25 @@ class RenderScene:
     def clear(self):
         _check(load().pgpu_scene_clear(self.id))
 
+    def set_guiding(self, enabled=True, train=True, alpha=0.5, lr=1e-2, batch=16384):
+        _check(load().pgpu_scene_set_guiding(self.id, int(enabled), int(train), alpha, lr, batch))
+
+    def guide_reset(self):
+        _check(load().pgpu_scene_guide_reset(self.id))
+
+    def guide_info(self, with_params=False):
+        loss = ctypes.c_float()
+        guided = ctypes.c_uint64()
+        ms = np.zeros(7, np.float64)
+        params = np.empty(29480, np.float32) if with_params else None
+        _check(load().pgpu_scene_guide_info(self.id, ctypes.byref(loss), ctypes.byref(guided), _ptr(ms, ctypes.c_double),
+                                            _ptr(params, ctypes.c_float) if with_params else None))
+        keys = ["prepare_ms", "regen_ms", "extend_ms", "shade_ms", "shadow_ms", "guide_infer_ms", "guide_train_ms"]
+        out = {"loss": loss.value, "guided_vertices": guided.value, "kernel_ms": dict(zip(keys, ms.tolist()))}
+        if with_params:
+            out["params"] = params
+        return out
+
 
 # ----------------------------------------------------------------------------------------------
 # Photon C API (ph_c_core.h) declared on the same library.
@@ -322,6 +345,7 @@ PH_SIGNATURES = [
     ("phGpuGetErrors", ctypes.c_int, [ctypes.c_uint64, _charpp]),
     ("phGpuSetMaxRayBounces", None, [ctypes.c_uint64, ctypes.c_uint32]),
     ("phGpuSetSeed", None, [ctypes.c_uint64, ctypes.c_uint64]),
+    ("phGpuSetGuiding", None, [ctypes.c_uint64, ctypes.c_int]),
     ("phGpuClearFilm", None, [ctypes.c_uint64]),
     ("phGpuGetRenderInfo", None, [ctypes.c_uint64, _dblp, _u64p, _u64p, _u64p, _dblp]),
     ("phGpuGetLaunchCount", ctypes.c_uint64, [ctypes.c_uint64]),
@@ -377,6 +401,9 @@ class PhotonEngine:
 
     def set_max_bounces(self, n: int) -> None:
         load().phGpuSetMaxRayBounces(self.id, n)
+
+    def set_guiding(self, enabled: bool) -> None:
+        load().phGpuSetGuiding(self.id, 1 if enabled else 0)
 
     def set_seed(self, seed: int) -> None:
         load().phGpuSetSeed(self.id, seed)

@@ -242,6 +242,41 @@ def cornell_glossy(width: int = 64, height: int = 64, spp: int = 64, max_bounces
     return sc
 
 
+def slit_room(width: int = 1024, height: int = 1024, spp: int = 64, max_bounces: int = 10,
+              num_boxes: int = 166_667, seed: int = 3, estimator: str = "bneept") -> Scene:
+    """Learned-guiding workload: a 10 x 10 x 4 room filled with seeded random furniture boxes
+    (12 triangles each; 166,667 boxes = 2M triangles), lit only by a 1 x 1 quad light behind a
+    dividing wall that has a single 0.05-wide vertical slit. 70 % of the boxes are Lambertian,
+    30 % rough GGX glass (IOR 1.5, roughness 0.1). Almost all light enters the room through the
+    slit, so BSDF sampling rarely finds it: the case path guiding is for."""
+    rng = np.random.default_rng(seed)
+    # room shell, faces pointing inwards
+    shell = boxes_axis_aligned(np.array([[0.0, 0.0, 0.0]]), np.array([[10.0, 4.0, 10.0]]))[:, [0, 2, 1]]
+    # dividing wall at x = 8 (0.1 thick) with a slit z in [4.975, 5.025], full height
+    wall = boxes_axis_aligned(np.array([[7.95, 0.0, 0.0], [7.95, 0.0, 5.025]]),
+                              np.array([[8.05, 4.0, 4.975], [8.05, 4.0, 10.0]]))
+    # the light: 1 x 1 quad at x = 9.5 facing -x, towards the slit
+    light = quad((9.5, 1.5, 4.5), (9.5, 1.5, 5.5), (9.5, 2.5, 5.5), (9.5, 2.5, 4.5))
+    # furniture in the main part of the room (x < 7.9), standing on the floor or floating
+    k = int(num_boxes)
+    size = rng.uniform(0.02, 0.25, (k, 3)) * np.array([1.0, 1.6, 1.0])
+    lo = np.stack([rng.uniform(0.1, 7.8, k), np.where(rng.random(k) < 0.6, 0.0, rng.uniform(0.0, 3.5, k)),
+                   rng.uniform(0.1, 9.9, k)], 1)
+    hi = np.minimum(lo + size, np.array([7.9, 3.95, 9.95]))
+    boxes = boxes_axis_aligned(lo, hi).reshape(k, 12, 3, 3)
+    glass = rng.random(k) < 0.3
+    groups = [
+        MeshGroup(np.concatenate([shell, wall]).astype(np.float32), Material("matte", albedo=(0.7, 0.7, 0.7))),
+        MeshGroup(boxes[~glass].reshape(-1, 3, 3), Material("matte", albedo=(0.6, 0.55, 0.5))),
+        MeshGroup(boxes[glass].reshape(-1, 3, 3), Material("dielectric", roughness=0.1, ior_outer=1.0, ior_inner=1.5)),
+        MeshGroup(light.astype(np.float32), BLACK, radiance=(400.0, 400.0, 400.0)),
+    ]
+    groups = [g for g in groups if g.tris.shape[0] > 0]
+    return Scene("slit_room", width, height, spp, max_bounces, cam_pos=(0.6, 2.2, 0.6),
+                 cam_dir=(0.55, -0.15, 0.8), cam_up=(0.0, 1.0, 0.0), fov_deg=70.0, groups=groups,
+                 estimator=estimator)
+
+
 def ggx_sphere(level: int = 8, width: int = 1024, height: int = 1024, spp: int = 256,
                max_bounces: int = 10, num_groups: int = 64, seed: int = 1,
                with_env: bool = True, estimator: str = "bneept") -> Scene:
