@@ -171,6 +171,50 @@ def cpu_sample(scene: scenes.Scene, tmp: str, target_seconds: float = 12.0, repe
     return records
 
 
+def rel_mse(x: np.ndarray, ref: np.ndarray, eps: float = 1e-2) -> float:
+    """Mean over pixels and channels of (x - ref)^2 / (ref^2 + eps)."""
+    return float(np.mean((x.astype(np.float64) - ref) ** 2 / (ref.astype(np.float64) ** 2 + eps)))
+
+
+def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 4096, plain_spp: int = 64,
+                      warmup_renders: int = 4) -> dict:
+    """Equal-time comparison of guided and plain GPU BNEEPT on the slit-light room (2M triangles).
+
+    A plain render of `plain_spp` samples sets the time budget; the guided renderer, after
+    `warmup_renders` training renders of plain_spp / 2 samples, renders as many samples as fit in
+    the same device time (its per-sample cost measured on a calibration render). Both are scored by
+    relMSE against a `ref_spp` plain render. `relmse_ratio` < 1 means guiding wins at equal time;
+    the ratio also estimates (time for guided to reach the plain error) / (plain time)."""
+    import photon_gpu
+
+    scene = scenes.slit_room(res, res, 1, 10, num_boxes=num_boxes)
+    with photon_gpu.RenderScene(scene) as rs:
+        rs.render(ref_spp, max_bounces=10, seed=1)
+        ref = rs.film()[0]
+        rs.clear()
+        plain = rs.render(plain_spp, max_bounces=10, seed=2)
+        plain_img = rs.film()[0]
+        rs.set_guiding(True, True, 0.5, 3e-3, 16384)
+        for k in range(warmup_renders):
+            rs.clear()
+            calib = rs.render(max(1, plain_spp // 2), max_bounces=10, seed=100 + k)
+        ms_per_spp = calib["ms"] / max(1, plain_spp // 2)
+        guided_spp = max(1, int(plain["ms"] / ms_per_spp))
+        rs.clear()
+        guided = rs.render(guided_spp, max_bounces=10, seed=3)
+        guided_img = rs.film()[0]
+        info = rs.guide_info()
+    e_plain, e_guided = rel_mse(plain_img, ref), rel_mse(guided_img, ref)
+    return {
+        "workload": f"slit_room {res}x{res}, {scene.num_tris} triangles, depth 10",
+        "reference_spp": ref_spp,
+        "plain": {"spp": plain_spp, "ms": plain["ms"], "relmse": e_plain},
+        "guided": {"spp": guided_spp, "ms": guided["ms"], "relmse": e_guided,
+                   "warmup_spp": warmup_renders * max(1, plain_spp // 2), "train_loss": info["loss"]},
+        "relmse_ratio": e_guided / e_plain if e_plain > 0 else None,
+    }
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -356,6 +400,8 @@ def run_ours(args) -> None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as tmp:
             line["cpu_baseline"] = cpu_sample(scene, tmp, target_seconds=args.cpu_seconds)[-1]
+    if rank == 0 and world == 1 and not args.no_guided:
+        line["guided_equal_time"] = guided_equal_time()
     if rank == 0:
         print(json.dumps(line))
     if dist:
@@ -372,6 +418,7 @@ def main() -> None:
     ap.add_argument("--spp", type=int, default=0, help="override samples per pixel")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-guided", action="store_true", help="skip the guided-vs-plain equal-time comparison")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -147,6 +147,10 @@ PGPU_API int pgpu_scene_render(uint64_t id, uint32_t spp, uint32_t max_bounces, 
 /* Developed frame (host float32 [h][w][3], row 0 = bottom, the reference's frame layout), the raw
  * FP64 sums (host double [h][w][3]) and the samples per pixel accumulated; any may be NULL. */
 PGPU_API int pgpu_scene_film(uint64_t id, float* out_rgb, double* out_sum, uint64_t* out_spp);
+/* A render into a scratch film with every kernel bracketed by CUDA events: per-kernel device
+ * milliseconds (prepare, regen, extend, shade, shadow, guide inference, guide training). */
+PGPU_API int pgpu_scene_profile(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator,
+                       uint64_t seed, double* out_kernel_ms);
 PGPU_API int pgpu_scene_clear(uint64_t id);
 
 /* Learned path guiding for the scene's subsequent BNEEPT renders (no reference counterpart). At

@@ -31,6 +31,9 @@ constexpr int kLobes = 8;
 constexpr int kOut = kLobes * 5;          // 40
 constexpr int kOutPad = 48;               // MMA N must be a multiple of 16 at M = 128
 constexpr int kTile = 128;                // rows per tcgen05 tile (MMA M)
+// Decoded mixture row written for the renderer: per lobe (weight, mean xyz, kappa, weight x vMF
+// normalisation), so that the density is sum_j c_j exp(kappa_j (mu_j . w - 1)).
+constexpr int kMixFloats = kLobes * 6;
 
 constexpr int kOffW0 = 0;
 constexpr int kOffB0 = kOffW0 + kIn * kHidden;

@@ -51,7 +51,11 @@ constexpr int kBiasCount = kHiddenLayers * kHidden + kOutPad;
 constexpr int kImageBytes = kOffImgBias + kBiasCount * 4;   // 60,576
 
 // ---- activation buffers
-constexpr int kActInBytes = kTile * kIn * 2;        // 57,344: input, later hidden ping
+// The input layer is fed in two K halves (one-blob inputs 0-3, then 4-6) so that the A buffer is
+// 32 KB and two CTAs fit on an SM.
+constexpr int kInHalf0 = 4 * kBins;                 // 128 columns
+constexpr int kInHalf1 = kIn - kInHalf0;            //  96 columns
+constexpr int kActInBytes = kTile * kInHalf0 * 2;   // 32,768: input half, later hidden ping
 constexpr int kActHBytes = kTile * kHidden * 2;     // 16,384: hidden pong
 constexpr int kOffSmemImage = 0;
 constexpr int kOffSmemActIn = (kImageBytes + 1023) / 1024 * 1024;
@@ -174,10 +178,16 @@ __device__ __forceinline__ void store_row8(unsigned char* buf, uint32_t r, uint3
 
 // ---- the fused forward kernel
 
-__global__ void __launch_bounds__(kThreads, 1)
+__device__ __forceinline__ float fast_blob(float s, int bin)
+{
+	const float z = (s - (static_cast<float>(bin) + 0.5f) * (1.0f / kBins)) * kBins;
+	return __expf(-0.5f * z * z);
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
 mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restrict__ features,
                    uint32_t n_max, const uint32_t* __restrict__ d_n, float* __restrict__ out_raw,
-                   __nv_bfloat16* __restrict__ out_acts, uint32_t* __restrict__ error)
+                   float* __restrict__ out_mix, __nv_bfloat16* __restrict__ out_acts, uint32_t* __restrict__ error)
 {
 	const uint32_t n = d_n ? min(*d_n, n_max) : n_max;
 	extern __shared__ __align__(128) unsigned char smem[];
@@ -226,68 +236,94 @@ mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restr
 		const uint32_t row = tile * kTile + tid;
 		const bool valid = row < n;
 
-		// 1. one-blob encoding of this thread's query into the input buffer
 		float f[kInputs];
 		#pragma unroll
 		for(int i = 0; i < kInputs; ++i)
 		{
 			f[i] = valid ? __ldg(features + static_cast<size_t>(row) * 8 + i) : -1.0f;
 		}
-		#pragma unroll
-		for(int i = 0; i < kInputs; ++i)
-		{
-			#pragma unroll
-			for(int c = 0; c < kBins / 8; ++c)
-			{
-				float v[8];
-				#pragma unroll
-				for(int j = 0; j < 8; ++j)
-				{
-					v[j] = valid ? one_blob(f[i], c * 8 + j) : 0.0f;
-				}
-				store_row8(act_in, tid, static_cast<uint32_t>(i * kBins + c * 8), v);
-			}
-		}
-		fence_async_smem();
-		fence_before_sync();
-		__syncthreads();
 
-		// 2./3. five layers: input -> H1 (act_h) -> H2 (act_in) -> H3 (act_h) -> H4 (act_in) -> out
-		#pragma unroll 1
-		for(int layer = 0; layer < 5; ++layer)
+		// One MMA chain (k_steps x K = 16) from A buffer a_buf against weights w_base starting at
+		// global K-step ks0, committed to the mbarrier; every thread then waits for it.
+		auto run_mma = [&](const unsigned char* a_buf, uint32_t k_steps, uint32_t w_base, uint32_t n_dim,
+		                   uint32_t ks0, bool accumulate) -> bool
 		{
-			const bool last = layer == 4;
-			const uint32_t k_dim = layer == 0 ? kIn : kHidden;
-			const uint32_t n_dim = last ? kOutPad : kHidden;
-			const unsigned char* a_buf = (layer & 1) ? act_h : act_in;
-			unsigned char* o_buf = (layer & 1) ? act_in : act_h;
 			if(tid == 0)
 			{
 				fence_after_sync();
 				const uint32_t a_base = smem_u32(a_buf);
 				const uint32_t idesc = instr_desc(kTile, n_dim);
-				for(uint32_t ks = 0; ks < k_dim / 16; ++ks)
+				for(uint32_t ks = 0; ks < k_steps; ++ks)
 				{
 					const uint64_t ad = smem_desc(a_base + ks * 2u * (kTile * 16u), kTile * 16u, 128u);
-					const uint64_t bd = smem_desc(w_addr[layer] + ks * 2u * (n_dim * 16u), n_dim * 16u, 128u);
-					mma_bf16(tmem, ad, bd, idesc, ks > 0 ? 1u : 0u);
+					const uint64_t bd = smem_desc(w_base + (ks0 + ks) * 2u * (n_dim * 16u), n_dim * 16u, 128u);
+					mma_bf16(tmem, ad, bd, idesc, (accumulate || ks > 0) ? 1u : 0u);
 				}
 				mma_commit(bar);
 			}
 			const bool ok = mbar_wait(bar, phase);
 			if(__syncthreads_or(ok ? 0 : 1))
 			{
-				// the tensor cores did not report back: stop, after one more bounded wait for the
-				// MMAs of this phase so that the accumulator is not freed under them
-				failed = true;
+				// the tensor cores did not report back: one more bounded wait for this phase so
+				// that the accumulator is not freed under running MMAs, then give up
 				if(!ok)
 				{
 					mbar_wait(bar, phase);
 				}
-				break;
+				return false;
 			}
 			phase ^= 1u;
 			fence_after_sync();
+			return true;
+		};
+
+		// 1. input layer in two K halves: one-blob encode, then accumulate into TMEM
+		bool tile_ok = true;
+		for(int half = 0; half < 2 && tile_ok; ++half)
+		{
+			const int i0 = half == 0 ? 0 : 4, i1 = half == 0 ? 4 : kInputs;
+			for(int i = i0; i < i1; ++i)
+			{
+				#pragma unroll
+				for(int c = 0; c < kBins / 8; ++c)
+				{
+					float v[8];
+					#pragma unroll
+					for(int j = 0; j < 8; ++j)
+					{
+						v[j] = valid ? fast_blob(f[i], c * 8 + j) : 0.0f;
+					}
+					store_row8(act_in, tid, static_cast<uint32_t>((i - i0) * kBins + c * 8), v);
+				}
+			}
+			fence_async_smem();
+			fence_before_sync();
+			__syncthreads();
+			const uint32_t k_steps = (half == 0 ? kInHalf0 : kInHalf1) / 16;
+			tile_ok = run_mma(act_in, k_steps, w_addr[0], kHidden, half == 0 ? 0u : kInHalf0 / 16, half == 1);
+		}
+		if(!tile_ok)
+		{
+			failed = true;
+			break;
+		}
+
+		// 2./3. H1 (act_h) -> H2 (act_in) -> H3 (act_h) -> H4 (act_in) -> out
+		#pragma unroll 1
+		for(int layer = 0; layer < 5; ++layer)
+		{
+			const bool last = layer == 4;
+			const uint32_t n_dim = last ? kOutPad : kHidden;
+			unsigned char* o_buf = (layer & 1) ? act_in : act_h;
+			if(layer > 0)
+			{
+				const unsigned char* a_buf = (layer & 1) ? act_h : act_in;
+				if(!run_mma(a_buf, kHidden / 16, w_addr[layer], n_dim, 0u, false))
+				{
+					failed = true;
+					break;
+				}
+			}
 
 			float acc[64];
 			#pragma unroll
@@ -327,12 +363,33 @@ mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restr
 			else if(valid)
 			{
 				const float* b = bias + kHiddenLayers * kHidden;
-				float4* dst = reinterpret_cast<float4*>(out_raw + static_cast<size_t>(row) * kOut);
 				#pragma unroll
-				for(int c = 0; c < kOut / 4; ++c)
+				for(int j = 0; j < kOut; ++j)
 				{
-					dst[c] = make_float4(acc[4 * c + 0] + b[4 * c + 0], acc[4 * c + 1] + b[4 * c + 1],
-					                     acc[4 * c + 2] + b[4 * c + 2], acc[4 * c + 3] + b[4 * c + 3]);
+					acc[j] += b[j];
+				}
+				if(out_raw)
+				{
+					float4* dst = reinterpret_cast<float4*>(out_raw + static_cast<size_t>(row) * kOut);
+					#pragma unroll
+					for(int c = 0; c < kOut / 4; ++c)
+					{
+						dst[c] = make_float4(acc[4 * c + 0], acc[4 * c + 1], acc[4 * c + 2], acc[4 * c + 3]);
+					}
+				}
+				if(out_mix)
+				{
+					const Mixture m = decode(acc);
+					float2* dst = reinterpret_cast<float2*>(out_mix + static_cast<size_t>(row) * kMixFloats);
+					#pragma unroll
+					for(int j = 0; j < kLobes; ++j)
+					{
+						const float k = m.kappa[j];
+						const float c = m.w[j] * k / (2.0f * kPi * (1.0f - expf(-2.0f * k)));
+						dst[3 * j + 0] = make_float2(m.w[j], m.mu[j].x);
+						dst[3 * j + 1] = make_float2(m.mu[j].y, m.mu[j].z);
+						dst[3 * j + 2] = make_float2(k, c);
+					}
 				}
 			}
 			fence_async_smem();
@@ -413,7 +470,8 @@ void pack_image(const float* d_params, unsigned char* d_image, cudaStream_t s)
 }
 
 void launch_forward(const unsigned char* d_image, const float* d_features, uint32_t n, float* d_out_raw,
-                    __nv_bfloat16* d_out_acts, uint32_t* d_error, cudaStream_t s, const uint32_t* d_n)
+                    __nv_bfloat16* d_out_acts, uint32_t* d_error, cudaStream_t s, const uint32_t* d_n,
+                    float* d_out_mix)
 {
 	if(n == 0)
 	{
@@ -426,8 +484,9 @@ void launch_forward(const unsigned char* d_image, const float* d_features, uint3
 	}();
 	(void)configured;
 	const uint32_t tiles = (n + kTile - 1) / kTile;
-	const uint32_t grid = std::min<uint32_t>(tiles, static_cast<uint32_t>(sm_count()));
-	mlp_forward_kernel<<<grid, kThreads, kSmemBytes, s>>>(d_image, d_features, n, d_n, d_out_raw, d_out_acts, d_error);
+	const uint32_t grid = std::min<uint32_t>(tiles, 2u * static_cast<uint32_t>(sm_count()));
+	mlp_forward_kernel<<<grid, kThreads, kSmemBytes, s>>>(d_image, d_features, n, d_n, d_out_raw, d_out_mix,
+	                                                     d_out_acts, d_error);
 	PG_CUDA_CHECK(cudaGetLastError());
 }
 

@@ -21,8 +21,10 @@ void pack_image(const float* d_params, unsigned char* d_image, cudaStream_t s);
 // outputs (decode() turns them into a mixture). d_out_acts (optional): [n][4][64] BF16 post-ReLU
 // hidden activations, for training. Errors are OR-ed into *d_error (PG_DEV_ERR_GUIDE_WAIT).
 // With d_n set, the kernel reads the row count from device memory (at most n): graph-safe.
+// d_out_raw may be null when d_out_mix ([n][kMixFloats], decoded mixture) is given.
 void launch_forward(const unsigned char* d_image, const float* d_features, uint32_t n, float* d_out_raw,
-                    __nv_bfloat16* d_out_acts, uint32_t* d_error, cudaStream_t s, const uint32_t* d_n = nullptr);
+                    __nv_bfloat16* d_out_acts, uint32_t* d_error, cudaStream_t s, const uint32_t* d_n = nullptr,
+                    float* d_out_mix = nullptr);
 
 // Loss and gradient of a batch (forward pass included): d_grads += d loss / d params, *d_loss +=
 // loss; d_total receives sum of weights. d_dirw: [n] (direction xyz, weight). d_raw: [n][40] and

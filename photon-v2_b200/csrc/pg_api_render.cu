@@ -183,6 +183,37 @@ int pgpu_scene_render(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t 
 	});
 }
 
+int pgpu_scene_profile(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator, uint64_t seed,
+                       double* out_kernel_ms)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		if(estimator > PG_EST_BVPT)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_profile: unknown estimator");
+		}
+		RenderParams p;
+		p.width = r->width;
+		p.height = r->height;
+		p.spp = spp;
+		p.max_bounces = max_bounces;
+		p.estimator = estimator;
+		p.seed = seed;
+		p.mode = PG_RENDER_TIMING;
+		DeviceBuffer<double> scratch(static_cast<std::size_t>(r->width) * r->height * 3);
+		PG_CUDA_CHECK(cudaMemsetAsync(scratch.get(), 0, scratch.bytes(), library_stream()));
+		r->scene->render(p, scratch.get());
+		if(out_kernel_ms)
+		{
+			for(int k = 0; k < 7; ++k)
+			{
+				out_kernel_ms[k] = r->scene->last_kernel_ms()[k];
+			}
+		}
+	});
+}
+
 int pgpu_scene_film(uint64_t id, float* out_rgb, double* out_sum, uint64_t* out_spp)
 {
 	return guarded([&]

@@ -214,30 +214,34 @@ regen_kernel(const RenderCounters* __restrict__ c, Camera cam, uint64_t seed, ui
 // ---------------------------------------------------------------------------------------------
 // Learned guiding at Lambertian vertices.
 
-__device__ __forceinline__ void load_raw(const float* __restrict__ raw, float* r)
+// Mixture density at unit direction w of a decoded network row (per lobe: weight, mean xyz,
+// kappa, weight x normalisation): sum_j c_j exp(kappa_j (mu_j . w - 1)).
+__device__ __noinline__ float guide_pdf(const float* __restrict__ mix, V3 w)
 {
-	const float4* q = reinterpret_cast<const float4*>(raw);
+	const float2* q = reinterpret_cast<const float2*>(mix);
+	float p = 0.0f;
 	#pragma unroll
-	for(int i = 0; i < guide::kOut / 4; ++i)
+	for(int j = 0; j < guide::kLobes; ++j)
 	{
-		const float4 v = __ldg(q + i);
-		r[4 * i + 0] = v.x; r[4 * i + 1] = v.y; r[4 * i + 2] = v.z; r[4 * i + 3] = v.w;
+		const float2 a = __ldg(q + 3 * j), b = __ldg(q + 3 * j + 1), c = __ldg(q + 3 * j + 2);
+		p += c.y * expf(c.x * (a.y * w.x + b.x * w.y + b.y * w.z - 1.0f));
 	}
+	return p;
 }
 
-// Mixture density of network row `raw` at unit direction w.
-__device__ __noinline__ float guide_pdf(const float* __restrict__ raw, V3 w)
+__device__ __noinline__ V3 guide_sample(const float* __restrict__ mix, float u0, float u1, float u2)
 {
-	float r[guide::kOut];
-	load_raw(raw, r);
-	return guide::mixture_pdf(guide::decode(r), w);
-}
-
-__device__ __noinline__ V3 guide_sample(const float* __restrict__ raw, float u0, float u1, float u2)
-{
-	float r[guide::kOut];
-	load_raw(raw, r);
-	return guide::mixture_sample(guide::decode(r), u0, u1, u2);
+	const float2* q = reinterpret_cast<const float2*>(mix);
+	guide::Mixture m;
+	#pragma unroll
+	for(int j = 0; j < guide::kLobes; ++j)
+	{
+		const float2 a = __ldg(q + 3 * j), b = __ldg(q + 3 * j + 1), c = __ldg(q + 3 * j + 2);
+		m.w[j] = a.x;
+		m.mu[j] = v3(a.y, b.x, b.y);
+		m.kappa[j] = c.x;
+	}
+	return guide::mixture_sample(m, u0, u1, u2);
 }
 
 __device__ __forceinline__ bool guidable(const Material& m)
@@ -481,7 +485,7 @@ shade_kernel(ShadeArgs a)
 		float sh_train = 0.0f;   // unweighted direct-light estimate (luminance) for the training sample
 		const uint32_t grow = GUIDED ? a.guide.map[i] : 0xFFFFFFFFu;
 		const bool guided = GUIDED && grow != 0xFFFFFFFFu;
-		const float* graw = guided ? a.guide.raw + static_cast<size_t>(grow) * guide::kOut : nullptr;
+		const float* graw = guided ? a.guide.raw + static_cast<size_t>(grow) * guide::kMixFloats : nullptr;
 		const float alpha = a.guide.alpha;
 		// Every material here is non-delta, so NEE applies at every vertex of BNEEPT
 		// (TDirectLightEstimator::isNeeSamplable); a black Lambertian surface can gain nothing
@@ -917,7 +921,7 @@ void RenderScene::ensure_guiding(uint32_t capacity)
 		m_st.resize(capacity);
 		m_gmap.resize(capacity);
 		m_gfeat.resize(static_cast<std::size_t>(capacity) * 8);
-		m_graw.resize(static_cast<std::size_t>(capacity) * guide::kOut);
+		m_graw.resize(static_cast<std::size_t>(capacity) * guide::kMixFloats);
 		m_guide_capacity = capacity;
 	}
 	const uint32_t batch = std::max<uint32_t>(m_guide_params.batch, guide::kTile);
@@ -1077,8 +1081,8 @@ float RenderScene::render(const RenderParams& params, double* film)
 			// network inputs of this iteration's guidable vertices, then the tensor-core forward pass
 			guide_query_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, cur, m_hits.get(), gargs, params.max_bounces);
 			PG_CUDA_CHECK(cudaGetLastError());
-			guide::launch_forward(m_gimage.get(), m_gfeat.get(), capacity, m_graw.get(), nullptr, m_gerr.get(), st,
-			                      &d_counters->n_guided);
+			guide::launch_forward(m_gimage.get(), m_gfeat.get(), capacity, nullptr, nullptr, m_gerr.get(), st,
+			                      &d_counters->n_guided, m_graw.get());
 		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[4], st)); }
 		ShadeArgs sa{m_dev, cur, nxt, m_hits.get(), sq, m_counters.get(), film, params.seed, first_global,

@@ -175,7 +175,7 @@ struct GuideArgs
 {
 	uint32_t*       map = nullptr;        // queue entry -> network row, 0xFFFFFFFF = not guided
 	float*          feat = nullptr;       // [capacity][8] network input rows
-	const float*    raw = nullptr;        // [capacity][40] network outputs
+	const float*    raw = nullptr;        // [capacity][48] decoded mixtures (guide::kMixFloats per row)
 	float*          train_feat = nullptr; // [batch][8]: features 0-6, |cos| / pdf
 	float4*         train_dirw = nullptr; // [batch]: direction, weight
 	uint32_t        train_cap = 0;        // 0: no training samples recorded

@@ -54,6 +54,8 @@ PGPU_SIGNATURES = [
       _f32p, _u64p, _u64p]),
     ("pgpu_scene_film", ctypes.c_int, [ctypes.c_uint64, _f32p, _dblp, _u64p]),
     ("pgpu_scene_clear", ctypes.c_int, [ctypes.c_uint64]),
+    ("pgpu_scene_profile", ctypes.c_int,
+     [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _dblp]),
     ("pgpu_scene_set_guiding", ctypes.c_int,
      [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_uint32]),
     ("pgpu_scene_guide_reset", ctypes.c_int, [ctypes.c_uint64]),
@@ -272,6 +274,13 @@ class RenderScene:
 
     def clear(self):
         _check(load().pgpu_scene_clear(self.id))
+
+    def profile(self, spp, max_bounces=10000, estimator=BNEEPT, seed=42):
+        """Per-kernel device ms of a timed render into a scratch film."""
+        ms = np.zeros(7, np.float64)
+        _check(load().pgpu_scene_profile(self.id, spp, max_bounces, estimator, seed, _ptr(ms, ctypes.c_double)))
+        keys = ["prepare_ms", "regen_ms", "extend_ms", "shade_ms", "shadow_ms", "guide_infer_ms", "guide_train_ms"]
+        return dict(zip(keys, ms.tolist()))
 
     def set_guiding(self, enabled=True, train=True, alpha=0.5, lr=1e-2, batch=16384):
         _check(load().pgpu_scene_set_guiding(self.id, int(enabled), int(train), alpha, lr, batch))
