@@ -258,10 +258,15 @@ def slit_room(width: int = 1024, height: int = 1024, spp: int = 64, max_bounces:
     # the light: 1 x 1 quad at x = 9.5 facing -x, towards the slit
     light = quad((9.5, 1.5, 4.5), (9.5, 1.5, 5.5), (9.5, 2.5, 5.5), (9.5, 2.5, 4.5))
     # furniture in the main part of the room (x < 7.9), standing on the floor or floating
+    # box sizes shrink with the count so that the filled volume stays ~2 % of the room; the corner
+    # around the camera is kept clear
     k = int(num_boxes)
-    size = rng.uniform(0.02, 0.25, (k, 3)) * np.array([1.0, 1.6, 1.0])
+    largest = float(np.clip(0.25 * (2000.0 / max(k, 1)) ** (1.0 / 3.0), 0.04, 0.25))
+    size = rng.uniform(0.08 * largest, largest, (k, 3)) * np.array([1.0, 1.6, 1.0])
     lo = np.stack([rng.uniform(0.1, 7.8, k), np.where(rng.random(k) < 0.6, 0.0, rng.uniform(0.0, 3.5, k)),
                    rng.uniform(0.1, 9.9, k)], 1)
+    near_camera = (lo[:, 0] < 1.6) & (lo[:, 2] < 1.6)
+    lo[near_camera, 0] += 1.6
     hi = np.minimum(lo + size, np.array([7.9, 3.95, 9.95]))
     boxes = boxes_axis_aligned(lo, hi).reshape(k, 12, 3, 3)
     glass = rng.random(k) < 0.3
