@@ -112,6 +112,12 @@ extern PH_API void phGpuSetSeed(PhUInt64 engineId, PhUInt64 seed);
  * Lambertian vertices (mixed with BSDF sampling by one-sample MIS, so results stay unbiased) and
  * is trained online on the render's own radiance samples. Off by default. */
 extern PH_API void phGpuSetGuiding(PhUInt64 engineId, PhBool enabled);
+/* Surface refinement of rays leaving surfaces, as the reference's EngineConfig.ini sets it
+ * (RefineMode / SelfIntersectDelta / NumIterativeSurfaceRefinements, which phInit also reads from
+ * ./Config/EngineConfig.ini when the file exists): mode 0 manual, 1 empirical, 2 iterative
+ * (the default). Invalid values are ignored. */
+extern PH_API void phGpuSetSurfaceRefine(PhUInt64 engineId, PhUInt32 mode, PhFloat32 selfIntersectDelta,
+                                         PhUInt32 numIterations);
 /* Clears the film; the next phRender starts a fresh image. */
 extern PH_API void phGpuClearFilm(PhUInt64 engineId);
 /* Device milliseconds, paths, closest-hit rays and shadow rays of the last phRender, and the

@@ -592,7 +592,9 @@ Offset offset_from(const Surface& x, const Tri& tri, Vec dir)
 	const Vec od = dot(x.ng, dir) > 0 ? x.ng : -x.ng;
 	const Vec ed = unit(dir);
 	const float ec = std::min(std::max(dot(ed, od), 0.0f), 1.0f);
-	float mx = len(x.pos) * 5e-8f + std::numeric_limits<float>::min(), mn = 0;
+	// HitDetail stores the triangle's error factors (5e-8, 2.5e-5) as powers of two, 2^-24 and 2^-15
+	// (Core/HitDetail.h:185-200)
+	float mx = len(x.pos) * 5.9604644775390625e-8f + std::numeric_limits<float>::min(), mn = 0;
 	for(int it = 0; it < 64; ++it)
 	{
 		float t;
@@ -615,7 +617,7 @@ Offset offset_from(const Surface& x, const Tri& tri, Vec dir)
 Offset mutual_offset(const Surface& x, const Tri& tri, Vec pos2, const Tri& tri2)
 {
 	const Offset r = offset_from(x, tri, pos2 - x.pos);
-	const float init = len(pos2) * (5e-8f * 5e2f) + std::numeric_limits<float>::min();
+	const float init = len(pos2) * 3.0517578125e-5f + std::numeric_limits<float>::min();
 	const Vec origin = x.pos + r.offset;
 	const float dist = len(origin - pos2);
 	float mx = init, mn = 0;

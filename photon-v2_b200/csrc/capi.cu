@@ -55,6 +55,8 @@ PhBool phInit(void)
 	{
 		require_device();
 		library_stream();
+		// the reference's engine settings file, when present (it is not created here)
+		load_engine_settings("./Config/EngineConfig.ini", engine_settings());
 		return PH_TRUE;
 	}
 	catch(const std::exception& e)
@@ -440,6 +442,17 @@ void phGpuSetSeed(PhUInt64 engineId, PhUInt64 seed)
 	if(auto e = engines().get(engineId))
 	{
 		e->engine.set_seed(seed);
+	}
+}
+
+void phGpuSetSurfaceRefine(PhUInt64 engineId, PhUInt32 mode, PhFloat32 selfIntersectDelta, PhUInt32 numIterations)
+{
+	if(auto e = engines().get(engineId))
+	{
+		if(mode <= 2u && selfIntersectDelta >= 0.0f && numIterations >= 1u)
+		{
+			e->engine.set_refine(mode, selfIntersectDelta, numIterations);
+		}
 	}
 }
 

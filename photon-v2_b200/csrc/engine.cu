@@ -774,6 +774,9 @@ void Engine::render()
 			p.spp = n;
 			p.max_bounces = m_max_bounces;
 			p.estimator = m_estimator;
+			p.refine_mode = m_refine.refine_mode;
+			p.refine_delta = m_refine.refine_delta;
+			p.refine_iters = m_refine.refine_iters;
 			p.seed = m_seed;
 			p.first_sample = m_first_sample + m_render->samples;
 			const float ms = m_render->scene->render(p, m_render->film.get());
@@ -811,6 +814,9 @@ void Engine::profile(uint32_t mode, uint32_t spp, double out_stats[14])
 	p.spp = spp;
 	p.max_bounces = m_max_bounces;
 	p.estimator = m_estimator;
+	p.refine_mode = m_refine.refine_mode;
+	p.refine_delta = m_refine.refine_delta;
+	p.refine_iters = m_refine.refine_iters;
 	p.seed = m_seed + 0x9E3779B97F4A7C15ull;
 	p.mode = mode;
 	RenderScene& rs = *m_render->scene;
@@ -949,6 +955,59 @@ bool read_pfm(const std::string& path, HdrFrame& frame)
 		for(int c = 0; c < 3; ++c)
 		{
 			frame.rgb[3 * i + c] = data[i * channels + (channels == 3 ? c : 0)];
+		}
+	}
+	return true;
+}
+
+EngineSettings& engine_settings()
+{
+	static EngineSettings settings;
+	return settings;
+}
+
+bool load_engine_settings(const std::string& path, EngineSettings& out)
+{
+	std::ifstream in(path);
+	if(!in)
+	{
+		return false;
+	}
+	auto trim = [](const std::string& x)
+	{
+		const auto b = x.find_first_not_of(" \t\r");
+		const auto e = x.find_last_not_of(" \t\r");
+		return b == std::string::npos ? std::string() : x.substr(b, e - b + 1);
+	};
+	std::string line;
+	while(std::getline(in, line))
+	{
+		const auto eq = line.find('=');
+		if(eq == std::string::npos)
+		{
+			continue;
+		}
+		const std::string key = trim(line.substr(0, eq)), value = trim(line.substr(eq + 1));
+		try
+		{
+			if(key == "RefineMode")
+			{
+				if(value == "manual") { out.refine_mode = 0; }
+				else if(value == "empirical") { out.refine_mode = 1; }
+				else if(value == "iterative") { out.refine_mode = 2; }
+			}
+			else if(key == "SelfIntersectDelta")
+			{
+				out.refine_delta = std::stof(value);
+			}
+			else if(key == "NumIterativeSurfaceRefinements")
+			{
+				out.refine_iters = std::max<uint32_t>(1u, static_cast<uint32_t>(std::stoul(value)));
+			}
+		}
+		catch(const std::exception&)
+		{
+			// a malformed number keeps the previous value, as an absent key would
 		}
 	}
 	return true;

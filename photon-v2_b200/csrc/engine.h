@@ -39,6 +39,22 @@ struct RenderInfo
 	uint64_t num_triangles = 0;
 };
 
+// The reference engine's global settings read at phInit from ./Config/EngineConfig.ini
+// (EngineInitSettings::loadStandardConfig / load, Engine/Source/EngineInitSettings.cpp:13-72):
+// the surface refiner's mode, self-intersection delta and number of bisection refinements.
+// Engines created afterwards start from these values.
+struct EngineSettings
+{
+	uint32_t refine_mode = 2;     // 0 manual, 1 empirical, 2 iterative (the reference default)
+	float    refine_delta = 2e-4f;
+	uint32_t refine_iters = 1;
+};
+
+EngineSettings& engine_settings();
+// Parses an EngineConfig.ini (keys RefineMode, SelfIntersectDelta, NumIterativeSurfaceRefinements);
+// returns false when the file cannot be read. Other keys are ignored.
+bool load_engine_settings(const std::string& path, EngineSettings& out);
+
 class Engine
 {
 public:
@@ -76,6 +92,7 @@ public:
 	void set_sample_offset(uint64_t first_sample) { m_first_sample = first_sample; }
 	// Learned path guiding of the BNEEPT estimator (network trained online during rendering).
 	void set_guiding(bool enabled) { m_guiding = enabled; }
+	void set_refine(uint32_t mode, float delta, uint32_t iters) { m_refine = EngineSettings{mode, delta, iters}; }
 	const RenderInfo& info() const { return m_info; }
 	uint64_t launch_count() const { return m_launches; }
 	// Renders into a scratch film with the given render mode and returns the statistics of
@@ -107,6 +124,7 @@ private:
 	uint64_t m_seed = 42;
 	uint64_t m_first_sample = 0;
 	bool m_guiding = false;
+	EngineSettings m_refine = engine_settings();
 
 	std::shared_ptr<RenderObject> m_render;
 	uint32_t m_width = 0, m_height = 0;

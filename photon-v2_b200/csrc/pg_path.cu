@@ -314,6 +314,7 @@ struct ShadeArgs
 	uint32_t      estimator;
 	uint32_t      width_height;
 	GuideArgs     guide;
+	RefineSettings refine;
 };
 
 __device__ __forceinline__ float4 cur_gf0(const ShadeArgs& a, uint32_t i) { return a.cur.gf0[i]; }
@@ -480,7 +481,7 @@ shade_kernel(ShadeArgs a)
 		//      TDirectLightEstimator.ipp:71-102; BNEEPTEstimator.cpp:103-149)
 		bool has_shadow = false;
 		V3 sh_o{}, sh_d{};
-		float sh_tmax = 0.0f;
+		float sh_tmin = 0.0f, sh_tmax = 0.0f;
 		RGB sh_c{};
 		float sh_train = 0.0f;   // unweighted direct-light estimate (luminance) for the training sample
 		const uint32_t grow = GUIDED ? a.guide.map[i] : 0xFFFFFFFFu;
@@ -515,10 +516,11 @@ shade_kernel(ShadeArgs a)
 				le = emitter_radiance(e);
 				if(sidedness_agreed(frame, to_light))
 				{
-					const OffsetResult off = iterative_offset(pos, ng, tri, to_light);
-					sh_o = pos + off.offset;
-					sh_d = off.unit_dir;
-					sh_tmax = kFloatMax;
+					const EscapeRay er = escape(a.refine, pos, ng, tri, to_light);
+					sh_o = er.origin;
+					sh_d = er.unit_dir;
+					sh_tmin = er.min_t;
+					sh_tmax = er.max_distance;
 					ok = true;
 				}
 			}
@@ -540,12 +542,13 @@ shade_kernel(ShadeArgs a)
 					const V3 target_to_emit = xe - pos;
 					if(pdf_w > 0.0f && isfinite(pdf_w) && sidedness_agreed(frame, target_to_emit))
 					{
-						const OffsetResult off = iterative_mutual_offset(pos, ng, tri, xe, lt);
-						if(off.max_distance > 0.0f && isfinite(off.max_distance))
+						const EscapeRay er = try_escape(a.refine, pos, ng, tri, xe, ne, lt);
+						if(er.ok)
 						{
-							sh_o = pos + off.offset;
-							sh_d = off.unit_dir;
-							sh_tmax = off.max_distance;
+							sh_o = er.origin;
+							sh_d = er.unit_dir;
+							sh_tmin = er.min_t;
+							sh_tmax = er.max_distance;
 							to_light = target_to_emit;
 							ok = true;
 						}
@@ -663,14 +666,14 @@ shade_kernel(ShadeArgs a)
 		if(continues)
 		{
 			slot = alloc_slot(&a.counters->n_next);
-			const OffsetResult off = iterative_offset(pos, ng, tri, bs.l);
-			const V3 o = pos + off.offset;
+			const EscapeRay off = escape(a.refine, pos, ng, tri, bs.l);
+			const V3 o = off.origin;
 			a.next.path[slot] = p;
 			a.next.meta[slot] = next_meta;
 			a.next.thr[slot] = make_float4(next_thr_emit.r, next_thr_emit.g, next_thr_emit.b, next_cont);
 			a.next.rad[slot] = make_float4(radiance.r, radiance.g, radiance.b, next_pdf);
 			a.next.prev[slot] = make_float4(pos.x, pos.y, pos.z, rr_scale);
-			a.next.ray_o[slot] = make_float4(o.x, o.y, o.z, 0.0f);
+			a.next.ray_o[slot] = make_float4(o.x, o.y, o.z, off.min_t);
 			a.next.ray_d[slot] = make_float4(off.unit_dir.x, off.unit_dir.y, off.unit_dir.z, kFloatMax);
 			if(GUIDED && (next_meta & kMetaGuideRec))
 			{
@@ -689,7 +692,7 @@ shade_kernel(ShadeArgs a)
 		{
 			const uint32_t k = alloc_slot(&a.counters->n_shadow);
 			const uint32_t target = continues ? slot : (kTargetFinal | pixel);
-			a.shadow.o[k] = make_float4(sh_o.x, sh_o.y, sh_o.z, 0.0f);
+			a.shadow.o[k] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_tmin);
 			a.shadow.d[k] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
 			a.shadow.c[k] = make_float4(sh_c.r, sh_c.g, sh_c.b, __uint_as_float(target));
 			if(GUIDED && a.shadow.t)
@@ -1088,6 +1091,9 @@ float RenderScene::render(const RenderParams& params, double* film)
 		ShadeArgs sa{m_dev, cur, nxt, m_hits.get(), sq, m_counters.get(), film, params.seed, first_global,
 		             params.max_bounces, params.estimator, static_cast<uint32_t>(wh)};
 		sa.guide = gargs;
+		sa.refine.mode = params.refine_mode;
+		sa.refine.delta = params.refine_delta;
+		sa.refine.iters = static_cast<int>(params.refine_iters);
 		if(guided)
 		{
 			shade_kernel<true><<<grid, kShadeBlock, 0, st>>>(sa);

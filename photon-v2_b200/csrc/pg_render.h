@@ -76,6 +76,11 @@ struct RenderParams
 	uint64_t first_sample = 0;          // sample index offset (resume / replicas)
 	uint32_t capacity = 1u << 21;       // path slots in flight
 	uint32_t mode = PG_RENDER_GRAPH;
+	// SurfaceHitRefinery settings (the reference's EngineInitSettings: RefineMode,
+	// SelfIntersectDelta, NumIterativeSurfaceRefinements): 0 manual, 1 empirical, 2 iterative.
+	uint32_t refine_mode = 2;
+	float    refine_delta = 2e-4f;
+	uint32_t refine_iters = 1;
 };
 
 // Learned path guiding (BNEEPT only). At Lambertian vertices the direction is drawn from the

@@ -25,6 +25,7 @@ struct RayTraits
 	float rdx, rdy, rdz;     // reciprocal direction for the slab test (zero components nudged)
 	float obx, oby, obz;     // origin * reciprocal direction
 	uint32_t oct;            // bit a set <=> direction component a is negative
+	float okx, oky, okz;     // origin permuted like the watertight test's axes
 };
 
 __device__ __forceinline__ float pick3(float a, float b, float c, int k)
@@ -67,6 +68,9 @@ __device__ __forceinline__ RayTraits make_ray_traits(float ox, float oy, float o
 	r.oby = oy * r.rdy;
 	r.obz = oz * r.rdz;
 	r.oct = (dx < 0.0f ? 1u : 0u) | (dy < 0.0f ? 2u : 0u) | (dz < 0.0f ? 4u : 0u);
+	r.okx = pick3(ox, oy, oz, r.kx);
+	r.oky = pick3(ox, oy, oz, r.ky);
+	r.okz = pick3(ox, oy, oz, r.kz);
 	return r;
 }
 
@@ -74,21 +78,23 @@ __device__ __forceinline__ RayTraits make_ray_traits(float ox, float oy, float o
 // (TWatertightTriangle.ipp:16-149) including operand order, the FP64 recomputation of zero edge
 // functions (:85-100) and the inclusive [minT, maxT] range in scaled form (:119-133). Every
 // FP32 operation is an explicitly rounded intrinsic so that no FMA contraction changes bits.
-__device__ __forceinline__ bool watertight_hit(
-	const RayTraits& r,
-	float ax, float ay, float az,
-	float bx, float by, float bz,
-	float cx, float cy, float cz,
+//
+// The core takes the vertices and the origin already permuted (component kx, ky, kz first); the
+// permutation commutes with the per-component subtraction, so permuting before or after it gives
+// the same bits. Callers that test one triangle from many origins along one direction (the
+// refinery) permute the triangle once.
+__device__ __forceinline__ bool watertight_core(
+	float okx, float oky, float okz, float sx, float sy, float sz,
+	float pax, float pay, float paz,
+	float pbx, float pby, float pbz,
+	float pcx, float pcy, float pcz,
 	float min_t, float max_t,
 	float* out_t, float* out_b0, float* out_b1, float* out_b2)
 {
-	const float Ax = __fsub_rn(ax, r.ox), Ay = __fsub_rn(ay, r.oy), Az = __fsub_rn(az, r.oz);
-	const float Bx = __fsub_rn(bx, r.ox), By = __fsub_rn(by, r.oy), Bz = __fsub_rn(bz, r.oz);
-	const float Cx = __fsub_rn(cx, r.ox), Cy = __fsub_rn(cy, r.oy), Cz = __fsub_rn(cz, r.oz);
-
-	float atx = pick3(Ax, Ay, Az, r.kx), aty = pick3(Ax, Ay, Az, r.ky), atz = pick3(Ax, Ay, Az, r.kz);
-	float btx = pick3(Bx, By, Bz, r.kx), bty = pick3(Bx, By, Bz, r.ky), btz = pick3(Bx, By, Bz, r.kz);
-	float ctx = pick3(Cx, Cy, Cz, r.kx), cty = pick3(Cx, Cy, Cz, r.ky), ctz = pick3(Cx, Cy, Cz, r.kz);
+	float atx = __fsub_rn(pax, okx), aty = __fsub_rn(pay, oky), atz = __fsub_rn(paz, okz);
+	float btx = __fsub_rn(pbx, okx), bty = __fsub_rn(pby, oky), btz = __fsub_rn(pbz, okz);
+	float ctx = __fsub_rn(pcx, okx), cty = __fsub_rn(pcy, oky), ctz = __fsub_rn(pcz, okz);
+	struct { float sx, sy, sz; } r{sx, sy, sz};
 
 	atx = __fadd_rn(atx, __fmul_rn(r.sx, atz));
 	aty = __fadd_rn(aty, __fmul_rn(r.sy, atz));
@@ -147,6 +153,21 @@ __device__ __forceinline__ bool watertight_hit(
 	*out_b2 = __fmul_rn(ec, rcp_det);
 	*out_t  = __fmul_rn(t_scaled, rcp_det);
 	return true;
+}
+
+__device__ __forceinline__ bool watertight_hit(
+	const RayTraits& r,
+	float ax, float ay, float az,
+	float bx, float by, float bz,
+	float cx, float cy, float cz,
+	float min_t, float max_t,
+	float* out_t, float* out_b0, float* out_b1, float* out_b2)
+{
+	return watertight_core(r.okx, r.oky, r.okz, r.sx, r.sy, r.sz,
+	                       pick3(ax, ay, az, r.kx), pick3(ax, ay, az, r.ky), pick3(ax, ay, az, r.kz),
+	                       pick3(bx, by, bz, r.kx), pick3(bx, by, bz, r.ky), pick3(bx, by, bz, r.kz),
+	                       pick3(cx, cy, cz, r.kx), pick3(cx, cy, cz, r.ky), pick3(cx, cy, cz, r.kz),
+	                       min_t, max_t, out_t, out_b0, out_b1, out_b2);
 }
 
 __device__ __forceinline__ bool watertight_hit_tri(

@@ -355,6 +355,7 @@ PH_SIGNATURES = [
     ("phGpuSetMaxRayBounces", None, [ctypes.c_uint64, ctypes.c_uint32]),
     ("phGpuSetSeed", None, [ctypes.c_uint64, ctypes.c_uint64]),
     ("phGpuSetGuiding", None, [ctypes.c_uint64, ctypes.c_int]),
+    ("phGpuSetSurfaceRefine", None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32]),
     ("phGpuClearFilm", None, [ctypes.c_uint64]),
     ("phGpuGetRenderInfo", None, [ctypes.c_uint64, _dblp, _u64p, _u64p, _u64p, _dblp]),
     ("phGpuGetLaunchCount", ctypes.c_uint64, [ctypes.c_uint64]),
@@ -413,6 +414,11 @@ class PhotonEngine:
 
     def set_guiding(self, enabled: bool) -> None:
         load().phGpuSetGuiding(self.id, 1 if enabled else 0)
+
+    def set_surface_refine(self, mode: str = "iterative", delta: float = 2e-4, iterations: int = 1) -> None:
+        """phGpuSetSurfaceRefine: the reference's RefineMode (manual / empirical / iterative)."""
+        m = {"manual": 0, "empirical": 1, "iterative": 2}[mode]
+        load().phGpuSetSurfaceRefine(self.id, m, delta, iterations)
 
     def set_seed(self, seed: int) -> None:
         load().phGpuSetSeed(self.id, seed)
