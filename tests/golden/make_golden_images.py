@@ -28,18 +28,26 @@ import scenes  # noqa: E402
 
 RENDER_TOOL = os.path.join(ROOT, "oracle", "_ref", "ph_ref_render")
 
-# name -> (scene factory, spp, max bounces)
+# name -> (scene factory, spp, max bounces[, the reference's RefineMode in its EngineConfig.ini])
 WORKLOADS = {
     "cornell_bneept": (lambda spp: scenes.cornell(64, 64, spp, 8, "bneept"), 8192, 8),
     "cornell_bvpt": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvpt"), 8192, 8),
     "cornell_glossy_bneept": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 8192, 8),
     "ggx_sphere_env_bneept": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
                                                             max_bounces=10), 4096, 10),
+    "cornell_glossy_bneept_empirical": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 8192, 8,
+                                        "empirical"),
+    "ggx_sphere_bneept_manual": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
+                                                               max_bounces=10), 4096, 10, "manual"),
 }
 
 
-def render(scene: scenes.Scene, max_bounces: int, threads: int) -> np.ndarray:
+def render(scene: scenes.Scene, max_bounces: int, threads: int, refine_mode: str = "iterative") -> np.ndarray:
     with tempfile.TemporaryDirectory() as tmp:
+        # the reference reads its surface refiner's mode from ./Config/EngineConfig.ini at phInit
+        os.makedirs(os.path.join(tmp, "Config"), exist_ok=True)
+        with open(os.path.join(tmp, "Config", "EngineConfig.ini"), "w") as f:
+            f.write(f"RefineMode={refine_mode}\nSelfIntersectDelta=2e-04\nNumIterativeSurfaceRefinements=1\n")
         p2 = os.path.join(tmp, "scene.p2")
         with open(p2, "w") as f:
             f.write(scenes.to_sdl(scene))
@@ -59,10 +67,10 @@ def main() -> None:
     path = os.path.join(HERE, "images.npz")
     only = sys.argv[1:]
     arrays = dict(np.load(path)) if only and os.path.exists(path) else {}
-    for name, (factory, spp, bounces) in WORKLOADS.items():
+    for name, (factory, spp, bounces, *mode) in WORKLOADS.items():
         if only and name not in only:
             continue
-        img = render(factory(spp), bounces, threads)
+        img = render(factory(spp), bounces, threads, *mode)
         arrays[name] = img
         arrays[name + "__spp"] = np.array(spp)
         arrays[name + "__bounces"] = np.array(bounces)

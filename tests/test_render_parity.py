@@ -4,7 +4,9 @@ Renders go through the Photon C API of this library (SDL text -> phLoadCommands 
 phRender -> phAquireFrameRaw), exactly as a reference user would drive it. References:
 
 * images.npz -- renders of the same SDL by the reference's own EqualSamplingRenderer +
-  BNEEPTEstimator / BVPTEstimator (tests/golden/make_golden_images.py, 64 x 64, 4096-8192 spp).
+  BNEEPTEstimator / BVPTEstimator (tests/golden/make_golden_images.py, 64 x 64, 4096-8192 spp),
+  in the reference's default iterative surface refinement and, for two scenes, in its empirical
+  and manual modes (the reference's EngineConfig.ini on its side, phGpuSetSurfaceRefine on ours).
   The bar is the north star's image tolerance: relMSE <= 1e-3, relMSE being the mean over pixels
   and channels of (x - ref)^2 / (ref^2 + 1e-2). Both images carry Monte Carlo noise, which the
   bound includes. BNEEPT images meet it at full resolution; BVPT (no light sampling, a small
@@ -39,6 +41,11 @@ WORKLOADS = {
     "cornell_glossy_bneept": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 16384),
     "ggx_sphere_env_bneept": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
                                                             max_bounces=10), 4096),
+    # the reference's other surface-refine modes (RefineMode in its EngineConfig.ini)
+    "cornell_glossy_bneept_empirical": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 16384,
+                                        "empirical"),
+    "ggx_sphere_bneept_manual": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
+                                                               max_bounces=10), 4096, "manual"),
 }
 
 
@@ -46,7 +53,7 @@ def rel_mse(x, ref, eps=1e-2):
     return float(np.mean((x.astype(np.float64) - ref) ** 2 / (ref.astype(np.float64) ** 2 + eps)))
 
 
-def render_via_c_api(scene, tmp_path, seed=1):
+def render_via_c_api(scene, tmp_path, seed=1, refine_mode="iterative"):
     import photon_gpu
 
     p2 = tmp_path / "scene.p2"
@@ -58,6 +65,7 @@ def render_via_c_api(scene, tmp_path, seed=1):
         assert eng.load_file(str(p2)), eng.errors()
         eng.set_max_bounces(scene.max_bounces)
         eng.set_seed(seed)
+        eng.set_surface_refine(refine_mode)
         eng.update()
         eng.render()
         img = eng.frame()
@@ -78,10 +86,10 @@ def test_golden_images_present():
 def test_image_matches_reference(gpu_lib, tmp_path, name):
     d = np.load(IMAGES)
     ref = d[name]
-    factory, spp = WORKLOADS[name]
+    factory, spp, *mode = WORKLOADS[name]
     scene = factory(spp)
     assert scene.max_bounces == int(d[name + "__bounces"])
-    img, _ = render_via_c_api(scene, tmp_path)
+    img, _ = render_via_c_api(scene, tmp_path, refine_mode=mode[0] if mode else "iterative")
     err = rel_mse(img, ref)
     block = lambda a: a.reshape(16, 4, 16, 4, 3).mean(axis=(1, 3))
     err_blocks = rel_mse(block(img), block(ref))
