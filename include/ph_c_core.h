@@ -112,6 +112,9 @@ extern PH_API void phGpuSetSeed(PhUInt64 engineId, PhUInt64 seed);
  * Lambertian vertices (mixed with BSDF sampling by one-sample MIS, so results stay unbiased) and
  * is trained online on the render's own radiance samples. Off by default. */
 extern PH_API void phGpuSetGuiding(PhUInt64 engineId, PhBool enabled);
+/* BVH builder of the next phUpdate: 0 host binned SAH (default), 1 on the GPU from Morton-ordered
+ * triangles (seconds faster on multi-million-triangle scenes, somewhat costlier to traverse). */
+extern PH_API void phGpuSetBvhBuilder(PhUInt64 engineId, PhUInt32 builder);
 /* Surface refinement of rays leaving surfaces, as the reference's EngineConfig.ini sets it
  * (RefineMode / SelfIntersectDelta / NumIterativeSurfaceRefinements, which phInit also reads from
  * ./Config/EngineConfig.ini when the file exists): mode 0 manual, 1 empirical, 2 iterative

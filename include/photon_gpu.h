@@ -39,6 +39,16 @@ PGPU_API int pgpu_device_count(void);
  * origin that will be traced (sizes the conservative box padding; 0 = scene bound only).
  */
 PGPU_API int pgpu_geometry_create(const float* tris, uint64_t num_tris, float max_origin_abs, uint64_t* out_id);
+/* As pgpu_geometry_create with a choice of builder: 0 = host binned SAH (the default above),
+ * 1 = on the GPU from Morton-ordered triangles (a radix tree collapsed to the same 8-wide layout;
+ * much faster to build on millions of triangles, somewhat costlier to traverse). Hits are the
+ * same either way: they depend only on the triangles. */
+PGPU_API int pgpu_geometry_create_ex(const float* tris, uint64_t num_tris, float max_origin_abs,
+                       uint32_t bvh_builder, uint64_t* out_id);
+/* Copies the built tree to the host: out_nodes [num_nodes] x 80-byte wide nodes, out_tris
+ * [num_tris] x 48-byte leaf triangles (either may be NULL to query the counts only). */
+PGPU_API int pgpu_geometry_export(uint64_t id, void* out_nodes, void* out_tris, uint64_t* out_num_nodes,
+                       uint64_t* out_num_tris);
 PGPU_API int pgpu_geometry_destroy(uint64_t id);
 /* num_nodes, num_tris, wide-tree depth, host build seconds. Any output may be NULL. */
 PGPU_API int pgpu_geometry_stats(uint64_t id, uint64_t* out_num_nodes, uint64_t* out_num_tris,
@@ -134,6 +144,11 @@ PGPU_API int pgpu_scene_create(const float* tris, const uint32_t* tri_material, 
                                uint64_t num_tris, const float* materials, uint32_t num_materials,
                                const float* emitters, uint32_t num_emitters, const float* camera,
                                uint64_t* out_id);
+/* As pgpu_scene_create with a choice of BVH builder (see pgpu_geometry_create_ex). */
+PGPU_API int pgpu_scene_create_ex(const float* tris, const uint32_t* tri_material, const uint32_t* tri_emitter,
+                       uint64_t num_tris, const float* materials, uint32_t num_materials,
+                       const float* emitters, uint32_t num_emitters, const float* camera,
+                       uint32_t bvh_builder, uint64_t* out_id);
 PGPU_API int pgpu_scene_destroy(uint64_t id);
 
 /* Renders spp samples per pixel (estimator 0 = BNEEPT, 1 = BVPT; max_bounces = the reference's

@@ -456,6 +456,17 @@ void phGpuSetSurfaceRefine(PhUInt64 engineId, PhUInt32 mode, PhFloat32 selfInter
 	}
 }
 
+void phGpuSetBvhBuilder(PhUInt64 engineId, PhUInt32 builder)
+{
+	if(auto e = engines().get(engineId))
+	{
+		if(builder <= 1u)
+		{
+			e->engine.set_bvh_builder(builder);
+		}
+	}
+}
+
 void phGpuSetGuiding(PhUInt64 engineId, PhBool enabled)
 {
 	if(auto e = engines().get(engineId))

@@ -249,6 +249,7 @@ void Engine::update()
 	{
 		SceneDesc desc;
 		cook(desc);
+		desc.bvh_builder = m_bvh_builder;
 		m_info.num_triangles = desc.tris.size() / 9;
 		m_render = make_render_object(std::move(desc));
 	}

@@ -93,6 +93,8 @@ public:
 	// Learned path guiding of the BNEEPT estimator (network trained online during rendering).
 	void set_guiding(bool enabled) { m_guiding = enabled; }
 	void set_refine(uint32_t mode, float delta, uint32_t iters) { m_refine = EngineSettings{mode, delta, iters}; }
+	// BVH builder used by the next update: 0 host binned SAH, 1 GPU Morton.
+	void set_bvh_builder(uint32_t builder) { m_bvh_builder = builder; }
 	const RenderInfo& info() const { return m_info; }
 	uint64_t launch_count() const { return m_launches; }
 	// Renders into a scratch film with the given render mode and returns the statistics of
@@ -125,6 +127,7 @@ private:
 	uint64_t m_first_sample = 0;
 	bool m_guiding = false;
 	EngineSettings m_refine = engine_settings();
+	uint32_t m_bvh_builder = 0;
 
 	std::shared_ptr<RenderObject> m_render;
 	uint32_t m_width = 0, m_height = 0;

@@ -80,8 +80,21 @@ int pgpu_scene_create(const float* tris, const uint32_t* tri_material, const uin
                       uint64_t num_tris, const float* materials, uint32_t num_materials,
                       const float* emitters, uint32_t num_emitters, const float* camera, uint64_t* out_id)
 {
+	return pgpu_scene_create_ex(tris, tri_material, tri_emitter, num_tris, materials, num_materials, emitters,
+	                            num_emitters, camera, PG_BVH_HOST_SAH, out_id);
+}
+
+int pgpu_scene_create_ex(const float* tris, const uint32_t* tri_material, const uint32_t* tri_emitter,
+                         uint64_t num_tris, const float* materials, uint32_t num_materials,
+                         const float* emitters, uint32_t num_emitters, const float* camera, uint32_t bvh_builder,
+                         uint64_t* out_id)
+{
 	return guarded([&]
 	{
+		if(bvh_builder > PG_BVH_GPU_MORTON)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create_ex: unknown BVH builder");
+		}
 		if(!tris || num_tris == 0 || !tri_material || !materials || num_materials == 0 || !camera || !out_id)
 		{
 			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create: missing input");
@@ -141,6 +154,7 @@ int pgpu_scene_create(const float* tris, const uint32_t* tri_material, const uin
 			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create: zero resolution");
 		}
 		d.camera = make_camera(camera, camera + 3, camera + 6, camera[9], w, h);
+		d.bvh_builder = bvh_builder;
 		*out_id = render_registry().add(make_render_object(std::move(d)));
 	});
 }

@@ -18,8 +18,16 @@ struct Geometry
 
 Registry<Geometry>& geometry_registry();
 
-// Builds the BVH on the host and uploads nodes and triangles on the library stream.
+// Builds the BVH on the host (binned SAH) and uploads nodes and triangles on the library stream.
 std::unique_ptr<Geometry> make_geometry(const BvhBuildInput& in);
+// Builds the same wide BVH layout on the device from Morton-ordered triangles (bvh_gpu.cu).
+std::unique_ptr<Geometry> make_geometry_gpu(const BvhBuildInput& in);
+
+enum BvhBuilder : uint32_t
+{
+	PG_BVH_HOST_SAH = 0,
+	PG_BVH_GPU_MORTON = 1,
+};
 
 // Launch helpers on a given stream (no synchronisation). d_rays: [n][8] float32;
 // d_hits: [n] x (uint32 leaf triangle or 0xFFFFFFFF, float32 t).

@@ -769,7 +769,7 @@ RenderScene::RenderScene(const SceneDesc& desc, float max_origin_abs)
 		throw Error(PG_ERR_SCENE, "scene has no triangles");
 	}
 	BvhBuildInput in{desc.tris.data(), desc.tri_material.data(), desc.tri_emitter.data(), n, max_origin_abs};
-	m_geometry = make_geometry(in);
+	m_geometry = desc.bvh_builder == PG_BVH_GPU_MORTON ? make_geometry_gpu(in) : make_geometry(in);
 
 	// scene bound, normalising the guiding network's position inputs
 	{

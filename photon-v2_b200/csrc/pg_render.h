@@ -113,6 +113,7 @@ struct SceneDesc
 	// times this area (LatLongEnvEmitter.cpp:36-68), which sets its share of NEE samples.
 	double env_area = 0.0;
 	Camera camera{};
+	uint32_t bvh_builder = 0;   // BvhBuilder: 0 host binned SAH, 1 GPU Morton
 };
 
 // Device view of a scene (all pointers are device memory).

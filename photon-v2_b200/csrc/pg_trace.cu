@@ -363,14 +363,45 @@ int pgpu_device_count(void)
 
 int pgpu_geometry_create(const float* tris, uint64_t num_tris, float max_origin_abs, uint64_t* out_id)
 {
+	return pgpu_geometry_create_ex(tris, num_tris, max_origin_abs, PG_BVH_HOST_SAH, out_id);
+}
+
+int pgpu_geometry_create_ex(const float* tris, uint64_t num_tris, float max_origin_abs, uint32_t bvh_builder,
+                            uint64_t* out_id)
+{
 	return guarded([&]
 	{
 		if(!tris || num_tris == 0 || !out_id)
 		{
 			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_geometry_create: empty input");
 		}
+		if(bvh_builder > PG_BVH_GPU_MORTON)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_geometry_create_ex: unknown BVH builder");
+		}
 		BvhBuildInput in{tris, nullptr, nullptr, static_cast<std::size_t>(num_tris), max_origin_abs};
-		*out_id = geometry_registry().add(make_geometry(in));
+		*out_id = geometry_registry().add(bvh_builder == PG_BVH_GPU_MORTON ? make_geometry_gpu(in) : make_geometry(in));
+	});
+}
+
+int pgpu_geometry_export(uint64_t id, void* out_nodes, void* out_tris, uint64_t* out_num_nodes, uint64_t* out_num_tris)
+{
+	return guarded([&]
+	{
+		auto g = get_geometry(id);
+		const uint64_t nn = g->stats.num_nodes, nt = g->stats.num_leaf_tris;
+		if(out_num_nodes) { *out_num_nodes = nn; }
+		if(out_num_tris) { *out_num_tris = nt; }
+		cudaStream_t s = library_stream();
+		if(out_nodes)
+		{
+			PG_CUDA_CHECK(cudaMemcpyAsync(out_nodes, g->nodes.get(), nn * sizeof(WideNode), cudaMemcpyDeviceToHost, s));
+		}
+		if(out_tris)
+		{
+			PG_CUDA_CHECK(cudaMemcpyAsync(out_tris, g->tris.get(), nt * sizeof(LeafTri), cudaMemcpyDeviceToHost, s));
+		}
+		PG_CUDA_CHECK(cudaStreamSynchronize(s));
 	});
 }
 

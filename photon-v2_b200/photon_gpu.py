@@ -29,6 +29,8 @@ PGPU_SIGNATURES = [
     ("pgpu_last_error", ctypes.c_char_p, []),
     ("pgpu_device_count", ctypes.c_int, []),
     ("pgpu_geometry_create", ctypes.c_int, [_f32p, ctypes.c_uint64, ctypes.c_float, _u64p]),
+    ("pgpu_geometry_create_ex", ctypes.c_int, [_f32p, ctypes.c_uint64, ctypes.c_float, ctypes.c_uint32, _u64p]),
+    ("pgpu_geometry_export", ctypes.c_int, [ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, _u64p, _u64p]),
     ("pgpu_geometry_destroy", ctypes.c_int, [ctypes.c_uint64]),
     ("pgpu_geometry_stats", ctypes.c_int, [ctypes.c_uint64, _u64p, _u64p, _i32p, _dblp]),
     ("pgpu_trace_closest", ctypes.c_int, [ctypes.c_uint64, _f32p, ctypes.c_uint64, _i32p, _f32p, _f32p]),
@@ -48,6 +50,9 @@ PGPU_SIGNATURES = [
      [_f32p, _f32p, _f32p, _f32p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _f32p]),
     ("pgpu_scene_create", ctypes.c_int,
      [_f32p, _u32p, _u32p, ctypes.c_uint64, _f32p, ctypes.c_uint32, _f32p, ctypes.c_uint32, _f32p, _u64p]),
+    ("pgpu_scene_create_ex", ctypes.c_int,
+     [_f32p, _u32p, _u32p, ctypes.c_uint64, _f32p, ctypes.c_uint32, _f32p, ctypes.c_uint32, _f32p, ctypes.c_uint32,
+      _u64p]),
     ("pgpu_scene_destroy", ctypes.c_int, [ctypes.c_uint64]),
     ("pgpu_scene_render", ctypes.c_int,
      [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64,
@@ -103,17 +108,34 @@ def device_count() -> int:
     return int(load().pgpu_device_count())
 
 
+BUILDERS = {"sah": 0, "gpu": 1}
+# 48-byte leaf triangle: v0 xyz, original index, v1 xyz, material, v2 xyz, emitter + 1
+LEAF_TRI_DTYPE = np.dtype([("v0", np.float32, 3), ("prim", np.uint32), ("v1", np.float32, 3),
+                           ("material", np.uint32), ("v2", np.float32, 3), ("emitter", np.uint32)])
+
+
 class Geometry:
     """Triangles [N, 3, 3] with their 8-wide BVH resident on the GPU."""
 
-    def __init__(self, tris: np.ndarray, max_origin_abs: float = 0.0):
+    def __init__(self, tris: np.ndarray, max_origin_abs: float = 0.0, builder: str = "sah"):
+        """builder: "sah" (host binned SAH) or "gpu" (Morton-ordered radix tree built on the GPU)."""
         lib = load()
         t = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
         self.num_tris = t.shape[0]
         gid = ctypes.c_uint64(0)
-        _check(lib.pgpu_geometry_create(_ptr(t, ctypes.c_float), t.shape[0], float(max_origin_abs),
-                                        ctypes.byref(gid)))
+        _check(lib.pgpu_geometry_create_ex(_ptr(t, ctypes.c_float), t.shape[0], float(max_origin_abs),
+                                           BUILDERS[builder], ctypes.byref(gid)))
         self.id = gid.value
+
+    def export(self):
+        """(nodes uint32 [N, 20], leaf triangles as a structured array) copied from the device."""
+        nn, nt = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(load().pgpu_geometry_export(self.id, None, None, ctypes.byref(nn), ctypes.byref(nt)))
+        nodes = np.empty((nn.value, 20), np.uint32)
+        tris = np.empty(nt.value, LEAF_TRI_DTYPE)
+        _check(load().pgpu_geometry_export(self.id, nodes.ctypes.data_as(ctypes.c_void_p),
+                                           tris.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nn), ctypes.byref(nt)))
+        return nodes, tris
 
     def close(self) -> None:
         if self.id:
@@ -233,16 +255,16 @@ def flatten_scene(scene):
 class RenderScene:
     """A scene resident on the GPU with its FP64 film (pgpu_scene_*)."""
 
-    def __init__(self, scene):
+    def __init__(self, scene, builder: str = "sah"):
         lib = load()
         tris, tri_mat, tri_em, mats, ems, cam = flatten_scene(scene)
         self.width, self.height = scene.width, scene.height
         sid = ctypes.c_uint64(0)
         em_ptr = _ptr(ems, ctypes.c_float) if ems.size else None
-        _check(lib.pgpu_scene_create(_ptr(tris, ctypes.c_float), _ptr(tri_mat, ctypes.c_uint32),
-                                     _ptr(tri_em, ctypes.c_uint32), tris.shape[0],
-                                     _ptr(mats, ctypes.c_float), mats.shape[0], em_ptr, ems.shape[0],
-                                     _ptr(cam, ctypes.c_float), ctypes.byref(sid)))
+        _check(lib.pgpu_scene_create_ex(_ptr(tris, ctypes.c_float), _ptr(tri_mat, ctypes.c_uint32),
+                                        _ptr(tri_em, ctypes.c_uint32), tris.shape[0],
+                                        _ptr(mats, ctypes.c_float), mats.shape[0], em_ptr, ems.shape[0],
+                                        _ptr(cam, ctypes.c_float), BUILDERS[builder], ctypes.byref(sid)))
         self.id = sid.value
 
     def close(self):
@@ -355,6 +377,7 @@ PH_SIGNATURES = [
     ("phGpuSetMaxRayBounces", None, [ctypes.c_uint64, ctypes.c_uint32]),
     ("phGpuSetSeed", None, [ctypes.c_uint64, ctypes.c_uint64]),
     ("phGpuSetGuiding", None, [ctypes.c_uint64, ctypes.c_int]),
+    ("phGpuSetBvhBuilder", None, [ctypes.c_uint64, ctypes.c_uint32]),
     ("phGpuSetSurfaceRefine", None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32]),
     ("phGpuClearFilm", None, [ctypes.c_uint64]),
     ("phGpuGetRenderInfo", None, [ctypes.c_uint64, _dblp, _u64p, _u64p, _u64p, _dblp]),
@@ -414,6 +437,9 @@ class PhotonEngine:
 
     def set_guiding(self, enabled: bool) -> None:
         load().phGpuSetGuiding(self.id, 1 if enabled else 0)
+
+    def set_bvh_builder(self, builder: str = "sah") -> None:
+        load().phGpuSetBvhBuilder(self.id, BUILDERS[builder])
 
     def set_surface_refine(self, mode: str = "iterative", delta: float = 2e-4, iterations: int = 1) -> None:
         """phGpuSetSurfaceRefine: the reference's RefineMode (manual / empirical / iterative)."""
