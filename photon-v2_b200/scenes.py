@@ -242,6 +242,76 @@ def cornell_glossy(width: int = 64, height: int = 64, spp: int = 64, max_bounces
     return sc
 
 
+def tessellated_boxes(mins: np.ndarray, maxs: np.ndarray, grid: int = 3) -> np.ndarray:
+    """Outward-facing boxes whose 6 faces are each split into grid x grid quads:
+    [K, 6 * grid^2 * 2, 3, 3] float32 (108 triangles per box at grid 3)."""
+    k = mins.shape[0]
+    u = np.linspace(0.0, 1.0, grid + 1)
+    tris = []
+    # each face: origin corner (in unit-box coordinates), two edge axes, sign for outward winding
+    faces = [((0, 0, 0), 2, 1), ((1, 0, 0), 1, 2),   # -x, +x
+             ((0, 0, 0), 0, 2), ((0, 1, 0), 2, 0),   # -y, +y
+             ((0, 0, 0), 1, 0), ((0, 0, 1), 0, 1)]   # -z, +z
+    ext = maxs - mins
+    for origin, ea, eb in faces:
+        for i in range(grid):
+            for j in range(grid):
+                def corner(a, b):
+                    c = np.array(origin, np.float64)
+                    c = np.broadcast_to(c, (k, 3)).copy()
+                    c[:, ea] = a
+                    c[:, eb] = b
+                    return mins + c * ext
+                p00, p10 = corner(u[i], u[j]), corner(u[i + 1], u[j])
+                p11, p01 = corner(u[i + 1], u[j + 1]), corner(u[i], u[j + 1])
+                tris.append(np.stack([p00, p10, p11], 1))
+                tris.append(np.stack([p00, p11, p01], 1))
+    return np.stack(tris, 1).astype(np.float32)
+
+
+def city(width: int = 1920, height: int = 1080, spp: int = 1024, max_bounces: int = 12,
+         blocks: int = 447, num_lights: int = 10_000, num_materials: int = 64, seed: int = 5,
+         estimator: str = "bneept") -> Scene:
+    """Many-light night city: a blocks x blocks grid of buildings (447^2 = 199,809) whose heights
+    are lognormal(mu 2, sigma 0.6), each a box with 3 x 3-tessellated faces (108 triangles, so
+    ~21.6M triangles), on a ground plane; GGX conductors with roughness ~ U[0.02, 0.8] in
+    `num_materials` groups; lit only by `num_lights` small emissive quads whose radiance is
+    lognormal (sigma 1), picked by the power alias table."""
+    rng = np.random.default_rng(seed)
+    lot = 12.0
+    gx, gz = np.meshgrid(np.arange(blocks), np.arange(blocks), indexing="ij")
+    gx, gz = gx.ravel(), gz.ravel()
+    k = gx.size
+    fw = rng.uniform(4.0, 9.0, (k, 2))
+    off = rng.uniform(0.0, 1.0, (k, 2)) * (lot - 1.0 - fw)
+    building_h = np.exp(rng.normal(2.0, 0.6, k))
+    mins = np.stack([gx * lot + 0.5 + off[:, 0], np.zeros(k), gz * lot + 0.5 + off[:, 1]], 1)
+    maxs = np.stack([mins[:, 0] + fw[:, 0], building_h, mins[:, 2] + fw[:, 1]], 1)
+    boxes = tessellated_boxes(mins, maxs, 3)
+    size = blocks * lot
+    ground = quad((0, 0, 0), (0, 0, size), (size, 0, size), (size, 0, 0))
+    group = rng.integers(0, num_materials, k)
+    groups = [MeshGroup(ground, Material("matte", albedo=(0.3, 0.3, 0.3)))]
+    for m in range(num_materials):
+        sel = boxes[group == m].reshape(-1, 3, 3)
+        if sel.shape[0]:
+            groups.append(MeshGroup(sel, Material("conductor", roughness=float(rng.uniform(0.02, 0.8)),
+                                                  f0=tuple(float(x) for x in rng.uniform(0.5, 1.0, 3)))))
+    # street lights: 1 x 1 quads facing down, 6 m above the street between lots
+    lx = (rng.integers(0, blocks, num_lights) + rng.uniform(0.0, 1.0, num_lights)) * lot
+    lz = rng.integers(0, blocks, num_lights) * lot + 0.25
+    radiance = np.exp(rng.normal(0.0, 1.0, num_lights)) * 400.0
+    tint = rng.uniform(0.7, 1.0, (num_lights, 3))
+    for i in range(num_lights):
+        x, z = float(lx[i]), float(lz[i])
+        q = quad((x, 6.0, z), (x + 1.0, 6.0, z), (x + 1.0, 6.0, z + 1.0), (x, 6.0, z + 1.0))  # normal -y
+        groups.append(MeshGroup(q, BLACK, radiance=tuple(float(radiance[i] * t) for t in tint[i])))
+    centre = size * 0.5
+    return Scene("city", width, height, spp, max_bounces, cam_pos=(centre - 60.0, 25.0, centre - 60.0),
+                 cam_dir=(0.7, -0.25, 0.7), cam_up=(0.0, 1.0, 0.0), fov_deg=60.0, groups=groups,
+                 estimator=estimator)
+
+
 def slit_room(width: int = 1024, height: int = 1024, spp: int = 64, max_bounces: int = 10,
               num_boxes: int = 166_667, seed: int = 3, estimator: str = "bneept") -> Scene:
     """Learned-guiding workload: a 10 x 10 x 4 room filled with seeded random furniture boxes
