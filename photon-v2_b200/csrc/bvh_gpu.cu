@@ -5,20 +5,20 @@
 // that build dominates turnaround, so this path builds on the device instead:
 //   1. per-triangle boxes and centroids, scene centroid bound (block reductions + atomics);
 //   2. 63-bit Morton codes of the centroids, sorted with their indices (CUB radix sort);
-//   3. the binary radix tree over the sorted codes (Karras 2012), one thread per internal node,
-//      equal codes ordered by index;
-//   4. node boxes bottom-up, the second child to arrive at a parent computing its box;
-//   5. collapse to 8-wide nodes level by level, one thread per wide node: open the largest
+//   3. the binary tree by parallel locally-ordered clustering (PLOC, Meister & Bittner 2018):
+//      every cluster finds, among its neighbours within a radius in Morton order, the one whose
+//      merged box has the least surface area; mutual nearest neighbours merge; the survivors
+//      are compacted and the pass repeats until one cluster is left;
+//   4. collapse to 8-wide nodes level by level, one thread per wide node: open the largest
 //      child holding more than 3 triangles until 8 children, assign octant slots and quantise
 //      the child boxes conservatively exactly as the host builder does.
-// Every subtree of the radix tree covers a contiguous range of sorted triangles, so a child with
-// at most 3 triangles becomes a leaf group directly. The closest hit a ray finds does not depend
-// on the tree (boxes are conservative, ties are resolved by primitive index), only traversal
-// cost does: a Morton tree visits more nodes than the SAH tree.
+// The closest hit a ray finds does not depend on the tree (boxes are conservative, ties are
+// resolved by primitive index), only traversal cost does.
 #include "pg_geometry.h"
 #include "pg_runtime.h"
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_select.cuh>
 
 #include <algorithm>
 #include <chrono>
@@ -138,72 +138,6 @@ __global__ void morton_kernel(const float4* __restrict__ lo, const float4* __res
 	}
 }
 
-// Length of the common prefix of sorted codes a and b; equal codes compare their indices.
-__device__ __forceinline__ int prefix(const uint64_t* __restrict__ keys, int n, int a, int b)
-{
-	if(b < 0 || b >= n)
-	{
-		return -1;
-	}
-	const uint64_t ka = keys[a], kb = keys[b];
-	if(ka == kb)
-	{
-		return 64 + __clz(static_cast<uint32_t>(a ^ b));
-	}
-	return __clzll(ka ^ kb);
-}
-
-// Karras 2012, "Maximizing parallelism in the construction of BVHs, octrees, and k-d trees".
-__global__ void radix_tree_kernel(const uint64_t* __restrict__ keys, int n, uint32_t* __restrict__ left,
-                                  uint32_t* __restrict__ right, uint32_t* __restrict__ first_of,
-                                  uint32_t* __restrict__ count_of, uint32_t* __restrict__ parent_internal,
-                                  uint32_t* __restrict__ parent_leaf)
-{
-	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x)
-	{
-		const int d = (prefix(keys, n, i, i + 1) - prefix(keys, n, i, i - 1)) >= 0 ? 1 : -1;
-		const int dmin = prefix(keys, n, i, i - d);
-		int lmax = 2;
-		while(prefix(keys, n, i, i + lmax * d) > dmin && lmax < 2 * n)
-		{
-			lmax *= 2;
-		}
-		int l = 0;
-		for(int t = lmax / 2; t >= 1; t /= 2)
-		{
-			if(prefix(keys, n, i, i + (l + t) * d) > dmin)
-			{
-				l += t;
-			}
-		}
-		const int j = i + l * d;
-		const int dnode = prefix(keys, n, i, j);
-		int s = 0;
-		for(int div = 2; ; div *= 2)
-		{
-			const int t = (l + div - 1) / div;
-			if(prefix(keys, n, i, i + (s + t) * d) > dnode)
-			{
-				s += t;
-			}
-			if(t <= 1)
-			{
-				break;
-			}
-		}
-		const int gamma = i + s * d + min(d, 0);
-		const int first = min(i, j), last = max(i, j);
-		const uint32_t lc = first == gamma ? (kLeafRef | static_cast<uint32_t>(gamma)) : static_cast<uint32_t>(gamma);
-		const uint32_t rc = last == gamma + 1 ? (kLeafRef | static_cast<uint32_t>(gamma + 1)) : static_cast<uint32_t>(gamma + 1);
-		left[i] = lc;
-		right[i] = rc;
-		first_of[i] = static_cast<uint32_t>(first);
-		count_of[i] = static_cast<uint32_t>(last - first + 1);
-		if(lc & kLeafRef) { parent_leaf[lc & ~kLeafRef] = static_cast<uint32_t>(i); } else { parent_internal[lc] = static_cast<uint32_t>(i); }
-		if(rc & kLeafRef) { parent_leaf[rc & ~kLeafRef] = static_cast<uint32_t>(i); } else { parent_internal[rc] = static_cast<uint32_t>(i); }
-	}
-}
-
 __device__ __forceinline__ void ref_box(uint32_t ref, const float4* __restrict__ plo, const float4* __restrict__ phi,
                                         const uint32_t* __restrict__ sorted, const float4* nlo, const float4* nhi,
                                         float4* l, float4* h)
@@ -221,31 +155,123 @@ __device__ __forceinline__ void ref_box(uint32_t ref, const float4* __restrict__
 	}
 }
 
-// Boxes bottom-up: each leaf walks to the root; at every parent the first arrival stops and the
-// second computes the parent's box from both children.
-__global__ void bounds_kernel(int n, const uint32_t* __restrict__ sorted, const float4* __restrict__ plo,
-                              const float4* __restrict__ phi, const uint32_t* __restrict__ left,
-                              const uint32_t* __restrict__ right, const uint32_t* __restrict__ parent_internal,
-                              const uint32_t* __restrict__ parent_leaf, uint32_t* __restrict__ arrivals,
-                              float4* nlo, float4* nhi)
+constexpr int kPlocRadius = 16;
+constexpr int kPlocBlock = 256;
+
+__device__ __forceinline__ float merged_area(float4 la, float4 ha, float4 lb, float4 hb)
 {
-	for(int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+	const float dx = fmaxf(ha.x, hb.x) - fminf(la.x, lb.x);
+	const float dy = fmaxf(ha.y, hb.y) - fminf(la.y, lb.y);
+	const float dz = fmaxf(ha.z, hb.z) - fminf(la.z, lb.z);
+	return dx * dy + dy * dz + dz * dx;
+}
+
+// Nearest neighbour of every cluster among the kPlocRadius clusters on each side. Pairs are
+// ordered by (merged area, index distance, parity of the lower index, lower index), a total
+// order, so the globally closest pair is always mutual and every pass merges at least once; the
+// parity term pairs equal-area runs (identical boxes) as (0,1), (2,3), ... so that they still
+// halve per pass instead of chaining. The block's clusters and the radius around them are staged
+// in shared memory.
+__global__ void __launch_bounds__(kPlocBlock)
+ploc_neighbour_kernel(const uint32_t* __restrict__ clusters, uint32_t m, const uint32_t* __restrict__ sorted,
+                      const float4* __restrict__ plo, const float4* __restrict__ phi, const float4* __restrict__ nlo,
+                      const float4* __restrict__ nhi, uint32_t* __restrict__ nn)
+{
+	__shared__ float4 slo[kPlocBlock + 2 * kPlocRadius], shi[kPlocBlock + 2 * kPlocRadius];
+	const int base = static_cast<int>(blockIdx.x) * kPlocBlock - kPlocRadius;
+	for(int t = threadIdx.x; t < kPlocBlock + 2 * kPlocRadius; t += kPlocBlock)
 	{
-		uint32_t node = parent_leaf[p];
-		for(int depth = 0; node != kNone && depth < n; ++depth)
+		const int c = base + t;
+		if(c >= 0 && c < static_cast<int>(m))
 		{
-			__threadfence();
-			if(atomicAdd(&arrivals[node], 1u) == 0u)
-			{
-				break;
-			}
-			float4 l0, h0, l1, h1;
-			ref_box(left[node], plo, phi, sorted, nlo, nhi, &l0, &h0);
-			ref_box(right[node], plo, phi, sorted, nlo, nhi, &l1, &h1);
-			__stcg(nlo + node, make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.0f));
-			__stcg(nhi + node, make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.0f));
-			node = parent_internal[node];
+			ref_box(clusters[c], plo, phi, sorted, nlo, nhi, &slo[t], &shi[t]);
 		}
+	}
+	__syncthreads();
+	const int i = static_cast<int>(blockIdx.x) * kPlocBlock + static_cast<int>(threadIdx.x);
+	if(i >= static_cast<int>(m))
+	{
+		return;
+	}
+	const int ti = i - base;
+	float best = 3.0e38f;
+	int bj = -1, best_dist = 0, best_par = 0, best_min = 0;
+	const int lo = max(0, i - kPlocRadius), hi = min(static_cast<int>(m) - 1, i + kPlocRadius);
+	for(int j = lo; j <= hi; ++j)
+	{
+		if(j == i)
+		{
+			continue;
+		}
+		const float area = merged_area(slo[ti], shi[ti], slo[j - base], shi[j - base]);
+		const int dist = abs(j - i), mn = min(i, j), par = mn & 1;
+		const bool better = bj < 0 || area < best ||
+			(area == best && (dist < best_dist || (dist == best_dist && (par < best_par ||
+			(par == best_par && mn < best_min)))));
+		if(better)
+		{
+			best = area;
+			bj = j;
+			best_dist = dist;
+			best_par = par;
+			best_min = mn;
+		}
+	}
+	nn[i] = bj < 0 ? kNone : static_cast<uint32_t>(bj);
+}
+
+// Mutual nearest neighbours merge into a new internal node kept at the lower position; the
+// higher position is dropped (flag 0).
+__global__ void ploc_merge_kernel(const uint32_t* __restrict__ clusters, uint32_t m, const uint32_t* __restrict__ nn,
+                                  const uint32_t* __restrict__ sorted, const float4* __restrict__ plo,
+                                  const float4* __restrict__ phi, uint32_t* __restrict__ next_node,
+                                  uint32_t* __restrict__ left, uint32_t* __restrict__ right,
+                                  uint32_t* __restrict__ count_of, float4* nlo, float4* nhi,
+                                  uint32_t* __restrict__ out, uint8_t* __restrict__ keep, uint32_t node_limit,
+                                  uint32_t* __restrict__ error)
+{
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+	{
+		const uint32_t j = nn[i];
+		const bool mutual = j != kNone && nn[j] == i;
+		if(!mutual)
+		{
+			out[i] = clusters[i];
+			keep[i] = 1;
+			continue;
+		}
+		if(i > j)
+		{
+			keep[i] = 0;
+			continue;
+		}
+		const uint32_t k = atomicAdd(next_node, 1u);
+		if(k >= node_limit)
+		{
+			atomicOr(error, BUILD_ERR_NODE_OVERFLOW);
+			out[i] = clusters[i];
+			keep[i] = 1;
+			continue;
+		}
+		const uint32_t a = clusters[i], b = clusters[j];
+		float4 la, ha, lb, hb;
+		ref_box(a, plo, phi, sorted, nlo, nhi, &la, &ha);
+		ref_box(b, plo, phi, sorted, nlo, nhi, &lb, &hb);
+		left[k] = a;
+		right[k] = b;
+		count_of[k] = ((a & kLeafRef) ? 1u : count_of[a]) + ((b & kLeafRef) ? 1u : count_of[b]);
+		nlo[k] = make_float4(fminf(la.x, lb.x), fminf(la.y, lb.y), fminf(la.z, lb.z), 0.0f);
+		nhi[k] = make_float4(fmaxf(ha.x, hb.x), fmaxf(ha.y, hb.y), fmaxf(ha.z, hb.z), 0.0f);
+		out[i] = k;
+		keep[i] = 1;
+	}
+}
+
+__global__ void leaf_refs_kernel(uint32_t n, uint32_t* __restrict__ clusters)
+{
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		clusters[i] = kLeafRef | i;
 	}
 }
 
@@ -261,7 +287,6 @@ struct CollapseArgs
 	const float4*   nhi;
 	const uint32_t* left;
 	const uint32_t* right;
-	const uint32_t* first_of;
 	const uint32_t* count_of;
 	WideNode*       nodes;
 	LeafTri*        leaf_tris;
@@ -481,12 +506,28 @@ __global__ void collapse_kernel(CollapseArgs a, const uint2* __restrict__ items,
 		}
 		else
 		{
-			const uint32_t cnt = count(ref);
-			const uint32_t first = (ref & kLeafRef) ? (ref & ~kLeafRef) : a.first_of[ref];
+			// the subtree's (at most 3) triangles
+			uint32_t leaves[kLeafMax], stack[2 * kLeafMax];
+			uint32_t cnt = 0;
+			int sp = 0;
+			stack[sp++] = ref;
+			while(sp > 0)
+			{
+				const uint32_t r = stack[--sp];
+				if(r & kLeafRef)
+				{
+					if(cnt < kLeafMax) { leaves[cnt++] = r & ~kLeafRef; }
+				}
+				else if(sp + 2 <= static_cast<int>(2 * kLeafMax))
+				{
+					stack[sp++] = a.right[r];
+					stack[sp++] = a.left[r];
+				}
+			}
 			meta = (((1u << cnt) - 1u) << 5) | tri_offset;
 			for(uint32_t t = 0; t < cnt; ++t)
 			{
-				const uint32_t p = a.sorted[first + t];
+				const uint32_t p = a.sorted[leaves[t]];
 				const float* v = a.tris + 9ull * p;
 				LeafTri lt;
 				lt.v0x = v[0]; lt.v0y = v[1]; lt.v0z = v[2]; lt.prim = p;
@@ -578,25 +619,49 @@ std::unique_ptr<Geometry> make_geometry_gpu(const BvhBuildInput& in)
 	PG_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(temp.get(), temp_bytes, keys.get(), keys_sorted.get(), idx.get(),
 	                                              sorted.get(), static_cast<int>(n), 0, 63, s));
 
-	// 3./4. radix tree and its boxes
+	// 3. the binary tree by locally-ordered clustering
 	const uint32_t ni = n > 1 ? n - 1 : 1;
-	DeviceBuffer<uint32_t> left(ni), right(ni), first_of(ni), count_of(ni), parent_internal(ni), parent_leaf(n),
-		arrivals(ni);
+	DeviceBuffer<uint32_t> left(ni), right(ni), count_of(ni);
 	DeviceBuffer<float4> nlo(ni), nhi(ni);
-	PG_CUDA_CHECK(cudaMemsetAsync(parent_internal.get(), 0xFF, parent_internal.bytes(), s));
-	PG_CUDA_CHECK(cudaMemsetAsync(parent_leaf.get(), 0xFF, parent_leaf.bytes(), s));
-	PG_CUDA_CHECK(cudaMemsetAsync(arrivals.get(), 0, arrivals.bytes(), s));
-	if(n > 1)
+	DeviceBuffer<uint32_t> clusters[2] = {DeviceBuffer<uint32_t>(n), DeviceBuffer<uint32_t>(n)};
+	DeviceBuffer<uint32_t> nn(n), merged(n), ploc_state(3);   // [0] next internal node, [1] selected, [2] errors
+	DeviceBuffer<uint8_t> keep(n);
+	PG_CUDA_CHECK(cudaMemsetAsync(ploc_state.get(), 0, ploc_state.bytes(), s));
+	leaf_refs_kernel<<<std::min(blocks_for(n), sm_count() * 8), kBlock, 0, s>>>(n, clusters[0].get());
+	PG_CUDA_CHECK(cudaGetLastError());
+	std::size_t select_bytes = 0;
+	PG_CUDA_CHECK(cub::DeviceSelect::Flagged(nullptr, select_bytes, merged.get(), keep.get(), clusters[1].get(),
+	                                         ploc_state.get() + 1, static_cast<int>(n), s));
+	DeviceBuffer<unsigned char> select_temp(std::max<std::size_t>(select_bytes, 16));
+	uint32_t m = n;
+	int cur = 0;
+	for(int pass = 0; m > 1; ++pass)
 	{
-		radix_tree_kernel<<<blocks_for(n - 1), kBlock, 0, s>>>(keys_sorted.get(), static_cast<int>(n), left.get(),
-		                                                       right.get(), first_of.get(), count_of.get(),
-		                                                       parent_internal.get(), parent_leaf.get());
+		if(pass > 100000)
+		{
+			throw Error(PG_ERR_SCENE, "GPU BVH build: clustering did not converge");
+		}
+		ploc_neighbour_kernel<<<(m + kPlocBlock - 1) / kPlocBlock, kPlocBlock, 0, s>>>(
+			clusters[cur].get(), m, sorted.get(), plo.get(), phi.get(), nlo.get(), nhi.get(), nn.get());
 		PG_CUDA_CHECK(cudaGetLastError());
-		bounds_kernel<<<blocks_for(n), kBlock, 0, s>>>(static_cast<int>(n), sorted.get(), plo.get(), phi.get(),
-		                                               left.get(), right.get(), parent_internal.get(),
-		                                               parent_leaf.get(), arrivals.get(), nlo.get(), nhi.get());
+		ploc_merge_kernel<<<std::min(blocks_for(m), sm_count() * 8), kBlock, 0, s>>>(
+			clusters[cur].get(), m, nn.get(), sorted.get(), plo.get(), phi.get(), ploc_state.get(), left.get(),
+			right.get(), count_of.get(), nlo.get(), nhi.get(), merged.get(), keep.get(), ni, ploc_state.get() + 2);
 		PG_CUDA_CHECK(cudaGetLastError());
+		PG_CUDA_CHECK(cub::DeviceSelect::Flagged(select_temp.get(), select_bytes, merged.get(), keep.get(),
+		                                         clusters[1 - cur].get(), ploc_state.get() + 1, static_cast<int>(m), s));
+		uint32_t state[3];
+		PG_CUDA_CHECK(cudaMemcpyAsync(state, ploc_state.get(), sizeof(state), cudaMemcpyDeviceToHost, s));
+		PG_CUDA_CHECK(cudaStreamSynchronize(s));
+		if(state[2] != 0u || state[1] >= m)
+		{
+			throw Error(PG_ERR_SCENE, "GPU BVH build: clustering made no progress");
+		}
+		m = state[1];
+		cur = 1 - cur;
 	}
+	uint32_t root_ref = kLeafRef;
+	PG_CUDA_CHECK(cudaMemcpyAsync(&root_ref, clusters[cur].get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
 	float h_stats[8];
 	PG_CUDA_CHECK(cudaMemcpyAsync(h_stats, stats.get(), sizeof(h_stats), cudaMemcpyDeviceToHost, s));
 	PG_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -612,12 +677,12 @@ std::unique_ptr<Geometry> make_geometry_gpu(const BvhBuildInput& in)
 	PG_CUDA_CHECK(cudaMemcpyAsync(counters.get(), init_counters, sizeof(init_counters), cudaMemcpyHostToDevice, s));
 	DeviceBuffer<uint2> items[2] = {DeviceBuffer<uint2>(node_capacity), DeviceBuffer<uint2>(node_capacity)};
 	DeviceBuffer<uint32_t> next_count(1);
-	const uint2 root = make_uint2(n > 1 ? 0u : kLeafRef, 0u);
+	const uint2 root = make_uint2(root_ref, 0u);
 	PG_CUDA_CHECK(cudaMemcpyAsync(items[0].get(), &root, sizeof(root), cudaMemcpyHostToDevice, s));
 
 	CollapseArgs args{d_tris.get(), in.materials ? d_mat.get() : nullptr, in.emitters ? d_em.get() : nullptr,
 	                  sorted.get(), plo.get(), phi.get(), nlo.get(), nhi.get(), left.get(), right.get(),
-	                  first_of.get(), count_of.get(), g->nodes.get(), g->tris.get(), node_capacity, n,
+	                  count_of.get(), g->nodes.get(), g->tris.get(), node_capacity, n,
 	                  4.0e-6f * max_abs, counters.get()};
 	uint32_t count = 1;
 	int depth = 0;
