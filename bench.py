@@ -153,7 +153,7 @@ def cpu_sample(scene: scenes.Scene, tmp: str, target_seconds: float = 12.0, repe
 
         scene_file = os.path.join(d, "scene.bin")
         oracle_port.write_scene_bin(scene_file, photon_gpu.flatten_scene(s), spp,
-                                    0 if s.estimator == "bneept" else 1)
+                                    {"bneept": 0, "bvpt": 1, "bvptdl": 2}[s.estimator])
     out = subprocess.run([tool, scene_file, str(threads), str(scene.max_bounces), os.path.join(d, "out.rgbf32"),
                           str(repeats)], cwd=d, capture_output=True, text=True, check=True)
     records = []

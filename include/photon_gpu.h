@@ -126,12 +126,13 @@ PGPU_API int pgpu_guide_train(float* params, const float* features, const float*
 PGPU_API int pgpu_bsdf_eval(const float* cases, const float* normals, uint64_t n, float* out);
 
 /* ---------------------------------------------------------------------------------------------
- * Render scenes: the full BNEEPT / BVPT estimator on the GPU.
+ * Render scenes: the full BNEEPT / BVPT / BVPTDL estimators on the GPU.
  *
  * Replaces EqualSamplingRenderer::doRender (Engine/Source/Core/Renderer/Sampling/
  * EqualSamplingRenderer.cpp:119-203) driving BNEEPTEstimator::estimate
- * (Engine/Source/Core/Estimator/BNEEPTEstimator.cpp:38-262) or BVPTEstimator::estimate
- * (Engine/Source/Core/Estimator/BVPTEstimator.cpp:25-160) into an HdrRgbFilm with a box filter.
+ * (Engine/Source/Core/Estimator/BNEEPTEstimator.cpp:38-262), BVPTEstimator::estimate
+ * (Engine/Source/Core/Estimator/BVPTEstimator.cpp:25-160) or BVPTDLEstimator::estimate
+ * (Engine/Source/Core/Estimator/BVPTDLEstimator.cpp:21-96) into an HdrRgbFilm with a box filter.
  *
  * tris: float32 [n][3][3]; tri_material: uint32 [n]; tri_emitter: uint32 [n] = emitter index + 1
  *   (0 = not emissive; may be NULL).
@@ -151,8 +152,8 @@ PGPU_API int pgpu_scene_create_ex(const float* tris, const uint32_t* tri_materia
                        uint32_t bvh_builder, uint64_t* out_id);
 PGPU_API int pgpu_scene_destroy(uint64_t id);
 
-/* Renders spp samples per pixel (estimator 0 = BNEEPT, 1 = BVPT; max_bounces = the reference's
- * MAX_RAY_BOUNCES) and adds them to the scene's FP64 film. Samples are numbered from first_sample
+/* Renders spp samples per pixel (estimator 0 = BNEEPT, 1 = BVPT, 2 = BVPTDL, which follows one
+ * bounce whatever max_bounces says; max_bounces = the reference's MAX_RAY_BOUNCES) and adds them to the scene's FP64 film. Samples are numbered from first_sample
  * so that separate calls draw independent random numbers. Optional outputs: device time of the
  * render (CUDA events), closest-hit rays and shadow rays traced. */
 PGPU_API int pgpu_scene_render(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator,

@@ -6,7 +6,7 @@
 // Library (C ABI, loaded by the tests through ctypes) and CLI:
 //   ph_port_render <scene.bin> <threads> <max-bounces> <out.rgbf32> [repeats]
 // scene.bin (little-endian): "PHPT" u32 version=1, u32 width, height, spp, estimator (0 BNEEPT,
-//   1 BVPT), f32 camera[12] (pos, dir, up, fov, width, height), u32 num_tris, num_materials,
+//   1 BVPT, 2 BVPTDL), f32 camera[12] (pos, dir, up, fov, width, height), u32 num_tris, num_materials,
 //   num_emitters, f32 tris[n][9], u32 tri_material[n], u32 tri_emitter[n] (index + 1),
 //   f32 materials[m][8], f32 emitters[e][4] -- the layout of pgpu_scene_create.
 #include <algorithm>
@@ -688,11 +688,15 @@ bool surface_at(const Scene& s, Vec o, Vec d, Surface* x, Vec* dir_in)
 	return true;
 }
 
-// One path of BNEEPTEstimator::estimate (Core/Estimator/BNEEPTEstimator.cpp:38-262) or
-// BVPTEstimator::estimate (Core/Estimator/BVPTEstimator.cpp:25-160).
+// One path of BNEEPTEstimator::estimate (Core/Estimator/BNEEPTEstimator.cpp:38-262),
+// BVPTEstimator::estimate (Core/Estimator/BVPTEstimator.cpp:25-160) or
+// BVPTDLEstimator::estimate (Core/Estimator/BVPTDLEstimator.cpp:21-96): BVPT cut after one
+// BSDF-sampled bounce, with the emitted radiance rather than the path weight clamped.
 Rgb estimate(const Scene& s, Vec o, Vec d, uint32_t max_bounces, Pcg32& rng)
 {
-	const bool bvpt = s.estimator == 1;
+	const bool bvpt = s.estimator == 1 || s.estimator == 2;
+	const bool dl = s.estimator == 2;
+	if(dl) { max_bounces = 1; }
 	Rgb energy;
 	Rgb thr{1, 1, 1};
 	float rr_scale = 1;
@@ -830,7 +834,7 @@ Rgb estimate(const Scene& s, Vec o, Vec d, uint32_t max_bounces, Pcg32& rng)
 		}
 		if(bvpt && have_le)
 		{
-			energy = energy + le * safe_clamp(thr);
+			energy = energy + (dl ? safe_clamp(le) * thr : le * safe_clamp(thr));
 		}
 		if(zero(thr) || !hit) { break; }
 		x = nx;

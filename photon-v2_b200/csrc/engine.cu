@@ -340,6 +340,7 @@ void Engine::cook(SceneDesc& desc)
 				const std::string e = lower(est->value);
 				if(e == "bvpt") { m_estimator = PG_EST_BVPT; }
 				else if(e == "bneept") { m_estimator = PG_EST_BNEEPT; }
+				else if(e == "bvptdl") { m_estimator = PG_EST_BVPTDL; }
 				else { throw std::runtime_error("estimator " + est->value + " is not supported by the GPU renderer"); }
 			}
 			if(const SdlClause* f = find(visualizer->clauses, "sample-filter"))

@@ -176,7 +176,7 @@ int pgpu_scene_render(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t 
 	return guarded([&]
 	{
 		auto r = get_render(id);
-		if(estimator > PG_EST_BVPT)
+		if(estimator > PG_EST_BVPTDL)
 		{
 			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_render: unknown estimator");
 		}
@@ -203,7 +203,7 @@ int pgpu_scene_profile(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t
 	return guarded([&]
 	{
 		auto r = get_render(id);
-		if(estimator > PG_EST_BVPT)
+		if(estimator > PG_EST_BVPTDL)
 		{
 			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_profile: unknown estimator");
 		}

@@ -348,7 +348,10 @@ shade_kernel(ShadeArgs a)
 		const V3 prev_pos = xyz(prev4);
 		float rr_scale = prev4.w;
 		const V3 d = xyz(rd);
-		const bool bvpt = a.estimator == PG_EST_BVPT;
+		// BVPT and BVPTDL add the emission their BSDF-sampled rays find; BVPTDL clamps the emitted
+		// radiance and not the path weight (BVPTDLEstimator.cpp:58-61, 88-91).
+		const bool bvpt = a.estimator != PG_EST_BNEEPT;
+		const bool dl = a.estimator == PG_EST_BVPTDL;
 
 		// ---- training sample for the guided vertex this ray left from: its incident radiance
 		//      is estimated by the emission found here plus the unoccluded NEE at this vertex
@@ -383,7 +386,8 @@ shade_kernel(ShadeArgs a)
 				const RGB le = RGB{s.env_r, s.env_g, s.env_b};
 				if(bvpt)
 				{
-					radiance = radiance + le * safe_clamp(thr_emit * cont, 0.0f, kClampMax);
+					radiance = radiance + (dl ? safe_clamp(le, 0.0f, kClampMax) * (thr_emit * cont)
+					                          : le * safe_clamp(thr_emit * cont, 0.0f, kClampMax));
 				}
 				else if(bounce == 0)
 				{
@@ -439,7 +443,8 @@ shade_kernel(ShadeArgs a)
 			}
 			if(bvpt)
 			{
-				radiance = radiance + le * safe_clamp(thr_emit * cont, 0.0f, kClampMax);
+				radiance = radiance + (dl ? safe_clamp(le, 0.0f, kClampMax) * (thr_emit * cont)
+				                          : le * safe_clamp(thr_emit * cont, 0.0f, kClampMax));
 			}
 			else if(bounce == 0)
 			{
@@ -1034,6 +1039,8 @@ float RenderScene::render(const RenderParams& params, double* film)
 	ShadowQueue sq{m_so.get(), m_sd.get(), m_sc.get()};
 	const uint64_t first_global = params.first_sample * wh;
 	const bool counting = params.mode == PG_RENDER_COUNT;
+	// BVPTDL follows one BSDF-sampled bounce whatever the configured depth (BVPTDLEstimator.cpp:62-95)
+	const uint32_t max_bounces = params.estimator == PG_EST_BVPTDL ? 1u : params.max_bounces;
 
 	// learned guiding (BNEEPT only)
 	const bool guided = m_guide_params.enabled && params.estimator == PG_EST_BNEEPT;
@@ -1082,14 +1089,14 @@ float RenderScene::render(const RenderParams& params, double* film)
 		if(guided)
 		{
 			// network inputs of this iteration's guidable vertices, then the tensor-core forward pass
-			guide_query_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, cur, m_hits.get(), gargs, params.max_bounces);
+			guide_query_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, cur, m_hits.get(), gargs, max_bounces);
 			PG_CUDA_CHECK(cudaGetLastError());
 			guide::launch_forward(m_gimage.get(), m_gfeat.get(), capacity, nullptr, nullptr, m_gerr.get(), st,
 			                      &d_counters->n_guided, m_graw.get());
 		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[4], st)); }
 		ShadeArgs sa{m_dev, cur, nxt, m_hits.get(), sq, m_counters.get(), film, params.seed, first_global,
-		             params.max_bounces, params.estimator, static_cast<uint32_t>(wh)};
+		             max_bounces, params.estimator, static_cast<uint32_t>(wh)};
 		sa.guide = gargs;
 		sa.refine.mode = params.refine_mode;
 		sa.refine.delta = params.refine_delta;

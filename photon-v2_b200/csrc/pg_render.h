@@ -57,6 +57,7 @@ enum Estimator : uint32_t
 {
 	PG_EST_BNEEPT = 0,
 	PG_EST_BVPT = 1,
+	PG_EST_BVPTDL = 2,   // zero- and one-bounce emission only (BVPTDLEstimator.cpp:21-96)
 };
 
 enum RenderMode : uint32_t

@@ -225,7 +225,7 @@ def guide_train(params, features, dirs, weights, steps, batch, lr=1e-2):
 
 
 MATTE, CONDUCTOR, DIELECTRIC = 0, 1, 2
-BNEEPT, BVPT = 0, 1
+BNEEPT, BVPT, BVPTDL = 0, 1, 2
 
 
 def flatten_scene(scene):

@@ -32,6 +32,7 @@ RENDER_TOOL = os.path.join(ROOT, "oracle", "_ref", "ph_ref_render")
 WORKLOADS = {
     "cornell_bneept": (lambda spp: scenes.cornell(64, 64, spp, 8, "bneept"), 8192, 8),
     "cornell_bvpt": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvpt"), 8192, 8),
+    "cornell_bvptdl": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvptdl"), 8192, 8),
     "cornell_glossy_bneept": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 8192, 8),
     "ggx_sphere_env_bneept": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
                                                             max_bounces=10), 4096, 10),

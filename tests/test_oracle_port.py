@@ -6,7 +6,7 @@ not at hand (it is plain C++ and travels), so it must itself reproduce the refer
 * closest hits and occlusion against the reference's TBinaryBvhIntersector answers (the same
   near-tie rule as the GPU traversal: a different primitive only where t agrees within 2 ulp);
 * BSDF eval / pdf / sample against the reference's SurfaceOptics answers (bsdf_cases.npz);
-* whole BNEEPT images against the reference renders of images.npz, at fewer samples (4 x 4 block
+* whole BNEEPT and BVPTDL images against the reference renders of images.npz, at fewer samples (4 x 4 block
   relMSE <= 1e-3 and per-channel means within 1 %, the bar of the GPU image tests).
 
 CPU only; builds the library with ``make -f oracle/Makefile.port`` when it is missing.
@@ -67,6 +67,7 @@ def test_port_bsdf_matches_reference(port):
 # image name -> (scene factory, oracle spp)
 IMAGES = {
     "cornell_bneept": (lambda spp: scenes.cornell(64, 64, spp, 8, "bneept"), 512),
+    "cornell_bvptdl": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvptdl"), 4096),
     "cornell_glossy_bneept": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 1024),
     "ggx_sphere_env_bneept": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
                                                             max_bounces=10), 512),
@@ -80,7 +81,8 @@ def test_port_image_matches_reference(port, name):
     d = np.load(os.path.join(GOLDEN, "images.npz"))
     factory, spp = IMAGES[name]
     scene = factory(spp)
-    img = port.render(photon_gpu.flatten_scene(scene), spp, scene.max_bounces, 0, seed=3)
+    estimator = {"bneept": 0, "bvpt": 1, "bvptdl": 2}[scene.estimator]
+    img = port.render(photon_gpu.flatten_scene(scene), spp, scene.max_bounces, estimator, seed=3)
     ref = d[name]
     block = lambda a: a.reshape(16, 4, 16, 4, 3).mean(axis=(1, 3)).astype(np.float64)
     err = float(np.mean((block(img) - block(ref)) ** 2 / (block(ref) ** 2 + 1e-2)))

@@ -4,13 +4,14 @@ Renders go through the Photon C API of this library (SDL text -> phLoadCommands 
 phRender -> phAquireFrameRaw), exactly as a reference user would drive it. References:
 
 * images.npz -- renders of the same SDL by the reference's own EqualSamplingRenderer +
-  BNEEPTEstimator / BVPTEstimator (tests/golden/make_golden_images.py, 64 x 64, 4096-8192 spp),
+  BNEEPTEstimator / BVPTEstimator / BVPTDLEstimator (tests/golden/make_golden_images.py, 64 x 64,
+  4096-8192 spp),
   in the reference's default iterative surface refinement and, for two scenes, in its empirical
   and manual modes (the reference's EngineConfig.ini on its side, phGpuSetSurfaceRefine on ours).
   The bar is the north star's image tolerance: relMSE <= 1e-3, relMSE being the mean over pixels
   and channels of (x - ref)^2 / (ref^2 + 1e-2). Both images carry Monte Carlo noise, which the
-  bound includes. BNEEPT images meet it at full resolution; BVPT (no light sampling, a small
-  light) is noise-dominated at these sample counts, so it is held to the bar on 4 x 4 block means
+  bound includes. BNEEPT images meet it at full resolution; BVPT and BVPTDL (no light sampling, a
+  small light) are noise-dominated at these sample counts, so it is held to the bar on 4 x 4 block means
   (16 x fewer noise, same expectation) and to a looser full-resolution bound. The glossy scene's
   caustics through the glass box are noisy at any spp, so its GPU side renders 16384 spp: the
   relMSE of two independent renders is the sum of their variances, and this keeps the GPU's
@@ -38,6 +39,7 @@ IMAGES = os.path.join(GOLDEN, "images.npz")
 WORKLOADS = {
     "cornell_bneept": (lambda spp: scenes.cornell(64, 64, spp, 8, "bneept"), 4096),
     "cornell_bvpt": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvpt"), 4096),
+    "cornell_bvptdl": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvptdl"), 4096),
     "cornell_glossy_bneept": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 16384),
     "ggx_sphere_env_bneept": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
                                                             max_bounces=10), 4096),

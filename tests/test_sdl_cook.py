@@ -43,6 +43,7 @@ def test_bvpt_and_materials():
     c = _cook(scenes.to_sdl(s))
     assert c.estimator == 1
     assert c.num_materials == len(s.groups)
+    assert _cook(scenes.to_sdl(scenes.cornell(estimator="bvptdl"))).estimator == 2
 
 
 def test_streamed_fragments_equal_whole_text():
