@@ -333,7 +333,7 @@ def run_ours(args) -> None:
         barrier()
         e2e_s = max_over_ranks(e2e_s)
         e2e_value = world * paths_per_step * args.steps / e2e_s / 1e6
-        d2h = int(scene.width * scene.height * 3 * 8)   # FP64 film sums read back to develop the frame
+        d2h = int(scene.width * scene.height * 3 * 4)   # the frame developed on the GPU (float32 RGB) read back
         mean_rgb = frame.reshape(-1, 3).mean(0).tolist()
         eng.close()
 

@@ -160,9 +160,15 @@ PGPU_API int pgpu_scene_render(uint64_t id, uint32_t spp, uint32_t max_bounces, 
                                uint64_t seed, uint64_t first_sample, float* out_ms,
                                uint64_t* out_rays, uint64_t* out_shadow_rays);
 
-/* Developed frame (host float32 [h][w][3], row 0 = bottom, the reference's frame layout), the raw
- * FP64 sums (host double [h][w][3]) and the samples per pixel accumulated; any may be NULL. */
+/* Developed frame (host float32 [h][w][3], row 0 = bottom, the reference's frame layout: RGB / W
+ * per pixel), the raw FP64 sums (host double [h][w][4] = filter-weighted R, G, B and the weight W,
+ * the reference's RadianceSensor, Engine/Source/Core/Receiver/RadianceSensor.h:13-16) and the
+ * samples per pixel accumulated; any may be NULL. */
 PGPU_API int pgpu_scene_film(uint64_t id, float* out_rgb, double* out_sum, uint64_t* out_spp);
+/* Sample filter of the scene's film (HdrRgbFilm::addRgbSample with SampleFilter::make*,
+ * Engine/Source/Core/Filmic/HdrRgbFilm.cpp:82-123, SampleFilter.cpp:12-61): 0 box (the default
+ * here), 1 gaussian, 2 mitchell-netravali, 3 blackman-harris. Clears the film. */
+PGPU_API int pgpu_scene_set_filter(uint64_t id, uint32_t filter);
 /* A render into a scratch film with every kernel bracketed by CUDA events: per-kernel device
  * milliseconds (prepare, regen, extend, shade, shadow, guide inference, guide training). */
 PGPU_API int pgpu_scene_profile(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator,
@@ -187,8 +193,8 @@ PGPU_API int pgpu_scene_guide_info(uint64_t id, float* out_loss, uint64_t* out_g
  * Scene cooking without a GPU: parses SDL text (the grammar of the reference's SdlCommandParser,
  * Engine/Source/SDL/SdlCommandParser.cpp:84-560) and cooks it the way phUpdate does (actors to
  * world-space triangles, materials, emitters, camera). Call once with NULL arrays to get the
- * counts, then again with arrays of those sizes. out_dims: uint32 [4] = width, height, spp,
- * estimator. out_emitters: float32 [e][4] = radiance rgb, type. out_camera: float32 [16] =
+ * counts, then again with arrays of those sizes. out_dims: uint32 [5] = width, height, spp,
+ * estimator, sample filter (pgpu_scene_set_filter's numbering). out_emitters: float32 [e][4] = radiance rgb, type. out_camera: float32 [16] =
  * position, camera x/y/z axes, sensor width, height, offset (metres), dome area. */
 PGPU_API int pgpu_sdl_cook(const char* sdl_text, const char* working_dir, uint64_t* out_num_tris,
                            uint32_t* out_num_materials, uint32_t* out_num_emitters, uint32_t* out_dims,

@@ -982,6 +982,114 @@ void render(const Scene& s, uint32_t spp, uint32_t max_bounces, uint32_t threads
 	for(auto& t : pool) { t.join(); }
 }
 
+// Sample filters as the reference evaluates them, in FP64 (SampleFilter::make*, SampleFilter.cpp:
+// 12-61: box 1 px; gaussian sigma 0.5, size 4, submerged by its value at (2, 2)
+// (TGaussian2D.h); Mitchell-Netravali B = C = 1/3, size 4 (TMitchellNetravaliCubic2D.h:35-67);
+// Blackman-Harris radius 2 (TBlackmanHarris2D.h:42-62)). 0 box, 1 gaussian, 2 mn, 3 bh.
+double filter_half(int filter) { return filter == 0 ? 0.5 : 2.0; }
+
+double filter_eval(int filter, double x, double y)
+{
+	if(filter == 1)
+	{
+		auto g = [](double a, double b) { return std::exp(-2.0 * a * a + -2.0 * b * b); };
+		return std::max(g(x, y) - g(2.0, 2.0), 0.0);
+	}
+	if(filter == 2)
+	{
+		const double b = 1.0 / 3.0, c = 1.0 / 3.0;
+		auto mn = [&](double v)
+		{
+			const double a = std::abs(v);
+			if(a < 1) { return ((12 - 9 * b - 6 * c) * a * a * a + (-18 + 12 * b + 6 * c) * a * a + (6 - 2 * b)) / 6; }
+			if(a < 2) { return ((-b - 6 * c) * a * a * a + (6 * b + 30 * c) * a * a + (-12 * b - 48 * c) * a + (8 * b + 24 * c)) / 6; }
+			return 0.0;
+		};
+		return mn(x) * mn(y);
+	}
+	if(filter == 3)
+	{
+		auto bh = [](double v)
+		{
+			const double n = (v * 0.5 + 1.0) * 0.5;
+			return 0.35875 - 0.48829 * std::cos(2 * M_PI * n) + 0.14128 * std::cos(4 * M_PI * n) -
+			       0.01174 * std::cos(6 * M_PI * n);
+		};
+		return bh(x) * bh(y);
+	}
+	return 1.0;
+}
+
+// HdrRgbFilm::addRgbSample (HdrRgbFilm.cpp:82-123): the filter-weighted sample into every pixel
+// whose centre lies within the filter's half size, and the weight into W; film [h][w][4].
+void add_filtered_sample(double* film, uint32_t w, uint32_t h, int filter, double rx, double ry, const Rgb& e)
+{
+	const double half = filter_half(filter);
+	const double fx0 = std::max(rx - half, 0.0), fy0 = std::max(ry - half, 0.0);
+	const double fx1 = std::min(rx + half, static_cast<double>(w)), fy1 = std::min(ry + half, static_cast<double>(h));
+	const int64_t x0 = static_cast<int64_t>(std::ceil(fx0 - 0.5)), y0 = static_cast<int64_t>(std::ceil(fy0 - 0.5));
+	const int64_t x1 = static_cast<int64_t>(std::floor(fx1 - 0.5)) + 1, y1 = static_cast<int64_t>(std::floor(fy1 - 0.5)) + 1;
+	for(int64_t y = y0; y < y1; ++y)
+	{
+		for(int64_t x = x0; x < x1; ++x)
+		{
+			const double f = filter_eval(filter, x - (rx - 0.5), y - (ry - 0.5));
+			double* p = film + 4 * (static_cast<std::size_t>(y) * w + x);
+			p[0] += e.r * f;
+			p[1] += e.g * f;
+			p[2] += e.b * f;
+			p[3] += f;
+		}
+	}
+}
+
+// The render with a sample filter: samples spread uniformly over the film's sample window (the
+// pixel-centre rectangle grown by the filter's half size, TSamplingFilm.ipp:102-119), one cell of
+// it per pixel and sample, splatted into per-worker films that are summed at the end (the
+// reference's per-worker films merged into the main film).
+void render_filtered(const Scene& s, uint32_t spp, uint32_t max_bounces, uint32_t threads, uint64_t seed, int filter,
+                     double* sums)
+{
+	const uint32_t w = s.width, h = s.height;
+	const double half = filter_half(filter);
+	const double wx0 = 0.5 - half, wy0 = 0.5 - half;
+	const double cell_x = (w - 1 + 2 * half) / w, cell_y = (h - 1 + 2 * half) / h;
+	const uint32_t nt = std::max(1u, threads);
+	std::vector<std::vector<double>> films(nt, std::vector<double>(static_cast<std::size_t>(w) * h * 4, 0.0));
+	std::atomic<uint32_t> next_row{0};
+	auto worker = [&](uint32_t wid)
+	{
+		Pcg32 rng(seed * 0x9E3779B97F4A7C15ull + wid + 1, wid * 2 + 1);
+		double* film = films[wid].data();
+		for(;;)
+		{
+			const uint32_t y = next_row.fetch_add(1);
+			if(y >= h) { break; }
+			for(uint32_t x = 0; x < w; ++x)
+			{
+				for(uint32_t k = 0; k < spp; ++k)
+				{
+					const double rx = wx0 + (x + static_cast<double>(rng.u01())) * cell_x;
+					const double ry = wy0 + (y + static_cast<double>(rng.u01())) * cell_y;
+					const float sx = -s.sensor_w / w * static_cast<float>(rx) + s.sensor_w * 0.5f;
+					const float sy = -s.sensor_h / h * static_cast<float>(ry) + s.sensor_h * 0.5f;
+					const Vec recv = unit(s.ax * sx + s.ay * sy + s.az * s.sensor_offset);
+					const Rgb e = estimate(s, s.cam_pos, -recv, max_bounces, rng);
+					add_filtered_sample(film, w, h, filter, rx, ry, e);
+				}
+			}
+		}
+	};
+	std::vector<std::thread> pool;
+	for(uint32_t t = 0; t < nt; ++t) { pool.emplace_back(worker, t); }
+	for(auto& t : pool) { t.join(); }
+	std::fill(sums, sums + static_cast<std::size_t>(w) * h * 4, 0.0);
+	for(const auto& f : films)
+	{
+		for(std::size_t i = 0; i < f.size(); ++i) { sums[i] += f[i]; }
+	}
+}
+
 }// end anonymous namespace
 
 extern "C" {
@@ -1055,6 +1163,22 @@ int port_render(const float* tris, const uint32_t* tri_material, const uint32_t*
 	}
 	s.estimator = estimator;
 	render(s, spp, max_bounces, threads, seed, out_sums);
+	return 0;
+}
+
+// The same with a sample filter (0 box, 1 gaussian, 2 mn, 3 bh): FP64 sums [h][w][4] = R, G, B, W.
+int port_render_filtered(const float* tris, const uint32_t* tri_material, const uint32_t* tri_emitter, uint32_t num_tris,
+                         const float* materials, uint32_t num_materials, const float* emitters, uint32_t num_emitters,
+                         const float* camera, uint32_t spp, uint32_t max_bounces, uint32_t estimator, uint32_t threads,
+                         uint64_t seed, uint32_t filter, double* out_sums)
+{
+	Scene s;
+	if(filter > 3 || !setup_scene(s, camera, tris, tri_material, tri_emitter, num_tris, materials, num_materials, emitters, num_emitters))
+	{
+		return 1;
+	}
+	s.estimator = estimator;
+	render_filtered(s, spp, max_bounces, threads, seed, static_cast<int>(filter), out_sums);
 	return 0;
 }
 

@@ -50,21 +50,35 @@ def bsdf(cases, normals):
     return out
 
 
-def render(flat_scene, spp, max_bounces, estimator=0, threads=None, seed=1):
-    """Renders the flat scene arrays of photon_gpu.flatten_scene; returns float32 [H, W, 3]."""
+FILTERS = {"box": 0, "gaussian": 1, "mn": 2, "bh": 3}
+
+
+def render(flat_scene, spp, max_bounces, estimator=0, threads=None, seed=1, sample_filter=None):
+    """Renders the flat scene arrays of photon_gpu.flatten_scene; returns float32 [H, W, 3].
+
+    Without `sample_filter` every pixel averages its own samples (box filter); with one of
+    FILTERS the samples are splatted through that filter into an (R, G, B, W) film."""
     tris, tri_mat, tri_em, mats, ems, cam = flat_scene
     w, h = int(cam[10]), int(cam[11])
-    sums = np.zeros((h, w, 3), np.float64)
     threads = threads or (os.cpu_count() or 1)
     ems = np.ascontiguousarray(ems, np.float32)
-    status = load().port_render(
+    args = [
         _p(np.ascontiguousarray(tris, np.float32), ctypes.c_float), _p(np.ascontiguousarray(tri_mat, np.uint32), ctypes.c_uint32),
         _p(np.ascontiguousarray(tri_em, np.uint32), ctypes.c_uint32), ctypes.c_uint32(tris.shape[0]),
         _p(np.ascontiguousarray(mats, np.float32), ctypes.c_float), ctypes.c_uint32(mats.shape[0]),
         _p(ems, ctypes.c_float) if ems.size else None, ctypes.c_uint32(ems.shape[0]),
         _p(np.ascontiguousarray(cam, np.float32), ctypes.c_float), ctypes.c_uint32(spp),
         ctypes.c_uint32(max_bounces), ctypes.c_uint32(estimator), ctypes.c_uint32(threads),
-        ctypes.c_uint64(seed), _p(sums, ctypes.c_double))
+        ctypes.c_uint64(seed)]
+    if sample_filter is not None:
+        sums = np.zeros((h, w, 4), np.float64)
+        status = load().port_render_filtered(*args, ctypes.c_uint32(FILTERS[sample_filter]), _p(sums, ctypes.c_double))
+        if status != 0:
+            raise RuntimeError("port_render_filtered failed")
+        wsum = sums[..., 3:4]
+        return (sums[..., :3] / np.where(wsum != 0, wsum, 1.0) * (wsum != 0)).astype(np.float32)
+    sums = np.zeros((h, w, 3), np.float64)
+    status = load().port_render(*args, _p(sums, ctypes.c_double))
     if status != 0:
         raise RuntimeError("port_render failed")
     return (sums / spp).astype(np.float32)

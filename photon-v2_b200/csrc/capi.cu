@@ -561,6 +561,7 @@ int pgpu_sdl_cook(const char* sdl_text, const char* working_dir, uint64_t* out_n
 			e.get_render_dimension(&out_dims[0], &out_dims[1]);
 			out_dims[2] = e.spp();
 			out_dims[3] = e.estimator();
+			out_dims[4] = e.sample_filter();
 		}
 		if(out_tris) { std::memcpy(out_tris, d.tris.data(), d.tris.size() * sizeof(float)); }
 		if(out_tri_material) { std::memcpy(out_tri_material, d.tri_material.data(), n * sizeof(uint32_t)); }

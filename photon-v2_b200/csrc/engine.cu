@@ -252,6 +252,7 @@ void Engine::update()
 		desc.bvh_builder = m_bvh_builder;
 		m_info.num_triangles = desc.tris.size() / 9;
 		m_render = make_render_object(std::move(desc));
+		m_render->filter = m_filter;
 	}
 	catch(const std::exception& e)
 	{
@@ -329,6 +330,7 @@ void Engine::cook(SceneDesc& desc)
 		}
 		m_spp = sampler ? static_cast<uint32_t>(get_real(sampler->clauses, "samples", 1.0)) : 1u;
 		m_estimator = PG_EST_BNEEPT;
+		m_filter = PG_FILTER_BLACKMAN_HARRIS;
 		if(visualizer)
 		{
 			if(visualizer->type != "path-tracing")
@@ -343,12 +345,16 @@ void Engine::cook(SceneDesc& desc)
 				else if(e == "bvptdl") { m_estimator = PG_EST_BVPTDL; }
 				else { throw std::runtime_error("estimator " + est->value + " is not supported by the GPU renderer"); }
 			}
+			// sample-filter: box | gaussian | mn | bh, Blackman-Harris when absent
+			// (sdl_sample_filter_type.h:18-38, PathTracingVisualizer.h:59-61)
 			if(const SdlClause* f = find(visualizer->clauses, "sample-filter"))
 			{
-				if(lower(f->value) != "box")
-				{
-					record_error("sample-filter " + f->value + " rendered with the box filter (only box is implemented)");
-				}
+				const std::string v = lower(f->value);
+				if(v == "box") { m_filter = PG_FILTER_BOX; }
+				else if(v == "gaussian") { m_filter = PG_FILTER_GAUSSIAN; }
+				else if(v == "mn") { m_filter = PG_FILTER_MITCHELL_NETRAVALI; }
+				else if(v == "bh" || v.empty()) { m_filter = PG_FILTER_BLACKMAN_HARRIS; }
+				else { throw std::runtime_error("unknown sample-filter " + f->value); }
 			}
 		}
 
@@ -776,6 +782,7 @@ void Engine::render()
 			p.spp = n;
 			p.max_bounces = m_max_bounces;
 			p.estimator = m_estimator;
+			p.filter = m_render->filter;
 			p.refine_mode = m_refine.refine_mode;
 			p.refine_delta = m_refine.refine_delta;
 			p.refine_iters = m_refine.refine_iters;
@@ -808,7 +815,7 @@ void Engine::profile(uint32_t mode, uint32_t spp, double out_stats[14])
 	{
 		throw std::runtime_error("profile: the scene was not updated successfully");
 	}
-	DeviceBuffer<double> scratch(static_cast<std::size_t>(m_width) * m_height * 3);
+	DeviceBuffer<double> scratch(static_cast<std::size_t>(m_width) * m_height * kFilmChannels);
 	PG_CUDA_CHECK(cudaMemsetAsync(scratch.get(), 0, scratch.bytes(), library_stream()));
 	RenderParams p;
 	p.width = m_width;
@@ -816,6 +823,7 @@ void Engine::profile(uint32_t mode, uint32_t spp, double out_stats[14])
 	p.spp = spp;
 	p.max_bounces = m_max_bounces;
 	p.estimator = m_estimator;
+	p.filter = m_render->filter;
 	p.refine_mode = m_refine.refine_mode;
 	p.refine_delta = m_refine.refine_delta;
 	p.refine_iters = m_refine.refine_iters;
@@ -859,9 +867,8 @@ void Engine::peek_frame(uint32_t x, uint32_t y, uint32_t w, uint32_t h, HdrFrame
 	{
 		return;
 	}
-	std::vector<double> sums(static_cast<std::size_t>(m_width) * m_height * 3);
-	download_film(*m_render, sums.data());
-	if(frame.width != m_width || frame.height != m_height || frame.rgb.size() != sums.size())
+	const std::size_t pixels = static_cast<std::size_t>(m_width) * m_height;
+	if(frame.width != m_width || frame.height != m_height || frame.rgb.size() != pixels * 3)
 	{
 		if(frame.width != 0 && (frame.width != m_width || frame.height != m_height))
 		{
@@ -870,21 +877,9 @@ void Engine::peek_frame(uint32_t x, uint32_t y, uint32_t w, uint32_t h, HdrFrame
 		}
 		frame.width = m_width;
 		frame.height = m_height;
-		frame.rgb.assign(sums.size(), 0.0f);
+		frame.rgb.assign(pixels * 3, 0.0f);
 	}
-	const double rcp = m_render->samples > 0 ? 1.0 / static_cast<double>(m_render->samples) : 0.0;
-	const uint32_t x1 = std::min(m_width, x + w), y1 = std::min(m_height, y + h);
-	for(uint32_t yy = y; yy < y1; ++yy)
-	{
-		for(uint32_t xx = x; xx < x1; ++xx)
-		{
-			const std::size_t i = (static_cast<std::size_t>(yy) * m_width + xx) * 3;
-			for(int c = 0; c < 3; ++c)
-			{
-				frame.rgb[i + c] = static_cast<float>(sums[i + c] * rcp);
-			}
-		}
-	}
+	develop_frame(*m_render, frame.rgb.data(), x, y, w, h);
 }
 
 void Engine::get_progress(uint64_t* total, uint64_t* done, uint64_t* elapsed_ms) const

@@ -7,6 +7,7 @@
 // film on retrieval.
 #pragma once
 
+#include "film.cuh"
 #include "sdl.h"
 
 #include <atomic>
@@ -73,6 +74,7 @@ public:
 	void cook(SceneDesc& out);
 	uint32_t spp() const { return m_spp; }
 	uint32_t estimator() const { return m_estimator; }
+	uint32_t sample_filter() const { return m_filter; }
 	// Renders all samples of the current scene (phRender).
 	void render();
 
@@ -133,6 +135,7 @@ private:
 	uint32_t m_width = 0, m_height = 0;
 	uint32_t m_spp = 0;
 	uint32_t m_estimator = 0;
+	uint32_t m_filter = PG_FILTER_BLACKMAN_HARRIS;   // the path-tracing visualizer's default
 
 	RenderInfo m_info;
 	uint64_t m_launches = 0;

@@ -57,15 +57,54 @@ std::unique_ptr<RenderObject> make_render_object(SceneDesc&& desc)
 	obj->scene = std::make_unique<RenderScene>(desc, max_abs);
 	obj->width = desc.camera.width;
 	obj->height = desc.camera.height;
-	obj->film.resize(static_cast<std::size_t>(obj->width) * obj->height * 3);
+	obj->film.resize(static_cast<std::size_t>(obj->width) * obj->height * kFilmChannels);
 	PG_CUDA_CHECK(cudaMemsetAsync(obj->film.get(), 0, obj->film.bytes(), library_stream()));
 	PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
 	return obj;
 }
 
+namespace
+{
+
+// RGB / W per pixel in FP64, rounded once to FP32; 0 where W is 0
+// (HdrRgbFilm::developRegion, Engine/Source/Core/Filmic/HdrRgbFilm.cpp:167-205).
+__global__ void develop_kernel(const double* __restrict__ sums, float* __restrict__ rgb, uint32_t num_pixels)
+{
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < num_pixels; i += gridDim.x * blockDim.x)
+	{
+		const double4 s = reinterpret_cast<const double4*>(sums)[i];
+		const double rcp = s.w == 0.0 ? 0.0 : 1.0 / s.w;
+		rgb[3 * static_cast<size_t>(i) + 0] = static_cast<float>(s.x * rcp);
+		rgb[3 * static_cast<size_t>(i) + 1] = static_cast<float>(s.y * rcp);
+		rgb[3 * static_cast<size_t>(i) + 2] = static_cast<float>(s.z * rcp);
+	}
+}
+
+}// end anonymous namespace
+
+void develop_frame(const RenderObject& r, float* out_rgb, uint32_t x, uint32_t y, uint32_t w, uint32_t h)
+{
+	const uint32_t pixels = r.width * r.height;
+	if(x >= r.width || y >= r.height || w == 0 || h == 0)
+	{
+		return;
+	}
+	w = std::min(w, r.width - x);
+	h = std::min(h, r.height - y);
+	r.frame.resize(static_cast<std::size_t>(pixels) * 3);
+	cudaStream_t st = library_stream();
+	develop_kernel<<<sm_count() * 4, 256, 0, st>>>(r.film.get(), r.frame.get(), pixels);
+	PG_CUDA_CHECK(cudaGetLastError());
+	const std::size_t pitch = static_cast<std::size_t>(r.width) * 3 * sizeof(float);
+	const std::size_t offset = (static_cast<std::size_t>(y) * r.width + x) * 3;
+	PG_CUDA_CHECK(cudaMemcpy2DAsync(out_rgb + offset, pitch, r.frame.get() + offset, pitch,
+	                                static_cast<std::size_t>(w) * 3 * sizeof(float), h, cudaMemcpyDeviceToHost, st));
+	PG_CUDA_CHECK(cudaStreamSynchronize(st));
+}
+
 void download_film(const RenderObject& r, double* out_sum)
 {
-	const std::size_t n = static_cast<std::size_t>(r.width) * r.height * 3;
+	const std::size_t n = static_cast<std::size_t>(r.width) * r.height * kFilmChannels;
 	PG_CUDA_CHECK(cudaMemcpyAsync(out_sum, r.film.get(), n * sizeof(double), cudaMemcpyDeviceToHost, library_stream()));
 	PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
 }
@@ -186,6 +225,7 @@ int pgpu_scene_render(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t 
 		p.spp = spp;
 		p.max_bounces = max_bounces;
 		p.estimator = estimator;
+		p.filter = r->filter;
 		p.seed = seed;
 		p.first_sample = first_sample;
 		const float ms = r->scene->render(p, r->film.get());
@@ -213,9 +253,10 @@ int pgpu_scene_profile(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t
 		p.spp = spp;
 		p.max_bounces = max_bounces;
 		p.estimator = estimator;
+		p.filter = r->filter;
 		p.seed = seed;
 		p.mode = PG_RENDER_TIMING;
-		DeviceBuffer<double> scratch(static_cast<std::size_t>(r->width) * r->height * 3);
+		DeviceBuffer<double> scratch(static_cast<std::size_t>(r->width) * r->height * kFilmChannels);
 		PG_CUDA_CHECK(cudaMemsetAsync(scratch.get(), 0, scratch.bytes(), library_stream()));
 		r->scene->render(p, scratch.get());
 		if(out_kernel_ms)
@@ -233,25 +274,31 @@ int pgpu_scene_film(uint64_t id, float* out_rgb, double* out_sum, uint64_t* out_
 	return guarded([&]
 	{
 		auto r = get_render(id);
-		const std::size_t n = static_cast<std::size_t>(r->width) * r->height * 3;
-		std::vector<double> sum(n);
-		PG_CUDA_CHECK(cudaMemcpyAsync(sum.data(), r->film.get(), n * sizeof(double), cudaMemcpyDeviceToHost, library_stream()));
-		PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
 		if(out_sum)
 		{
-			std::copy(sum.begin(), sum.end(), out_sum);
+			download_film(*r, out_sum);
 		}
 		if(out_rgb)
 		{
-			// develop: per-pixel weighted mean; the box filter gives every sample weight 1
-			// (HdrRgbFilm::developRegion, Engine/Source/Core/Filmic/HdrRgbFilm.cpp:167-205)
-			const double rcp = r->samples > 0 ? 1.0 / static_cast<double>(r->samples) : 0.0;
-			for(std::size_t i = 0; i < n; ++i)
-			{
-				out_rgb[i] = static_cast<float>(sum[i] * rcp);
-			}
+			develop_frame(*r, out_rgb, 0, 0, r->width, r->height);
 		}
 		if(out_spp) { *out_spp = r->samples; }
+	});
+}
+
+int pgpu_scene_set_filter(uint64_t id, uint32_t filter)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		if(filter > PG_FILTER_BLACKMAN_HARRIS)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_set_filter: unknown sample filter");
+		}
+		r->filter = filter;
+		PG_CUDA_CHECK(cudaMemsetAsync(r->film.get(), 0, r->film.bytes(), library_stream()));
+		PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
+		r->samples = 0;
 	});
 }
 

@@ -126,11 +126,37 @@ __device__ __forceinline__ uint32_t alias_pick(const float2* alias, uint32_t n, 
 	return frac < a.x ? i : __float_as_uint(a.y);
 }
 
-__device__ __forceinline__ void splat(double* film, uint32_t pixel, RGB c)
+// Raster position of a path's camera sample: a uniform point in its pixel's cell of the film's
+// sample window (film.cuh).
+__device__ __forceinline__ float2 raster_position(const FilmView& f, uint32_t pixel, const PathRng& rng)
 {
-	if(c.r != 0.0f) { atomicAdd(&film[3 * pixel + 0], static_cast<double>(c.r)); }
-	if(c.g != 0.0f) { atomicAdd(&film[3 * pixel + 1], static_cast<double>(c.g)); }
-	if(c.b != 0.0f) { atomicAdd(&film[3 * pixel + 2], static_cast<double>(c.b)); }
+	const uint32_t x = pixel % f.width;
+	const uint32_t y = pixel / f.width;
+	return make_float2(f.x0 + (static_cast<float>(x) + rng.u01(0, DIM_CAM_X)) * f.sx,
+	                   f.y0 + (static_cast<float>(y) + rng.u01(0, DIM_CAM_Y)) * f.sy);
+}
+
+// Radiance of a finished path (or a part of it) into the film.
+__device__ __forceinline__ void splat(const FilmView& f, uint32_t pixel, const PathRng& rng, RGB c)
+{
+	if(f.filter == PG_FILTER_BOX)
+	{
+		film_add_box(f, pixel, c.r, c.g, c.b);
+	}
+	else if(!is_zero(c))
+	{
+		const float2 r = raster_position(f, pixel, rng);
+		film_deposit(f, r.x, r.y, make_float4(c.r, c.g, c.b, 0.0f));
+	}
+}
+
+// Box filter: every pixel received spp samples of weight 1.
+__global__ void box_weights_kernel(double* sums, uint32_t num_pixels, double spp)
+{
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < num_pixels; i += gridDim.x * blockDim.x)
+	{
+		sums[static_cast<size_t>(i) * kFilmChannels + 3] += spp;
+	}
 }
 
 // Warp-aggregated slot allocation on a queue counter.
@@ -175,8 +201,8 @@ __global__ void prepare_kernel(RenderCounters* c, uint32_t capacity)
 // Camera rays of new paths into the tail of the current queue
 // (PinholeCamera::receiveRay, then BNEEPTEstimator.cpp:63-64: reversed, range [0, max]).
 __global__ void __launch_bounds__(kShadeBlock)
-regen_kernel(const RenderCounters* __restrict__ c, Camera cam, uint64_t seed, uint64_t first_global,
-             PathBuffers cur)
+regen_kernel(const RenderCounters* __restrict__ c, Camera cam, FilmView film, uint64_t seed,
+             uint64_t first_global, PathBuffers cur)
 {
 	const uint32_t active = c->n_active;
 	const uint32_t total = c->n_total;
@@ -186,11 +212,14 @@ regen_kernel(const RenderCounters* __restrict__ c, Camera cam, uint64_t seed, ui
 	{
 		const uint32_t p = static_cast<uint32_t>(base + (i - active));
 		const uint32_t pixel = p % wh;
-		const uint32_t x = pixel % cam.width;
-		const uint32_t y = pixel / cam.width;
 		const PathRng rng = make_rng(seed, first_global + p);
-		const float rx = static_cast<float>(x) + rng.u01(0, DIM_CAM_X);
-		const float ry = static_cast<float>(y) + rng.u01(0, DIM_CAM_Y);
+		const float2 raster = raster_position(film, pixel, rng);
+		const float rx = raster.x;
+		const float ry = raster.y;
+		if(film.filter != PG_FILTER_BOX)
+		{
+			film_deposit(film, rx, ry, make_float4(0.0f, 0.0f, 0.0f, 1.0f));   // the sample's filter weights
+		}
 
 		// raster -> sensor (SingleLensObserver::makeRasterToSensor)
 		const float sx = -cam.sensor_w / static_cast<float>(cam.width) * rx + cam.sensor_w * 0.5f;
@@ -307,7 +336,7 @@ struct ShadeArgs
 	const uint2*  hits;
 	ShadowQueue   shadow;
 	RenderCounters* counters;
-	double*       film;
+	FilmView      film;
 	uint64_t      seed;
 	uint64_t      first_global;
 	uint32_t      max_bounces;
@@ -409,7 +438,7 @@ shade_kernel(ShadeArgs a)
 					radiance = radiance + le * safe_clamp(thr_emit, 0.0f, kClampMax);
 				}
 			}
-			splat(a.film, pixel, radiance);
+			splat(a.film, pixel, rng, radiance);
 			continue;
 		}
 
@@ -427,7 +456,7 @@ shade_kernel(ShadeArgs a)
 		// traceNextSurface rejects hits whose sidedness disagrees (SurfaceTracer.h:126-141).
 		if(!(dot(ng, d) * dot(frame.ns, d) > 0.0f))
 		{
-			splat(a.film, pixel, radiance);
+			splat(a.film, pixel, rng, radiance);
 			continue;
 		}
 
@@ -475,7 +504,7 @@ shade_kernel(ShadeArgs a)
 		// ---- does the path continue past this vertex?
 		if((meta & kMetaStopAfter) || bounce >= a.max_bounces)
 		{
-			splat(a.film, pixel, radiance);
+			splat(a.film, pixel, rng, radiance);
 			continue;
 		}
 		const RGB throughput = thr_emit * cont;
@@ -690,7 +719,7 @@ shade_kernel(ShadeArgs a)
 		}
 		else
 		{
-			splat(a.film, pixel, radiance);
+			splat(a.film, pixel, rng, radiance);
 		}
 
 		if(has_shadow)
@@ -703,6 +732,10 @@ shade_kernel(ShadeArgs a)
 			if(GUIDED && a.shadow.t)
 			{
 				a.shadow.t[k] = make_float2(__uint_as_float(train_row), sh_train);
+			}
+			if(!continues && a.film.filter != PG_FILTER_BOX)
+			{
+				a.shadow.r[k] = raster_position(a.film, pixel, rng);
 			}
 		}
 	}
@@ -891,7 +924,17 @@ RenderScene::RenderScene(const SceneDesc& desc, float max_origin_abs)
 	m_dev.cam = desc.camera;
 }
 
-RenderScene::~RenderScene() = default;
+RenderScene::~RenderScene()
+{
+	if(m_exec)
+	{
+		cudaGraphExecDestroy(m_exec);
+	}
+	if(m_host_counters)
+	{
+		cudaFreeHost(m_host_counters);
+	}
+}
 
 void RenderScene::ensure_capacity(uint32_t capacity)
 {
@@ -913,6 +956,7 @@ void RenderScene::ensure_capacity(uint32_t capacity)
 	m_so.resize(capacity);
 	m_sd.resize(capacity);
 	m_sc.resize(capacity);
+	m_sr.resize(capacity);
 	m_capacity = capacity;
 }
 
@@ -1004,7 +1048,7 @@ void RenderScene::guide_params(float* out) const
 	PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
 }
 
-float RenderScene::render(const RenderParams& params, double* film)
+float RenderScene::render(const RenderParams& params, double* film_sums)
 {
 	if(params.width == 0 || params.height == 0 || params.spp == 0)
 	{
@@ -1037,6 +1081,8 @@ float RenderScene::render(const RenderParams& params, double* film)
 		                     m_prev[b].get(), m_ro[b].get(), m_rd[b].get()};
 	}
 	ShadowQueue sq{m_so.get(), m_sd.get(), m_sc.get()};
+	sq.r = m_sr.get();
+	const FilmView film = make_film_view(film_sums, params.width, params.height, params.filter);
 	const uint64_t first_global = params.first_sample * wh;
 	const bool counting = params.mode == PG_RENDER_COUNT;
 	// BVPTDL follows one BSDF-sampled bounce whatever the configured depth (BVPTDLEstimator.cpp:62-95)
@@ -1082,7 +1128,7 @@ float RenderScene::render(const RenderParams& params, double* film)
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[0], st)); }
 		prepare_kernel<<<1, 32, 0, st>>>(m_counters.get(), capacity);
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[1], st)); }
-		regen_kernel<<<grid, kShadeBlock, 0, st>>>(m_counters.get(), m_dev.cam, params.seed, first_global, cur);
+		regen_kernel<<<grid, kShadeBlock, 0, st>>>(m_counters.get(), m_dev.cam, film, params.seed, first_global, cur);
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[2], st)); }
 		launch_extend(m_dev, m_counters.get(), cur.ray_o, cur.ray_d, m_hits.get(), grid, 128, st, counting);
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[3], st)); }
@@ -1131,8 +1177,21 @@ float RenderScene::render(const RenderParams& params, double* film)
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[7], st)); }
 	};
 
-	RenderCounters* host_counters = nullptr;
-	PG_CUDA_CHECK(cudaMallocHost(&host_counters, sizeof(RenderCounters)));
+	// the box filter's W: spp per pixel, added once (film.cuh)
+	auto add_box_weights = [&]
+	{
+		if(params.filter == PG_FILTER_BOX)
+		{
+			box_weights_kernel<<<sms * 4, 256, 0, st>>>(film_sums, static_cast<uint32_t>(wh), static_cast<double>(params.spp));
+			PG_CUDA_CHECK(cudaGetLastError());
+		}
+	};
+
+	if(!m_host_counters)
+	{
+		PG_CUDA_CHECK(cudaMallocHost(&m_host_counters, sizeof(RenderCounters)));
+	}
+	RenderCounters* const host_counters = m_host_counters;
 	cudaEvent_t e0, e1;
 	PG_CUDA_CHECK(cudaEventCreate(&e0));
 	PG_CUDA_CHECK(cudaEventCreate(&e1));
@@ -1143,15 +1202,40 @@ float RenderScene::render(const RenderParams& params, double* film)
 
 	if(params.mode == PG_RENDER_GRAPH)
 	{
-		// One graph = two iterations (ping -> pong -> ping).
+		// One graph = two iterations (ping -> pong -> ping). The launch sequence only depends on
+		// whether guiding and training run, so the executable graph of the previous render is
+		// updated with this render's kernel arguments and instantiated again only when its
+		// topology changed.
 		cudaGraph_t graph;
-		cudaGraphExec_t exec;
 		PG_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
 		iteration(0, nullptr);
 		iteration(1, nullptr);
 		PG_CUDA_CHECK(cudaStreamEndCapture(st, &graph));
-		PG_CUDA_CHECK(cudaGraphInstantiate(&exec, graph, 0));
+		const int key = (guided ? 1 : 0) | (training ? 2 : 0);
+		bool updated = false;
+		if(m_exec && m_exec_key == key)
+		{
+			cudaGraphExecUpdateResultInfo info;
+			updated = cudaGraphExecUpdate(m_exec, graph, &info) == cudaSuccess;
+			if(!updated)
+			{
+				(void)cudaGetLastError();   // a failed update is not sticky; instantiate anew
+			}
+		}
+		if(!updated)
+		{
+			if(m_exec)
+			{
+				PG_CUDA_CHECK(cudaGraphExecDestroy(m_exec));
+				m_exec = nullptr;
+			}
+			PG_CUDA_CHECK(cudaGraphInstantiate(&m_exec, graph, 0));
+			m_exec_key = key;
+		}
+		PG_CUDA_CHECK(cudaGraphDestroy(graph));
+		cudaGraphExec_t exec = m_exec;
 		PG_CUDA_CHECK(cudaEventRecord(e0, st));
+		add_box_weights();
 		int batch = 4;
 		while(!done && iterations < max_iterations)
 		{
@@ -1171,8 +1255,6 @@ float RenderScene::render(const RenderParams& params, double* film)
 		}
 		PG_CUDA_CHECK(cudaEventRecord(e1, st));
 		PG_CUDA_CHECK(cudaEventSynchronize(e1));
-		cudaGraphExecDestroy(exec);
-		cudaGraphDestroy(graph);
 	}
 	else
 	{
@@ -1182,6 +1264,7 @@ float RenderScene::render(const RenderParams& params, double* film)
 		const bool timing = params.mode == PG_RENDER_TIMING;
 		for(cudaEvent_t& e : ev) { PG_CUDA_CHECK(cudaEventCreate(&e)); }
 		PG_CUDA_CHECK(cudaEventRecord(e0, st));
+		add_box_weights();
 		int b = 0;
 		while(!done && iterations < max_iterations)
 		{
@@ -1217,7 +1300,6 @@ float RenderScene::render(const RenderParams& params, double* film)
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	const RenderCounters final_counters = *host_counters;
-	cudaFreeHost(host_counters);
 
 	m_last_rays = final_counters.rays_traced;
 	m_last_shadow = final_counters.shadow_rays;

@@ -14,6 +14,7 @@
 #pragma once
 
 #include "bsdf.cuh"
+#include "film.cuh"
 #include "pg_common.cuh"
 #include "pg_geometry.h"
 
@@ -73,6 +74,7 @@ struct RenderParams
 	uint32_t spp = 1;
 	uint32_t max_bounces = 10000;       // MAX_RAY_BOUNCES of the reference estimators
 	uint32_t estimator = PG_EST_BNEEPT;
+	uint32_t filter = PG_FILTER_BOX;    // SampleFilterType of the film being rendered into
 	uint64_t seed = 42;
 	uint64_t first_sample = 0;          // sample index offset (resume / replicas)
 	uint32_t capacity = 1u << 21;       // path slots in flight
@@ -175,6 +177,7 @@ struct ShadowQueue
 	float4* d;          // direction, tmax
 	float4* c;          // contribution rgb, target (slot in next buffer, or 0x80000000|pixel)
 	float2* t;          // guided renders: training sample index (bits, or ~0), weight added if unoccluded
+	float2* r;          // filtered films: raster position of the sample a final contribution belongs to
 };
 
 // Device view of the guiding buffers for one render iteration.
@@ -201,7 +204,7 @@ constexpr uint32_t kTargetFinal = 0x80000000u;
 void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4* ray_o,
                    const float4* ray_d, uint2* hits, int grid, int block, cudaStream_t st, bool count);
 void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
-                   float4* rad_next, double* film, int grid, int block, cudaStream_t st, bool count,
+                   float4* rad_next, const FilmView& film, int grid, int block, cudaStream_t st, bool count,
                    float4* train_dirw = nullptr);
 
 // A scene resident on the GPU together with its render buffers.
@@ -211,8 +214,8 @@ public:
 	explicit RenderScene(const SceneDesc& desc, float max_origin_abs);
 	~RenderScene();
 
-	// Renders `params` and accumulates into the FP64 film (sum of RGB per pixel). Returns the
-	// device time of the render in milliseconds (CUDA events on the library stream).
+	// Renders `params` and accumulates into the FP64 film (R, G, B, W sums per pixel, film.cuh).
+	// Returns the device time of the render in milliseconds (CUDA events on the library stream).
 	float render(const RenderParams& params, double* film_device);
 
 	const DeviceScene& device() const { return m_dev; }
@@ -254,6 +257,7 @@ private:
 	DeviceBuffer<float4>   m_thr[2], m_rad[2], m_prev[2], m_ro[2], m_rd[2];
 	DeviceBuffer<uint2>    m_hits;
 	DeviceBuffer<float4>   m_so, m_sd, m_sc;
+	DeviceBuffer<float2>   m_sr;
 	DeviceBuffer<RenderCounters> m_counters;
 
 	// learned guiding
@@ -273,6 +277,12 @@ private:
 	DeviceBuffer<uint32_t> m_gstep, m_gerr;
 	float m_last_guide_loss = 0.0f;
 	unsigned long long m_last_guided = 0;
+
+	// pinned readback of the counters, and the instantiated two-iteration graph of the last
+	// render (kept across renders and updated in place when only kernel arguments change)
+	RenderCounters* m_host_counters = nullptr;
+	cudaGraphExec_t m_exec = nullptr;
+	int m_exec_key = -1;
 
 	unsigned long long m_last_rays = 0, m_last_shadow = 0, m_last_iterations = 0;
 	unsigned long long m_last_counts[4] = {0, 0, 0, 0};

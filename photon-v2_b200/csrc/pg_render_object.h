@@ -9,7 +9,9 @@ namespace pg
 struct RenderObject
 {
 	std::unique_ptr<RenderScene> scene;
-	DeviceBuffer<double> film;      // [h][w][3] sums of sample radiance
+	DeviceBuffer<double> film;      // [h][w][4] sums of filter-weighted radiance and weight (film.cuh)
+	uint32_t filter = PG_FILTER_BOX;
+	mutable DeviceBuffer<float> frame;   // [h][w][3] developed frame (develop_frame)
 	uint32_t width = 0, height = 0;
 	uint64_t samples = 0;           // samples per pixel accumulated in the film
 	float last_ms = 0.0f;
@@ -18,7 +20,13 @@ struct RenderObject
 // Builds the BVH, uploads the scene and allocates a cleared film.
 std::unique_ptr<RenderObject> make_render_object(SceneDesc&& desc);
 
-// Copies the film sums to the host (double [h][w][3]).
+// Copies the film sums to the host (double [h][w][4]).
 void download_film(const RenderObject& r, double* out_sum);
+
+// Develops the film on the GPU and copies the rectangle [x, x + w) x [y, y + h) of the developed
+// frame into `out_rgb`, a host frame of the film's full size (float [height][width][3]); pixels
+// outside the rectangle are left untouched.
+void develop_frame(const RenderObject& r, float* out_rgb, uint32_t x, uint32_t y, uint32_t w, uint32_t h);
+
 
 }// end namespace pg

@@ -218,8 +218,8 @@ __global__ void __launch_bounds__(kTraceBlock)
 shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
               RenderCounters* __restrict__ counters,
               const float4* __restrict__ so, const float4* __restrict__ sd, const float4* __restrict__ sc,
-              const float2* __restrict__ st, float4* __restrict__ rad_next, double* __restrict__ film,
-              float4* __restrict__ train_dirw)
+              const float2* __restrict__ st, const float2* __restrict__ sr, float4* __restrict__ rad_next,
+              FilmView film, float4* __restrict__ train_dirw)
 {
 	const uint32_t n = counters->n_shadow;
 	if(blockIdx.x == 0 && threadIdx.x == 0)
@@ -249,10 +249,15 @@ shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tr
 			const uint32_t target = __float_as_uint(c.w);
 			if(target & kTargetFinal)
 			{
-				const uint32_t pixel = target & ~kTargetFinal;
-				if(c.x != 0.0f) { atomicAdd(&film[3 * pixel + 0], static_cast<double>(c.x)); }
-				if(c.y != 0.0f) { atomicAdd(&film[3 * pixel + 1], static_cast<double>(c.y)); }
-				if(c.z != 0.0f) { atomicAdd(&film[3 * pixel + 2], static_cast<double>(c.z)); }
+				if(film.filter == PG_FILTER_BOX)
+				{
+					film_add_box(film, target & ~kTargetFinal, c.x, c.y, c.z);
+				}
+				else
+				{
+					const float2 r = __ldg(sr + i);
+					film_deposit(film, r.x, r.y, make_float4(c.x, c.y, c.z, 0.0f));
+				}
 			}
 			else
 			{
@@ -294,19 +299,19 @@ void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4*
 }
 
 void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
-                   float4* rad_next, double* film, int, int, cudaStream_t st, bool count, float4* train_dirw)
+                   float4* rad_next, const FilmView& film, int, int, cudaStream_t st, bool count, float4* train_dirw)
 {
 	if(count)
 	{
 		static const int grid = persistent_grid(shadow_kernel<true>);
-		shadow_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, q.t, rad_next,
-		                                                  film, train_dirw);
+		shadow_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, q.t, q.r,
+		                                                  rad_next, film, train_dirw);
 	}
 	else
 	{
 		static const int grid = persistent_grid(shadow_kernel<false>);
-		shadow_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, q.t, rad_next,
-		                                                   film, train_dirw);
+		shadow_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, q.t, q.r,
+		                                                   rad_next, film, train_dirw);
 	}
 	PG_CUDA_CHECK(cudaGetLastError());
 }

@@ -59,6 +59,7 @@ PGPU_SIGNATURES = [
       _f32p, _u64p, _u64p]),
     ("pgpu_scene_film", ctypes.c_int, [ctypes.c_uint64, _f32p, _dblp, _u64p]),
     ("pgpu_scene_clear", ctypes.c_int, [ctypes.c_uint64]),
+    ("pgpu_scene_set_filter", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32]),
     ("pgpu_scene_profile", ctypes.c_int,
      [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _dblp]),
     ("pgpu_scene_set_guiding", ctypes.c_int,
@@ -226,6 +227,8 @@ def guide_train(params, features, dirs, weights, steps, batch, lr=1e-2):
 
 MATTE, CONDUCTOR, DIELECTRIC = 0, 1, 2
 BNEEPT, BVPT, BVPTDL = 0, 1, 2
+# sample-filter names of the reference's SDL (sdl_sample_filter_type.h) -> pgpu_scene_set_filter
+FILTERS = {"box": 0, "gaussian": 1, "mn": 2, "bh": 3}
 
 
 def flatten_scene(scene):
@@ -286,9 +289,9 @@ class RenderScene:
         return {"ms": ms.value, "rays": rays.value, "shadow_rays": shadow.value}
 
     def film(self):
-        """(developed float32 [H, W, 3], FP64 sums [H, W, 3], spp)."""
+        """(developed float32 [H, W, 3], FP64 sums [H, W, 4] = R, G, B, W, spp)."""
         rgb = np.empty((self.height, self.width, 3), np.float32)
-        sums = np.empty((self.height, self.width, 3), np.float64)
+        sums = np.empty((self.height, self.width, 4), np.float64)
         spp = ctypes.c_uint64()
         _check(load().pgpu_scene_film(self.id, _ptr(rgb, ctypes.c_float), _ptr(sums, ctypes.c_double),
                                       ctypes.byref(spp)))
@@ -296,6 +299,10 @@ class RenderScene:
 
     def clear(self):
         _check(load().pgpu_scene_clear(self.id))
+
+    def set_filter(self, name: str) -> None:
+        """Sample filter of the film ("box", "gaussian", "mn", "bh"); clears the film."""
+        _check(load().pgpu_scene_set_filter(self.id, FILTERS[name]))
 
     def profile(self, spp, max_bounces=10000, estimator=BNEEPT, seed=42):
         """Per-kernel device ms of a timed render into a scratch film."""
@@ -395,7 +402,7 @@ class CookedScene:
         wd = working_dir.encode()
         n = ctypes.c_uint64()
         nm, ne = ctypes.c_uint32(), ctypes.c_uint32()
-        dims = np.zeros(4, np.uint32)
+        dims = np.zeros(5, np.uint32)
         _check(lib.pgpu_sdl_cook(txt, wd, ctypes.byref(n), ctypes.byref(nm), ctypes.byref(ne),
                                  _ptr(dims, ctypes.c_uint32), None, None, None, None, None))
         self.tris = np.empty((n.value, 3, 3), np.float32)
@@ -409,7 +416,7 @@ class CookedScene:
                                  _ptr(self.emitters, ctypes.c_float) if ne.value else None,
                                  _ptr(self.camera, ctypes.c_float)))
         self.num_materials = nm.value
-        self.width, self.height, self.spp, self.estimator = (int(x) for x in dims)
+        self.width, self.height, self.spp, self.estimator, self.sample_filter = (int(x) for x in dims)
 
 
 class PhotonEngine:

@@ -4,12 +4,13 @@ Paths are independent, so a render of S samples per pixel splits into disjoint, 
 sample ranges, one per rank. Every rank renders its range on its own GPU with the same seed. The
 path generator keys each path by its global index (sample index x pixels + pixel), so the union
 of the ranges is exactly the set of paths one GPU would trace for all S samples. The FP64 film
-sums then meet in a single all-reduce, and the developed image is sum / S.
+sums (filter-weighted R, G, B and the weight W per pixel) then meet in a single all-reduce, and
+the developed image is RGB / W.
 
 This is the multi-device analogue of the reference's split of one render across worker threads,
 each with its own film merged into the main film (EqualSamplingRenderer::doRender,
 Engine/Engine/Source/Core/Renderer/Sampling/EqualSamplingRenderer.cpp:123-190). There is no
-exchange on the data path: the only collective is the final reduction of W x H x 3 doubles.
+exchange on the data path: the only collective is the final reduction of W x H x 4 doubles.
 """
 
 from __future__ import annotations
@@ -44,12 +45,14 @@ def reduce_film(sums: np.ndarray, group=None, device: str = "cpu") -> np.ndarray
     return t.cpu().numpy()
 
 
-def develop(sums: np.ndarray, spp: int) -> np.ndarray:
-    """Box-filter develop of FP64 RGB sums: sum / spp (HdrRgbFilm::developRegion with unit
-    weights, Engine/Engine/Source/Core/Filmic/HdrRgbFilm.cpp:167-205)."""
-    if spp <= 0:
-        raise ValueError("no samples to develop")
-    return (sums / float(spp)).astype(np.float32)
+def develop(sums: np.ndarray) -> np.ndarray:
+    """Develop of FP64 (R, G, B, W) sums [..., 4]: RGB / W, 0 where W is 0
+    (HdrRgbFilm::developRegion, Engine/Engine/Source/Core/Filmic/HdrRgbFilm.cpp:167-205)."""
+    if sums.shape[-1] != 4:
+        raise ValueError("film sums must be [..., 4] (R, G, B, W)")
+    w = sums[..., 3:4]
+    rcp = np.divide(1.0, w, out=np.zeros_like(w), where=w != 0)
+    return (sums[..., :3] * rcp).astype(np.float32)
 
 
 def render_replicated(scene, spp: int, rank: int, world: int, max_bounces: int = 10000,
@@ -64,4 +67,4 @@ def render_replicated(scene, spp: int, rank: int, world: int, max_bounces: int =
             rs.render(count, max_bounces=max_bounces, estimator=estimator, seed=seed, first_sample=first)
         _, sums, _ = rs.film()
     total = reduce_film(sums, group=group, device=reduce_device)
-    return develop(total, spp)
+    return develop(total)

@@ -73,6 +73,7 @@ class Scene:
     groups: List[MeshGroup]
     estimator: str = "bneept"
     env_radiance: Optional[RGB] = None
+    sample_filter: str = "box"      # box | gaussian | mn | bh (the reference's sample-filter enum)
 
     @property
     def num_tris(self) -> int:
@@ -433,7 +434,7 @@ def to_sdl(scene: Scene, env_image_name: str = "env.pfm") -> str:
         f'[vector3 pos "{_v3(scene.cam_pos)}"] [vector3 dir "{_v3(scene.cam_dir)}"] '
         f'[vector3 up-axis "{_v3(scene.cam_up)}"];',
         f"sample-source(stratified) @sampler = [integer samples {scene.spp}];",
-        "visualizer(path-tracing) @visualizer = [enum sample-filter box] "
+        f"visualizer(path-tracing) @visualizer = [enum sample-filter {scene.sample_filter}] "
         f"[enum estimator {scene.estimator}];",
     ]
     for gi, g in enumerate(scene.groups):

@@ -18,6 +18,8 @@ import subprocess
 import sys
 import tempfile
 
+import dataclasses
+
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -33,6 +35,13 @@ WORKLOADS = {
     "cornell_bneept": (lambda spp: scenes.cornell(64, 64, spp, 8, "bneept"), 8192, 8),
     "cornell_bvpt": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvpt"), 8192, 8),
     "cornell_bvptdl": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvptdl"), 8192, 8),
+    # the reference's other sample filters (sample-filter of the path-tracing visualizer)
+    "cornell_bneept_gaussian": (lambda spp: dataclasses.replace(scenes.cornell(64, 64, spp, 8, "bneept"),
+                                                                sample_filter="gaussian"), 8192, 8),
+    "cornell_bneept_mn": (lambda spp: dataclasses.replace(scenes.cornell(64, 64, spp, 8, "bneept"),
+                                                          sample_filter="mn"), 8192, 8),
+    "cornell_bneept_bh": (lambda spp: dataclasses.replace(scenes.cornell(64, 64, spp, 8, "bneept"),
+                                                          sample_filter="bh"), 8192, 8),
     "cornell_glossy_bneept": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 8192, 8),
     "ggx_sphere_env_bneept": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
                                                             max_bounces=10), 4096, 10),

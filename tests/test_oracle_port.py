@@ -7,11 +7,15 @@ not at hand (it is plain C++ and travels), so it must itself reproduce the refer
   near-tie rule as the GPU traversal: a different primitive only where t agrees within 2 ulp);
 * BSDF eval / pdf / sample against the reference's SurfaceOptics answers (bsdf_cases.npz);
 * whole BNEEPT and BVPTDL images against the reference renders of images.npz, at fewer samples (4 x 4 block
-  relMSE <= 1e-3 and per-channel means within 1 %, the bar of the GPU image tests).
+  relMSE <= 1e-3 and per-channel means within 1 %, the bar of the GPU image tests);
+* images through the reference's gaussian, Mitchell-Netravali and Blackman-Harris sample filters
+  at full resolution (relMSE <= 1e-3; the same scene through the box filter is 3.5e-3 or more
+  away from each of them, so the bar tells the filters apart).
 
 CPU only; builds the library with ``make -f oracle/Makefile.port`` when it is missing.
 """
 
+import dataclasses
 import os
 import subprocess
 
@@ -68,6 +72,12 @@ def test_port_bsdf_matches_reference(port):
 IMAGES = {
     "cornell_bneept": (lambda spp: scenes.cornell(64, 64, spp, 8, "bneept"), 512),
     "cornell_bvptdl": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvptdl"), 4096),
+    "cornell_bneept_gaussian": (lambda spp: dataclasses.replace(scenes.cornell(64, 64, spp, 8, "bneept"),
+                                                                sample_filter="gaussian"), 1024),
+    "cornell_bneept_mn": (lambda spp: dataclasses.replace(scenes.cornell(64, 64, spp, 8, "bneept"),
+                                                          sample_filter="mn"), 1024),
+    "cornell_bneept_bh": (lambda spp: dataclasses.replace(scenes.cornell(64, 64, spp, 8, "bneept"),
+                                                          sample_filter="bh"), 1024),
     "cornell_glossy_bneept": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 1024),
     "ggx_sphere_env_bneept": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
                                                             max_bounces=10), 512),
@@ -82,10 +92,15 @@ def test_port_image_matches_reference(port, name):
     factory, spp = IMAGES[name]
     scene = factory(spp)
     estimator = {"bneept": 0, "bvpt": 1, "bvptdl": 2}[scene.estimator]
-    img = port.render(photon_gpu.flatten_scene(scene), spp, scene.max_bounces, estimator, seed=3)
+    filtered = scene.sample_filter != "box"
+    img = port.render(photon_gpu.flatten_scene(scene), spp, scene.max_bounces, estimator, seed=3,
+                      sample_filter=scene.sample_filter if filtered else None)
     ref = d[name]
     block = lambda a: a.reshape(16, 4, 16, 4, 3).mean(axis=(1, 3)).astype(np.float64)
     err = float(np.mean((block(img) - block(ref)) ** 2 / (block(ref) ** 2 + 1e-2)))
     means = img.mean(axis=(0, 1)) / ref.mean(axis=(0, 1))
     assert err <= 1e-3, f"block relMSE {err:.3e}"
     assert np.all(np.abs(means - 1.0) < 0.01), means
+    if filtered:
+        full = float(np.mean((img.astype(np.float64) - ref) ** 2 / (ref.astype(np.float64) ** 2 + 1e-2)))
+        assert full <= 1e-3, f"relMSE {full:.3e}"

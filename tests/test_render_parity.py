@@ -24,6 +24,7 @@ phRender -> phAquireFrameRaw), exactly as a reference user would drive it. Refer
   emitters of radiance 1 sees exactly 1 in every pixel.
 """
 
+import dataclasses
 import os
 
 import numpy as np
@@ -48,6 +49,13 @@ WORKLOADS = {
                                         "empirical"),
     "ggx_sphere_bneept_manual": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
                                                                max_bounces=10), 4096, "manual"),
+    # the reference's other sample filters (HdrRgbFilm::addRgbSample through SampleFilter)
+    "cornell_bneept_gaussian": (lambda spp: dataclasses.replace(scenes.cornell(64, 64, spp, 8, "bneept"),
+                                                                sample_filter="gaussian"), 4096),
+    "cornell_bneept_mn": (lambda spp: dataclasses.replace(scenes.cornell(64, 64, spp, 8, "bneept"),
+                                                          sample_filter="mn"), 4096),
+    "cornell_bneept_bh": (lambda spp: dataclasses.replace(scenes.cornell(64, 64, spp, 8, "bneept"),
+                                                          sample_filter="bh"), 4096),
 }
 
 
@@ -102,18 +110,21 @@ def test_image_matches_reference(gpu_lib, tmp_path, name):
     assert np.all(np.abs(means - 1.0) < 0.01), f"channel means differ: {means}"
 
 
-def _furnace_scene(estimator):
+def _furnace_scene(estimator, sample_filter="box"):
     sphere = scenes.icosphere(3).astype(np.float32)
     groups = [scenes.MeshGroup(sphere, scenes.Material("matte", albedo=(0.5, 0.5, 0.5)))]
     return scenes.Scene("furnace", 32, 32, 1024, 10000, cam_pos=(0.0, 0.0, -4.0), cam_dir=(0.0, 0.0, 1.0),
                         cam_up=(0.0, 1.0, 0.0), fov_deg=30.0, groups=groups, estimator=estimator,
-                        env_radiance=(1.0, 1.0, 1.0))
+                        env_radiance=(1.0, 1.0, 1.0), sample_filter=sample_filter)
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("estimator", ["bneept", "bvpt"])
-def test_furnace(gpu_lib, tmp_path, estimator):
-    img, _ = render_via_c_api(_furnace_scene(estimator), tmp_path)
+@pytest.mark.parametrize("estimator,sample_filter", [("bneept", "box"), ("bvpt", "box"), ("bneept", "gaussian"),
+                                                     ("bneept", "mn"), ("bneept", "bh")])
+def test_furnace(gpu_lib, tmp_path, estimator, sample_filter):
+    # with a filter, light found by NEE at a path's last vertex reaches the film from the any-hit
+    # kernel, the rest from the shading kernel: both must weight it like the sample's W
+    img, _ = render_via_c_api(_furnace_scene(estimator, sample_filter), tmp_path)
     # the central pixels see only the sphere; the corners see only the environment
     centre = img[12:20, 12:20]
     assert abs(centre.mean() - 0.5) < 1e-3, centre.mean()
@@ -121,11 +132,34 @@ def test_furnace(gpu_lib, tmp_path, estimator):
 
 
 @pytest.mark.gpu
-def test_unit_radiance(gpu_lib, tmp_path):
+@pytest.mark.parametrize("sample_filter", ["box", "gaussian", "mn", "bh"])
+def test_unit_radiance(gpu_lib, tmp_path, sample_filter):
     walls = scenes.boxes_axis_aligned(np.array([[-10.0, -10.0, -10.0]]), np.array([[10.0, 10.0, 10.0]]))
     walls = walls[:, [0, 2, 1]]   # flip winding so the faces (and their emission) point inwards
     groups = [scenes.MeshGroup(walls, scenes.Material("matte", albedo=(0.0, 0.0, 0.0)), radiance=(1.0, 1.0, 1.0))]
     scene = scenes.Scene("unit", 16, 16, 16, 10000, cam_pos=(0.0, 0.0, 0.0), cam_dir=(0.0, 0.0, 1.0),
-                         cam_up=(0.0, 1.0, 0.0), fov_deg=60.0, groups=groups)
+                         cam_up=(0.0, 1.0, 0.0), fov_deg=60.0, groups=groups, sample_filter=sample_filter)
     img, _ = render_via_c_api(scene, tmp_path)
     assert np.allclose(img, 1.0, atol=1e-6), (img.min(), img.max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sample_filter", ["box", "bh"])
+def test_developed_frame_is_sums_over_weight(gpu_lib, sample_filter):
+    """The GPU develop equals RGB / W of the FP64 sums, rounded once to FP32, bit for bit; the box
+    filter's W is the sample count."""
+    import photon_gpu
+
+    scene = scenes.cornell(32, 24, 8, 8, "bneept")
+    with photon_gpu.RenderScene(scene) as rs:
+        rs.set_filter(sample_filter)
+        rs.render(8, max_bounces=8, seed=5)
+        rs.render(3, max_bounces=8, seed=5, first_sample=8)
+        rgb, sums, spp = rs.film()
+    assert spp == 11 and rgb.shape == (24, 32, 3) and sums.shape == (24, 32, 4)
+    w = sums[..., 3:4]
+    assert np.all(w > 0)
+    if sample_filter == "box":
+        assert np.all(w == 11.0)
+    want = (sums[..., :3] * (1.0 / w)).astype(np.float32)
+    assert np.array_equal(rgb.view(np.uint32), want.view(np.uint32))

@@ -46,10 +46,11 @@ def _reduce_worker(rank, world, port, out_dir):
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
     try:
         first, count = replicas.sample_range(10, rank, world)
-        # a film whose every sample adds (sample index + 1) to every channel
-        sums = np.full((4, 5, 3), float(sum(range(first + 1, first + count + 1))), np.float64)
+        # a film whose every sample adds (sample index + 1) to every colour channel, weight 1
+        sums = np.full((4, 5, 4), float(sum(range(first + 1, first + count + 1))), np.float64)
+        sums[..., 3] = count
         total = replicas.reduce_film(sums, device="cpu")
-        np.save(os.path.join(out_dir, f"rank{rank}.npy"), replicas.develop(total, 10))
+        np.save(os.path.join(out_dir, f"rank{rank}.npy"), replicas.develop(total))
     finally:
         dist.destroy_process_group()
 
@@ -68,17 +69,20 @@ def test_film_reduction_over_two_gloo_ranks(tmp_path):
 
 
 @pytest.mark.gpu
-def test_split_sample_ranges_reproduce_one_render(gpu_lib):
+@pytest.mark.parametrize("sample_filter", ["box", "bh"])
+def test_split_sample_ranges_reproduce_one_render(gpu_lib, sample_filter):
     import photon_gpu
 
     scene = scenes.cornell_glossy(32, 32, 8, 8, "bneept")
     with photon_gpu.RenderScene(scene) as whole:
+        whole.set_filter(sample_filter)
         whole.render(8, max_bounces=8, seed=9)
         _, ref, _ = whole.film()
     parts = []
     for rank in range(2):
         first, count = replicas.sample_range(8, rank, 2)
         with photon_gpu.RenderScene(scene) as rs:
+            rs.set_filter(sample_filter)
             rs.render(count, max_bounces=8, seed=9, first_sample=first)
             parts.append(rs.film()[1])
     total = parts[0] + parts[1]

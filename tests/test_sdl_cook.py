@@ -46,6 +46,18 @@ def test_bvpt_and_materials():
     assert _cook(scenes.to_sdl(scenes.cornell(estimator="bvptdl"))).estimator == 2
 
 
+def test_sample_filters():
+    import dataclasses
+
+    for name, code in photon_gpu.FILTERS.items():
+        s = dataclasses.replace(scenes.cornell(8, 8, 1), sample_filter=name)
+        assert _cook(scenes.to_sdl(s)).sample_filter == code
+    # without a sample-filter clause the path-tracing visualizer uses Blackman-Harris
+    text = scenes.to_sdl(scenes.cornell(8, 8, 1)).replace("[enum sample-filter box] ", "")
+    assert "sample-filter" not in text
+    assert _cook(text).sample_filter == photon_gpu.FILTERS["bh"]
+
+
 def test_streamed_fragments_equal_whole_text():
     text = scenes.to_sdl(scenes.cornell(32, 32, 4))
     whole = _cook(text)
