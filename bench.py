@@ -2,6 +2,9 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
+Workloads: ggx_1m (default), cornell (256^2, 64 spp, 36 triangles) through the Photon C API;
+city, batched and slit_room through the flat scene ABI (see FLAT_WORKLOADS).
+
 Default workload: the 1M-triangle GGX scene -- an icosphere subdivided 8 times (1,310,720
 triangles) with seeded 3-octave value-noise radial displacement (5 % of the radius) on a
 2-triangle ground, GGX conductors in 64 groups (roughness U[0.05, 0.5], F0 U[0.5, 1]), 2 quad
@@ -132,17 +135,18 @@ def measured_peaks() -> dict:
 EST_CPU_PATHS_PER_CORE_S = 0.13e6
 
 
-def cpu_sample(scene: scenes.Scene, tmp: str, target_seconds: float = 12.0, repeats: int = 1) -> list:
+def cpu_sample(scene: scenes.Scene, tmp: str, target_seconds: float = 12.0, repeats: int = 1,
+               force_port: bool = False, paths_per_core_s: float = EST_CPU_PATHS_PER_CORE_S) -> list:
     """Times the reference CPU renderer (or, without it, the oracle port) on a bounded sample of
     the same workload -- the same scene with fewer samples per pixel -- on all host threads.
     Returns one record per repeat (phUpdate untimed, phRender timed)."""
     threads = os.cpu_count() or 1
-    tool, kind = (REF_RENDER, "reference") if os.path.exists(REF_RENDER) else (PORT_RENDER, "port")
+    tool, kind = (REF_RENDER, "reference") if os.path.exists(REF_RENDER) and not force_port else (PORT_RENDER, "port")
     if not os.path.exists(tool):
         return [{"value": None, "unit": "Mpaths/s", "cores": threads, "kind": kind,
                  "sample": "unavailable: neither oracle/_ref/ph_ref_render nor the port is built"}]
     per_spp_paths = scene.width * scene.height
-    spp = int(max(1, min(scene.spp, round(target_seconds * EST_CPU_PATHS_PER_CORE_S * threads / per_spp_paths))))
+    spp = int(max(1, min(scene.spp, round(target_seconds * paths_per_core_s * threads / per_spp_paths))))
     s = scenes.Scene(**{**scene.__dict__, "spp": spp})
     d = tempfile.mkdtemp(dir=tmp)
     if kind == "reference":
@@ -163,12 +167,51 @@ def cpu_sample(scene: scenes.Scene, tmp: str, target_seconds: float = 12.0, repe
         r = json.loads(line)
         paths = per_spp_paths * spp
         records.append({
-            "value": paths / r["render_s"] / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": kind,
+            "value": paths / r["render_s"] / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": kind, "paths": paths,
             "sample": f"{scene.width}x{scene.height} x {spp} spp of the same scene ({paths} paths), "
                       f"{'phRender' if kind == 'reference' else 'oracle port render'} only "
                       f"({r['render_s']:.2f} s); scene load {r['load_s']:.1f} s and update "
                       f"{r['update_s']:.1f} s excluded"})
     return records
+
+
+def roofline_of(kernel_ms: dict, rays: float, shadow_rays: float, iterations: float, counts: dict) -> dict:
+    """HBM roofline of the kernel with the largest device time: algorithmic bytes (the traversal
+    model from the counted nodes and triangles per ray) over its measured time, against the
+    measured copy bandwidth; `traffic` is DRAM bytes per launch from the committed ncu capture,
+    scaled by queue entries to this workload's average launch."""
+    peaks = measured_peaks()
+    nodes_per_ray = counts["nodes_closest"] / max(1.0, counts["rays"])
+    tris_per_ray = counts["tris_closest"] / max(1.0, counts["rays"])
+    s_nodes = counts["nodes_any"] / max(1.0, counts["shadow_rays"])
+    s_tris = counts["tris_any"] / max(1.0, counts["shadow_rays"])
+    # bytes per closest-hit ray: 32 ray in + 8 hit out + 80 per node + 48 per triangle
+    bytes_closest = 40.0 + 80.0 * nodes_per_ray + 48.0 * tris_per_ray
+    bytes_shadow = 48.0 + 80.0 * s_nodes + 48.0 * s_tris
+    dominant = max(("extend_ms", "shadow_ms", "shade_ms"), key=lambda k: kernel_ms[k])
+    if dominant == "shadow_ms":
+        alg_bytes, kname = bytes_shadow * shadow_rays, "shadow (any hit)"
+    elif dominant == "extend_ms":
+        alg_bytes, kname = bytes_closest * rays, "extend (closest hit)"
+    else:
+        # shade: ray + hit + state in/out + triangle + shadow record per queued ray
+        alg_bytes, kname = (32 + 8 + 80 + 48 + 112 + 48) * rays, "shade"
+    achieved = alg_bytes / (kernel_ms[dominant] / 1e3) / 1e9
+    traffic = None
+    prof_path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(prof_path):
+        with open(prof_path) as f:
+            rec = json.load(f).get(dominant) or {}
+        if rec.get("dram_bytes_per_entry"):
+            entries = (shadow_rays if dominant == "shadow_ms" else rays) / max(1, iterations)
+            traffic = rec["dram_bytes_per_entry"] * entries
+    return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peaks["hbm_gbs"],
+            "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+            "algorithmic_bytes_per_launch": alg_bytes / max(1, iterations),
+            "peak_source": peaks["source"],
+            "model": {"bytes_per_closest_ray": bytes_closest, "nodes_per_closest_ray": nodes_per_ray,
+                      "tris_per_closest_ray": tris_per_ray, "bytes_per_shadow_ray": bytes_shadow,
+                      "nodes_per_shadow_ray": s_nodes, "tris_per_shadow_ray": s_tris}}
 
 
 def rel_mse(x: np.ndarray, ref: np.ndarray, eps: float = 1e-2) -> float:
@@ -218,6 +261,18 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 4
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
+        return
+    if args.workload in FLAT_WORKLOADS:
+        scene_list = FLAT_WORKLOADS[args.workload]()
+        rec = cpu_sample_many(scene_list, args.cpu_seconds, PORT_PATHS_PER_CORE_S[args.workload])
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": rec["value"], "unit": "Mpaths/s",
+            "n_gpus": args.gpus, "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes)",
+            "config": {"workload": args.workload, "scenes": len(scene_list),
+                       "triangles": int(sum(sc.num_tris for sc in scene_list))},
+            "cpu_baseline": rec,
+            "e2e": {"value": rec["value"], "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
     scene = workload(args.workload)
     with tempfile.TemporaryDirectory() as tmp:
@@ -338,39 +393,11 @@ def run_ours(args) -> None:
         eng.close()
 
         # ---- roofline of the dominant kernel
-        peaks = measured_peaks()
         kernel_ms = {k: kprof[k] for k in ("prepare_ms", "regen_ms", "extend_ms", "shade_ms", "shadow_ms")}
         total_k = sum(kernel_ms.values())
         rays = kprof["rays"]
         shadow_rays = kprof["shadow_rays"]
-        nodes_per_ray = counts["nodes_closest"] / max(1.0, counts["rays"])
-        tris_per_ray = counts["tris_closest"] / max(1.0, counts["rays"])
-        s_nodes = counts["nodes_any"] / max(1.0, counts["shadow_rays"])
-        s_tris = counts["tris_any"] / max(1.0, counts["shadow_rays"])
-        # bytes per closest-hit ray: 32 ray in + 8 hit out + 80 per node + 48 per triangle
-        bytes_closest = 40.0 + 80.0 * nodes_per_ray + 48.0 * tris_per_ray
-        bytes_shadow = 48.0 + 80.0 * s_nodes + 48.0 * s_tris
-        dominant = max(("extend_ms", "shadow_ms", "shade_ms"), key=lambda k: kernel_ms[k])
-        if dominant == "shadow_ms":
-            alg_bytes, launches_k, kname = bytes_shadow * shadow_rays, kprof["iterations"], "shadow (any hit)"
-        elif dominant == "extend_ms":
-            alg_bytes, launches_k, kname = bytes_closest * rays, kprof["iterations"], "extend (closest hit)"
-        else:
-            # shade: ray + hit + state in/out + triangle + shadow record per queued ray
-            alg_bytes = (32 + 8 + 80 + 48 + 112 + 48) * rays
-            launches_k, kname = kprof["iterations"], "shade"
-        achieved = alg_bytes / (kernel_ms[dominant] / 1e3) / 1e9
-        # DRAM bytes per launch from an ncu capture of a full-queue launch, scaled by queue
-        # entries to this workload's average launch (rays / iterations)
-        traffic = None
-        prof_path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-        if os.path.exists(prof_path):
-            with open(prof_path) as f:
-                rec = json.load(f).get(dominant) or {}
-            if rec.get("dram_bytes_per_entry"):
-                entries = (shadow_rays if dominant == "shadow_ms" else rays) / max(1, kprof["iterations"])
-                traffic = rec["dram_bytes_per_entry"] * entries
-        achieved_per_launch = alg_bytes / max(1, launches_k)
+        roofline = roofline_of(kernel_ms, rays, shadow_rays, kprof["iterations"], counts)
 
     clock = clocks.summary()
     line = {
@@ -383,13 +410,7 @@ def run_ours(args) -> None:
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
                 "path": "phRender + phAquireFrameRaw + phGetFrameRgbData (scene resident after phUpdate)"},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peaks["hbm_gbs"],
-                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                     "algorithmic_bytes_per_launch": achieved_per_launch,
-                     "peak_source": peaks["source"],
-                     "model": {"bytes_per_closest_ray": bytes_closest, "nodes_per_closest_ray": nodes_per_ray,
-                               "tris_per_closest_ray": tris_per_ray, "bytes_per_shadow_ray": bytes_shadow,
-                               "nodes_per_shadow_ray": s_nodes, "tris_per_shadow_ray": s_tris}},
+        "roofline": roofline,
         "kernel_ms_per_step": {k: v for k, v in kernel_ms.items()},
         "kernel_share": {k: v / total_k for k, v in kernel_ms.items()},
         "rays_per_step": {"closest": rays, "shadow": shadow_rays},
@@ -408,6 +429,145 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+# Workloads too large for SDL text (the SDL vector3-array is text only): built and rendered
+# through the flat scene ABI (pgpu_scene_create / pgpu_scene_render), one RenderScene each.
+FLAT_WORKLOADS = {
+    # many-light city: 447^2 lognormal buildings, 21.6M triangles, 10,000 lights, 1920x1080, 1024 spp
+    "city": lambda: [scenes.city()],
+    # 64 seeded scenes, 1k-500k triangles, 128^2-1024^2, 16-256 spp, rendered one after another
+    "batched": lambda: [scenes.batch_scene(i) for i in range(64)],
+    # the learned-guiding room rendered plain: 2M triangles, one light behind a slit, 1024^2, 64 spp
+    "slit_room": lambda: [scenes.slit_room()],
+}
+# The oracle port's cost on these workloads (Mpaths/s per host thread, measured on the GPU box's
+# 16 threads); only used to size the bounded CPU sample, the reported rate is always measured.
+PORT_PATHS_PER_CORE_S = {"city": 0.054e6, "batched": 0.10e6, "slit_room": 0.012e6}
+
+
+def run_flat(args) -> None:
+    """One step = every scene of the workload rendered once with its own spp (device time summed);
+    e2e adds each developed frame's copy to host memory."""
+    import torch
+
+    import photon_gpu
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    photon_gpu.load()
+    t0 = time.time()
+    scene_list = FLAT_WORKLOADS[args.workload]()
+    gen_s = time.time() - t0
+    if args.spp:
+        for sc in scene_list:
+            sc.spp = args.spp
+    t0 = time.time()
+    rss = [photon_gpu.RenderScene(sc, builder=args.builder) for sc in scene_list]
+    build_s = time.time() - t0
+    paths_per_step = sum(sc.width * sc.height * sc.spp for sc in scene_list)
+    l2_flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > 126 MB L2
+    seed = 1000003 * rank + 7
+
+    def one_pass(read_back: bool = False):
+        ms, launches = 0.0, 0
+        for sc, rs in zip(scene_list, rss):
+            rs.clear()
+            ms += rs.render(sc.spp, max_bounces=sc.max_bounces, seed=seed)["ms"]
+            launches += rs.launches()
+            if read_back:
+                rs.film(with_sums=False)
+        return ms, launches
+
+    for _ in range(args.warmup):
+        one_pass()
+    torch.cuda.synchronize()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        device_ms, launches = 0.0, 0
+        wall0 = time.time()
+        for _ in range(args.steps):
+            l2_flush.fill_(1.0)
+            torch.cuda.synchronize()
+            ms, n = one_pass()
+            device_ms += ms
+            launches += n
+        wall = time.time() - wall0
+    value = paths_per_step * args.steps / (device_ms / 1e3) / 1e6
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        t = time.time()
+        one_pass(read_back=True)
+        e2e_s += time.time() - t
+    e2e_value = paths_per_step * args.steps / e2e_s / 1e6
+    d2h = sum(sc.width * sc.height * 3 * 4 for sc in scene_list)
+
+    # per-kernel device time (events around every launch) and traversal counts, untimed
+    kernel_ms = dict.fromkeys(("prepare_ms", "regen_ms", "extend_ms", "shade_ms", "shadow_ms"), 0.0)
+    counts = dict.fromkeys(("rays", "shadow_rays", "nodes_closest", "tris_closest", "nodes_any", "tris_any"), 0)
+    rays = shadow_rays = iterations = 0
+    for sc, rs in zip(scene_list, rss):
+        prof = rs.profile(sc.spp, max_bounces=sc.max_bounces, seed=seed)
+        for k in kernel_ms:
+            kernel_ms[k] += prof[k]
+        full = rs.count(sc.spp, max_bounces=sc.max_bounces, seed=seed)
+        rays += full["rays"]
+        shadow_rays += full["shadow_rays"]
+        iterations += full["iterations"]
+        for k in counts:
+            counts[k] += full[k]
+    for rs in rss:
+        rs.close()
+    total_k = sum(kernel_ms.values())
+    clock = clocks.summary()
+    spps = sorted({sc.spp for sc in scene_list})
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": device_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes)",
+        "config": {"workload": args.workload, "scenes": len(scene_list),
+                   "triangles": int(sum(sc.num_tris for sc in scene_list)), "paths_per_step": paths_per_step,
+                   "resolution": sorted({f"{sc.width}x{sc.height}" for sc in scene_list})[:4],
+                   "spp": spps if len(spps) <= 4 else [spps[0], spps[-1]],
+                   "max_bounces": scene_list[0].max_bounces, "estimator": "bneept", "bvh": args.builder,
+                   "l2": "256 MiB write between timed steps", "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
+                "path": "pgpu_scene_render + pgpu_scene_film (frame developed on the GPU, copied to host)"},
+        "gpu_launches": launches,
+        "roofline": roofline_of(kernel_ms, rays, shadow_rays, iterations, counts),
+        "kernel_ms_per_step": kernel_ms,
+        "kernel_share": {k: v / total_k for k, v in kernel_ms.items()},
+        "rays_per_step": {"closest": rays, "shadow": shadow_rays},
+        "mrays_per_s": (rays + shadow_rays) / (device_ms / args.steps / 1e3) / 1e6,
+        "clocks": {"sm_mhz": clock["sm_mhz"], "sm_max_mhz": clock["sm_max_mhz"], "reasons": clock["reasons"]},
+        "host": {"scene_generation_s": gen_s, "bvh_build_and_upload_s": build_s, "wall_s_timed": wall},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample_many(scene_list, args.cpu_seconds, PORT_PATHS_PER_CORE_S[args.workload])
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def cpu_sample_many(scene_list, target_seconds: float, paths_per_core_s: float = EST_CPU_PATHS_PER_CORE_S) -> dict:
+    """CPU baseline of a multi-scene or very large workload: the oracle port (binary scene file;
+    SDL text of tens of millions of triangles is impractical to parse) on the first scenes, each
+    with spp reduced to a bounded sample, paths summed over render time."""
+    picked = scene_list[:4]
+    paths = secs = 0.0
+    cores, kinds = os.cpu_count() or 1, set()
+    with tempfile.TemporaryDirectory() as tmp:
+        for sc in picked:
+            rec = cpu_sample(sc, tmp, target_seconds=target_seconds / len(picked), force_port=True,
+                             paths_per_core_s=paths_per_core_s)[-1]
+            if not rec["value"]:
+                return rec
+            n = rec["paths"]
+            paths += n
+            secs += n / (rec["value"] * 1e6)
+            kinds.add(rec["kind"])
+    return {"value": paths / secs / 1e6, "unit": "Mpaths/s", "cores": cores, "kind": "/".join(sorted(kinds)),
+            "sample": f"{len(picked)} of {len(scene_list)} scenes at reduced spp ({int(paths)} paths, "
+                      f"{secs:.1f} s of render time; BVH build excluded)"}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -419,9 +579,12 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-guided", action="store_true", help="skip the guided-vs-plain equal-time comparison")
+    ap.add_argument("--builder", default="sah", choices=["sah", "gpu"], help="BVH builder of flat workloads")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload in FLAT_WORKLOADS:
+        run_flat(args)
     else:
         run_ours(args)
 

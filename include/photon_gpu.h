@@ -174,6 +174,14 @@ PGPU_API int pgpu_scene_set_filter(uint64_t id, uint32_t filter);
 PGPU_API int pgpu_scene_profile(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator,
                        uint64_t seed, double* out_kernel_ms);
 PGPU_API int pgpu_scene_clear(uint64_t id);
+/* Kernels the scene's last render launched (all iterations, including the empty ones that end the
+ * last CUDA-graph batch). */
+PGPU_API int pgpu_scene_launches(uint64_t id, uint64_t* out_launches);
+/* A render into a scratch film whose traversal kernels count their work: out_counts uint64 [7] =
+ * closest-hit rays, shadow rays, BVH nodes and triangles visited by closest-hit queries, the same
+ * for shadow queries, render iterations. */
+PGPU_API int pgpu_scene_count(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator,
+                              uint64_t seed, uint64_t* out_counts);
 
 /* Learned path guiding for the scene's subsequent BNEEPT renders (no reference counterpart). At
  * Lambertian vertices the next direction comes from the network's vMF mixture with probability

@@ -794,7 +794,7 @@ void Engine::render()
 			m_info.paths += wh * n;
 			m_info.rays += m_render->scene->last_rays();
 			m_info.shadow_rays += m_render->scene->last_shadow_rays();
-			m_launches += 5ull * m_render->scene->last_iterations();
+			m_launches += m_render->scene->last_launches();
 			done += n;
 			m_work_done = done;
 			const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -269,6 +269,44 @@ int pgpu_scene_profile(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t
 	});
 }
 
+int pgpu_scene_launches(uint64_t id, uint64_t* out_launches)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		if(out_launches) { *out_launches = r->scene->last_launches(); }
+	});
+}
+
+int pgpu_scene_count(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator, uint64_t seed,
+                     uint64_t* out_counts)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		if(estimator > PG_EST_BVPTDL || !out_counts)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_count: unknown estimator or null output");
+		}
+		RenderParams p;
+		p.width = r->width;
+		p.height = r->height;
+		p.spp = spp;
+		p.max_bounces = max_bounces;
+		p.estimator = estimator;
+		p.filter = r->filter;
+		p.seed = seed;
+		p.mode = PG_RENDER_COUNT;
+		DeviceBuffer<double> scratch(static_cast<std::size_t>(r->width) * r->height * kFilmChannels);
+		PG_CUDA_CHECK(cudaMemsetAsync(scratch.get(), 0, scratch.bytes(), library_stream()));
+		r->scene->render(p, scratch.get());
+		out_counts[0] = r->scene->last_rays();
+		out_counts[1] = r->scene->last_shadow_rays();
+		for(int k = 0; k < 4; ++k) { out_counts[2 + k] = r->scene->last_counts()[k]; }
+		out_counts[6] = r->scene->last_iterations();
+	});
+}
+
 int pgpu_scene_film(uint64_t id, float* out_rgb, double* out_sum, uint64_t* out_spp)
 {
 	return guarded([&]

@@ -1304,6 +1304,13 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 	m_last_rays = final_counters.rays_traced;
 	m_last_shadow = final_counters.shadow_rays;
 	m_last_iterations = iterations;
+	{
+		// prepare, regen, extend, shade, shadow; guide query + forward; training: weight sums
+		// (and clamp), forward, backward, Adam, step, repack, loss
+		const unsigned long long per_iteration = 5ull + (guided ? 2ull : 0ull) +
+		                                         (training ? (m_guide_params.clamp > 0.0f ? 8ull : 6ull) : 0ull);
+		m_last_launches = iterations * per_iteration + (params.filter == PG_FILTER_BOX ? 1ull : 0ull);
+	}
 	m_last_counts[0] = final_counters.nodes_closest;
 	m_last_counts[1] = final_counters.tris_closest;
 	m_last_counts[2] = final_counters.nodes_any;

@@ -223,6 +223,9 @@ public:
 	unsigned long long last_rays() const { return m_last_rays; }
 	unsigned long long last_shadow_rays() const { return m_last_shadow; }
 	unsigned long long last_iterations() const { return m_last_iterations; }
+	// Kernels launched by the last render (every iteration's launches, empty trailing iterations
+	// of the last graph batch included, and the per-render film launch).
+	unsigned long long last_launches() const { return m_last_launches; }
 	// Per-kernel device milliseconds of the last timing-mode render: prepare, regen, extend,
 	// shade, shadow, guiding inference (query + network), guiding training.
 	const double* last_kernel_ms() const { return m_kernel_ms; }
@@ -284,7 +287,7 @@ private:
 	cudaGraphExec_t m_exec = nullptr;
 	int m_exec_key = -1;
 
-	unsigned long long m_last_rays = 0, m_last_shadow = 0, m_last_iterations = 0;
+	unsigned long long m_last_rays = 0, m_last_shadow = 0, m_last_iterations = 0, m_last_launches = 0;
 	unsigned long long m_last_counts[4] = {0, 0, 0, 0};
 	double m_kernel_ms[7] = {0, 0, 0, 0, 0, 0, 0};
 };

@@ -60,6 +60,9 @@ PGPU_SIGNATURES = [
     ("pgpu_scene_film", ctypes.c_int, [ctypes.c_uint64, _f32p, _dblp, _u64p]),
     ("pgpu_scene_clear", ctypes.c_int, [ctypes.c_uint64]),
     ("pgpu_scene_set_filter", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32]),
+    ("pgpu_scene_launches", ctypes.c_int, [ctypes.c_uint64, _u64p]),
+    ("pgpu_scene_count", ctypes.c_int,
+     [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _u64p]),
     ("pgpu_scene_profile", ctypes.c_int,
      [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _dblp]),
     ("pgpu_scene_set_guiding", ctypes.c_int,
@@ -288,13 +291,13 @@ class RenderScene:
                                         ctypes.byref(ms), ctypes.byref(rays), ctypes.byref(shadow)))
         return {"ms": ms.value, "rays": rays.value, "shadow_rays": shadow.value}
 
-    def film(self):
-        """(developed float32 [H, W, 3], FP64 sums [H, W, 4] = R, G, B, W, spp)."""
+    def film(self, with_sums: bool = True):
+        """(developed float32 [H, W, 3], FP64 sums [H, W, 4] = R, G, B, W or None, spp)."""
         rgb = np.empty((self.height, self.width, 3), np.float32)
-        sums = np.empty((self.height, self.width, 4), np.float64)
+        sums = np.empty((self.height, self.width, 4), np.float64) if with_sums else None
         spp = ctypes.c_uint64()
-        _check(load().pgpu_scene_film(self.id, _ptr(rgb, ctypes.c_float), _ptr(sums, ctypes.c_double),
-                                      ctypes.byref(spp)))
+        _check(load().pgpu_scene_film(self.id, _ptr(rgb, ctypes.c_float),
+                                      _ptr(sums, ctypes.c_double) if with_sums else None, ctypes.byref(spp)))
         return rgb, sums, spp.value
 
     def clear(self):
@@ -310,6 +313,19 @@ class RenderScene:
         _check(load().pgpu_scene_profile(self.id, spp, max_bounces, estimator, seed, _ptr(ms, ctypes.c_double)))
         keys = ["prepare_ms", "regen_ms", "extend_ms", "shade_ms", "shadow_ms", "guide_infer_ms", "guide_train_ms"]
         return dict(zip(keys, ms.tolist()))
+
+    def launches(self) -> int:
+        """Kernels launched by the last render (pgpu_scene_launches)."""
+        n = ctypes.c_uint64()
+        _check(load().pgpu_scene_launches(self.id, ctypes.byref(n)))
+        return n.value
+
+    def count(self, spp, max_bounces=10000, estimator=BNEEPT, seed=42):
+        """Traversal work of a render into a scratch film (pgpu_scene_count)."""
+        c = np.zeros(7, np.uint64)
+        _check(load().pgpu_scene_count(self.id, spp, max_bounces, estimator, seed, _ptr(c, ctypes.c_uint64)))
+        keys = ["rays", "shadow_rays", "nodes_closest", "tris_closest", "nodes_any", "tris_any", "iterations"]
+        return dict(zip(keys, (int(x) for x in c)))
 
     def set_guiding(self, enabled=True, train=True, alpha=0.5, lr=1e-2, batch=16384):
         _check(load().pgpu_scene_set_guiding(self.id, int(enabled), int(train), alpha, lr, batch))

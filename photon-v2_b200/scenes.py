@@ -385,6 +385,62 @@ def ggx_sphere(level: int = 8, width: int = 1024, height: int = 1024, spp: int =
                  env_radiance=(0.1, 0.1, 0.1) if with_env else None)
 
 
+def batch_scene(index: int, max_bounces: int = 10, estimator: str = "bneept") -> Scene:
+    """Scene `index` (0..63) of the batched workload: seeded by its index, ~U[1k, 500k] triangles
+    of random boxes (even indices) or a displaced icosphere (odd indices; 20 * 4**level triangles,
+    the level nearest the drawn count), resolution ~U{128..1024} squared, spp ~U{16..256}, eight
+    material groups each Lambertian or GGX conductor with probability 1/2, 1-4 quad lights."""
+    rng = np.random.default_rng(7000 + index)
+    target = int(rng.integers(1000, 500_001))
+    res = int(rng.integers(128, 1025))
+    spp = int(rng.integers(16, 257))
+    num_lights = int(rng.integers(1, 5))
+    if index % 2 == 0:
+        k = max(target // 12, 1)
+        # boxes scattered over a 10 x 10 floor, sizes shrinking with the count (~5 % filled)
+        largest = float(np.clip(1.2 * (300.0 / k) ** (1.0 / 3.0), 0.02, 1.2))
+        size = rng.uniform(0.2 * largest, largest, (k, 3))
+        lo = np.stack([rng.uniform(-5.0, 5.0, k), np.where(rng.random(k) < 0.5, 0.0, rng.uniform(0.0, 3.0, k)),
+                       rng.uniform(-5.0, 5.0, k)], 1)
+        tris = boxes_axis_aligned(lo, lo + size).reshape(-1, 3, 3)
+        centre, extent = np.array([0.0, 1.0, 0.0]), 6.0
+    else:
+        level = int(np.clip(np.round(np.log(target / 20.0) / np.log(4.0)), 3, 7))
+        tris = icosphere(level)
+        flat = tris.reshape(-1, 3)
+        flat = flat * (1.0 + 0.08 * value_noise3(flat * 2.0, index))[:, None] * 2.0
+        tris = flat.reshape(-1, 3, 3)
+        tris[:, :, 1] += 2.1
+        centre, extent = np.array([0.0, 2.0, 0.0]), 3.5
+    gid = rng.integers(0, 8, tris.shape[0])
+    groups = []
+    for g in range(8):
+        sel = tris[gid == g].astype(np.float32)
+        if sel.shape[0] == 0:
+            continue
+        if rng.random() < 0.5:
+            m = Material("matte", albedo=tuple(float(x) for x in rng.uniform(0.2, 0.8, 3)))
+        else:
+            m = Material("conductor", roughness=float(rng.uniform(0.05, 0.6)),
+                         f0=tuple(float(x) for x in rng.uniform(0.5, 1.0, 3)))
+        groups.append(MeshGroup(sel, m))
+    G = 60.0
+    groups.append(MeshGroup(quad((-G, 0, -G), (-G, 0, G), (G, 0, G), (G, 0, -G)),
+                            Material("matte", albedo=(0.5, 0.5, 0.5))))
+    for _ in range(num_lights):
+        x, z = rng.uniform(-4.0, 3.0, 2)
+        w = float(rng.uniform(0.5, 1.5))
+        y = float(rng.uniform(5.0, 7.0))
+        radiance = float(rng.uniform(4.0, 12.0))
+        groups.append(MeshGroup(quad((x, y, z), (x + w, y, z), (x + w, y, z + w), (x, y, z + w)), BLACK,
+                                radiance=(radiance, radiance, radiance)))
+    cam = centre + np.array([0.0, 1.0 * extent, -1.4 * extent])
+    look = centre - cam
+    return Scene(f"batch_{index}", res, res, spp, max_bounces, cam_pos=tuple(float(v) for v in cam),
+                 cam_dir=tuple(float(v) for v in look / np.linalg.norm(look)), cam_up=(0.0, 1.0, 0.0),
+                 fov_deg=50.0, groups=groups, estimator=estimator)
+
+
 # ----------------------------------------------------------------------------------------------
 # SDL serialisation
 
