@@ -195,6 +195,8 @@ __global__ void prepare_kernel(RenderCounters* c, uint32_t capacity)
 	c->guided_total += c->n_guided;
 	c->n_guided = 0;
 	c->n_train = 0;
+	c->n_refine = 0;
+	c->n_refine_mutual = 0;
 	c->rays_traced += c->n_total;
 }
 
@@ -344,6 +346,7 @@ struct ShadeArgs
 	uint32_t      width_height;
 	GuideArgs     guide;
 	RefineSettings refine;
+	RefineQueue   refine_queue;   // iterative refine mode: requests for refine_kernel
 };
 
 __device__ __forceinline__ float4 cur_gf0(const ShadeArgs& a, uint32_t i) { return a.cur.gf0[i]; }
@@ -515,7 +518,11 @@ shade_kernel(ShadeArgs a)
 		//      TDirectLightEstimator.ipp:71-102; BNEEPTEstimator.cpp:103-149)
 		bool has_shadow = false;
 		V3 sh_o{}, sh_d{};
-		float sh_tmin = 0.0f, sh_tmax = 0.0f;
+		float sh_tmin = 0.0f, sh_tmax = 0.0f;   // the record's .w words: range, or refinery inputs
+		uint32_t sh_refine = 0u;   // 1: escape towards a direction, 2: towards a light-triangle point
+		// In the iterative refine mode the re-intersection loops run in refine_kernel, whose warps
+		// all execute the same loop; this kernel leaves the hit point, its triangle and the target.
+		const bool defer_refine = a.refine.mode == PG_REFINE_ITERATIVE;
 		RGB sh_c{};
 		float sh_train = 0.0f;   // unweighted direct-light estimate (luminance) for the training sample
 		const uint32_t grow = GUIDED ? a.guide.map[i] : 0xFFFFFFFFu;
@@ -550,18 +557,30 @@ shade_kernel(ShadeArgs a)
 				le = emitter_radiance(e);
 				if(sidedness_agreed(frame, to_light))
 				{
-					const EscapeRay er = escape(a.refine, pos, ng, tri, to_light);
-					sh_o = er.origin;
-					sh_d = er.unit_dir;
-					sh_tmin = er.min_t;
-					sh_tmax = er.max_distance;
+					if(defer_refine)
+					{
+						sh_o = pos;
+						sh_d = to_light;
+						sh_tmin = __uint_as_float(hit.x);
+						sh_tmax = kFloatMax;
+						sh_refine = 1u;
+					}
+					else
+					{
+						const EscapeRay er = escape_fixed(a.refine, pos, ng, to_light);
+						sh_o = er.origin;
+						sh_d = er.unit_dir;
+						sh_tmin = er.min_t;
+						sh_tmax = er.max_distance;
+					}
 					ok = true;
 				}
 			}
 			else if(e.count > 0u)
 			{
 				const uint32_t j = e.first + min(static_cast<uint32_t>(rng.u01(bounce, DIM_NEE_TRI) * e.count), e.count - 1u);
-				const TriVerts lt = load_tri(s.tris, s.emitter_tris ? s.emitter_tris[j] : 0u, nullptr, nullptr);
+				const uint32_t light_tri = s.emitter_tris ? s.emitter_tris[j] : 0u;
+				const TriVerts lt = load_tri(s.tris, light_tri, nullptr, nullptr);
 				// Osada uniform triangle sampling (TBasicTriangle::sampleToBarycentricOsada)
 				const float su = sqrtf(rng.u01(bounce, DIM_NEE_U));
 				const float sv = rng.u01(bounce, DIM_NEE_V);
@@ -576,15 +595,29 @@ shade_kernel(ShadeArgs a)
 					const V3 target_to_emit = xe - pos;
 					if(pdf_w > 0.0f && isfinite(pdf_w) && sidedness_agreed(frame, target_to_emit))
 					{
-						const EscapeRay er = try_escape(a.refine, pos, ng, tri, xe, ne, lt);
-						if(er.ok)
+						if(defer_refine)
 						{
-							sh_o = er.origin;
-							sh_d = er.unit_dir;
-							sh_tmin = er.min_t;
-							sh_tmax = er.max_distance;
+							// a failed mutual escape zeroes the contribution in refine_kernel
+							sh_o = pos;
+							sh_d = xe;
+							sh_tmin = __uint_as_float(hit.x);
+							sh_tmax = __uint_as_float(light_tri);
+							sh_refine = 2u;
 							to_light = target_to_emit;
 							ok = true;
+						}
+						else
+						{
+							const EscapeRay er = try_escape_fixed(a.refine, pos, ng, xe, ne);
+							if(er.ok)
+							{
+								sh_o = er.origin;
+								sh_d = er.unit_dir;
+								sh_tmin = er.min_t;
+								sh_tmax = er.max_distance;
+								to_light = target_to_emit;
+								ok = true;
+							}
 						}
 					}
 				}
@@ -700,15 +733,24 @@ shade_kernel(ShadeArgs a)
 		if(continues)
 		{
 			slot = alloc_slot(&a.counters->n_next);
-			const EscapeRay off = escape(a.refine, pos, ng, tri, bs.l);
-			const V3 o = off.origin;
 			a.next.path[slot] = p;
 			a.next.meta[slot] = next_meta;
 			a.next.thr[slot] = make_float4(next_thr_emit.r, next_thr_emit.g, next_thr_emit.b, next_cont);
 			a.next.rad[slot] = make_float4(radiance.r, radiance.g, radiance.b, next_pdf);
 			a.next.prev[slot] = make_float4(pos.x, pos.y, pos.z, rr_scale);
-			a.next.ray_o[slot] = make_float4(o.x, o.y, o.z, off.min_t);
-			a.next.ray_d[slot] = make_float4(off.unit_dir.x, off.unit_dir.y, off.unit_dir.z, kFloatMax);
+			if(defer_refine)
+			{
+				a.next.ray_o[slot] = make_float4(pos.x, pos.y, pos.z, __uint_as_float(hit.x));
+				a.next.ray_d[slot] = make_float4(bs.l.x, bs.l.y, bs.l.z, kFloatMax);
+				a.refine_queue.single[alloc_slot(&a.counters->n_refine)] = slot;
+			}
+			else
+			{
+				const EscapeRay off = escape_fixed(a.refine, pos, ng, bs.l);
+				const V3 o = off.origin;
+				a.next.ray_o[slot] = make_float4(o.x, o.y, o.z, off.min_t);
+				a.next.ray_d[slot] = make_float4(off.unit_dir.x, off.unit_dir.y, off.unit_dir.z, kFloatMax);
+			}
 			if(GUIDED && (next_meta & kMetaGuideRec))
 			{
 				const float4* fr = reinterpret_cast<const float4*>(a.guide.feat + static_cast<size_t>(grow) * 8);
@@ -736,6 +778,68 @@ shade_kernel(ShadeArgs a)
 			if(!continues && a.film.filter != PG_FILTER_BOX)
 			{
 				a.shadow.r[k] = raster_position(a.film, pixel, rng);
+			}
+			if(sh_refine == 1u)
+			{
+				a.refine_queue.single[alloc_slot(&a.counters->n_refine)] = k | 0x80000000u;
+			}
+			else if(sh_refine == 2u)
+			{
+				a.refine_queue.mutual[alloc_slot(&a.counters->n_refine_mutual)] = k;
+			}
+		}
+	}
+}
+
+// The surface refinery of one iteration (iterative refine mode): every queued ray slot holds the
+// hit point and its leaf triangle (and, towards a light, the light point and its triangle); the
+// slot is rewritten with the refined origin, unit direction and range (SurfaceHitRefinery::escape
+// / tryEscape, SurfaceHitRefinery.h:200-360). One-sided escapes come first in the grid-stride
+// order and mutual ones after them, so nearly every warp runs one loop.
+__global__ void __launch_bounds__(kShadeBlock)
+refine_kernel(DeviceScene s, const RenderCounters* __restrict__ c, PathBuffers next, ShadowQueue shadow,
+              RefineQueue q, int iters)
+{
+	const uint32_t n_single = c->n_refine;
+	const uint32_t n = n_single + c->n_refine_mutual;
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		if(i < n_single)
+		{
+			const uint32_t r = q.single[i];
+			const uint32_t k = r & 0x7FFFFFFFu;
+			float4* o = (r & 0x80000000u) ? shadow.o + k : next.ray_o + k;
+			float4* d = (r & 0x80000000u) ? shadow.d + k : next.ray_d + k;
+			const float4 o4 = *o, d4 = *d;
+			const TriVerts tri = load_tri(s.tris, __float_as_uint(o4.w), nullptr, nullptr);
+			const EscapeRay e = escape_iterative(xyz(o4), face_normal(tri), tri, xyz(d4), iters);
+			*o = make_float4(e.origin.x, e.origin.y, e.origin.z, e.min_t);
+			*d = make_float4(e.unit_dir.x, e.unit_dir.y, e.unit_dir.z, e.max_distance);
+		}
+		else
+		{
+			const uint32_t k = q.mutual[i - n_single];
+			const float4 o4 = shadow.o[k], d4 = shadow.d[k];
+			const TriVerts tri = load_tri(s.tris, __float_as_uint(o4.w), nullptr, nullptr);
+			const TriVerts tri2 = load_tri(s.tris, __float_as_uint(d4.w), nullptr, nullptr);
+			const EscapeRay e = try_escape_iterative(xyz(o4), face_normal(tri), tri, xyz(d4), tri2, iters);
+			if(e.ok)
+			{
+				shadow.o[k] = make_float4(e.origin.x, e.origin.y, e.origin.z, e.min_t);
+				shadow.d[k] = make_float4(e.unit_dir.x, e.unit_dir.y, e.unit_dir.z, e.max_distance);
+			}
+			else
+			{
+				// no self-intersection-free segment: the light sample contributes nothing
+				// (the shading kernel counted it only if the escape succeeds)
+				const float4 c4 = shadow.c[k];
+				shadow.c[k] = make_float4(0.0f, 0.0f, 0.0f, c4.w);
+				if(shadow.t)
+				{
+					shadow.t[k].y = 0.0f;
+				}
+				shadow.o[k] = make_float4(o4.x, o4.y, o4.z, 0.0f);
+				shadow.d[k] = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
 			}
 		}
 	}
@@ -957,6 +1061,8 @@ void RenderScene::ensure_capacity(uint32_t capacity)
 	m_sd.resize(capacity);
 	m_sc.resize(capacity);
 	m_sr.resize(capacity);
+	m_req_single.resize(2 * static_cast<size_t>(capacity));   // continuation + environment NEE per path
+	m_req_mutual.resize(capacity);
 	m_capacity = capacity;
 }
 
@@ -1147,6 +1253,7 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 		sa.refine.mode = params.refine_mode;
 		sa.refine.delta = params.refine_delta;
 		sa.refine.iters = static_cast<int>(params.refine_iters);
+		sa.refine_queue = RefineQueue{m_req_single.get(), m_req_mutual.get()};
 		if(guided)
 		{
 			shade_kernel<true><<<grid, kShadeBlock, 0, st>>>(sa);
@@ -1156,6 +1263,12 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 			shade_kernel<false><<<grid, kShadeBlock, 0, st>>>(sa);
 		}
 		PG_CUDA_CHECK(cudaGetLastError());
+		if(params.refine_mode == PG_REFINE_ITERATIVE)
+		{
+			refine_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, nxt, sq, sa.refine_queue,
+			                                              static_cast<int>(params.refine_iters));
+			PG_CUDA_CHECK(cudaGetLastError());
+		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[5], st)); }
 		launch_shadow(m_dev, m_counters.get(), sq, nxt.rad, film, grid, 128, st, counting,
 		              training ? m_tdirw.get() : nullptr);
@@ -1305,9 +1418,10 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 	m_last_shadow = final_counters.shadow_rays;
 	m_last_iterations = iterations;
 	{
-		// prepare, regen, extend, shade, shadow; guide query + forward; training: weight sums
-		// (and clamp), forward, backward, Adam, step, repack, loss
-		const unsigned long long per_iteration = 5ull + (guided ? 2ull : 0ull) +
+		// prepare, regen, extend, shade, shadow (+ refine in the iterative mode); guide query +
+		// forward; training: weight sums (and clamp), forward, backward, Adam, step, repack, loss
+		const unsigned long long per_iteration = 5ull + (params.refine_mode == PG_REFINE_ITERATIVE ? 1ull : 0ull) +
+		                                         (guided ? 2ull : 0ull) +
 		                                         (training ? (m_guide_params.clamp > 0.0f ? 8ull : 6ull) : 0ull);
 		m_last_launches = iterations * per_iteration + (params.filter == PG_FILTER_BOX ? 1ull : 0ull);
 	}

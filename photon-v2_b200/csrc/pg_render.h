@@ -155,6 +155,19 @@ struct alignas(16) RenderCounters
 	uint32_t fetch_shadow;   // zeroed by prepare_kernel at the start of every iteration
 	uint32_t n_guided;       // guided vertices this iteration (network rows)
 	uint32_t n_train;        // training samples recorded this iteration (may exceed the batch)
+	uint32_t n_refine;       // surface-refinery requests this iteration: one-sided escapes
+	uint32_t n_refine_mutual;// and escapes towards a light-triangle point
+};
+
+// Surface-refinery requests of one iteration (iterative refine mode). The shading kernel leaves
+// the hit point and triangle in the ray slot it fills and queues the slot; the refinery kernel
+// replaces them with the refined origin and range. `single` entries are (slot | kind << 31):
+// kind 0 = a continuation ray in the next path buffer, 1 = a shadow ray towards a direction
+// (environment light); `mutual` entries are shadow rays towards a point on a light triangle.
+struct RefineQueue
+{
+	uint32_t* single;
+	uint32_t* mutual;
 };
 
 // Per-path state, one buffer of the ping-pong pair (structure of arrays).
@@ -261,6 +274,7 @@ private:
 	DeviceBuffer<uint2>    m_hits;
 	DeviceBuffer<float4>   m_so, m_sd, m_sc;
 	DeviceBuffer<float2>   m_sr;
+	DeviceBuffer<uint32_t> m_req_single, m_req_mutual;
 	DeviceBuffer<RenderCounters> m_counters;
 
 	// learned guiding

@@ -210,21 +210,41 @@ struct EscapeRay
 	bool  ok;
 };
 
-// SurfaceHitRefinery::escape (SurfaceHitRefinery.h:200-263).
-__device__ __forceinline__ EscapeRay escape(const RefineSettings& rs, V3 pos, V3 ng, const TriVerts& tri, V3 dir)
+// SurfaceHitRefinery::escape (SurfaceHitRefinery.h:200-263) in the iterative mode.
+__device__ __forceinline__ EscapeRay escape_iterative(V3 pos, V3 ng, const TriVerts& tri, V3 dir, int iters)
+{
+	const OffsetResult r = iterative_offset(pos, ng, tri, dir, iters);
+	EscapeRay e;
+	e.ok = true;
+	e.min_t = 0.0f;
+	e.origin = pos + r.offset;
+	e.unit_dir = r.unit_dir;
+	e.max_distance = r.max_distance;
+	return e;
+}
+
+// SurfaceHitRefinery::tryEscape (SurfaceHitRefinery.h:265-360) in the iterative mode.
+__device__ __forceinline__ EscapeRay try_escape_iterative(V3 pos, V3 ng, const TriVerts& tri, V3 pos2,
+                                                          const TriVerts& tri2, int iters)
+{
+	const OffsetResult r = iterative_mutual_offset(pos, ng, tri, pos2, tri2, iters);
+	EscapeRay e;
+	e.min_t = 0.0f;
+	e.origin = pos + r.offset;
+	e.unit_dir = r.unit_dir;
+	e.max_distance = r.max_distance;
+	e.ok = r.max_distance > 0.0f && isfinite(r.max_distance);
+	return e;
+}
+
+// SurfaceHitRefinery::escape in the empirical and manual modes (no re-intersection).
+__device__ __forceinline__ EscapeRay escape_fixed(const RefineSettings& rs, V3 pos, V3 ng, V3 dir)
 {
 	EscapeRay e;
 	e.ok = true;
 	e.min_t = 0.0f;
 	e.max_distance = kFloatMax;
-	if(rs.mode == PG_REFINE_ITERATIVE)
-	{
-		const OffsetResult r = iterative_offset(pos, ng, tri, dir, rs.iters);
-		e.origin = pos + r.offset;
-		e.unit_dir = r.unit_dir;
-		e.max_distance = r.max_distance;
-	}
-	else if(rs.mode == PG_REFINE_EMPIRICAL)
+	if(rs.mode == PG_REFINE_EMPIRICAL)
 	{
 		e.origin = pos + empirical_offset_vec(pos, ng, dir);
 		e.unit_dir = normalize(dir);
@@ -238,23 +258,14 @@ __device__ __forceinline__ EscapeRay escape(const RefineSettings& rs, V3 pos, V3
 	return e;
 }
 
-// SurfaceHitRefinery::tryEscape towards a point on another triangle (SurfaceHitRefinery.h:265-360).
-__device__ __forceinline__ EscapeRay try_escape(const RefineSettings& rs, V3 pos, V3 ng, const TriVerts& tri,
-                                                V3 pos2, V3 ng2, const TriVerts& tri2)
+// SurfaceHitRefinery::tryEscape in the empirical and manual modes.
+__device__ __forceinline__ EscapeRay try_escape_fixed(const RefineSettings& rs, V3 pos, V3 ng, V3 pos2, V3 ng2)
 {
 	EscapeRay e;
 	e.ok = false;
 	e.min_t = 0.0f;
 	e.max_distance = 0.0f;
-	if(rs.mode == PG_REFINE_ITERATIVE)
-	{
-		const OffsetResult r = iterative_mutual_offset(pos, ng, tri, pos2, tri2, rs.iters);
-		e.origin = pos + r.offset;
-		e.unit_dir = r.unit_dir;
-		e.max_distance = r.max_distance;
-		e.ok = r.max_distance > 0.0f && isfinite(r.max_distance);
-	}
-	else if(rs.mode == PG_REFINE_EMPIRICAL)
+	if(rs.mode == PG_REFINE_EMPIRICAL)
 	{
 		const V3 x_to_x2 = pos2 - pos;
 		const V3 origin = pos + empirical_offset_vec(pos, ng, x_to_x2);
