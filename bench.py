@@ -189,8 +189,12 @@ def roofline_of(kernel_ms: dict, rays: float, shadow_rays: float, iterations: fl
     bytes_closest = 40.0 + 80.0 * nodes_per_ray + 48.0 * tris_per_ray
     bytes_shadow = 48.0 + 80.0 * s_nodes + 48.0 * s_tris
     dominant = max(("extend_ms", "shadow_ms", "shade_ms"), key=lambda k: kernel_ms[k])
+    # one trace launch serves both queues (the any-hit slot then only times two empty events)
+    merged = kernel_ms["shadow_ms"] < 0.02 * kernel_ms["extend_ms"]
     if dominant == "shadow_ms":
         alg_bytes, kname = bytes_shadow * shadow_rays, "shadow (any hit)"
+    elif dominant == "extend_ms" and merged:
+        alg_bytes, kname = bytes_closest * rays + bytes_shadow * shadow_rays, "trace (closest + any hit)"
     elif dominant == "extend_ms":
         alg_bytes, kname = bytes_closest * rays, "extend (closest hit)"
     else:
@@ -203,7 +207,8 @@ def roofline_of(kernel_ms: dict, rays: float, shadow_rays: float, iterations: fl
         with open(prof_path) as f:
             rec = json.load(f).get(dominant) or {}
         if rec.get("dram_bytes_per_entry"):
-            entries = (shadow_rays if dominant == "shadow_ms" else rays) / max(1, iterations)
+            entries = (shadow_rays if dominant == "shadow_ms" else
+                       rays + shadow_rays if dominant == "extend_ms" and merged else rays) / max(1, iterations)
             traffic = rec["dram_bytes_per_entry"] * entries
     return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peaks["hbm_gbs"],
             "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,

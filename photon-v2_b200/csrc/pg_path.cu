@@ -189,6 +189,7 @@ __global__ void prepare_kernel(RenderCounters* c, uint32_t capacity)
 	c->gen_base = c->next_path;
 	c->next_path += n_new;
 	c->n_next = 0;
+	c->n_shadow_prev = c->n_shadow;
 	c->n_shadow = 0;
 	c->fetch_extend = 0;
 	c->fetch_shadow = 0;
@@ -1057,10 +1058,13 @@ void RenderScene::ensure_capacity(uint32_t capacity)
 		m_rd[b].resize(capacity);
 	}
 	m_hits.resize(capacity);
-	m_so.resize(capacity);
-	m_sd.resize(capacity);
-	m_sc.resize(capacity);
-	m_sr.resize(capacity);
+	for(int b = 0; b < 2; ++b)
+	{
+		m_so[b].resize(capacity);
+		m_sd[b].resize(capacity);
+		m_sc[b].resize(capacity);
+		m_sr[b].resize(capacity);
+	}
 	m_req_single.resize(2 * static_cast<size_t>(capacity));   // continuation + environment NEE per path
 	m_req_mutual.resize(capacity);
 	m_capacity = capacity;
@@ -1186,8 +1190,12 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 		buf[b] = PathBuffers{m_path[b].get(), m_meta[b].get(), m_thr[b].get(), m_rad[b].get(),
 		                     m_prev[b].get(), m_ro[b].get(), m_rd[b].get()};
 	}
-	ShadowQueue sq{m_so.get(), m_sd.get(), m_sc.get()};
-	sq.r = m_sr.get();
+	ShadowQueue sqs[2];
+	for(int b = 0; b < 2; ++b)
+	{
+		sqs[b] = ShadowQueue{m_so[b].get(), m_sd[b].get(), m_sc[b].get()};
+		sqs[b].r = m_sr[b].get();
+	}
 	const FilmView film = make_film_view(film_sums, params.width, params.height, params.filter);
 	const uint64_t first_global = params.first_sample * wh;
 	const bool counting = params.mode == PG_RENDER_COUNT;
@@ -1208,7 +1216,10 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 			buf[b].gf0 = m_gf0[b].get();
 			buf[b].gf1 = m_gf1[b].get();
 		}
-		sq.t = m_st.get();
+		if(training)
+		{
+			sqs[0].t = m_st.get();
+		}
 		gargs.map = m_gmap.get();
 		gargs.feat = m_gfeat.get();
 		gargs.raw = m_graw.get();
@@ -1225,6 +1236,11 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 		PG_CUDA_CHECK(cudaMemsetAsync(m_gscalars.get(), 0, 4 * sizeof(float), st));
 	}
 	RenderCounters* const d_counters = m_counters.get();
+	// The NEE segments made by an iteration's shading are traced by the next iteration's
+	// trace_kernel together with its closest-hit rays (one launch, one tail). Training renders
+	// keep a separate any-hit launch at the end of the iteration instead: the training step that
+	// ends the iteration needs the unoccluded NEE of its own samples.
+	const bool merged_shadows = !training;
 
 	// The five launches of one iteration; `ev` (optional) brackets each with events.
 	auto iteration = [&](int b, cudaEvent_t* ev)
@@ -1236,7 +1252,16 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[1], st)); }
 		regen_kernel<<<grid, kShadeBlock, 0, st>>>(m_counters.get(), m_dev.cam, film, params.seed, first_global, cur);
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[2], st)); }
-		launch_extend(m_dev, m_counters.get(), cur.ray_o, cur.ray_d, m_hits.get(), grid, 128, st, counting);
+		const ShadowQueue& sq = sqs[merged_shadows ? b : 0];   // this iteration's NEE segments
+		if(merged_shadows)
+		{
+			launch_trace(m_dev, d_counters, cur.ray_o, cur.ray_d, m_hits.get(), sqs[1 - b], cur.rad, film, st,
+			             counting);
+		}
+		else
+		{
+			launch_extend(m_dev, d_counters, cur.ray_o, cur.ray_d, m_hits.get(), grid, 128, st, counting);
+		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[3], st)); }
 		if(guided)
 		{
@@ -1270,8 +1295,11 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 			PG_CUDA_CHECK(cudaGetLastError());
 		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[5], st)); }
-		launch_shadow(m_dev, m_counters.get(), sq, nxt.rad, film, grid, 128, st, counting,
-		              training ? m_tdirw.get() : nullptr);
+		if(!merged_shadows)
+		{
+			launch_shadow(m_dev, d_counters, sq, nxt.rad, film, grid, 128, st, counting,
+			              training ? m_tdirw.get() : nullptr);
+		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[6], st)); }
 		if(training)
 		{
@@ -1359,7 +1387,8 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 			iterations += 2ull * batch;
 			PG_CUDA_CHECK(cudaMemcpyAsync(host_counters, m_counters.get(), sizeof(RenderCounters), cudaMemcpyDeviceToHost, st));
 			PG_CUDA_CHECK(cudaStreamSynchronize(st));
-			done = host_counters->next_path >= host_counters->total_paths && host_counters->n_next == 0;
+			done = host_counters->next_path >= host_counters->total_paths && host_counters->n_next == 0 &&
+			       (!merged_shadows || host_counters->n_shadow == 0);
 			if(host_counters->error)
 			{
 				break;
@@ -1397,7 +1426,8 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 					m_kernel_ms[slot[k]] += ms;
 				}
 			}
-			done = host_counters->next_path >= host_counters->total_paths && host_counters->n_next == 0;
+			done = host_counters->next_path >= host_counters->total_paths && host_counters->n_next == 0 &&
+			       (!merged_shadows || host_counters->n_shadow == 0);
 			if(host_counters->error)
 			{
 				break;
@@ -1418,9 +1448,11 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 	m_last_shadow = final_counters.shadow_rays;
 	m_last_iterations = iterations;
 	{
-		// prepare, regen, extend, shade, shadow (+ refine in the iterative mode); guide query +
-		// forward; training: weight sums (and clamp), forward, backward, Adam, step, repack, loss
-		const unsigned long long per_iteration = 5ull + (params.refine_mode == PG_REFINE_ITERATIVE ? 1ull : 0ull) +
+		// prepare, regen, trace (or extend + shadow), shade (+ refine in the iterative mode);
+		// guide query + forward; training: weight sums (and clamp), forward, backward, Adam, step,
+		// repack, loss
+		const unsigned long long per_iteration = (merged_shadows ? 4ull : 5ull) +
+		                                         (params.refine_mode == PG_REFINE_ITERATIVE ? 1ull : 0ull) +
 		                                         (guided ? 2ull : 0ull) +
 		                                         (training ? (m_guide_params.clamp > 0.0f ? 8ull : 6ull) : 0ull);
 		m_last_launches = iterations * per_iteration + (params.filter == PG_FILTER_BOX ? 1ull : 0ull);

@@ -140,7 +140,7 @@ struct alignas(16) RenderCounters
 	uint32_t n_active;      // continuing paths at the head of the current queue
 	uint32_t n_total;       // n_active + newly generated paths this iteration
 	uint32_t n_next;        // compaction counter of the next queue
-	uint32_t n_shadow;      // shadow queue length
+	uint32_t n_shadow;      // shadow queue length (records made this iteration)
 	unsigned long long next_path;   // next path index to generate
 	unsigned long long total_paths;
 	unsigned long long gen_base;    // first path index generated this iteration
@@ -155,6 +155,7 @@ struct alignas(16) RenderCounters
 	uint32_t fetch_shadow;   // zeroed by prepare_kernel at the start of every iteration
 	uint32_t n_guided;       // guided vertices this iteration (network rows)
 	uint32_t n_train;        // training samples recorded this iteration (may exceed the batch)
+	uint32_t n_shadow_prev;  // records made by the previous iteration, traced by this one's trace_kernel
 	uint32_t n_refine;       // surface-refinery requests this iteration: one-sided escapes
 	uint32_t n_refine_mutual;// and escapes towards a light-triangle point
 };
@@ -216,6 +217,11 @@ constexpr uint32_t kTargetFinal = 0x80000000u;
 // Launchers implemented in pg_trace.cu (FMA-enabled traversal kernels).
 void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4* ray_o,
                    const float4* ray_d, uint2* hits, int grid, int block, cudaStream_t st, bool count);
+// Closest hits of this iteration's queue and visibility of the previous iteration's shadow
+// queue `prev` in one persistent launch; unoccluded contributions go to rad_cur / the film.
+void launch_trace(const DeviceScene& s, RenderCounters* counters, const float4* ray_o, const float4* ray_d,
+                  uint2* hits, const ShadowQueue& prev, float4* rad_cur, const FilmView& film, cudaStream_t st,
+                  bool count);
 void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
                    float4* rad_next, const FilmView& film, int grid, int block, cudaStream_t st, bool count,
                    float4* train_dirw = nullptr);
@@ -272,8 +278,8 @@ private:
 	DeviceBuffer<uint32_t> m_path[2], m_meta[2];
 	DeviceBuffer<float4>   m_thr[2], m_rad[2], m_prev[2], m_ro[2], m_rd[2];
 	DeviceBuffer<uint2>    m_hits;
-	DeviceBuffer<float4>   m_so, m_sd, m_sc;
-	DeviceBuffer<float2>   m_sr;
+	DeviceBuffer<float4>   m_so[2], m_sd[2], m_sc[2];   // shadow queues, one per iteration parity
+	DeviceBuffer<float2>   m_sr[2];
 	DeviceBuffer<uint32_t> m_req_single, m_req_mutual;
 	DeviceBuffer<RenderCounters> m_counters;
 

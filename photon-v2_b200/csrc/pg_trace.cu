@@ -211,8 +211,107 @@ extend_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tr
 	}
 }
 
-// Visibility of the NEE segments; unoccluded contributions go to the owning path (slot in the
-// next state buffer) or, for paths that ended at that vertex, straight to the FP64 film.
+// An unoccluded NEE contribution (shadow record i): to the owning path's radiance (slot in the
+// path buffer the record was made for) or, for paths that ended at that vertex, straight to the
+// FP64 film; guided renders also credit the training sample the record belongs to.
+__device__ __forceinline__ void add_unoccluded(uint32_t i, const float4* __restrict__ sc,
+                                               const float2* __restrict__ st, const float2* __restrict__ sr,
+                                               float4* __restrict__ rad_target, const FilmView& film,
+                                               float4* __restrict__ train_dirw)
+{
+	if(train_dirw)
+	{
+		const float2 tr = __ldg(st + i);
+		const uint32_t row = __float_as_uint(tr.x);
+		if(row != 0xFFFFFFFFu && tr.y != 0.0f)
+		{
+			atomicAdd(&train_dirw[row].w, tr.y);
+		}
+	}
+	const float4 c = __ldg(sc + i);
+	const uint32_t target = __float_as_uint(c.w);
+	if(target & kTargetFinal)
+	{
+		if(film.filter == PG_FILTER_BOX)
+		{
+			film_add_box(film, target & ~kTargetFinal, c.x, c.y, c.z);
+		}
+		else
+		{
+			const float2 r = __ldg(sr + i);
+			film_deposit(film, r.x, r.y, make_float4(c.x, c.y, c.z, 0.0f));
+		}
+	}
+	else
+	{
+		float4 rv = rad_target[target];
+		rv.x += c.x;
+		rv.y += c.y;
+		rv.z += c.z;
+		rad_target[target] = rv;
+	}
+}
+
+// One launch for both traversal queues of an iteration: the closest hits of this iteration's
+// rays, then the visibility of the previous iteration's NEE segments, whose owning paths sit in
+// this iteration's path buffer (their radiance is read by this iteration's shading, after this
+// kernel). A single dynamic-fetch cursor runs over both queues, so the launch has one tail.
+template<bool COUNT>
+__global__ void __launch_bounds__(kTraceBlock)
+trace_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
+             RenderCounters* __restrict__ counters,
+             const float4* __restrict__ ray_o, const float4* __restrict__ ray_d, uint2* __restrict__ hits,
+             const float4* __restrict__ so, const float4* __restrict__ sd, const float4* __restrict__ sc,
+             const float2* __restrict__ sr, float4* __restrict__ rad_cur, FilmView film)
+{
+	const uint32_t n_closest = counters->n_total;
+	const uint32_t n_shadow = counters->n_shadow_prev;
+	if(blockIdx.x == 0 && threadIdx.x == 0)
+	{
+		counters->shadow_rays += n_shadow;
+	}
+	uint32_t err = 0, node_count[2] = {0u, 0u}, tri_count[2] = {0u, 0u};
+	traverse_persistent<false, COUNT, true>(nodes, tris, n_closest + n_shadow, &counters->fetch_extend,
+		[&](uint32_t i, float4* a, float4* b)
+		{
+			if(i < n_closest)
+			{
+				*a = __ldg(ray_o + i);
+				*b = __ldg(ray_d + i);
+			}
+			else
+			{
+				*a = __ldg(so + (i - n_closest));
+				*b = __ldg(sd + (i - n_closest));
+			}
+		},
+		[&](uint32_t i, bool hit, uint32_t tri, float t)
+		{
+			if(i < n_closest)
+			{
+				hits[i] = make_uint2(hit ? tri : 0xFFFFFFFFu, __float_as_uint(t));
+			}
+			else if(!hit)
+			{
+				add_unoccluded(i - n_closest, sc, nullptr, sr, rad_cur, film, nullptr);
+			}
+		},
+		&err, node_count, tri_count, n_closest);
+	if(COUNT)
+	{
+		atomicAdd(&counters->nodes_closest, static_cast<unsigned long long>(node_count[0]));
+		atomicAdd(&counters->tris_closest, static_cast<unsigned long long>(tri_count[0]));
+		atomicAdd(&counters->nodes_any, static_cast<unsigned long long>(node_count[1]));
+		atomicAdd(&counters->tris_any, static_cast<unsigned long long>(tri_count[1]));
+	}
+	if(err)
+	{
+		atomicOr(&counters->error, err);
+	}
+}
+
+// Visibility of the NEE segments of this iteration (guided training renders, whose training
+// step at the end of the iteration needs them); see add_unoccluded.
 template<bool COUNT>
 __global__ void __launch_bounds__(kTraceBlock)
 shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
@@ -231,41 +330,9 @@ shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tr
 		[&](uint32_t i, float4* a, float4* b) { *a = __ldg(so + i); *b = __ldg(sd + i); },
 		[&](uint32_t i, bool occluded, uint32_t, float)
 		{
-			if(occluded)
+			if(!occluded)
 			{
-				return;
-			}
-			if(train_dirw)
-			{
-				// guided renders: the unoccluded direct light joins the training sample it belongs to
-				const float2 tr = __ldg(st + i);
-				const uint32_t row = __float_as_uint(tr.x);
-				if(row != 0xFFFFFFFFu && tr.y != 0.0f)
-				{
-					atomicAdd(&train_dirw[row].w, tr.y);
-				}
-			}
-			const float4 c = __ldg(sc + i);
-			const uint32_t target = __float_as_uint(c.w);
-			if(target & kTargetFinal)
-			{
-				if(film.filter == PG_FILTER_BOX)
-				{
-					film_add_box(film, target & ~kTargetFinal, c.x, c.y, c.z);
-				}
-				else
-				{
-					const float2 r = __ldg(sr + i);
-					film_deposit(film, r.x, r.y, make_float4(c.x, c.y, c.z, 0.0f));
-				}
-			}
-			else
-			{
-				float4 rv = rad_next[target];
-				rv.x += c.x;
-				rv.y += c.y;
-				rv.z += c.z;
-				rad_next[target] = rv;
+				add_unoccluded(i, sc, st, sr, rad_next, film, train_dirw);
 			}
 		},
 		&err, &node_count, &tri_count);
@@ -294,6 +361,25 @@ void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4*
 	{
 		static const int grid = persistent_grid(extend_kernel<false>);
 		extend_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits);
+	}
+	PG_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_trace(const DeviceScene& s, RenderCounters* counters, const float4* ray_o, const float4* ray_d,
+                  uint2* hits, const ShadowQueue& prev, float4* rad_cur, const FilmView& film, cudaStream_t st,
+                  bool count)
+{
+	if(count)
+	{
+		static const int grid = persistent_grid(trace_kernel<true>);
+		trace_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
+		                                                 prev.o, prev.d, prev.c, prev.r, rad_cur, film);
+	}
+	else
+	{
+		static const int grid = persistent_grid(trace_kernel<false>);
+		trace_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
+		                                                  prev.o, prev.d, prev.c, prev.r, rad_cur, film);
 	}
 	PG_CUDA_CHECK(cudaGetLastError());
 }

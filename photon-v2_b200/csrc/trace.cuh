@@ -367,17 +367,22 @@ __device__ __forceinline__ bool traverse(
 // Fetch(uint32_t i, float4* origin_tmin, float4* dir_tmax) loads ray i; Finish(uint32_t i,
 // bool hit, uint32_t leaf_tri, float t) consumes its result. n rays are taken from *next_ray,
 // which must be zero when the launch starts. Every lane of the warp must call this function.
+//
+// MIXED: rays [0, n_closest) are closest-hit queries and rays [n_closest, n) any-hit queries, so
+// one launch serves both queues (each lane switches per ray); counts go to node_count[0] /
+// tri_count[0] for closest-hit rays and [1] for any-hit rays.
 
 constexpr uint32_t kFullWarp = 0xFFFFFFFFu;
 constexpr int kRefillMinIdle = 8;
 
-template<bool ANY_HIT, bool COUNT, class Fetch, class Finish>
+template<bool ANY_HIT, bool COUNT, bool MIXED = false, class Fetch, class Finish>
 __device__ __forceinline__ void traverse_persistent(
 	const WideNode* __restrict__ nodes,
 	const LeafTri* __restrict__ tris,
 	uint32_t n, uint32_t* __restrict__ next_ray,
 	Fetch fetch, Finish finish,
-	uint32_t* out_error, uint32_t* node_count = nullptr, uint32_t* tri_count = nullptr)
+	uint32_t* out_error, uint32_t* node_count = nullptr, uint32_t* tri_count = nullptr,
+	uint32_t n_closest = 0)
 {
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint32_t lanes_below = (1u << lane) - 1u;
@@ -392,6 +397,7 @@ __device__ __forceinline__ void traverse_persistent(
 	uint32_t tri_base = 0, tri_hits = 0;
 	uint32_t ray = 0;
 	bool has_ray = false;
+	bool any_hit = ANY_HIT;   // this lane's query (varies per ray only when MIXED)
 	bool exhausted = false;   // warp-uniform: the counter has passed n
 
 	while(true)
@@ -428,6 +434,7 @@ __device__ __forceinline__ void traverse_persistent(
 					sp = 0;
 					ray = i;
 					has_ray = true;
+					if(MIXED) { any_hit = i >= n_closest; }
 				}
 			}
 		}
@@ -446,11 +453,11 @@ __device__ __forceinline__ void traverse_persistent(
 			const uint32_t bit = __ffs(tri_hits) - 1u;
 			tri_hits &= tri_hits - 1u;
 			const uint32_t k = tri_base + bit;
-			if(COUNT) { ++*tri_count; }
+			if(COUNT) { ++tri_count[MIXED && any_hit ? 1 : 0]; }
 			float t, b0, b1, b2;
 			if(watertight_hit_tri(r, tris, k, t_min, best_t, &t, &b0, &b1, &b2))
 			{
-				if(ANY_HIT)
+				if(MIXED ? any_hit : ANY_HIT)
 				{
 					best_t = t;
 					best_tri = k;
@@ -497,7 +504,7 @@ __device__ __forceinline__ void traverse_persistent(
 					}
 				}
 				const uint32_t hits = intersect_children(r, nodes, child, t_min, best_t, &child_base, &tri_base, &imask);
-				if(COUNT) { ++*node_count; }
+				if(COUNT) { ++node_count[MIXED && any_hit ? 1 : 0]; }
 				node_hits = hits >> 24;
 				tri_hits = hits & 0x00FFFFFFu;
 			}
