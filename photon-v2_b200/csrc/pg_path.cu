@@ -159,6 +159,29 @@ __global__ void box_weights_kernel(double* sums, uint32_t num_pixels, double spp
 	}
 }
 
+// Lists every slot of the current queue under its shading class (kShadeClasses): 0 for a miss,
+// 1 + the material type of the hit surface. Lanes of one class share one atomic.
+__global__ void __launch_bounds__(kShadeBlock)
+classify_kernel(DeviceScene s, RenderCounters* __restrict__ c, const uint2* __restrict__ hits,
+                uint32_t* __restrict__ order, uint32_t capacity)
+{
+	const uint32_t n = c->n_total;
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		const uint32_t tri = hits[i].x;
+		const uint32_t cls = tri == 0xFFFFFFFFu ? 0u
+		                                        : min(1u + s.materials[__ldg(&s.tris[tri].material)].type, kShadeClasses - 1u);
+		const cg::coalesced_group peers = cg::labeled_partition(cg::coalesced_threads(), cls);
+		uint32_t base = 0;
+		if(peers.thread_rank() == 0)
+		{
+			base = atomicAdd(&c->n_class[cls], peers.size());
+		}
+		base = peers.shfl(base, 0);
+		order[cls * capacity + base + peers.thread_rank()] = i;
+	}
+}
+
 // Warp-aggregated slot allocation on a queue counter.
 __device__ __forceinline__ uint32_t alloc_slot(uint32_t* counter)
 {
@@ -198,6 +221,10 @@ __global__ void prepare_kernel(RenderCounters* c, uint32_t capacity)
 	c->n_train = 0;
 	c->n_refine = 0;
 	c->n_refine_mutual = 0;
+	for(uint32_t k = 0; k < kShadeClasses; ++k)
+	{
+		c->n_class[k] = 0;
+	}
 	c->rays_traced += c->n_total;
 }
 
@@ -348,6 +375,8 @@ struct ShadeArgs
 	GuideArgs     guide;
 	RefineSettings refine;
 	RefineQueue   refine_queue;   // iterative refine mode: requests for refine_kernel
+	const uint32_t* order;        // slots listed per shading class (classify_kernel), or null: slot order
+	uint32_t      order_capacity; // slots per class region of `order`
 };
 
 __device__ __forceinline__ float4 cur_gf0(const ShadeArgs& a, uint32_t i) { return a.cur.gf0[i]; }
@@ -360,8 +389,30 @@ shade_kernel(ShadeArgs a)
 {
 	const uint32_t total = a.counters->n_total;
 	const DeviceScene& s = a.scene;
-	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+	// work item w -> queue slot: class by class through the lists trace_kernel made
+	__shared__ uint32_t class_end[kShadeClasses];
+	if(a.order && threadIdx.x == 0)
 	{
+		uint32_t end = 0;
+		for(uint32_t c = 0; c < kShadeClasses; ++c)
+		{
+			end += a.counters->n_class[c];
+			class_end[c] = end;
+		}
+	}
+	__syncthreads();
+	for(uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < total; w += gridDim.x * blockDim.x)
+	{
+		uint32_t i = w;
+		if(a.order)
+		{
+			uint32_t c = 0;
+			while(c + 1 < kShadeClasses && w >= class_end[c])
+			{
+				++c;
+			}
+			i = a.order[c * a.order_capacity + (w - (c ? class_end[c - 1] : 0u))];
+		}
 		const uint32_t p = a.cur.path[i];
 		const uint32_t meta = a.cur.meta[i];
 		const uint32_t bounce = meta & kMetaBounceMask;
@@ -1067,6 +1118,7 @@ void RenderScene::ensure_capacity(uint32_t capacity)
 	}
 	m_req_single.resize(2 * static_cast<size_t>(capacity));   // continuation + environment NEE per path
 	m_req_mutual.resize(capacity);
+	m_order.resize(static_cast<size_t>(kShadeClasses) * capacity);
 	m_capacity = capacity;
 }
 
@@ -1257,6 +1309,8 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 		{
 			launch_trace(m_dev, d_counters, cur.ray_o, cur.ray_d, m_hits.get(), sqs[1 - b], cur.rad, film, st,
 			             counting);
+			classify_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, m_hits.get(), m_order.get(), m_capacity);
+			PG_CUDA_CHECK(cudaGetLastError());
 		}
 		else
 		{
@@ -1279,6 +1333,8 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 		sa.refine.delta = params.refine_delta;
 		sa.refine.iters = static_cast<int>(params.refine_iters);
 		sa.refine_queue = RefineQueue{m_req_single.get(), m_req_mutual.get()};
+		sa.order = merged_shadows ? m_order.get() : nullptr;
+		sa.order_capacity = m_capacity;
 		if(guided)
 		{
 			shade_kernel<true><<<grid, kShadeBlock, 0, st>>>(sa);
@@ -1448,10 +1504,10 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 	m_last_shadow = final_counters.shadow_rays;
 	m_last_iterations = iterations;
 	{
-		// prepare, regen, trace (or extend + shadow), shade (+ refine in the iterative mode);
-		// guide query + forward; training: weight sums (and clamp), forward, backward, Adam, step,
-		// repack, loss
-		const unsigned long long per_iteration = (merged_shadows ? 4ull : 5ull) +
+		// prepare, regen, trace + classify (or extend + shadow), shade (+ refine in the iterative
+		// mode); guide query + forward; training: weight sums (and clamp), forward, backward, Adam,
+		// step, repack, loss
+		const unsigned long long per_iteration = 5ull +
 		                                         (params.refine_mode == PG_REFINE_ITERATIVE ? 1ull : 0ull) +
 		                                         (guided ? 2ull : 0ull) +
 		                                         (training ? (m_guide_params.clamp > 0.0f ? 8ull : 6ull) : 0ull);

@@ -134,6 +134,11 @@ struct DeviceScene
 	Camera            cam;
 };
 
+// Shading classes of a closest-hit result: 0 = miss, then 1 + the hit surface's material type
+// (matte, conductor, dielectric, absorber). classify_kernel lists the queue slots of each class
+// so that the shading kernel's warps mostly run one material's code.
+constexpr uint32_t kShadeClasses = 5;
+
 // Counters shared by the kernels of one render (device memory).
 struct alignas(16) RenderCounters
 {
@@ -156,6 +161,7 @@ struct alignas(16) RenderCounters
 	uint32_t n_guided;       // guided vertices this iteration (network rows)
 	uint32_t n_train;        // training samples recorded this iteration (may exceed the batch)
 	uint32_t n_shadow_prev;  // records made by the previous iteration, traced by this one's trace_kernel
+	uint32_t n_class[kShadeClasses];   // closest-hit results per shading class (classify_kernel)
 	uint32_t n_refine;       // surface-refinery requests this iteration: one-sided escapes
 	uint32_t n_refine_mutual;// and escapes towards a light-triangle point
 };
@@ -281,6 +287,7 @@ private:
 	DeviceBuffer<float4>   m_so[2], m_sd[2], m_sc[2];   // shadow queues, one per iteration parity
 	DeviceBuffer<float2>   m_sr[2];
 	DeviceBuffer<uint32_t> m_req_single, m_req_mutual;
+	DeviceBuffer<uint32_t> m_order;   // shading order: kShadeClasses regions of m_capacity slots
 	DeviceBuffer<RenderCounters> m_counters;
 
 	// learned guiding
