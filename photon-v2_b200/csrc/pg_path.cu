@@ -160,25 +160,29 @@ __global__ void box_weights_kernel(double* sums, uint32_t num_pixels, double spp
 }
 
 // Lists every slot of the current queue under its shading class (kShadeClasses): 0 for a miss,
-// 1 + the material type of the hit surface. Lanes of one class share one atomic.
+// 1 + the material type of the hit surface, in the list of that class for this block's residue
+// (kClassLists). Lanes of one class share one atomic. `list_capacity` bounds the slots one list
+// can receive: the slots all blocks of one residue visit in the grid-stride loop.
 __global__ void __launch_bounds__(kShadeBlock)
 classify_kernel(DeviceScene s, RenderCounters* __restrict__ c, const uint2* __restrict__ hits,
-                uint32_t* __restrict__ order, uint32_t capacity)
+                uint32_t* __restrict__ order, uint32_t list_capacity)
 {
 	const uint32_t n = c->n_total;
+	const uint32_t residue = blockIdx.x % kClassLists;
 	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		const uint32_t tri = hits[i].x;
 		const uint32_t cls = tri == 0xFFFFFFFFu ? 0u
 		                                        : min(1u + s.materials[__ldg(&s.tris[tri].material)].type, kShadeClasses - 1u);
+		const uint32_t list = cls * kClassLists + residue;
 		const cg::coalesced_group peers = cg::labeled_partition(cg::coalesced_threads(), cls);
 		uint32_t base = 0;
 		if(peers.thread_rank() == 0)
 		{
-			base = atomicAdd(&c->n_class[cls], peers.size());
+			base = atomicAdd(&c->n_class[list], peers.size());
 		}
 		base = peers.shfl(base, 0);
-		order[cls * capacity + base + peers.thread_rank()] = i;
+		order[list * list_capacity + base + peers.thread_rank()] = i;
 	}
 }
 
@@ -221,7 +225,7 @@ __global__ void prepare_kernel(RenderCounters* c, uint32_t capacity)
 	c->n_train = 0;
 	c->n_refine = 0;
 	c->n_refine_mutual = 0;
-	for(uint32_t k = 0; k < kShadeClasses; ++k)
+	for(uint32_t k = 0; k < kOrderLists; ++k)
 	{
 		c->n_class[k] = 0;
 	}
@@ -376,7 +380,7 @@ struct ShadeArgs
 	RefineSettings refine;
 	RefineQueue   refine_queue;   // iterative refine mode: requests for refine_kernel
 	const uint32_t* order;        // slots listed per shading class (classify_kernel), or null: slot order
-	uint32_t      order_capacity; // slots per class region of `order`
+	uint32_t      order_capacity; // slots per list of `order`
 };
 
 __device__ __forceinline__ float4 cur_gf0(const ShadeArgs& a, uint32_t i) { return a.cur.gf0[i]; }
@@ -389,15 +393,15 @@ shade_kernel(ShadeArgs a)
 {
 	const uint32_t total = a.counters->n_total;
 	const DeviceScene& s = a.scene;
-	// work item w -> queue slot: class by class through the lists trace_kernel made
-	__shared__ uint32_t class_end[kShadeClasses];
+	// work item w -> queue slot: list by list (class-major) through the lists classify_kernel made
+	__shared__ uint32_t list_end[kOrderLists];
 	if(a.order && threadIdx.x == 0)
 	{
 		uint32_t end = 0;
-		for(uint32_t c = 0; c < kShadeClasses; ++c)
+		for(uint32_t l = 0; l < kOrderLists; ++l)
 		{
-			end += a.counters->n_class[c];
-			class_end[c] = end;
+			end += a.counters->n_class[l];
+			list_end[l] = end;
 		}
 	}
 	__syncthreads();
@@ -406,12 +410,14 @@ shade_kernel(ShadeArgs a)
 		uint32_t i = w;
 		if(a.order)
 		{
-			uint32_t c = 0;
-			while(c + 1 < kShadeClasses && w >= class_end[c])
+			// first list whose end exceeds w
+			uint32_t lo = 0, hi = kOrderLists - 1u;
+			while(lo < hi)
 			{
-				++c;
+				const uint32_t mid = (lo + hi) >> 1;
+				if(w < list_end[mid]) { hi = mid; } else { lo = mid + 1u; }
 			}
-			i = a.order[c * a.order_capacity + (w - (c ? class_end[c - 1] : 0u))];
+			i = a.order[lo * a.order_capacity + (w - (lo ? list_end[lo - 1u] : 0u))];
 		}
 		const uint32_t p = a.cur.path[i];
 		const uint32_t meta = a.cur.meta[i];
@@ -1118,7 +1124,13 @@ void RenderScene::ensure_capacity(uint32_t capacity)
 	}
 	m_req_single.resize(2 * static_cast<size_t>(capacity));   // continuation + environment NEE per path
 	m_req_mutual.resize(capacity);
-	m_order.resize(static_cast<size_t>(kShadeClasses) * capacity);
+	{
+		// the slots the blocks of one residue visit in classify_kernel's grid-stride loop
+		const uint32_t grid = static_cast<uint32_t>(sm_count()) * 8u;
+		const uint32_t rounds = (capacity + grid * kShadeBlock - 1u) / (grid * kShadeBlock);
+		m_order_list = (grid + kClassLists - 1u) / kClassLists * rounds * kShadeBlock;
+		m_order.resize(static_cast<size_t>(kOrderLists) * m_order_list);
+	}
 	m_capacity = capacity;
 }
 
@@ -1309,7 +1321,7 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 		{
 			launch_trace(m_dev, d_counters, cur.ray_o, cur.ray_d, m_hits.get(), sqs[1 - b], cur.rad, film, st,
 			             counting);
-			classify_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, m_hits.get(), m_order.get(), m_capacity);
+			classify_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, m_hits.get(), m_order.get(), m_order_list);
 			PG_CUDA_CHECK(cudaGetLastError());
 		}
 		else
@@ -1334,7 +1346,7 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 		sa.refine.iters = static_cast<int>(params.refine_iters);
 		sa.refine_queue = RefineQueue{m_req_single.get(), m_req_mutual.get()};
 		sa.order = merged_shadows ? m_order.get() : nullptr;
-		sa.order_capacity = m_capacity;
+		sa.order_capacity = m_order_list;
 		if(guided)
 		{
 			shade_kernel<true><<<grid, kShadeBlock, 0, st>>>(sa);

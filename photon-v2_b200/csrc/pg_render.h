@@ -136,8 +136,12 @@ struct DeviceScene
 
 // Shading classes of a closest-hit result: 0 = miss, then 1 + the hit surface's material type
 // (matte, conductor, dielectric, absorber). classify_kernel lists the queue slots of each class
-// so that the shading kernel's warps mostly run one material's code.
+// so that the shading kernel's warps mostly run one material's code. Each class has kClassLists
+// lists, one per residue of the block index, so that the list counters' atomics spread over
+// kOrderLists addresses instead of queuing on five.
 constexpr uint32_t kShadeClasses = 5;
+constexpr uint32_t kClassLists = 16;
+constexpr uint32_t kOrderLists = kShadeClasses * kClassLists;
 
 // Counters shared by the kernels of one render (device memory).
 struct alignas(16) RenderCounters
@@ -161,7 +165,7 @@ struct alignas(16) RenderCounters
 	uint32_t n_guided;       // guided vertices this iteration (network rows)
 	uint32_t n_train;        // training samples recorded this iteration (may exceed the batch)
 	uint32_t n_shadow_prev;  // records made by the previous iteration, traced by this one's trace_kernel
-	uint32_t n_class[kShadeClasses];   // closest-hit results per shading class (classify_kernel)
+	uint32_t n_class[kOrderLists];   // closest-hit results per shading-class list (classify_kernel)
 	uint32_t n_refine;       // surface-refinery requests this iteration: one-sided escapes
 	uint32_t n_refine_mutual;// and escapes towards a light-triangle point
 };
@@ -287,7 +291,8 @@ private:
 	DeviceBuffer<float4>   m_so[2], m_sd[2], m_sc[2];   // shadow queues, one per iteration parity
 	DeviceBuffer<float2>   m_sr[2];
 	DeviceBuffer<uint32_t> m_req_single, m_req_mutual;
-	DeviceBuffer<uint32_t> m_order;   // shading order: kShadeClasses regions of m_capacity slots
+	DeviceBuffer<uint32_t> m_order;   // shading order: kOrderLists lists of m_order_list slots
+	uint32_t m_order_list = 0;
 	DeviceBuffer<RenderCounters> m_counters;
 
 	// learned guiding
