@@ -57,9 +57,7 @@ def write_scene(scene: scenes.Scene, directory: str) -> str:
     path = os.path.join(directory, "scene.p2")
     with open(path, "w") as f:
         f.write(scenes.to_sdl(scene))
-    if scene.env_radiance is not None:
-        scenes.write_pfm(os.path.join(directory, "env.pfm"),
-                         np.array(scene.env_radiance, np.float32).reshape(1, 1, 3))
+    scenes.write_env(scene, directory)
     return path
 
 

@@ -115,6 +115,11 @@ extern PH_API void phGpuSetGuiding(PhUInt64 engineId, PhBool enabled);
 /* BVH builder of the next phUpdate: 0 host binned SAH (default), 1 on the GPU from Morton-ordered
  * triangles (seconds faster on multi-million-triangle scenes, somewhat costlier to traverse). */
 extern PH_API void phGpuSetBvhBuilder(PhUInt64 engineId, PhUInt32 builder);
+/* Densities of dome (image-dome) light samples: 0 (the default) as the reference computes them on
+ * its finite dome sphere (Core/Intersection/PLatLongEnvSphere.cpp:125-186, lta::pdfA_to_pdfW),
+ * which matches its images but is biased away from the dome centre; 1 the exact density of the
+ * sampled direction (unbiased). Invalid values are ignored. */
+extern PH_API void phGpuSetDomePdf(PhUInt64 engineId, PhUInt32 mode);
 /* Surface refinement of rays leaving surfaces, as the reference's EngineConfig.ini sets it
  * (RefineMode / SelfIntersectDelta / NumIterativeSurfaceRefinements, which phInit also reads from
  * ./Config/EngineConfig.ini when the file exists): mode 0 manual, 1 empirical, 2 iterative

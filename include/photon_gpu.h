@@ -169,6 +169,9 @@ PGPU_API int pgpu_scene_film(uint64_t id, float* out_rgb, double* out_sum, uint6
  * Engine/Source/Core/Filmic/HdrRgbFilm.cpp:82-123, SampleFilter.cpp:12-61): 0 box (the default
  * here), 1 gaussian, 2 mitchell-netravali, 3 blackman-harris. Clears the film. */
 PGPU_API int pgpu_scene_set_filter(uint64_t id, uint32_t filter);
+/* Densities of environment light samples: 0 the reference's (default), 1 exact; see
+ * phGpuSetDomePdf in ph_c_core.h. */
+PGPU_API int pgpu_scene_set_dome_pdf(uint64_t id, uint32_t mode);
 /* A render into a scratch film with every kernel bracketed by CUDA events: per-kernel device
  * milliseconds (prepare, regen, extend, shade, shadow, guide inference, guide training). */
 PGPU_API int pgpu_scene_profile(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator,

@@ -467,6 +467,17 @@ void phGpuSetBvhBuilder(PhUInt64 engineId, PhUInt32 builder)
 	}
 }
 
+void phGpuSetDomePdf(PhUInt64 engineId, PhUInt32 mode)
+{
+	if(auto e = engines().get(engineId))
+	{
+		if(mode <= 1u)
+		{
+			e->engine.set_dome_pdf(mode);
+		}
+	}
+}
+
 void phGpuSetGuiding(PhUInt64 engineId, PhBool enabled)
 {
 	if(auto e = engines().get(engineId))

@@ -253,6 +253,7 @@ void Engine::update()
 		m_info.num_triangles = desc.tris.size() / 9;
 		m_render = make_render_object(std::move(desc));
 		m_render->filter = m_filter;
+		m_render->scene->set_dome_exact(m_dome_pdf == 1u);
 	}
 	catch(const std::exception& e)
 	{
@@ -711,13 +712,39 @@ void Engine::cook(SceneDesc& desc)
 				{
 					throw std::runtime_error("cannot read dome image " + path + " (PFM only)");
 				}
-				if(img.width != 1 || img.height != 1)
+				if(img.width == 0 || img.height == 0 || img.rgb.size() != static_cast<std::size_t>(img.width) * img.height * 3)
 				{
-					throw std::runtime_error("only constant (1x1) dome images are supported by the GPU renderer");
+					throw std::runtime_error("dome image " + path + " is empty");
 				}
 				const double scale = get_real(a.clauses, "energy-scale", 1.0);
 				desc.has_env = true;
-				for(int k = 0; k < 3; ++k) { desc.env_rgb[k] = static_cast<float>(img.rgb[k] * scale); }
+				if(img.width == 1 && img.height == 1)
+				{
+					// constant environment
+					for(int k = 0; k < 3; ++k) { desc.env_rgb[k] = static_cast<float>(img.rgb[k] * scale); }
+				}
+				else
+				{
+					// lat-long image, row 0 at the bottom (looking down), and the dome's rotation
+					// (its scale has no effect, ADome.cpp:25-40)
+					desc.env_width = img.width;
+					desc.env_height = img.height;
+					desc.env_image.resize(img.rgb.size());
+					double mean[3] = {0, 0, 0};
+					for(std::size_t k = 0; k < img.rgb.size(); ++k)
+					{
+						desc.env_image[k] = static_cast<float>(img.rgb[k] * scale);
+						mean[k % 3] += desc.env_image[k];
+					}
+					for(int k = 0; k < 3; ++k) { desc.env_rgb[k] = static_cast<float>(mean[k] / (img.width * img.height)); }
+					for(int c = 0; c < 3; ++c)
+					{
+						const double axis[3] = {c == 0 ? 1.0 : 0.0, c == 1 ? 1.0 : 0.0, c == 2 ? 1.0 : 0.0};
+						double col[3];
+						quat_rotate(a.rot, axis, col);
+						for(int r = 0; r < 3; ++r) { desc.env_rot[3 * r + c] = static_cast<float>(col[r]); }
+					}
+				}
 				for(int k = 0; k < 3; ++k) { dome_center[k] = a.pos[k]; }
 				has_dome = true;
 			}
@@ -734,6 +761,7 @@ void Engine::cook(SceneDesc& desc)
 			desc.emitters.push_back(e);
 			const float c[3] = {static_cast<float>(dome_center[0]), static_cast<float>(dome_center[1]), static_cast<float>(dome_center[2])};
 			desc.env_area = dome_area(desc.tris, c);
+			for(int k = 0; k < 3; ++k) { desc.env_center[k] = c[k]; }
 		}
 		if(desc.tris.empty())
 		{
@@ -745,6 +773,15 @@ void Engine::cook(SceneDesc& desc)
 		desc.camera = make_camera(p3, d3, u3, static_cast<float>(fov), width, height, static_cast<float>(sensor_w));
 		m_width = width;
 		m_height = height;
+	}
+}
+
+void Engine::set_dome_pdf(uint32_t mode)
+{
+	m_dome_pdf = mode;
+	if(m_render)
+	{
+		m_render->scene->set_dome_exact(mode == 1u);
 	}
 }
 

@@ -97,6 +97,8 @@ public:
 	void set_refine(uint32_t mode, float delta, uint32_t iters) { m_refine = EngineSettings{mode, delta, iters}; }
 	// BVH builder used by the next update: 0 host binned SAH, 1 GPU Morton.
 	void set_bvh_builder(uint32_t builder) { m_bvh_builder = builder; }
+	// Environment (dome) densities: 0 as the reference computes them (default), 1 exact.
+	void set_dome_pdf(uint32_t mode);
 	const RenderInfo& info() const { return m_info; }
 	uint64_t launch_count() const { return m_launches; }
 	// Renders into a scratch film with the given render mode and returns the statistics of
@@ -130,6 +132,7 @@ private:
 	bool m_guiding = false;
 	EngineSettings m_refine = engine_settings();
 	uint32_t m_bvh_builder = 0;
+	uint32_t m_dome_pdf = 0;
 
 	std::shared_ptr<RenderObject> m_render;
 	uint32_t m_width = 0, m_height = 0;

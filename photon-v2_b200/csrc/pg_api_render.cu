@@ -324,6 +324,19 @@ int pgpu_scene_film(uint64_t id, float* out_rgb, double* out_sum, uint64_t* out_
 	});
 }
 
+int pgpu_scene_set_dome_pdf(uint64_t id, uint32_t mode)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		if(mode > 1u)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_set_dome_pdf: mode must be 0 or 1");
+		}
+		r->scene->set_dome_exact(mode == 1u);
+	});
+}
+
 int pgpu_scene_set_filter(uint64_t id, uint32_t filter)
 {
 	return guarded([&]

@@ -467,13 +467,13 @@ shade_kernel(ShadeArgs a)
 		// ---- miss: environment (the dome primitive is hit after every triangle missed)
 		if(hit.x == 0xFFFFFFFFu)
 		{
+			const RGB le = s.env_emitter < 0 ? RGB{0.0f, 0.0f, 0.0f} : env_lookup(s.env_map, env_uv(s.env_map, d));
 			if(train_row != 0xFFFFFFFFu && s.env_emitter >= 0)
 			{
-				a.guide.train_dirw[train_row].w = luminance(RGB{s.env_r, s.env_g, s.env_b}) * train_wfac;
+				a.guide.train_dirw[train_row].w = luminance(le) * train_wfac;
 			}
 			if(s.env_emitter >= 0)
 			{
-				const RGB le = RGB{s.env_r, s.env_g, s.env_b};
 				if(bvpt)
 				{
 					radiance = radiance + (dl ? safe_clamp(le, 0.0f, kClampMax) * (thr_emit * cont)
@@ -488,7 +488,7 @@ shade_kernel(ShadeArgs a)
 					if(prev_bsdf_pdf > 0.0f)
 					{
 						const EmitterRec e = s.emitters[s.env_emitter];
-						const float light_pdf = e.pmf * (1.0f / (4.0f * kPi));
+						const float light_pdf = e.pmf * env_pdf_hit(s.env_map, prev_pos, d);
 						const float mis = prev_bsdf_pdf * prev_bsdf_pdf /
 						                  (prev_bsdf_pdf * prev_bsdf_pdf + light_pdf * light_pdf);
 						radiance = radiance + le * safe_clamp(thr_emit * mis, 0.0f, kClampMax);
@@ -604,28 +604,25 @@ shade_kernel(ShadeArgs a)
 			RGB le{};
 			if(e.type == PG_EMITTER_ENV)
 			{
-				// uniform sphere direction
-				const float u = rng.u01(bounce, DIM_NEE_U), w = rng.u01(bounce, DIM_NEE_V);
-				const float z = 1.0f - 2.0f * u;
-				const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
-				float sp, cp;
-				sincosf(kTwoPi * w, &sp, &cp);
-				to_light = v3(r * cp, r * sp, z);
-				pdf_w = e.pmf * (1.0f / (4.0f * kPi));
-				le = emitter_radiance(e);
-				if(sidedness_agreed(frame, to_light))
+				// a texel by the image's luminance x sin(theta) distribution, a point inside it
+				float env_pdf = 0.0f;
+				V3 shadow_dir{};
+				const bool env_ok = env_sample(s.env_map, pos, rng.u01(bounce, DIM_NEE_TRI), rng.u01(bounce, DIM_NEE_U),
+				                               rng.u01(bounce, DIM_NEE_V), &to_light, &env_pdf, &le, &shadow_dir);
+				pdf_w = e.pmf * env_pdf;
+				if(env_ok && sidedness_agreed(frame, to_light))
 				{
 					if(defer_refine)
 					{
 						sh_o = pos;
-						sh_d = to_light;
+						sh_d = shadow_dir;
 						sh_tmin = __uint_as_float(hit.x);
 						sh_tmax = kFloatMax;
 						sh_refine = 1u;
 					}
 					else
 					{
-						const EscapeRay er = escape_fixed(a.refine, pos, ng, to_light);
+						const EscapeRay er = escape_fixed(a.refine, pos, ng, shadow_dir);
 						sh_o = er.origin;
 						sh_d = er.unit_dir;
 						sh_tmin = er.min_t;
@@ -1017,6 +1014,51 @@ RenderScene::RenderScene(const SceneDesc& desc, float max_origin_abs)
 	std::vector<uint32_t> emitter_tris;
 	std::vector<double> weights(emitters.size(), 0.0);
 	int32_t env_index = -1;
+
+	// the dome image (a constant environment is a 1 x 1 image): texel sampling weights
+	// max(luminance, 1e-6) * sin(theta) at texel centres (LatLongEnvEmitter.cpp:52-79), their alias
+	// table, and each texel's uv-space density
+	const bool env_image = !desc.env_image.empty() && desc.env_width > 0 && desc.env_height > 0;
+	double env_weight_sum = 0.0;
+	std::vector<float4> env_texels;
+	std::vector<float2> env_alias;
+	if(desc.has_env)
+	{
+		std::vector<float> constant_image;
+		if(!env_image)
+		{
+			constant_image.assign(desc.env_rgb, desc.env_rgb + 3);
+		}
+		const std::vector<float>& image = env_image ? desc.env_image : constant_image;
+		const uint32_t w = env_image ? desc.env_width : 1u, h = env_image ? desc.env_height : 1u;
+		if(image.size() != static_cast<std::size_t>(w) * h * 3)
+		{
+			throw Error(PG_ERR_SCENE, "environment image size does not match its dimensions");
+		}
+		std::vector<double> texel_weights(static_cast<std::size_t>(w) * h);
+		for(uint32_t j = 0; j < h; ++j)
+		{
+			const double v = (j + 0.5) / h;
+			const double sin_theta = std::sin((1.0 - v) * 3.14159265358979323846);
+			for(uint32_t i = 0; i < w; ++i)
+			{
+				const float* c = &image[3 * (static_cast<std::size_t>(j) * w + i)];
+				const double lum = kLumR * c[0] + kLumG * c[1] + kLumB * c[2];
+				texel_weights[static_cast<std::size_t>(j) * w + i] = std::max(lum, 1e-6) * sin_theta;
+				env_weight_sum += texel_weights[static_cast<std::size_t>(j) * w + i];
+			}
+		}
+		std::vector<double> texel_pmf;
+		build_alias(texel_weights, env_alias, texel_pmf);
+		env_texels.resize(texel_weights.size());
+		for(std::size_t k = 0; k < texel_weights.size(); ++k)
+		{
+			const float* c = &image[3 * k];
+			env_texels[k] = make_float4(c[0], c[1], c[2], static_cast<float>(texel_pmf[k] * texel_weights.size()));
+		}
+		m_dev.env_map.width = w;
+		m_dev.env_map.height = h;
+	}
 	for(std::size_t e = 0; e < emitters.size(); ++e)
 	{
 		auto& list = per_emitter[e];
@@ -1027,11 +1069,10 @@ RenderScene::RenderScene(const SceneDesc& desc, float max_origin_abs)
 		emitter_tris.insert(emitter_tris.end(), list.begin(), list.end());
 		if(emitters[e].type == PG_EMITTER_ENV)
 		{
-			// luminance x sin(theta) summed over the 1x1 image, times the dome area
-			// (LatLongEnvEmitter.cpp:36-68)
+			// luminance x sin(theta) summed over the image's texels, times the dome area
+			// (LatLongEnvEmitter.cpp:36-80); a constant environment is a 1 x 1 image
 			env_index = static_cast<int32_t>(e);
-			const double lum = kLumR * emitters[e].r + kLumG * emitters[e].g + kLumB * emitters[e].b;
-			weights[e] = std::max(lum, 1e-6) * desc.env_area;
+			weights[e] = env_weight_sum * desc.env_area;
 		}
 		else
 		{
@@ -1069,6 +1110,20 @@ RenderScene::RenderScene(const SceneDesc& desc, float max_origin_abs)
 	{
 		PG_CUDA_CHECK(cudaMemcpyAsync(m_alias.get(), alias.data(), alias.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
 	}
+	if(desc.has_env)
+	{
+		m_env_texels.resize(env_texels.size());
+		m_env_alias.resize(env_alias.size());
+		PG_CUDA_CHECK(cudaMemcpyAsync(m_env_texels.get(), env_texels.data(), env_texels.size() * sizeof(float4),
+		                              cudaMemcpyHostToDevice, st));
+		PG_CUDA_CHECK(cudaMemcpyAsync(m_env_alias.get(), env_alias.data(), env_alias.size() * sizeof(float2),
+		                              cudaMemcpyHostToDevice, st));
+		m_dev.env_map.texels = m_env_texels.get();
+		m_dev.env_map.alias = m_env_alias.get();
+		for(int k = 0; k < 9; ++k) { m_dev.env_map.rot[k] = desc.env_rot[k]; }
+		for(int k = 0; k < 3; ++k) { m_dev.env_map.center[k] = desc.env_center[k]; }
+		m_dev.env_map.radius = static_cast<float>(std::sqrt(desc.env_area / (4.0 * 3.14159265358979323846)));
+	}
 	m_counters.resize(1);
 	PG_CUDA_CHECK(cudaStreamSynchronize(st));
 
@@ -1080,9 +1135,6 @@ RenderScene::RenderScene(const SceneDesc& desc, float max_origin_abs)
 	m_dev.alias = m_alias.get();
 	m_dev.num_emitters = static_cast<uint32_t>(emitters.size());
 	m_dev.env_emitter = env_index;
-	m_dev.env_r = desc.env_rgb[0];
-	m_dev.env_g = desc.env_rgb[1];
-	m_dev.env_b = desc.env_rgb[2];
 	m_dev.cam = desc.camera;
 }
 

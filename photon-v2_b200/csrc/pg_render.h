@@ -14,6 +14,7 @@
 #pragma once
 
 #include "bsdf.cuh"
+#include "env.cuh"
 #include "film.cuh"
 #include "pg_common.cuh"
 #include "pg_geometry.h"
@@ -111,6 +112,13 @@ struct SceneDesc
 	std::vector<EmitterRec> emitters;     // pmf / first / count filled by the scene builder
 	float env_rgb[3] = {0.0f, 0.0f, 0.0f};
 	bool  has_env = false;
+	// An image dome larger than 1 x 1: linear sRGB radiance [env_height][env_width][3], row 0 at the
+	// bottom (looking down), and the dome's local-to-world rotation (row-major). Empty: the
+	// environment is the constant env_rgb.
+	std::vector<float> env_image;
+	uint32_t env_width = 0, env_height = 0;
+	float env_rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+	float env_center[3] = {0.0f, 0.0f, 0.0f};   // dome centre (its actor position)
 	// Surface area of the dome sphere (4 pi r^2, r = 1.01 x the farthest scene-bound corner from
 	// the dome centre, ADome.cpp:45-60); the environment's flux approximation is its luminance
 	// times this area (LatLongEnvEmitter.cpp:36-68), which sets its share of NEE samples.
@@ -130,7 +138,7 @@ struct DeviceScene
 	const float2*     alias;            // per emitter: (accept probability, alias index bits)
 	uint32_t          num_emitters;
 	int32_t           env_emitter;      // index of the environment emitter or -1
-	float             env_r, env_g, env_b;
+	EnvMap            env_map;          // the dome (a constant environment is a 1 x 1 image)
 	Camera            cam;
 };
 
@@ -264,6 +272,8 @@ public:
 	// Learned guiding for subsequent renders; the network is created (He-initialised, fixed seed)
 	// on first use and keeps its training state until reset_guiding().
 	void set_guiding(const GuideParams& g) { m_guide_params = g; }
+	// Dome densities: false (default) the reference's finite-dome densities, true exact ones (env.cuh).
+	void set_dome_exact(bool exact) { m_dev.env_map.exact = exact ? 1u : 0u; }
 	const GuideParams& guiding() const { return m_guide_params; }
 	void reset_guiding();
 	// Mean training loss over the training steps of the last guided render, and its number of
@@ -282,6 +292,8 @@ private:
 	DeviceBuffer<EmitterRec>  m_emitters;
 	DeviceBuffer<uint32_t>    m_emitter_tris;
 	DeviceBuffer<float2>      m_alias;
+	DeviceBuffer<float4>      m_env_texels;
+	DeviceBuffer<float2>      m_env_alias;
 	DeviceScene               m_dev{};
 
 	uint32_t m_capacity = 0;

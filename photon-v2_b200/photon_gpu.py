@@ -60,6 +60,7 @@ PGPU_SIGNATURES = [
     ("pgpu_scene_film", ctypes.c_int, [ctypes.c_uint64, _f32p, _dblp, _u64p]),
     ("pgpu_scene_clear", ctypes.c_int, [ctypes.c_uint64]),
     ("pgpu_scene_set_filter", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32]),
+    ("pgpu_scene_set_dome_pdf", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32]),
     ("pgpu_scene_launches", ctypes.c_int, [ctypes.c_uint64, _u64p]),
     ("pgpu_scene_count", ctypes.c_int,
      [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _u64p]),
@@ -232,6 +233,8 @@ MATTE, CONDUCTOR, DIELECTRIC = 0, 1, 2
 BNEEPT, BVPT, BVPTDL = 0, 1, 2
 # sample-filter names of the reference's SDL (sdl_sample_filter_type.h) -> pgpu_scene_set_filter
 FILTERS = {"box": 0, "gaussian": 1, "mn": 2, "bh": 3}
+# phGpuSetDomePdf / pgpu_scene_set_dome_pdf modes
+DOME_PDF = {"reference": 0, "exact": 1}
 
 
 def flatten_scene(scene):
@@ -250,6 +253,9 @@ def flatten_scene(scene):
             tri_em.append(np.full(n, len(ems), np.uint32))
         else:
             tri_em.append(np.zeros(n, np.uint32))
+    if scene.env_image is not None:
+        raise ValueError("the flat scene ABI takes constant environments only; render image domes through the "
+                         "Photon C API (SDL image-dome)")
     if scene.env_radiance is not None:
         ems.append([scene.env_radiance[0], scene.env_radiance[1], scene.env_radiance[2], 1.0])
     cam = np.array(list(scene.cam_pos) + list(scene.cam_dir) + list(scene.cam_up)
@@ -302,6 +308,10 @@ class RenderScene:
 
     def clear(self):
         _check(load().pgpu_scene_clear(self.id))
+
+    def set_dome_pdf(self, mode: str) -> None:
+        """Environment sample densities: "reference" (default) or "exact"."""
+        _check(load().pgpu_scene_set_dome_pdf(self.id, DOME_PDF[mode]))
 
     def set_filter(self, name: str) -> None:
         """Sample filter of the film ("box", "gaussian", "mn", "bh"); clears the film."""
@@ -401,6 +411,7 @@ PH_SIGNATURES = [
     ("phGpuSetSeed", None, [ctypes.c_uint64, ctypes.c_uint64]),
     ("phGpuSetGuiding", None, [ctypes.c_uint64, ctypes.c_int]),
     ("phGpuSetBvhBuilder", None, [ctypes.c_uint64, ctypes.c_uint32]),
+    ("phGpuSetDomePdf", None, [ctypes.c_uint64, ctypes.c_uint32]),
     ("phGpuSetSurfaceRefine", None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32]),
     ("phGpuClearFilm", None, [ctypes.c_uint64]),
     ("phGpuGetRenderInfo", None, [ctypes.c_uint64, _dblp, _u64p, _u64p, _u64p, _dblp]),
@@ -463,6 +474,10 @@ class PhotonEngine:
 
     def set_bvh_builder(self, builder: str = "sah") -> None:
         load().phGpuSetBvhBuilder(self.id, BUILDERS[builder])
+
+    def set_dome_pdf(self, mode: str = "reference") -> None:
+        """phGpuSetDomePdf: environment sample densities as the reference computes them, or exact."""
+        load().phGpuSetDomePdf(self.id, DOME_PDF[mode])
 
     def set_surface_refine(self, mode: str = "iterative", delta: float = 2e-4, iterations: int = 1) -> None:
         """phGpuSetSurfaceRefine: the reference's RefineMode (manual / empirical / iterative)."""

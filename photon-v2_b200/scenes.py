@@ -25,6 +25,7 @@ the reference then intersects plain ``PTriangle`` primitives (Engine/Source/Acto
 from __future__ import annotations
 
 import dataclasses
+import os
 import math
 from typing import List, Optional, Sequence, Tuple
 
@@ -74,6 +75,14 @@ class Scene:
     estimator: str = "bneept"
     env_radiance: Optional[RGB] = None
     sample_filter: str = "box"      # box | gaussian | mn | bh (the reference's sample-filter enum)
+    # lat-long dome image [H, W, 3] (row 0 = top), used instead of env_radiance when set, and the
+    # dome's rotation (axis, degrees)
+    env_image: Optional[np.ndarray] = None
+    env_rotation: Optional[Tuple[RGB, float]] = None
+
+    @property
+    def has_env(self) -> bool:
+        return self.env_radiance is not None or self.env_image is not None
 
     @property
     def num_tris(self) -> int:
@@ -385,6 +394,17 @@ def ggx_sphere(level: int = 8, width: int = 1024, height: int = 1024, spp: int =
                  env_radiance=(0.1, 0.1, 0.1) if with_env else None)
 
 
+def furnace(spp: int = 1024, estimator: str = "bneept", sample_filter: str = "box") -> Scene:
+    """Grey-furnace known answer (the reference's RenderTest test_gray_furnace_box.py): a convex
+    Lambertian icosphere of albedo 0.5 under a constant unit dome, 32 x 32; with exact densities
+    every pixel that sees only the sphere is 0.5."""
+    sphere = icosphere(3).astype(np.float32)
+    groups = [MeshGroup(sphere, Material("matte", albedo=(0.5, 0.5, 0.5)))]
+    return Scene("furnace", 32, 32, spp, 10000, cam_pos=(0.0, 0.0, -4.0), cam_dir=(0.0, 0.0, 1.0),
+                 cam_up=(0.0, 1.0, 0.0), fov_deg=30.0, groups=groups, estimator=estimator,
+                 env_radiance=(1.0, 1.0, 1.0), sample_filter=sample_filter)
+
+
 def batch_scene(index: int, max_bounces: int = 10, estimator: str = "bneept") -> Scene:
     """Scene `index` (0..63) of the batched workload: seeded by its index, ~U[1k, 500k] triangles
     of random boxes (even indices) or a displaced icosphere (odd indices; 20 * 4**level triangles,
@@ -508,9 +528,41 @@ def to_sdl(scene: Scene, env_image_name: str = "env.pfm") -> str:
                          f"[enum color-space LSRGB];")
             lines.append(f"actor(model-light) @a{gi} = [geometry geometry @g{gi}] "
                          f"[material material @{mname}] [image emitted-energy @e{gi}];")
-    if scene.env_radiance is not None:
+    if scene.has_env:
         lines.append(f'actor(image-dome) @dome = [PRI image-file ":{env_image_name}"];')
+        if scene.env_rotation is not None:
+            axis, degrees = scene.env_rotation
+            lines.append(f'rotate(@dome) = [vector3 axis "{_v3(axis)}"] [real degrees {_f(degrees)}];')
     return "\n".join(lines) + "\n"
+
+
+def write_env(scene: Scene, directory: str, name: str = "env.pfm") -> None:
+    """Writes the scene's dome image (or its 1 x 1 constant radiance) where to_sdl refers to it."""
+    if scene.env_image is not None:
+        write_pfm(os.path.join(directory, name), np.asarray(scene.env_image, np.float32))
+    elif scene.env_radiance is not None:
+        write_pfm(os.path.join(directory, name), np.array(scene.env_radiance, np.float32).reshape(1, 1, 3))
+
+
+def sky_image(width: int = 64, height: int = 32, sun_uv: Tuple[float, float] = (0.3, 0.78),
+              sun_radiance: float = 60.0, seed: int = 11) -> np.ndarray:
+    """A lat-long sky [height, width, 3] (row 0 = top): a blue-to-white gradient above the
+    horizon, a dim brown ground below, seeded per-texel variation, and a small bright sun disk
+    centred at lat-long `sun_uv` (u = azimuth / 2 pi, v = 1 at the zenith)."""
+    rng = np.random.default_rng(seed)
+    v = 1.0 - (np.arange(height) + 0.5) / height          # row 0 = top = v near 1
+    u = (np.arange(width) + 0.5) / width
+    uu, vv = np.meshgrid(u, v)
+    elev = (vv - 0.5) * np.pi                              # -pi/2 .. pi/2
+    s = np.sin(np.clip(elev, 0, None))[..., None]          # 0 at the horizon, 1 at the zenith
+    sky = (1 - s) * np.array([0.45, 0.5, 0.6]) + s * np.array([0.15, 0.3, 0.7])
+    ground = np.stack([0.12 + 0 * uu, 0.09 + 0 * uu, 0.06 + 0 * uu], -1)
+    img = np.where((elev >= 0)[..., None], sky, ground)
+    img *= 1.0 + 0.15 * rng.random(img.shape[:2])[..., None]
+    du = np.minimum(np.abs(uu - sun_uv[0]), 1 - np.abs(uu - sun_uv[0])) * width
+    dv = np.abs(vv - sun_uv[1]) * height
+    img[(du * du + dv * dv) <= 2.0 ** 2] = sun_radiance * np.array([1.0, 0.9, 0.75])
+    return img.astype(np.float32)
 
 
 def write_pfm(path: str, rgb: np.ndarray) -> None:

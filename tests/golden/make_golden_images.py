@@ -35,6 +35,12 @@ WORKLOADS = {
     "cornell_bneept": (lambda spp: scenes.cornell(64, 64, spp, 8, "bneept"), 8192, 8),
     "cornell_bvpt": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvpt"), 8192, 8),
     "cornell_bvptdl": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvptdl"), 8192, 8),
+    # the grey furnace (32 x 32): the reference's finite-dome densities bias it above 0.5
+    "furnace_bneept_ref": (lambda spp: scenes.furnace(spp), 8192, 10000),
+    # a lat-long image dome (sky with a small sun), rotated 60 degrees about +y
+    "ggx_sphere_envmap_bneept": (lambda spp: dataclasses.replace(
+        scenes.ggx_sphere(level=3, width=64, height=64, spp=spp, max_bounces=10),
+        env_radiance=None, env_image=scenes.sky_image(), env_rotation=((0.0, 1.0, 0.0), 60.0)), 8192, 10),
     # the reference's other sample filters (sample-filter of the path-tracing visualizer)
     "cornell_bneept_gaussian": (lambda spp: dataclasses.replace(scenes.cornell(64, 64, spp, 8, "bneept"),
                                                                 sample_filter="gaussian"), 8192, 8),
@@ -61,9 +67,7 @@ def render(scene: scenes.Scene, max_bounces: int, threads: int, refine_mode: str
         p2 = os.path.join(tmp, "scene.p2")
         with open(p2, "w") as f:
             f.write(scenes.to_sdl(scene))
-        if scene.env_radiance is not None:
-            scenes.write_pfm(os.path.join(tmp, "env.pfm"),
-                             np.array(scene.env_radiance, np.float32).reshape(1, 1, 3))
+        scenes.write_env(scene, tmp)
         out = os.path.join(tmp, "out.rgbf32")
         subprocess.run([RENDER_TOOL, p2, str(threads), str(max_bounces), out], check=True, cwd=tmp,
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)

@@ -41,6 +41,10 @@ WORKLOADS = {
     "cornell_bneept": (lambda spp: scenes.cornell(64, 64, spp, 8, "bneept"), 4096),
     "cornell_bvpt": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvpt"), 4096),
     "cornell_bvptdl": (lambda spp: scenes.cornell(64, 64, spp, 8, "bvptdl"), 4096),
+    # lat-long image dome, importance-sampled by its luminance x sin(theta), rotated dome
+    "ggx_sphere_envmap_bneept": (lambda spp: dataclasses.replace(
+        scenes.ggx_sphere(level=3, width=64, height=64, spp=spp, max_bounces=10),
+        env_radiance=None, env_image=scenes.sky_image(), env_rotation=((0.0, 1.0, 0.0), 60.0)), 8192),
     "cornell_glossy_bneept": (lambda spp: scenes.cornell_glossy(64, 64, spp, 8, "bneept"), 16384),
     "ggx_sphere_env_bneept": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
                                                             max_bounces=10), 4096),
@@ -63,19 +67,19 @@ def rel_mse(x, ref, eps=1e-2):
     return float(np.mean((x.astype(np.float64) - ref) ** 2 / (ref.astype(np.float64) ** 2 + eps)))
 
 
-def render_via_c_api(scene, tmp_path, seed=1, refine_mode="iterative"):
+def render_via_c_api(scene, tmp_path, seed=1, refine_mode="iterative", dome_pdf="reference"):
     import photon_gpu
 
     p2 = tmp_path / "scene.p2"
     p2.write_text(scenes.to_sdl(scene))
-    if scene.env_radiance is not None:
-        scenes.write_pfm(str(tmp_path / "env.pfm"), np.array(scene.env_radiance, np.float32).reshape(1, 1, 3))
+    scenes.write_env(scene, str(tmp_path))
     with photon_gpu.PhotonEngine() as eng:
         eng.set_working_directory(str(tmp_path))
         assert eng.load_file(str(p2)), eng.errors()
         eng.set_max_bounces(scene.max_bounces)
         eng.set_seed(seed)
         eng.set_surface_refine(refine_mode)
+        eng.set_dome_pdf(dome_pdf)
         eng.update()
         eng.render()
         img = eng.frame()
@@ -110,25 +114,32 @@ def test_image_matches_reference(gpu_lib, tmp_path, name):
     assert np.all(np.abs(means - 1.0) < 0.01), f"channel means differ: {means}"
 
 
-def _furnace_scene(estimator, sample_filter="box"):
-    sphere = scenes.icosphere(3).astype(np.float32)
-    groups = [scenes.MeshGroup(sphere, scenes.Material("matte", albedo=(0.5, 0.5, 0.5)))]
-    return scenes.Scene("furnace", 32, 32, 1024, 10000, cam_pos=(0.0, 0.0, -4.0), cam_dir=(0.0, 0.0, 1.0),
-                        cam_up=(0.0, 1.0, 0.0), fov_deg=30.0, groups=groups, estimator=estimator,
-                        env_radiance=(1.0, 1.0, 1.0), sample_filter=sample_filter)
-
-
 @pytest.mark.gpu
 @pytest.mark.parametrize("estimator,sample_filter", [("bneept", "box"), ("bvpt", "box"), ("bneept", "gaussian"),
                                                      ("bneept", "mn"), ("bneept", "bh")])
 def test_furnace(gpu_lib, tmp_path, estimator, sample_filter):
-    # with a filter, light found by NEE at a path's last vertex reaches the film from the any-hit
-    # kernel, the rest from the shading kernel: both must weight it like the sample's W
-    img, _ = render_via_c_api(_furnace_scene(estimator, sample_filter), tmp_path)
+    # exact dome densities: the analytic answer. With a filter, light found by NEE at a path's last
+    # vertex reaches the film from the traversal kernel, the rest from the shading kernel: both
+    # must weight it like the sample's W.
+    img, _ = render_via_c_api(scenes.furnace(1024, estimator, sample_filter), tmp_path, dome_pdf="exact")
     # the central pixels see only the sphere; the corners see only the environment
     centre = img[12:20, 12:20]
     assert abs(centre.mean() - 0.5) < 1e-3, centre.mean()
     assert np.allclose(img[0, 0], 1.0) and np.allclose(img[-1, -1], 1.0)
+
+
+@pytest.mark.gpu
+def test_furnace_with_the_reference_dome_densities(gpu_lib, tmp_path):
+    """The reference's own densities on its finite dome sphere overestimate the furnace (its render
+    gives 0.512, not 0.5, at the sphere's centre pixels); by default the GPU renderer computes
+    them the same way and must land near the reference's render, not near 0.5. This dome is only
+    1.75 x the sphere's radius, the most the densities deviate; the GPU render comes out 0.45 %
+    above the reference's (0.514), against 2.4 % for the exact densities, so the bar is 1 %."""
+    ref = np.load(IMAGES)["furnace_bneept_ref"][12:20, 12:20].mean()
+    assert ref > 0.505
+    img, _ = render_via_c_api(scenes.furnace(4096), tmp_path)
+    centre = img[12:20, 12:20].mean()
+    assert abs(centre / ref - 1.0) < 1e-2, (centre, ref)
 
 
 @pytest.mark.gpu
