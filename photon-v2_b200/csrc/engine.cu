@@ -1,4 +1,5 @@
 #include "engine.h"
+#include "ply.h"
 #include "pg_render_object.h"
 #include "scene_build.h"
 
@@ -539,6 +540,24 @@ void Engine::cook(SceneDesc& desc)
 				}
 				out.assign(pos_f.begin(), pos_f.end());
 			}
+			else if(g.type == "ply")
+			{
+				const SdlClause* f = find(g.clauses, "ply-file");
+				if(!f)
+				{
+					throw std::runtime_error("ply geometry without ply-file");
+				}
+				PlyMesh mesh = read_ply(resolve_resource(f->value));
+				if(mesh.has_normals)
+				{
+					record_error("vertex normals are ignored: the GPU renderer shades with face normals");
+				}
+				if(mesh.tris.empty())
+				{
+					throw std::runtime_error("ply geometry without faces");
+				}
+				out = std::move(mesh.tris);
+			}
 			else if(g.type == "rectangle")
 			{
 				// GRectangle::genTriangleMesh (Engine/Source/Actor/Geometry/GRectangle.cpp:70-100)
@@ -701,12 +720,7 @@ void Engine::cook(SceneDesc& desc)
 				{
 					throw std::runtime_error("image dome without image-file");
 				}
-				// SDL resource identifiers: ":rel/path" is relative to the scene's working directory,
-				// "ext:/abs/path" is external (SdlResourceLocator.cpp:20-43, 190-210).
-				std::string path = f->value;
-				if(path.rfind("ext:", 0) == 0) { path = path.substr(4); }
-				else if(!path.empty() && path[0] == ':') { path = m_working_dir + "/" + path.substr(1); }
-				else if(path.empty() || path[0] != '/') { path = m_working_dir + "/" + path; }
+				const std::string path = resolve_resource(f->value);
 				HdrFrame img;
 				if(!read_pfm(path, img))
 				{
@@ -774,6 +788,16 @@ void Engine::cook(SceneDesc& desc)
 		m_width = width;
 		m_height = height;
 	}
+}
+
+std::string Engine::resolve_resource(const std::string& identifier) const
+{
+	// SDL resource identifiers: ":rel/path" is relative to the scene's working directory,
+	// "ext:/abs/path" is external (SdlResourceLocator.cpp:20-43, 190-210).
+	if(identifier.rfind("ext:", 0) == 0) { return identifier.substr(4); }
+	if(!identifier.empty() && identifier[0] == ':') { return m_working_dir + "/" + identifier.substr(1); }
+	if(identifier.empty() || identifier[0] != '/') { return m_working_dir + "/" + identifier; }
+	return identifier;
 }
 
 void Engine::set_dome_pdf(uint32_t mode)

@@ -99,6 +99,8 @@ public:
 	void set_bvh_builder(uint32_t builder) { m_bvh_builder = builder; }
 	// Environment (dome) densities: 0 as the reference computes them (default), 1 exact.
 	void set_dome_pdf(uint32_t mode);
+	// Path of an SDL resource identifier (":relative" to the working directory, "ext:/absolute").
+	std::string resolve_resource(const std::string& identifier) const;
 	const RenderInfo& info() const { return m_info; }
 	uint64_t launch_count() const { return m_launches; }
 	// Renders into a scratch film with the given render mode and returns the statistics of

@@ -499,8 +499,10 @@ def _material_sdl(name: str, m: Material, lines: List[str]) -> None:
         raise ValueError(f"unknown material kind {m.kind}")
 
 
-def to_sdl(scene: Scene, env_image_name: str = "env.pfm") -> str:
-    """The whole scene as SDL 1.1 command text."""
+def to_sdl(scene: Scene, env_image_name: str = "env.pfm", mesh_format: str = "text") -> str:
+    """The whole scene as SDL 1.1 command text. mesh_format "ply" refers every mesh group to a
+    file g<i>.ply in the scene's directory (write them with write_meshes) instead of spelling its
+    vertices out as vector3-array text."""
     lines = [
         "#version 1.1.0;",
         "option(single-frame-render-session) @session = "
@@ -517,10 +519,13 @@ def to_sdl(scene: Scene, env_image_name: str = "env.pfm") -> str:
         mname = f"m{gi}"
         _material_sdl(mname, g.material, lines)
         n = g.tris.shape[0] * 3
-        lines.append(f"geometry(triangle-mesh) @g{gi} = "
-                     f"[vector3-array positions {_vec3_array(g.tris)}] "
-                     f"[vector3-array texture-coordinates {_zeros_array(n)}] "
-                     f"[vector3-array normals {_zeros_array(n)}];")
+        if mesh_format == "ply":
+            lines.append(f'geometry(ply) @g{gi} = [PRI ply-file ":g{gi}.ply"];')
+        else:
+            lines.append(f"geometry(triangle-mesh) @g{gi} = "
+                         f"[vector3-array positions {_vec3_array(g.tris)}] "
+                         f"[vector3-array texture-coordinates {_zeros_array(n)}] "
+                         f"[vector3-array normals {_zeros_array(n)}];")
         if g.radiance is None:
             lines.append(f"actor(model) @a{gi} = [geometry geometry @g{gi}] [material material @{mname}];")
         else:
@@ -534,6 +539,35 @@ def to_sdl(scene: Scene, env_image_name: str = "env.pfm") -> str:
             axis, degrees = scene.env_rotation
             lines.append(f'rotate(@dome) = [vector3 axis "{_v3(axis)}"] [real degrees {_f(degrees)}];')
     return "\n".join(lines) + "\n"
+
+
+def write_ply(path: str, tris: np.ndarray, fmt: str = "binary_little_endian") -> None:
+    """Triangles [n, 3, 3] as a PLY mesh: three float32 vertices per face (not shared), faces as
+    `list uchar int vertex_indices`. fmt: binary_little_endian, binary_big_endian or ascii."""
+    t = np.asarray(tris, np.float32).reshape(-1, 3)
+    n = t.shape[0] // 3
+    header = (f"ply\nformat {fmt} 1.0\ncomment photon-v2_b200 scenes.write_ply\n"
+              f"element vertex {t.shape[0]}\nproperty float x\nproperty float y\nproperty float z\n"
+              f"element face {n}\nproperty list uchar int vertex_indices\nend_header\n")
+    idx = np.arange(3 * n, dtype=np.int64).reshape(n, 3)
+    with open(path, "wb") as f:
+        f.write(header.encode())
+        if fmt == "ascii":
+            f.write("".join(f"{a!r} {b!r} {c!r}\n" for a, b, c in t.tolist()).encode())
+            f.write("".join(f"3 {a} {b} {c}\n" for a, b, c in idx.tolist()).encode())
+            return
+        order = "<" if fmt == "binary_little_endian" else ">"
+        f.write(t.astype(order + "f4").tobytes())
+        faces = np.zeros(n, dtype=[("k", "u1"), ("i", order + "i4", (3,))])
+        faces["k"] = 3
+        faces["i"] = idx
+        f.write(faces.tobytes())
+
+
+def write_meshes(scene: Scene, directory: str, fmt: str = "binary_little_endian") -> None:
+    """The PLY files to_sdl(mesh_format="ply") refers to."""
+    for gi, g in enumerate(scene.groups):
+        write_ply(os.path.join(directory, f"g{gi}.ply"), g.tris, fmt)
 
 
 def write_env(scene: Scene, directory: str, name: str = "env.pfm") -> None:

@@ -67,11 +67,13 @@ def rel_mse(x, ref, eps=1e-2):
     return float(np.mean((x.astype(np.float64) - ref) ** 2 / (ref.astype(np.float64) ** 2 + eps)))
 
 
-def render_via_c_api(scene, tmp_path, seed=1, refine_mode="iterative", dome_pdf="reference"):
+def render_via_c_api(scene, tmp_path, seed=1, refine_mode="iterative", dome_pdf="reference", mesh_format="text"):
     import photon_gpu
 
     p2 = tmp_path / "scene.p2"
-    p2.write_text(scenes.to_sdl(scene))
+    p2.write_text(scenes.to_sdl(scene, mesh_format=mesh_format))
+    if mesh_format == "ply":
+        scenes.write_meshes(scene, str(tmp_path))
     scenes.write_env(scene, str(tmp_path))
     with photon_gpu.PhotonEngine() as eng:
         eng.set_working_directory(str(tmp_path))
@@ -112,6 +114,16 @@ def test_image_matches_reference(gpu_lib, tmp_path, name):
     assert err_blocks <= 1e-3, f"block relMSE {err_blocks:.3e}"
     assert err <= (1e-3 if scene.estimator == "bneept" else 2e-2), f"relMSE {err:.3e}"
     assert np.all(np.abs(means - 1.0) < 0.01), f"channel means differ: {means}"
+
+
+@pytest.mark.gpu
+def test_ply_meshes_match_reference(gpu_lib, tmp_path):
+    """The Cornell box with every mesh loaded from binary PLY files (geometry(ply)) renders the
+    reference's Cornell image (the reference loads the same files: GPlyPolygonMesh)."""
+    ref = np.load(IMAGES)["cornell_bneept"]
+    img, _ = render_via_c_api(scenes.cornell(64, 64, 4096, 8, "bneept"), tmp_path, mesh_format="ply")
+    assert rel_mse(img, ref) <= 1e-3
+    assert np.all(np.abs(img.mean(axis=(0, 1)) / ref.mean(axis=(0, 1)) - 1.0) < 0.01)
 
 
 @pytest.mark.gpu

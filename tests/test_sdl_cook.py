@@ -139,3 +139,53 @@ def test_degenerate_triangles_are_dropped():
     g.tris = np.concatenate([g.tris, bad])
     c = _cook(scenes.to_sdl(s))
     assert c.tris.shape[0] == 36
+
+
+@pytest.mark.parametrize("fmt", ["binary_little_endian", "binary_big_endian", "ascii"])
+def test_ply_meshes_cook_to_the_same_triangles(fmt, tmp_path):
+    s = scenes.cornell(16, 16, 4)
+    scenes.write_meshes(s, str(tmp_path), fmt)
+    c = _cook(scenes.to_sdl(s, mesh_format="ply"), str(tmp_path))
+    ref = np.concatenate([g.tris for g in s.groups])
+    assert np.array_equal(c.tris.view(np.uint32), ref.view(np.uint32))
+
+
+def _write_custom_ply(path, header_props, vertex_rows, face_rows, extra=""):
+    with open(path, "w") as f:
+        f.write("ply\nformat ascii 1.0\n")
+        f.write(f"element vertex {len(vertex_rows)}\n{header_props}")
+        f.write(f"element face {len(face_rows)}\nproperty list uchar int vertex_indices\n{extra}end_header\n")
+        for r in vertex_rows:
+            f.write(" ".join(str(x) for x in r) + "\n")
+        for r in face_rows:
+            f.write(" ".join(str(x) for x in r) + "\n")
+
+
+def _ply_scene_text():
+    """A one-mesh scene whose mesh is read from g0.ply."""
+    tri = np.array([[[0, 0, 0], [1, 0, 0], [0, 1, 0]]], np.float32)
+    s = scenes.Scene("ply", 8, 8, 1, 8, cam_pos=(0.5, 0.5, -3.0), cam_dir=(0.0, 0.0, 1.0), cam_up=(0.0, 1.0, 0.0),
+                     fov_deg=40.0, groups=[scenes.MeshGroup(tri, scenes.WHITE)])
+    return scenes.to_sdl(s, mesh_format="ply")
+
+
+def test_ply_extra_properties_and_elements(tmp_path):
+    # shared vertices, an extra per-vertex colour, a trailing edge element with a list
+    props = "property double x\nproperty double y\nproperty double z\nproperty uchar red\n"
+    verts = [(0, 0, 0, 1), (1, 0, 0, 2), (0, 1, 0, 3), (1, 1, 0, 4)]
+    faces = [(3, 0, 1, 2), (3, 2, 1, 3)]
+    path = tmp_path / "g0.ply"
+    _write_custom_ply(path, props, verts, faces, extra="element edge 1\nproperty list uchar int vertex_pair\n")
+    with open(path, "a") as f:
+        f.write("2 0 3\n")
+    c = _cook(_ply_scene_text(), str(tmp_path))
+    want = np.array([[[0, 0, 0], [1, 0, 0], [0, 1, 0]], [[0, 1, 0], [1, 0, 0], [1, 1, 0]]], np.float32)
+    assert np.array_equal(c.tris, want)
+
+
+@pytest.mark.parametrize("faces", [[(4, 0, 1, 2, 3)], [(3, 0, 1, 7)]])
+def test_ply_rejects_polygons_and_bad_indices(faces, tmp_path):
+    props = "property float x\nproperty float y\nproperty float z\n"
+    _write_custom_ply(tmp_path / "g0.ply", props, [(0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 0)], faces)
+    with pytest.raises(photon_gpu.PhotonGpuError, match="PLY"):
+        _cook(_ply_scene_text(), str(tmp_path))
