@@ -481,6 +481,18 @@ def run_flat(args) -> None:
 
     def one_pass(read_back: bool = False):
         ms, launches = 0.0, 0
+        if args.concurrency > 1 and len(scene_list) > 1:
+            # all scenes of the step at once, `concurrency` of them in flight on their own streams;
+            # the step's time is the batch's span
+            for rs in rss:
+                rs.clear()
+            ms = photon_gpu.render_scenes(rss, [sc.spp for sc in scene_list], max_bounces=scene_list[0].max_bounces,
+                                          seed=seed, concurrency=args.concurrency)
+            launches = sum(rs.launches() for rs in rss)
+            if read_back:
+                for rs in rss:
+                    rs.film(with_sums=False)
+            return ms, launches
         for sc, rs in zip(scene_list, rss):
             rs.clear()
             ms += rs.render(sc.spp, max_bounces=sc.max_bounces, seed=seed)["ms"]
@@ -539,6 +551,7 @@ def run_flat(args) -> None:
                    "resolution": sorted({f"{sc.width}x{sc.height}" for sc in scene_list})[:4],
                    "spp": spps if len(spps) <= 4 else [spps[0], spps[-1]],
                    "max_bounces": scene_list[0].max_bounces, "estimator": "bneept", "bvh": args.builder,
+                   "concurrency": args.concurrency if len(scene_list) > 1 else 1,
                    "l2": "256 MiB write between timed steps", "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
                 "path": "pgpu_scene_render + pgpu_scene_film (frame developed on the GPU, copied to host)"},
@@ -591,6 +604,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-guided", action="store_true", help="skip the guided-vs-plain equal-time comparison")
     ap.add_argument("--builder", default="sah", choices=["sah", "gpu"], help="BVH builder of flat workloads")
+    ap.add_argument("--concurrency", type=int, default=4,
+                    help="scenes of a multi-scene workload rendered at once (1: one after another)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

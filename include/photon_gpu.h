@@ -177,6 +177,13 @@ PGPU_API int pgpu_scene_set_dome_pdf(uint64_t id, uint32_t mode);
 PGPU_API int pgpu_scene_profile(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator,
                        uint64_t seed, double* out_kernel_ms);
 PGPU_API int pgpu_scene_clear(uint64_t id);
+/* Renders several scenes at once: scene ids[i] gets spp[i] more samples (numbered after its
+ * earlier ones) with the same bounce cap, estimator and seed. Up to `concurrency` host threads
+ * render one scene each at a time on the scene's own stream, so small scenes fill the GPU
+ * together. out_ms: time from the batch's start to its last scene's end (CUDA events on the
+ * library stream around the whole batch). Each id may appear once. */
+PGPU_API int pgpu_scenes_render(const uint64_t* ids, uint32_t n, const uint32_t* spp, uint32_t max_bounces,
+                                uint32_t estimator, uint64_t seed, uint32_t concurrency, float* out_ms);
 /* Kernels the scene's last render launched (all iterations, including the empty ones that end the
  * last CUDA-graph batch). */
 PGPU_API int pgpu_scene_launches(uint64_t id, uint64_t* out_launches);

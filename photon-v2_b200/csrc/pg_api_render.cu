@@ -6,7 +6,10 @@
 #include "../../include/photon_gpu.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <exception>
+#include <thread>
 #include <vector>
 
 namespace pg
@@ -266,6 +269,101 @@ int pgpu_scene_profile(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t
 				out_kernel_ms[k] = r->scene->last_kernel_ms()[k];
 			}
 		}
+	});
+}
+
+int pgpu_scenes_render(const uint64_t* ids, uint32_t n, const uint32_t* spp, uint32_t max_bounces,
+                       uint32_t estimator, uint64_t seed, uint32_t concurrency, float* out_ms)
+{
+	return guarded([&]
+	{
+		if(n == 0)
+		{
+			if(out_ms) { *out_ms = 0.0f; }
+			return;
+		}
+		if(!ids || !spp)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scenes_render: null ids or spp");
+		}
+		if(estimator > PG_EST_BVPTDL)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scenes_render: unknown estimator");
+		}
+		std::vector<std::shared_ptr<RenderObject>> objects;
+		for(uint32_t i = 0; i < n; ++i)
+		{
+			for(uint32_t k = 0; k < i; ++k)
+			{
+				if(ids[k] == ids[i])
+				{
+					throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scenes_render: a scene appears twice");
+				}
+			}
+			objects.push_back(get_render(ids[i]));
+		}
+		int device = 0;
+		PG_CUDA_CHECK(cudaGetDevice(&device));
+		const uint32_t workers = std::max(1u, std::min(concurrency, n));
+		cudaEvent_t e0, e1;
+		PG_CUDA_CHECK(cudaEventCreate(&e0));
+		PG_CUDA_CHECK(cudaEventCreate(&e1));
+		PG_CUDA_CHECK(cudaEventRecord(e0, library_stream()));
+		// scenes are handed out in order to `workers` host threads, each rendering on its scene's
+		// own stream, so the scenes' kernels overlap on the device
+		std::atomic<uint32_t> next{0};
+		std::vector<std::exception_ptr> errors(workers);
+		auto work = [&](uint32_t w)
+		{
+			try
+			{
+				PG_CUDA_CHECK(cudaSetDevice(device));
+				for(uint32_t i = next++; i < n; i = next++)
+				{
+					RenderObject& r = *objects[i];
+					RenderParams p;
+					p.width = r.width;
+					p.height = r.height;
+					p.spp = spp[i];
+					p.max_bounces = max_bounces;
+					p.estimator = estimator;
+					p.filter = r.filter;
+					p.seed = seed;
+					p.first_sample = r.samples;
+					r.last_ms = r.scene->render(p, r.film.get());
+					r.samples += spp[i];
+				}
+			}
+			catch(...)
+			{
+				errors[w] = std::current_exception();
+				next = n;   // hand out no further scenes
+			}
+		};
+		std::vector<std::thread> pool;
+		for(uint32_t w = 1; w < workers; ++w)
+		{
+			pool.emplace_back(work, w);
+		}
+		work(0);
+		for(auto& t : pool)
+		{
+			t.join();
+		}
+		PG_CUDA_CHECK(cudaEventRecord(e1, library_stream()));
+		PG_CUDA_CHECK(cudaEventSynchronize(e1));
+		float ms = 0.0f;
+		PG_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+		cudaEventDestroy(e0);
+		cudaEventDestroy(e1);
+		for(const auto& e : errors)
+		{
+			if(e)
+			{
+				std::rethrow_exception(e);
+			}
+		}
+		if(out_ms) { *out_ms = ms; }
 	});
 }
 

@@ -960,6 +960,7 @@ void build_alias(const std::vector<double>& weights, std::vector<float2>& out_al
 RenderScene::RenderScene(const SceneDesc& desc, float max_origin_abs)
 {
 	require_device();
+	PG_CUDA_CHECK(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking));
 	const std::size_t n = desc.tris.size() / 9;
 	if(n == 0)
 	{
@@ -1144,6 +1145,11 @@ RenderScene::~RenderScene()
 	{
 		cudaGraphExecDestroy(m_exec);
 	}
+	if(m_stream)
+	{
+		cudaStreamSynchronize(m_stream);
+		cudaStreamDestroy(m_stream);
+	}
 	if(m_host_counters)
 	{
 		cudaFreeHost(m_host_counters);
@@ -1188,7 +1194,7 @@ void RenderScene::ensure_capacity(uint32_t capacity)
 
 void RenderScene::ensure_guiding(uint32_t capacity)
 {
-	cudaStream_t st = library_stream();
+	cudaStream_t st = m_stream;
 	if(capacity > m_guide_capacity)
 	{
 		for(int b = 0; b < 2; ++b)
@@ -1293,7 +1299,7 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 	const uint32_t capacity = static_cast<uint32_t>(std::min<unsigned long long>(params.capacity, total));
 	ensure_capacity(std::max<uint32_t>(capacity, 1024u));
 
-	cudaStream_t st = library_stream();
+	cudaStream_t st = m_stream;
 	RenderCounters init{};
 	init.total_paths = total;
 	PG_CUDA_CHECK(cudaMemcpyAsync(m_counters.get(), &init, sizeof(init), cudaMemcpyHostToDevice, st));

@@ -325,6 +325,8 @@ private:
 	float m_last_guide_loss = 0.0f;
 	unsigned long long m_last_guided = 0;
 
+	// the scene's own stream: renders of different scenes, from different host threads, overlap
+	cudaStream_t m_stream = nullptr;
 	// pinned readback of the counters, and the instantiated two-iteration graph of the last
 	// render (kept across renders and updated in place when only kernel arguments change)
 	RenderCounters* m_host_counters = nullptr;

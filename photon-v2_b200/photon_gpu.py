@@ -62,6 +62,8 @@ PGPU_SIGNATURES = [
     ("pgpu_scene_set_filter", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32]),
     ("pgpu_scene_set_dome_pdf", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32]),
     ("pgpu_scene_launches", ctypes.c_int, [ctypes.c_uint64, _u64p]),
+    ("pgpu_scenes_render", ctypes.c_int,
+     [_u64p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32, _f32p]),
     ("pgpu_scene_count", ctypes.c_int,
      [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _u64p]),
     ("pgpu_scene_profile", ctypes.c_int,
@@ -262,6 +264,17 @@ def flatten_scene(scene):
                    + [scene.fov_deg, scene.width, scene.height], np.float32)
     return (np.ascontiguousarray(np.concatenate(tris)), np.concatenate(tri_mat), np.concatenate(tri_em),
             np.asarray(mats, np.float32).reshape(-1, 8), np.asarray(ems, np.float32).reshape(-1, 4), cam)
+
+
+def render_scenes(render_scenes, spp, max_bounces=10000, estimator=BNEEPT, seed=42, concurrency=4) -> float:
+    """pgpu_scenes_render: renders RenderScenes together (spp[i] more samples each), up to
+    `concurrency` at a time on their own streams; returns the batch's device span in ms."""
+    ids = np.array([rs.id for rs in render_scenes], np.uint64)
+    counts = np.array(spp, np.uint32)
+    ms = ctypes.c_float()
+    _check(load().pgpu_scenes_render(_ptr(ids, ctypes.c_uint64), len(ids), _ptr(counts, ctypes.c_uint32), max_bounces,
+                                     estimator, seed, concurrency, ctypes.byref(ms)))
+    return ms.value
 
 
 class RenderScene:

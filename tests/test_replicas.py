@@ -88,3 +88,28 @@ def test_split_sample_ranges_reproduce_one_render(gpu_lib, sample_filter):
     total = parts[0] + parts[1]
     assert np.allclose(total, ref, rtol=1e-12, atol=1e-12)
     assert ref.sum() > 0
+
+
+@pytest.mark.gpu
+def test_concurrent_batch_equals_renders_one_by_one(gpu_lib):
+    """pgpu_scenes_render with several scenes in flight gives each scene the film it gets from its
+    own render (same paths, same generator keys; FP64 atomics only change the addition order)."""
+    import photon_gpu
+
+    batch = [scenes.cornell(32, 32, 8, 8, "bneept"), scenes.cornell_glossy(24, 24, 5, 8, "bneept"),
+             scenes.ggx_sphere(level=2, width=16, height=16, spp=3, max_bounces=6)]
+    alone = []
+    for sc in batch:
+        with photon_gpu.RenderScene(sc) as rs:
+            rs.render(sc.spp, max_bounces=8, seed=5)
+            alone.append(rs.film()[1])
+    rss = [photon_gpu.RenderScene(sc) for sc in batch]
+    try:
+        ms = photon_gpu.render_scenes(rss, [sc.spp for sc in batch], max_bounces=8, seed=5, concurrency=3)
+        together = [rs.film()[1] for rs in rss]
+    finally:
+        for rs in rss:
+            rs.close()
+    assert ms > 0.0
+    for a, b in zip(alone, together):
+        assert np.allclose(a, b, rtol=1e-12, atol=1e-12)
