@@ -6,7 +6,11 @@
 //
 // A sample at raster position (rx, ry) adds f(px + 0.5 - rx, py + 0.5 - ry) times its radiance to
 // every pixel whose centre lies within the filter's half size, and the same weight to W
-// (HdrRgbFilm::addRgbSample, HdrRgbFilm.cpp:82-123). Samples are spread over the film's sample
+// (HdrRgbFilm::addRgbSample, HdrRgbFilm.cpp:82-123). With the 4 x 4 filters the renderer first
+// collects every path's radiance in a per-path buffer (the shading kernel stores it when the path
+// ends, the traversal kernel adds the NEE light found at its last vertex), and one pass in path
+// order then splats all samples: consecutive paths are neighbouring pixels, so a warp's atomics
+// land in a few adjacent cache lines instead of all over the film. Samples are spread over the film's sample
 // window, the pixel-centre rectangle grown by the half size on every side, so that border pixels
 // see the whole filter support (TSamplingFilm::updateSampleDimensions with soft edges,
 // Engine/Source/Core/Filmic/TSamplingFilm.ipp:102-119). Here the window is cut into W x H equal
@@ -47,6 +51,7 @@ struct FilmView
 	float    half = 0.5f;      // filter half size (pixels)
 	float    x0 = 0.0f, y0 = 0.0f;   // sample window corner
 	float    sx = 1.0f, sy = 1.0f;   // sample window cell size (window extent / resolution)
+	float4*  samples = nullptr;      // 4 x 4 filters: radiance of every path of the pass (by path index)
 };
 
 inline FilmView make_film_view(double* sums, uint32_t width, uint32_t height, uint32_t filter)

@@ -137,16 +137,30 @@ __device__ __forceinline__ float2 raster_position(const FilmView& f, uint32_t pi
 }
 
 // Radiance of a finished path (or a part of it) into the film.
-__device__ __forceinline__ void splat(const FilmView& f, uint32_t pixel, const PathRng& rng, RGB c)
+__device__ __forceinline__ void splat(const FilmView& f, uint32_t pixel, uint32_t path, RGB c)
 {
 	if(f.filter == PG_FILTER_BOX)
 	{
 		film_add_box(f, pixel, c.r, c.g, c.b);
 	}
-	else if(!is_zero(c))
+	else
 	{
-		const float2 r = raster_position(f, pixel, rng);
-		film_deposit(f, r.x, r.y, make_float4(c.r, c.g, c.b, 0.0f));
+		f.samples[path] = make_float4(c.r, c.g, c.b, 0.0f);   // splatted by splat_samples_kernel
+	}
+}
+
+// 4 x 4 filters: every path of the pass into the film, in path order (its raster position from
+// the same counter-based draws the camera ray used), radiance and weight W together.
+__global__ void __launch_bounds__(kShadeBlock)
+splat_samples_kernel(FilmView film, uint64_t seed, uint64_t first_global, uint32_t num_paths)
+{
+	const uint32_t wh = film.width * film.height;
+	for(uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < num_paths; p += gridDim.x * blockDim.x)
+	{
+		const float4 c = film.samples[p];
+		const PathRng rng = make_rng(seed, first_global + p);
+		const float2 r = raster_position(film, p % wh, rng);
+		film_deposit(film, r.x, r.y, make_float4(c.x, c.y, c.z, 1.0f));
 	}
 }
 
@@ -250,10 +264,6 @@ regen_kernel(const RenderCounters* __restrict__ c, Camera cam, FilmView film, ui
 		const float2 raster = raster_position(film, pixel, rng);
 		const float rx = raster.x;
 		const float ry = raster.y;
-		if(film.filter != PG_FILTER_BOX)
-		{
-			film_deposit(film, rx, ry, make_float4(0.0f, 0.0f, 0.0f, 1.0f));   // the sample's filter weights
-		}
 
 		// raster -> sensor (SingleLensObserver::makeRasterToSensor)
 		const float sx = -cam.sensor_w / static_cast<float>(cam.width) * rx + cam.sensor_w * 0.5f;
@@ -499,7 +509,7 @@ shade_kernel(ShadeArgs a)
 					radiance = radiance + le * safe_clamp(thr_emit, 0.0f, kClampMax);
 				}
 			}
-			splat(a.film, pixel, rng, radiance);
+			splat(a.film, pixel, p, radiance);
 			continue;
 		}
 
@@ -517,7 +527,7 @@ shade_kernel(ShadeArgs a)
 		// traceNextSurface rejects hits whose sidedness disagrees (SurfaceTracer.h:126-141).
 		if(!(dot(ng, d) * dot(frame.ns, d) > 0.0f))
 		{
-			splat(a.film, pixel, rng, radiance);
+			splat(a.film, pixel, p, radiance);
 			continue;
 		}
 
@@ -565,7 +575,7 @@ shade_kernel(ShadeArgs a)
 		// ---- does the path continue past this vertex?
 		if((meta & kMetaStopAfter) || bounce >= a.max_bounces)
 		{
-			splat(a.film, pixel, rng, radiance);
+			splat(a.film, pixel, p, radiance);
 			continue;
 		}
 		const RGB throughput = thr_emit * cont;
@@ -816,7 +826,7 @@ shade_kernel(ShadeArgs a)
 		}
 		else
 		{
-			splat(a.film, pixel, rng, radiance);
+			splat(a.film, pixel, p, radiance);
 		}
 
 		if(has_shadow)
@@ -832,7 +842,7 @@ shade_kernel(ShadeArgs a)
 			}
 			if(!continues && a.film.filter != PG_FILTER_BOX)
 			{
-				a.shadow.r[k] = raster_position(a.film, pixel, rng);
+				a.shadow.r[k] = make_float2(__uint_as_float(p), 0.0f);   // the path, for its sample slot
 			}
 			if(sh_refine == 1u)
 			{
@@ -1280,7 +1290,45 @@ void RenderScene::guide_params(float* out) const
 	PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
 }
 
+// Paths whose radiance a pass of a 4 x 4-filter render keeps (16 B each): larger renders are
+// split into passes of whole samples per pixel.
+constexpr unsigned long long kMaxFilteredPassPaths = 1ull << 27;
+
 float RenderScene::render(const RenderParams& params, double* film_sums)
+{
+	const unsigned long long wh = static_cast<unsigned long long>(params.width) * params.height;
+	if(params.filter == PG_FILTER_BOX || wh == 0 || wh * params.spp <= kMaxFilteredPassPaths)
+	{
+		return render_pass(params, film_sums);
+	}
+	const uint32_t pass_spp = static_cast<uint32_t>(std::max<unsigned long long>(1ull, kMaxFilteredPassPaths / wh));
+	float ms = 0.0f;
+	unsigned long long rays = 0, shadow = 0, iterations = 0, launches = 0, counts[4] = {0, 0, 0, 0};
+	double kernel_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+	for(uint32_t done = 0; done < params.spp; )
+	{
+		RenderParams p = params;
+		p.spp = std::min(pass_spp, params.spp - done);
+		p.first_sample = params.first_sample + done;
+		ms += render_pass(p, film_sums);
+		rays += m_last_rays;
+		shadow += m_last_shadow;
+		iterations += m_last_iterations;
+		launches += m_last_launches;
+		for(int k = 0; k < 4; ++k) { counts[k] += m_last_counts[k]; }
+		for(int k = 0; k < 7; ++k) { kernel_ms[k] += m_kernel_ms[k]; }
+		done += p.spp;
+	}
+	m_last_rays = rays;
+	m_last_shadow = shadow;
+	m_last_iterations = iterations;
+	m_last_launches = launches;
+	for(int k = 0; k < 4; ++k) { m_last_counts[k] = counts[k]; }
+	for(int k = 0; k < 7; ++k) { m_kernel_ms[k] = kernel_ms[k]; }
+	return ms;
+}
+
+float RenderScene::render_pass(const RenderParams& params, double* film_sums)
 {
 	if(params.width == 0 || params.height == 0 || params.spp == 0)
 	{
@@ -1318,7 +1366,15 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 		sqs[b] = ShadowQueue{m_so[b].get(), m_sd[b].get(), m_sc[b].get()};
 		sqs[b].r = m_sr[b].get();
 	}
-	const FilmView film = make_film_view(film_sums, params.width, params.height, params.filter);
+	FilmView film = make_film_view(film_sums, params.width, params.height, params.filter);
+	if(params.filter != PG_FILTER_BOX)
+	{
+		if(m_samples.size() < total)
+		{
+			m_samples.resize(total);
+		}
+		film.samples = m_samples.get();
+	}
 	const uint64_t first_global = params.first_sample * wh;
 	const bool counting = params.mode == PG_RENDER_COUNT;
 	// BVPTDL follows one BSDF-sampled bounce whatever the configured depth (BVPTDLEstimator.cpp:62-95)
@@ -1453,6 +1509,15 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 			PG_CUDA_CHECK(cudaGetLastError());
 		}
 	};
+	// the 4 x 4 filters: every path's radiance, kept per path during the pass, into the film
+	auto splat_samples = [&]
+	{
+		if(params.filter != PG_FILTER_BOX)
+		{
+			splat_samples_kernel<<<grid, kShadeBlock, 0, st>>>(film, params.seed, first_global, static_cast<uint32_t>(total));
+			PG_CUDA_CHECK(cudaGetLastError());
+		}
+	};
 
 	if(!m_host_counters)
 	{
@@ -1521,6 +1586,7 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 			}
 			batch = std::min(batch * 2, 64);
 		}
+		splat_samples();
 		PG_CUDA_CHECK(cudaEventRecord(e1, st));
 		PG_CUDA_CHECK(cudaEventSynchronize(e1));
 	}
@@ -1559,6 +1625,7 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 				break;
 			}
 		}
+		splat_samples();
 		PG_CUDA_CHECK(cudaEventRecord(e1, st));
 		PG_CUDA_CHECK(cudaEventSynchronize(e1));
 		for(cudaEvent_t& e : ev) { cudaEventDestroy(e); }
@@ -1581,7 +1648,7 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 		                                         (params.refine_mode == PG_REFINE_ITERATIVE ? 1ull : 0ull) +
 		                                         (guided ? 2ull : 0ull) +
 		                                         (training ? (m_guide_params.clamp > 0.0f ? 8ull : 6ull) : 0ull);
-		m_last_launches = iterations * per_iteration + (params.filter == PG_FILTER_BOX ? 1ull : 0ull);
+		m_last_launches = iterations * per_iteration + 1ull;   // + the film's box-weight or splat launch
 	}
 	m_last_counts[0] = final_counters.nodes_closest;
 	m_last_counts[1] = final_counters.tris_closest;

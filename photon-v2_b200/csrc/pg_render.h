@@ -284,6 +284,7 @@ public:
 	void guide_params(float* out) const;
 
 private:
+	float render_pass(const RenderParams& params, double* film_device);
 	void ensure_capacity(uint32_t capacity);
 	void ensure_guiding(uint32_t capacity);
 
@@ -304,6 +305,7 @@ private:
 	DeviceBuffer<float2>   m_sr[2];
 	DeviceBuffer<uint32_t> m_req_single, m_req_mutual;
 	DeviceBuffer<uint32_t> m_order;   // shading order: kOrderLists lists of m_order_list slots
+	DeviceBuffer<float4>   m_samples; // 4 x 4 filters: radiance of every path of a pass
 	uint32_t m_order_list = 0;
 	DeviceBuffer<RenderCounters> m_counters;
 

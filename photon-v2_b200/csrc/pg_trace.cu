@@ -238,8 +238,14 @@ __device__ __forceinline__ void add_unoccluded(uint32_t i, const float4* __restr
 		}
 		else
 		{
-			const float2 r = __ldg(sr + i);
-			film_deposit(film, r.x, r.y, make_float4(c.x, c.y, c.z, 0.0f));
+			// the path already stored its radiance in its sample slot (it ended in an earlier
+			// kernel); each path has at most one such contribution
+			float4* s = film.samples + __float_as_uint(__ldg(sr + i).x);
+			float4 v = *s;
+			v.x += c.x;
+			v.y += c.y;
+			v.z += c.z;
+			*s = v;
 		}
 	}
 	else
