@@ -232,7 +232,8 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 4
     relMSE against a `ref_spp` plain render, averaged over `trials` independent renders of each
     (single renders of this scene are dominated by rare bright paths). `relmse_ratio` < 1 means
     guiding wins at equal time; the ratio also estimates (time for guided to reach the plain
-    error) / (plain time)."""
+    error) / (plain time). `guided_frozen` repeats the guided renders with training switched off
+    after the warm-up (inference only), at its own equal-time sample count."""
     import photon_gpu
 
     scene = scenes.slit_room(res, res, 1, 10, num_boxes=num_boxes)
@@ -256,7 +257,17 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 4
             guided_ms.append(rs.render(guided_spp, max_bounces=10, seed=3 + 1000 * t)["ms"])
             e_guided.append(rel_mse(rs.film()[0], ref))
         info = rs.guide_info()
-    mp, mg = float(np.mean(e_plain)), float(np.mean(e_guided))
+        # the same network frozen (inference only, no training step): its own equal-time spp
+        rs.set_guiding(True, False, 0.5, 3e-3, 16384)
+        rs.clear()
+        calib = rs.render(max(1, plain_spp // 2), max_bounces=10, seed=200)
+        frozen_spp = max(1, int(statistics.median(plain_ms) / (calib["ms"] / max(1, plain_spp // 2))))
+        e_frozen, frozen_ms = [], []
+        for t in range(trials):
+            rs.clear()
+            frozen_ms.append(rs.render(frozen_spp, max_bounces=10, seed=4 + 1000 * t)["ms"])
+            e_frozen.append(rel_mse(rs.film()[0], ref))
+    mp, mg, mf = float(np.mean(e_plain)), float(np.mean(e_guided)), float(np.mean(e_frozen))
     return {
         "workload": f"slit_room {res}x{res}, {scene.num_tris} triangles, depth 10",
         "reference_spp": ref_spp, "trials": trials,
@@ -266,6 +277,9 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 4
                    "relmse_trials": e_guided, "warmup_spp": warmup_renders * max(1, plain_spp // 2),
                    "train_loss": info["loss"]},
         "relmse_ratio": mg / mp if mp > 0 else None,
+        "guided_frozen": {"spp": frozen_spp, "ms": statistics.median(frozen_ms), "relmse": mf,
+                          "relmse_trials": e_frozen, "note": "the trained network without further training steps"},
+        "relmse_ratio_frozen": mf / mp if mp > 0 else None,
     }
 
 
