@@ -8,7 +8,7 @@ phRender -> phAquireFrameRaw), exactly as a reference user would drive it. Refer
   4096-8192 spp),
   in the reference's default iterative surface refinement and, for two scenes, in its empirical
   and manual modes (the reference's EngineConfig.ini on its side, phGpuSetSurfaceRefine on ours).
-  The bar is the north star's image tolerance: relMSE <= 1e-3, relMSE being the mean over pixels
+  The bar is an image tolerance of relMSE <= 1e-3, relMSE being the mean over pixels
   and channels of (x - ref)^2 / (ref^2 + 1e-2). Both images carry Monte Carlo noise, which the
   bound includes. BNEEPT images meet it at full resolution; BVPT and BVPTDL (no light sampling, a
   small light) are noise-dominated at these sample counts, so it is held to the bar on 4 x 4 block means

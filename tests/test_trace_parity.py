@@ -8,7 +8,7 @@ arithmetic), except for near-ties: where two triangles meet (shared edges and ve
 starting on a surface) both report hits whose t differ by at most an ulp or two, and which one
 wins depends on traversal order -- the reference's scaled range check (tScaled <= maxT * det)
 lets a later triangle replace an earlier one whose t is a rounding step smaller. For those rays
-the hit primitive may differ but t must agree within 2 ulp, the bound the north star sets; they
+the hit primitive may differ but t must agree within 2 ulp; they
 are counted and bounded. Same primitive means bit-identical t and barycentrics.
 """
 
