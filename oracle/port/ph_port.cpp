@@ -147,6 +147,18 @@ struct Scene
 	std::vector<float> cdf;        // emitter pick CDF (TPwcDistribution1D semantics)
 	int env = -1;
 	Rgb env_radiance;
+	// the dome (LatLongEnvEmitter over PLatLongEnvSphere): lat-long image (row 0 = bottom; a
+	// constant environment is 1 x 1), rotation, sphere, and the texel distribution
+	// (TPwcDistribution2D: marginal CDF over rows, conditional CDFs within rows)
+	uint32_t env_w = 0, env_h = 0;
+	std::vector<Rgb> env_texels;
+	double env_rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+	double env_center[3] = {0, 0, 0};
+	double env_radius = 1;
+	bool env_exact = false;
+	std::vector<double> env_row_cdf;    // [h + 1]
+	std::vector<double> env_col_cdf;    // [h][w + 1]
+	std::vector<double> env_pdf_uv;     // [h][w]
 	// camera
 	Vec cam_pos, ax, ay, az;
 	float sensor_w = 0, sensor_h = 0, sensor_offset = 0;
@@ -688,6 +700,129 @@ bool surface_at(const Scene& s, Vec o, Vec d, Surface* x, Vec* dir_in)
 	return true;
 }
 
+// ---- the dome (Core/Emitter/LatLongEnvEmitter.cpp:36-150, Core/Intersection/PLatLongEnvSphere.cpp)
+
+struct EnvConfig
+{
+	std::vector<float> rgb;
+	uint32_t w = 0, h = 0;
+	double rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+	double center[3] = {0, 0, 0};
+	bool exact = false;
+};
+
+EnvConfig& env_config()
+{
+	static EnvConfig cfg;
+	return cfg;
+}
+
+// Lat-long coordinates of a world direction (TSphere::surfaceToLatLong01 in the dome's frame).
+void env_uv(const Scene& s, Vec d, double* u, double* v)
+{
+	const double* R = s.env_rot;
+	const double lx = R[0] * d.x + R[3] * d.y + R[6] * d.z;
+	const double ly = R[1] * d.x + R[4] * d.y + R[7] * d.z;
+	const double lz = R[2] * d.x + R[5] * d.y + R[8] * d.z;
+	const double len = std::sqrt(lx * lx + ly * ly + lz * lz);
+	const double theta = std::acos(std::min(std::max(len > 0 ? ly / len : 1.0, -1.0), 1.0));
+	double phi = std::atan2(lx, lz);
+	if(phi < 0) { phi += 2 * M_PI; }
+	*u = phi / (2 * M_PI);
+	*v = (M_PI - theta) / M_PI;
+}
+
+// Bilinear with clamped edges (TPixelTexture2D::samplePixelBufferBilinear).
+Rgb env_lookup(const Scene& s, double u, double v)
+{
+	const int w = static_cast<int>(s.env_w), h = static_cast<int>(s.env_h);
+	const double x = std::min(std::max(u, 0.0), 1.0) * w - 0.5, y = std::min(std::max(v, 0.0), 1.0) * h - 0.5;
+	const double fx = std::floor(x), fy = std::floor(y), ax = x - fx, ay = y - fy;
+	auto at = [&](int i, int j)
+	{
+		i = std::min(std::max(i, 0), w - 1);
+		j = std::min(std::max(j, 0), h - 1);
+		return s.env_texels[static_cast<std::size_t>(j) * w + i];
+	};
+	const int i0 = static_cast<int>(fx), j0 = static_cast<int>(fy);
+	return at(i0, j0) * static_cast<float>((1 - ax) * (1 - ay)) + at(i0, j0 + 1) * static_cast<float>((1 - ax) * ay) +
+	       at(i0 + 1, j0) * static_cast<float>(ax * (1 - ay)) + at(i0 + 1, j0 + 1) * static_cast<float>(ax * ay);
+}
+
+double env_distance(const Scene& s, Vec x, Vec w)
+{
+	const double ox = x.x - s.env_center[0], oy = x.y - s.env_center[1], oz = x.z - s.env_center[2];
+	const double b = ox * w.x + oy * w.y + oz * w.z;
+	const double c = ox * ox + oy * oy + oz * oz - s.env_radius * s.env_radius;
+	return -b + std::sqrt(std::max(b * b - c, 0.0));
+}
+
+double env_texel_pdf(const Scene& s, double u, double v)
+{
+	const uint32_t i = std::min(static_cast<uint32_t>(std::max(u, 0.0) * s.env_w), s.env_w - 1);
+	const uint32_t j = std::min(static_cast<uint32_t>(std::max(v, 0.0) * s.env_h), s.env_h - 1);
+	return s.env_pdf_uv[static_cast<std::size_t>(j) * s.env_w + i];
+}
+
+// Solid-angle density the reference assigns to a BSDF-sampled ray from x along w that leaves
+// the scene (LatLongEnvEmitter::calcDirectPdf: area density on the dome sphere, converted with
+// the distance and cosine at the ray's hit on it), or the exact density.
+double env_pdf_hit(const Scene& s, Vec x, Vec w)
+{
+	double u, v;
+	env_uv(s, w, &u, &v);
+	double pdf = env_texel_pdf(s, u, v) / (2 * M_PI * M_PI * std::sin(M_PI * (1 - v)));
+	if(!s.env_exact)
+	{
+		const double d = env_distance(s, x, w);
+		const double px = x.x + d * w.x - s.env_center[0], py = x.y + d * w.y - s.env_center[1], pz = x.z + d * w.z - s.env_center[2];
+		const double cos_p = std::abs(px * w.x + py * w.y + pz * w.z) / s.env_radius;
+		pdf *= d * d / (s.env_radius * s.env_radius * cos_p);
+	}
+	return std::isfinite(pdf) && pdf > 0 ? pdf : 0;
+}
+
+// A dome sample for NEE at x (LatLongEnvEmitter::genDirectSample with
+// PLatLongEnvSphere::genPosSampleWithObservationPos): uv from the 2D piecewise-constant
+// distribution, its direction w, the reference's density (the cosine at the end of an observation
+// ray of length r, projected onto the sphere, where the shadow ray also aims) or the exact one.
+bool env_sample(const Scene& s, Vec x, float r0, float r1, Vec* w_out, double* pdf_out, Rgb* le, Vec* shadow_dir)
+{
+	const std::size_t h = s.env_h, wdt = s.env_w;
+	std::size_t j = std::min<std::size_t>(std::upper_bound(s.env_row_cdf.begin() + 1, s.env_row_cdf.end(), r0) -
+	                                      (s.env_row_cdf.begin() + 1), h - 1);
+	const double rj0 = s.env_row_cdf[j], rj1 = s.env_row_cdf[j + 1];
+	const double fv = rj1 > rj0 ? (r0 - rj0) / (rj1 - rj0) : 0.5;
+	const double* col = &s.env_col_cdf[j * (wdt + 1)];
+	std::size_t i = std::min<std::size_t>(std::upper_bound(col + 1, col + wdt + 1, r1) - (col + 1), wdt - 1);
+	const double fu = col[i + 1] > col[i] ? (r1 - col[i]) / (col[i + 1] - col[i]) : 0.5;
+	const double u = (i + std::min(std::max(fu, 0.0), 1.0)) / wdt, v = (j + std::min(std::max(fv, 0.0), 1.0)) / h;
+	const double theta = (1 - v) * M_PI, phi = 2 * M_PI * u, st = std::sin(theta);
+	const double lx = st * std::sin(phi), ly = std::cos(theta), lz = st * std::cos(phi);
+	const double* R = s.env_rot;
+	const Vec w = mk(static_cast<float>(R[0] * lx + R[1] * ly + R[2] * lz), static_cast<float>(R[3] * lx + R[4] * ly + R[5] * lz),
+	                 static_cast<float>(R[6] * lx + R[7] * ly + R[8] * lz));
+	double pdf = s.env_pdf_uv[j * wdt + i] / (2 * M_PI * M_PI * st);
+	Vec sd = w;
+	if(!s.env_exact)
+	{
+		const double d = env_distance(s, x, w);
+		double qx = x.x + s.env_radius * w.x - s.env_center[0], qy = x.y + s.env_radius * w.y - s.env_center[1],
+		       qz = x.z + s.env_radius * w.z - s.env_center[2];
+		const double ql = std::sqrt(qx * qx + qy * qy + qz * qz);
+		qx /= ql; qy /= ql; qz /= ql;
+		pdf *= d * d / (s.env_radius * s.env_radius * std::abs(qx * w.x + qy * w.y + qz * w.z));
+		sd = mk(static_cast<float>(s.env_center[0] + s.env_radius * qx - x.x), static_cast<float>(s.env_center[1] + s.env_radius * qy - x.y),
+		        static_cast<float>(s.env_center[2] + s.env_radius * qz - x.z));
+	}
+	if(!(st > 0) || !std::isfinite(pdf) || !(pdf > 0)) { return false; }
+	*w_out = w;
+	*pdf_out = pdf;
+	*le = env_lookup(s, u, v);
+	*shadow_dir = sd;
+	return true;
+}
+
 // One path of BNEEPTEstimator::estimate (Core/Estimator/BNEEPTEstimator.cpp:38-262),
 // BVPTEstimator::estimate (Core/Estimator/BVPTEstimator.cpp:25-160) or
 // BVPTDLEstimator::estimate (Core/Estimator/BVPTDLEstimator.cpp:21-96): BVPT cut after one
@@ -702,11 +837,18 @@ Rgb estimate(const Scene& s, Vec o, Vec d, uint32_t max_bounces, Pcg32& rng)
 	float rr_scale = 1;
 	Surface x;
 	Vec din;
-	auto env_hit = [&](Rgb* le) { *le = s.env_radiance; return s.env >= 0; };
+	auto env_hit = [&](Vec dir, Rgb* le)
+	{
+		if(s.env < 0) { return false; }
+		double u, v;
+		env_uv(s, dir, &u, &v);
+		*le = env_lookup(s, u, v);
+		return true;
+	};
 	if(!surface_at(s, o, d, &x, &din))
 	{
 		Rgb le;
-		if(env_hit(&le)) { energy = energy + le; }
+		if(env_hit(d, &le)) { energy = energy + le; }
 		return energy;
 	}
 	if(!(dot(x.ng, d) * dot(x.ns, d) > 0)) { return energy; }
@@ -733,15 +875,23 @@ Rgb estimate(const Scene& s, Vec o, Vec d, uint32_t max_bounces, Pcg32& rng)
 				std::upper_bound(s.cdf.begin(), s.cdf.end(), u) - s.cdf.begin(), s.emitters.size() - 1);
 			const Emitter& e = s.emitters[ei];
 			Vec to_light;
+			Rgb env_radiance_nee = e.radiance;
 			float pdfw = 0;
 			Offset vis{};
 			bool ok = false;
 			if(e.type == 1)
 			{
-				const float zz = 1 - 2 * rng.u01(), r = std::sqrt(std::max(0.0f, 1 - zz * zz)), ph = 2 * kPi * rng.u01();
-				to_light = mk(r * std::cos(ph), r * std::sin(ph), zz);
-				pdfw = e.pmf / (4 * kPi);
-				if(agreed(x, to_light)) { vis = offset_from(x, s.tris[x.tri], to_light); ok = true; }
+				const float r0 = rng.u01(), r1 = rng.u01();
+				double env_pdf = 0;
+				Vec shadow_dir;
+				Rgb env_le;
+				if(env_sample(s, x.pos, r0, r1, &to_light, &env_pdf, &env_le, &shadow_dir) && agreed(x, to_light))
+				{
+					pdfw = static_cast<float>(e.pmf * env_pdf);
+					env_radiance_nee = env_le;
+					vis = offset_from(x, s.tris[x.tri], shadow_dir);
+					ok = pdfw > 0;
+				}
 			}
 			else if(!e.tris.empty())
 			{
@@ -774,7 +924,7 @@ Rgb estimate(const Scene& s, Vec o, Vec d, uint32_t max_bounces, Pcg32& rng)
 					Rgb w = f * std::abs(dot(x.ns, l));
 					w = w * thr;
 					w = w * (mis / pdfw);
-					energy = energy + e.radiance * safe_clamp(w);
+					energy = energy + (e.type == 1 ? env_radiance_nee : e.radiance) * safe_clamp(w);
 				}
 			}
 		}
@@ -796,7 +946,7 @@ Rgb estimate(const Scene& s, Vec o, Vec d, uint32_t max_bounces, Pcg32& rng)
 		int emitter = -1;
 		bool have_le = false;
 		if(hit) { emitter = emitted(nx, nd, &le); have_le = emitter >= 0; }
-		else { have_le = env_hit(&le); emitter = s.env; }
+		else { have_le = env_hit(nd, &le); emitter = s.env; }
 		if(have_le)
 		{
 			if(bvpt)
@@ -810,7 +960,7 @@ Rgb estimate(const Scene& s, Vec o, Vec d, uint32_t max_bounces, Pcg32& rng)
 				{
 					float lp = 0;
 					const Emitter& e = s.emitters[emitter];
-					if(e.type == 1) { lp = e.pmf / (4 * kPi); }
+					if(e.type == 1) { lp = static_cast<float>(e.pmf * env_pdf_hit(s, x.pos, nd)); }
 					else
 					{
 						const Vec tt = x.pos - nx.pos;
@@ -903,13 +1053,56 @@ bool setup_scene(Scene& s, const float* cam, const float* tris, const uint32_t* 
 	{
 		if(e.type == 1)
 		{
+			// the dome sphere around the scene bound (ADome.cpp:42-60) and its texel distribution
+			// (LatLongEnvEmitter.cpp:52-79): weights max(luminance, 1e-6) * sin(theta) at texel centres
+			const EnvConfig& cfg = env_config();
+			std::copy(cfg.rot, cfg.rot + 9, s.env_rot);
+			std::copy(cfg.center, cfg.center + 3, s.env_center);
+			s.env_exact = cfg.exact;
 			double r = 1;
 			for(int c = 0; c < 8; ++c)
 			{
-				const double px = (c & 1) ? hi[0] : lo[0], py = (c & 2) ? hi[1] : lo[1], pz = (c & 4) ? hi[2] : lo[2];
+				const double px = ((c & 1) ? hi[0] : lo[0]) - s.env_center[0], py = ((c & 2) ? hi[1] : lo[1]) - s.env_center[1];
+				const double pz = ((c & 4) ? hi[2] : lo[2]) - s.env_center[2];
 				r = std::max(r, std::sqrt(px * px + py * py + pz * pz) * 1.01);
 			}
-			e.weight = std::max<double>(lum(e.radiance), 1e-6) * 4 * M_PI * r * r;
+			s.env_radius = r;
+			s.env_w = cfg.w ? cfg.w : 1;
+			s.env_h = cfg.w ? cfg.h : 1;
+			s.env_texels.clear();
+			for(std::size_t k = 0; k < static_cast<std::size_t>(s.env_w) * s.env_h; ++k)
+			{
+				s.env_texels.push_back(cfg.w ? Rgb{cfg.rgb[3 * k], cfg.rgb[3 * k + 1], cfg.rgb[3 * k + 2]} : e.radiance);
+			}
+			std::vector<double> wts(s.env_texels.size());
+			double sum = 0;
+			for(uint32_t j = 0; j < s.env_h; ++j)
+			{
+				const double sin_theta = std::sin((1 - (j + 0.5) / s.env_h) * M_PI);
+				for(uint32_t i = 0; i < s.env_w; ++i)
+				{
+					const std::size_t k = static_cast<std::size_t>(j) * s.env_w + i;
+					wts[k] = std::max<double>(lum(s.env_texels[k]), 1e-6) * sin_theta;
+					sum += wts[k];
+				}
+			}
+			s.env_row_cdf.assign(s.env_h + 1, 0.0);
+			s.env_col_cdf.assign(static_cast<std::size_t>(s.env_h) * (s.env_w + 1), 0.0);
+			s.env_pdf_uv.assign(wts.size(), 0.0);
+			for(uint32_t j = 0; j < s.env_h; ++j)
+			{
+				double row = 0;
+				double* col = &s.env_col_cdf[static_cast<std::size_t>(j) * (s.env_w + 1)];
+				for(uint32_t i = 0; i < s.env_w; ++i) { row += wts[static_cast<std::size_t>(j) * s.env_w + i]; col[i + 1] = row; }
+				for(uint32_t i = 0; i <= s.env_w; ++i) { col[i] = row > 0 ? col[i] / row : (double)i / s.env_w; }
+				s.env_row_cdf[j + 1] = s.env_row_cdf[j] + row / sum;
+				for(uint32_t i = 0; i < s.env_w; ++i)
+				{
+					const std::size_t k = static_cast<std::size_t>(j) * s.env_w + i;
+					s.env_pdf_uv[k] = wts[k] / sum * wts.size();
+				}
+			}
+			e.weight = sum * 4 * M_PI * r * r;
 		}
 		else
 		{
@@ -1093,6 +1286,21 @@ void render_filtered(const Scene& s, uint32_t spp, uint32_t max_bounces, uint32_
 }// end anonymous namespace
 
 extern "C" {
+
+// The dome of the next renders: a lat-long image [h][w][3] (row 0 = bottom) with its rotation
+// (row-major, dome local -> world) and centre; w = 0 keeps the emitter's constant radiance as a
+// 1 x 1 image. exact != 0 uses the true densities instead of the reference's.
+int port_set_environment(const float* rgb, uint32_t w, uint32_t h, const float* rot, const float* center, uint32_t exact)
+{
+	EnvConfig& cfg = env_config();
+	cfg.w = rgb && w && h ? w : 0;
+	cfg.h = rgb && w && h ? h : 0;
+	cfg.rgb.assign(rgb && w && h ? rgb : nullptr, rgb && w && h ? rgb + static_cast<std::size_t>(w) * h * 3 : nullptr);
+	for(int k = 0; k < 9; ++k) { cfg.rot[k] = rot ? rot[k] : (k % 4 == 0 ? 1.0 : 0.0); }
+	for(int k = 0; k < 3; ++k) { cfg.center[k] = center ? center[k] : 0.0; }
+	cfg.exact = exact != 0;
+	return 0;
+}
 
 // Closest hit / occlusion over host triangles: rays [n][8] = origin, minT, direction, maxT.
 int port_trace(const float* tris, uint32_t num_tris, const float* rays, uint32_t n,

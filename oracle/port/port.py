@@ -84,6 +84,29 @@ def render(flat_scene, spp, max_bounces, estimator=0, threads=None, seed=1, samp
     return (sums / spp).astype(np.float32)
 
 
+def rotation_matrix(axis, degrees):
+    """Row-major rotation by `degrees` about `axis` (right-handed), as an actor's rotate() sets it."""
+    a = np.asarray(axis, np.float64)
+    a = a / np.linalg.norm(a)
+    t = np.radians(degrees)
+    k = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+    return np.eye(3) + np.sin(t) * k + (1 - np.cos(t)) * (k @ k)
+
+
+def set_environment(image=None, rotation=None, center=(0.0, 0.0, 0.0), exact=False):
+    """The dome of the following renders: `image` [H, W, 3] with row 0 at the top (as written to a
+    PFM by scenes.write_pfm), or None for the scene's constant environment; `rotation` (axis,
+    degrees) of the dome; `exact` for the true sample densities instead of the reference's."""
+    rot = np.ascontiguousarray(rotation_matrix(*rotation) if rotation else np.eye(3), np.float32)
+    c = np.ascontiguousarray(center, np.float32)
+    if image is None:
+        load().port_set_environment(None, 0, 0, _p(rot, ctypes.c_float), _p(c, ctypes.c_float), int(exact))
+        return
+    img = np.ascontiguousarray(np.asarray(image, np.float32)[::-1])   # row 0 = bottom
+    load().port_set_environment(_p(img, ctypes.c_float), img.shape[1], img.shape[0], _p(rot, ctypes.c_float),
+                                _p(c, ctypes.c_float), int(exact))
+
+
 def write_scene_bin(path, flat_scene, spp, estimator=0):
     """The scene file ph_port_render reads (see oracle/port/ph_port.cpp)."""
     tris, tri_mat, tri_em, mats, ems, cam = flat_scene
