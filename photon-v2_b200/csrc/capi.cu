@@ -198,11 +198,19 @@ void phCreateFrame(PhUInt64* out_frameId, PhUInt32 widthPx, PhUInt32 heightPx)
 	{
 		return;
 	}
-	auto f = std::make_unique<HdrFrame>();
-	f->width = widthPx;
-	f->height = heightPx;
-	f->rgb.assign(static_cast<std::size_t>(widthPx) * heightPx * 3, 0.0f);
-	*out_frameId = frames().add(std::move(f));
+	*out_frameId = 0;
+	try
+	{
+		auto f = std::make_unique<HdrFrame>();
+		f->width = widthPx;
+		f->height = heightPx;
+		f->rgb.assign(static_cast<std::size_t>(widthPx) * heightPx * 3, 0.0f);
+		*out_frameId = frames().add(std::move(f));
+	}
+	catch(const std::exception& ex)
+	{
+		log_error("phCreateFrame", ex);   // no frame: the id stays 0
+	}
 }
 
 void phGetFrameDimension(PhUInt64 frameId, PhUInt32* out_widthPx, PhUInt32* out_heightPx)

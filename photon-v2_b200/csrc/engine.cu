@@ -296,8 +296,11 @@ void Engine::cook(SceneDesc& desc)
 		if(const SdlClause* fs = find(session->clauses, "frame-size"))
 		{
 			const auto v = sdl_numbers(fs->value);
-			width = static_cast<uint32_t>(v.at(0));
-			height = static_cast<uint32_t>(v.at(1));
+			if(v.size() != 2)
+			{
+				throw std::runtime_error("frame-size needs two numbers");
+			}
+			checked_resolution(v[0], v[1], "frame-size", &width, &height);
 		}
 		const Resource* observer = ref(*session, "observer");
 		const Resource* sampler = ref(*session, "sample-source");
@@ -330,7 +333,12 @@ void Engine::cook(SceneDesc& desc)
 			const double offset = get_real(observer->clauses, "sensor-offset-mm", 36.0);
 			fov = 2.0 * std::atan((sensor_w * 0.5) / offset) * 180.0 / kPiD;
 		}
-		m_spp = sampler ? static_cast<uint32_t>(get_real(sampler->clauses, "samples", 1.0)) : 1u;
+		const double samples = sampler ? get_real(sampler->clauses, "samples", 1.0) : 1.0;
+		if(!(samples >= 1.0 && samples <= 4294967295.0 && samples == std::floor(samples)))
+		{
+			throw std::runtime_error("sample-source samples must be a whole number in [1, 2^32 - 1]");
+		}
+		m_spp = static_cast<uint32_t>(samples);
 		m_estimator = PG_EST_BNEEPT;
 		m_filter = PG_FILTER_BLACKMAN_HARRIS;
 		if(visualizer)

@@ -137,10 +137,13 @@ int pgpu_scene_create_ex(const float* tris, const uint32_t* tri_material, const 
 		{
 			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create_ex: unknown BVH builder");
 		}
-		if(!tris || num_tris == 0 || !tri_material || !materials || num_materials == 0 || !camera || !out_id)
+		if(!tris || num_tris == 0 || !tri_material || !materials || num_materials == 0 || !camera || !out_id ||
+		   (num_emitters > 0 && !emitters))
 		{
 			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create: missing input");
 		}
+		uint32_t w = 0, h = 0;
+		checked_resolution(camera[10], camera[11], "pgpu_scene_create", &w, &h);
 		SceneDesc d;
 		d.tris.assign(tris, tris + 9 * num_tris);
 		d.tri_material.assign(tri_material, tri_material + num_tris);
@@ -163,10 +166,10 @@ int pgpu_scene_create_ex(const float* tris, const uint32_t* tri_material, const 
 		for(uint32_t m = 0; m < num_materials; ++m)
 		{
 			const float* p = materials + 8 * m;
-			const int type = static_cast<int>(p[0]);
-			if(type == 0)      { d.materials.push_back(make_matte(p[1], p[2], p[3])); }
-			else if(type == 1) { d.materials.push_back(make_conductor(p[4], p[1], p[2], p[3])); }
-			else if(type == 2) { d.materials.push_back(make_dielectric(p[4], p[5], p[6])); }
+			const float type = p[0];
+			if(type == 0.0f)      { d.materials.push_back(make_matte(p[1], p[2], p[3])); }
+			else if(type == 1.0f) { d.materials.push_back(make_conductor(p[4], p[1], p[2], p[3])); }
+			else if(type == 2.0f) { d.materials.push_back(make_dielectric(p[4], p[5], p[6])); }
 			else
 			{
 				throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create: unknown material type");
@@ -175,6 +178,10 @@ int pgpu_scene_create_ex(const float* tris, const uint32_t* tri_material, const 
 		for(uint32_t e = 0; e < num_emitters; ++e)
 		{
 			const float* p = emitters + 4 * e;
+			if(p[3] != static_cast<float>(PG_EMITTER_TRIANGLES) && p[3] != static_cast<float>(PG_EMITTER_ENV))
+			{
+				throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create: unknown emitter type");
+			}
 			EmitterRec rec{};
 			rec.r = p[0]; rec.g = p[1]; rec.b = p[2];
 			rec.type = static_cast<uint32_t>(p[3]);
@@ -188,12 +195,6 @@ int pgpu_scene_create_ex(const float* tris, const uint32_t* tri_material, const 
 				d.env_rgb[0] = p[0]; d.env_rgb[1] = p[1]; d.env_rgb[2] = p[2];
 			}
 			d.emitters.push_back(rec);
-		}
-		const uint32_t w = static_cast<uint32_t>(camera[10]);
-		const uint32_t h = static_cast<uint32_t>(camera[11]);
-		if(w == 0 || h == 0)
-		{
-			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_create: zero resolution");
 		}
 		d.camera = make_camera(camera, camera + 3, camera + 6, camera[9], w, h);
 		d.bvh_builder = bvh_builder;

@@ -2,9 +2,22 @@
 
 #include <algorithm>
 #include <cmath>
+#include <string>
 
 namespace pg
 {
+
+void checked_resolution(double width, double height, const char* who, uint32_t* out_width, uint32_t* out_height)
+{
+	auto whole = [](double v) { return std::isfinite(v) && v >= 1.0 && v <= 2147483648.0 && v == std::floor(v); };
+	if(!whole(width) || !whole(height) || width * height > 2147483648.0)
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, std::string(who) + ": the resolution must be two whole numbers of at least 1 "
+		                                     "with at most 2^31 pixels in all");
+	}
+	*out_width = static_cast<uint32_t>(width);
+	*out_height = static_cast<uint32_t>(height);
+}
 
 Camera make_camera(const float pos[3], const float dir[3], const float up[3], float fov_degrees,
                    uint32_t width, uint32_t height, float sensor_width_mm)

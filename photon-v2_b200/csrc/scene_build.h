@@ -14,6 +14,12 @@ namespace pg
 Camera make_camera(const float pos[3], const float dir[3], const float up[3], float fov_degrees,
                    uint32_t width, uint32_t height, float sensor_width_mm = 36.0f);
 
+// Film resolution from caller-supplied numbers (the session's frame-size, a vector of two uint32,
+// SingleFrameRenderSession.h:43): each a whole number of at least 1, and at most 2^31 pixels in
+// all, so that every per-pixel kernel's 32-bit grid-stride index stays below 2^32. Throws Error
+// (PG_ERR_INVALID_ARGUMENT) naming `who` otherwise.
+void checked_resolution(double width, double height, const char* who, uint32_t* out_width, uint32_t* out_height);
+
 // Material record from the SDL-level parameters. Roughness maps to alpha = roughness^2
 // (RoughnessToAlphaMapping::Squared, the MicrosurfaceInfo default) with the floor of
 // IsoTrowbridgeReitzConstant (alpha >= 0.001).

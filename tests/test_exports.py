@@ -3,6 +3,7 @@
 import os
 import re
 
+import pytest
 from conftest import ROOT
 
 import photon_gpu
@@ -38,3 +39,64 @@ def test_calls_without_device_fail_loudly():
         assert "no CUDA device" in str(e)
     else:
         raise AssertionError("geometry creation succeeded without a device")
+
+
+def _create_status(tris, tri_mat, tri_em, mats, ems, cam, emitters_null=False):
+    import ctypes
+
+    import numpy as np
+
+    lib = photon_gpu.load()
+    sid = ctypes.c_uint64(0)
+
+    def ptr(a, t):
+        return a.ctypes.data_as(ctypes.POINTER(t))
+
+    em_ptr = None if emitters_null else ptr(ems, ctypes.c_float)
+    status = lib.pgpu_scene_create_ex(ptr(tris, ctypes.c_float), ptr(tri_mat, ctypes.c_uint32),
+                                      ptr(tri_em, ctypes.c_uint32), tris.shape[0], ptr(mats, ctypes.c_float),
+                                      mats.shape[0], em_ptr, ems.shape[0], ptr(cam, ctypes.c_float), 0,
+                                      ctypes.byref(sid))
+    assert sid.value == 0
+    return status, lib.pgpu_last_error().decode()
+
+
+@pytest.mark.parametrize("case, message", [
+    ("width0", "resolution"), ("height_negative", "resolution"), ("width_nan", "resolution"),
+    ("width_fraction", "resolution"), ("too_many_pixels", "resolution"), ("emitters_null", "missing input"),
+    ("emitter_type", "unknown emitter type"), ("material_type", "unknown material type"),
+    ("material_type_nan", "unknown material type"), ("material_index", "material index out of range"),
+])
+def test_scene_create_rejects_bad_input_before_device_work(case, message):
+    # every check runs before the library touches a device, so these need no GPU
+    import numpy as np
+
+    import scenes
+
+    tris, tri_mat, tri_em, mats, ems, cam = photon_gpu.flatten_scene(scenes.cornell(8, 8, 1))
+    tris, tri_mat, tri_em, mats, ems, cam = (a.copy() for a in (tris, tri_mat, tri_em, mats, ems, cam))
+    assert ems.shape[0] > 0
+    emitters_null = False
+    if case == "width0":
+        cam[10] = 0
+    elif case == "height_negative":
+        cam[11] = -8
+    elif case == "width_nan":
+        cam[10] = np.nan
+    elif case == "width_fraction":
+        cam[10] = 8.5
+    elif case == "too_many_pixels":
+        cam[10], cam[11] = 65536, 65537
+    elif case == "emitters_null":
+        emitters_null = True
+    elif case == "emitter_type":
+        ems[0, 3] = 7
+    elif case == "material_type":
+        mats[0, 0] = 3
+    elif case == "material_type_nan":
+        mats[0, 0] = np.nan
+    elif case == "material_index":
+        tri_mat[0] = mats.shape[0]
+    status, text = _create_status(tris, tri_mat, tri_em, mats, ems, cam, emitters_null)
+    assert status == 1, (status, text)   # PG_ERR_INVALID_ARGUMENT
+    assert message in text, text

@@ -132,6 +132,23 @@ def test_errors_are_reported(snippet, message):
     assert message in str(err.value)
 
 
+@pytest.mark.parametrize("old, new, message", [
+    ('frame-size "8 8"', 'frame-size "0 8"', "resolution"),
+    ('frame-size "8 8"', 'frame-size "8 -2"', "resolution"),
+    ('frame-size "8 8"', 'frame-size "8.5 8"', "resolution"),
+    ('frame-size "8 8"', 'frame-size "65536 65537"', "resolution"),
+    ('frame-size "8 8"', 'frame-size "8"', "two numbers"),
+    ("[integer samples 1]", "[integer samples 0]", "whole number"),
+    ("[integer samples 1]", "[integer samples -3]", "whole number"),
+])
+def test_bad_session_numbers_are_reported(old, new, message):
+    base = scenes.to_sdl(scenes.cornell(8, 8, 1))
+    assert old in base
+    with pytest.raises(photon_gpu.PhotonGpuError) as err:
+        _cook(base.replace(old, new))
+    assert message in str(err.value)
+
+
 def test_degenerate_triangles_are_dropped():
     s = scenes.cornell(8, 8, 1)
     g = s.groups[0]
