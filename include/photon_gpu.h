@@ -132,14 +132,18 @@ PGPU_API int pgpu_bsdf_eval(const float* cases, const float* normals, uint64_t n
  * EqualSamplingRenderer.cpp:119-203) driving BNEEPTEstimator::estimate
  * (Engine/Source/Core/Estimator/BNEEPTEstimator.cpp:38-262), BVPTEstimator::estimate
  * (Engine/Source/Core/Estimator/BVPTEstimator.cpp:25-160) or BVPTDLEstimator::estimate
- * (Engine/Source/Core/Estimator/BVPTDLEstimator.cpp:21-96) into an HdrRgbFilm with a box filter.
+ * (Engine/Source/Core/Estimator/BVPTDLEstimator.cpp:21-96) into an HdrRgbFilm (box filter unless
+ * pgpu_scene_set_filter picks another).
  *
  * tris: float32 [n][3][3]; tri_material: uint32 [n]; tri_emitter: uint32 [n] = emitter index + 1
  *   (0 = not emissive; may be NULL).
  * materials: float32 [m][8] = type (0 matte, 1 GGX conductor, 2 GGX dielectric), c0, c1, c2,
  *   roughness, ior_outer, ior_inner, 0 -- c = albedo (matte) or F0 (conductor).
  * emitters: float32 [e][4] = radiance r, g, b, type (0 triangle group, 1 constant environment).
- * camera: float32 [12] = position(3), direction(3), up(3), horizontal fov (degrees), width, height.
+ * camera: float32 [12] = position(3), direction(3), up(3), horizontal fov (degrees), width, height;
+ *   width and height whole numbers of at least 1, at most 2^31 pixels in all.
+ * Every check (null arrays, index and type ranges, resolution) runs before any device work and
+ * fails with PG_ERR_INVALID_ARGUMENT.
  */
 PGPU_API int pgpu_scene_create(const float* tris, const uint32_t* tri_material, const uint32_t* tri_emitter,
                                uint64_t num_tris, const float* materials, uint32_t num_materials,

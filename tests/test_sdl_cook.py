@@ -206,3 +206,44 @@ def test_ply_rejects_polygons_and_bad_indices(faces, tmp_path):
     _write_custom_ply(tmp_path / "g0.ply", props, [(0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 0)], faces)
     with pytest.raises(photon_gpu.PhotonGpuError, match="PLY"):
         _cook(_ply_scene_text(), str(tmp_path))
+
+
+_PLY_XYZ = b"property float x\nproperty float y\nproperty float z\n"
+_PLY_FACE = b"element face 1\nproperty list uchar int vertex_indices\n"
+
+
+@pytest.mark.parametrize("content, message", [
+    (b"plx\nformat ascii 1.0\n", "not a PLY file"),
+    (b"ply\nformat ascii 1.0\nelement vertex 3\n" + _PLY_XYZ + _PLY_FACE, "no end_header"),
+    (b"ply\nformat binary_middle_endian 1.0\nelement vertex 3\n" + _PLY_XYZ + _PLY_FACE + b"end_header\n",
+     "unknown format"),
+    (b"ply\nformat ascii 1.0\nelement vertex 3\nproperty float x\nproperty float y\n" + _PLY_FACE
+     + b"end_header\n0 0\n1 0\n0 1\n3 0 1 2\n", "needs x, y and z"),
+    (b"ply\nformat ascii 1.0\n" + _PLY_FACE + b"element vertex 3\n" + _PLY_XYZ
+     + b"end_header\n3 0 1 2\n0 0 0\n1 0 0\n0 1 0\n", "must follow the vertex element"),
+    (b"ply\nformat ascii 1.0\nelement vertex 3\n" + _PLY_XYZ
+     + b"element face 1\nproperty list uchar float vertex_indices\nend_header\n0 0 0\n1 0 0\n0 1 0\n3 0 1 2\n",
+     "must be integers"),
+    (b"ply\nformat ascii 1.0\nelement vertex 3\n" + _PLY_XYZ + b"property short q\n" + _PLY_FACE
+     .replace(b"int", b"int128") + b"end_header\n", "unknown property type"),
+    (b"ply\nformat ascii 1.0\nelement vertex 3\n" + _PLY_XYZ + _PLY_FACE + b"end_header\n0 0 0\n1 0 0\n0 1\n",
+     "truncated or malformed ASCII body"),
+    (b"ply\nformat binary_little_endian 1.0\nelement vertex 3\n" + _PLY_XYZ + _PLY_FACE + b"end_header\n"
+     + np.zeros(9, "<f4").tobytes() + b"\x03" + np.arange(2, dtype="<i4").tobytes(), "truncated binary body"),
+])
+def test_ply_malformed_files_are_reported(content, message, tmp_path):
+    (tmp_path / "g0.ply").write_bytes(content)
+    with pytest.raises(photon_gpu.PhotonGpuError) as err:
+        _cook(_ply_scene_text(), str(tmp_path))
+    assert message in str(err.value)
+
+
+def test_ply_big_endian_doubles_and_short_indices(tmp_path):
+    # scalar types other than float / int, in big-endian order
+    verts = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], ">f8")
+    body = verts.tobytes() + b"\x03" + np.array([0, 1, 2], ">u2").tobytes()
+    head = (b"ply\nformat binary_big_endian 1.0\nelement vertex 3\nproperty double x\nproperty double y\n"
+            b"property double z\nelement face 1\nproperty list uchar ushort vertex_indices\nend_header\n")
+    (tmp_path / "g0.ply").write_bytes(head + body)
+    c = _cook(_ply_scene_text(), str(tmp_path))
+    assert np.array_equal(c.tris, verts.astype(np.float32)[None])
