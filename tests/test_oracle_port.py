@@ -54,6 +54,29 @@ def test_port_hits_match_reference(port, name):
     assert np.array_equal(occ, d["occluded"])
 
 
+def test_smoke_checker_on_port_hits(port):
+    """smoke()'s closest-hit check accepts the port's answers on the Cornell fixture (including
+    rays that start on a surface, hit at t = +0 where the reference reports -0), and rejects a
+    wrong primitive, a hit turned into a miss and a t moved by 3 ulp."""
+    import __graft_entry__ as entry
+
+    d = dict(np.load(os.path.join(GOLDEN, "hits_cornell.npz")))
+    prim, t, _, _ = port.trace(d["tris"], d["rays"])
+    assert np.any((t == 0) & (d["t"] == 0) & np.signbit(d["t"]) & ~np.signbit(t))
+    assert entry.hits_agree(prim, t, d["prim"], d["t"]).all()
+    hit = np.flatnonzero((prim >= 0) & (prim == d["prim"]) & (t > 0))
+    k = hit[0]
+    bad = prim.copy()
+    bad[k] = (prim[k] + 1) % d["tris"].shape[0]
+    far = t.copy()
+    far.view(np.int32)[k] += 3
+    missed = prim.copy()
+    missed[k] = -1
+    assert not entry.hits_agree(missed, t, d["prim"], d["t"])[k]
+    moved = entry.hits_agree(bad, far, d["prim"], d["t"])
+    assert not moved[k] and moved.sum() == len(prim) - 1
+
+
 def test_port_bsdf_matches_reference(port):
     d = np.load(os.path.join(GOLDEN, "bsdf_cases.npz"))
     cases, ref = d["cases"], d["out"]
