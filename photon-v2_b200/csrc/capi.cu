@@ -246,7 +246,15 @@ PhBool phLoadFrame(PhUInt64 frameId, const PhChar* filePath)
 	{
 		return PH_FALSE;
 	}
-	return read_pfm(filePath, *f) ? PH_TRUE : PH_FALSE;
+	try
+	{
+		return read_pfm(filePath, *f) ? PH_TRUE : PH_FALSE;
+	}
+	catch(const std::exception& ex)
+	{
+		log_error("phLoadFrame", ex);
+		return PH_FALSE;
+	}
 }
 
 PhBool phSaveFrame(PhUInt64 frameId, const PhChar* filePath, const PhFrameSaveInfo* /*saveInfo*/)

@@ -992,12 +992,26 @@ bool read_pfm(const std::string& path, HdrFrame& frame)
 	{
 		return false;
 	}
-	uint32_t w = 0, h = 0;
+	long long w = 0, h = 0;
 	double scale = 0.0;
 	in >> w >> h >> scale;
 	in.get();
+	if(!in || w < 0 || h < 0 || w > 0x7FFFFFFFll || h > 0x7FFFFFFFll || !std::isfinite(scale) || scale == 0.0)
+	{
+		return false;
+	}
 	const int channels = magic == "PF" ? 3 : 1;
-	std::vector<float> data(static_cast<std::size_t>(w) * h * channels);
+	// the header's size must be backed by the bytes that follow it (checked before allocating)
+	const std::streamoff body_begin = in.tellg();
+	in.seekg(0, std::ios::end);
+	const std::streamoff body_bytes = in.tellg() - body_begin;
+	in.seekg(body_begin);
+	const unsigned long long needed = static_cast<unsigned long long>(w) * static_cast<unsigned long long>(h) * channels * 4ull;
+	if(body_begin < 0 || body_bytes < 0 || static_cast<unsigned long long>(body_bytes) < needed)
+	{
+		return false;
+	}
+	std::vector<float> data(static_cast<std::size_t>(w) * static_cast<std::size_t>(h) * channels);
 	in.read(reinterpret_cast<char*>(data.data()), static_cast<std::streamsize>(data.size() * sizeof(float)));
 	if(!in)
 	{
@@ -1013,10 +1027,10 @@ bool read_pfm(const std::string& path, HdrFrame& frame)
 			std::memcpy(&v, &u, 4);
 		}
 	}
-	frame.width = w;
-	frame.height = h;
-	frame.rgb.resize(static_cast<std::size_t>(w) * h * 3);
-	for(std::size_t i = 0; i < static_cast<std::size_t>(w) * h; ++i)
+	frame.width = static_cast<uint32_t>(w);
+	frame.height = static_cast<uint32_t>(h);
+	frame.rgb.resize(static_cast<std::size_t>(w) * static_cast<std::size_t>(h) * 3);
+	for(std::size_t i = 0; i < static_cast<std::size_t>(w) * static_cast<std::size_t>(h); ++i)
 	{
 		for(int c = 0; c < 3; ++c)
 		{

@@ -100,3 +100,38 @@ def test_scene_create_rejects_bad_input_before_device_work(case, message):
     status, text = _create_status(tris, tri_mat, tri_em, mats, ems, cam, emitters_null)
     assert status == 1, (status, text)   # PG_ERR_INVALID_ARGUMENT
     assert message in text, text
+
+
+def test_frames_load_and_save_pfm_without_a_device(tmp_path):
+    # frames live on the host: phCreateFrame / phLoadFrame / phSaveFrame / phGetFrameRgbData
+    import ctypes
+
+    import numpy as np
+
+    lib = photon_gpu.load()
+    fid = ctypes.c_uint64(0)
+    lib.phCreateFrame(ctypes.byref(fid), 2, 2)
+    assert fid.value != 0
+    try:
+        rgb = np.arange(12, dtype=np.float32).reshape(2, 2, 3) / 7.0
+        good = tmp_path / "a.pfm"
+        good.write_bytes(b"PF\n2 2\n-1.0\n" + rgb.astype("<f4").tobytes())
+        assert lib.phLoadFrame(fid.value, str(good).encode()) == 1
+        w, h = ctypes.c_uint32(), ctypes.c_uint32()
+        lib.phGetFrameDimension(fid.value, ctypes.byref(w), ctypes.byref(h))
+        assert (w.value, h.value) == (2, 2)
+        data = ctypes.POINTER(ctypes.c_float)()
+        lib.phGetFrameRgbData(fid.value, ctypes.byref(data))
+        assert np.array_equal(np.ctypeslib.as_array(data, (12,)), rgb.reshape(-1))
+        out = tmp_path / "b.pfm"
+        assert lib.phSaveFrame(fid.value, str(out).encode(), None) == 1
+        assert out.read_bytes() == good.read_bytes()
+        huge = tmp_path / "huge.pfm"
+        huge.write_bytes(b"PF\n100000 100000\n-1.0\n" + bytes(48))
+        assert lib.phLoadFrame(fid.value, str(huge).encode()) == 0
+        short = tmp_path / "short.pfm"
+        short.write_bytes(b"PF\n2 2\n-1.0\n" + bytes(44))
+        assert lib.phLoadFrame(fid.value, str(short).encode()) == 0
+        assert lib.phLoadFrame(fid.value, str(tmp_path / "missing.pfm").encode()) == 0
+    finally:
+        lib.phDeleteFrame(fid.value)

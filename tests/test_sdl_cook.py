@@ -120,6 +120,30 @@ def test_environment_dome(tmp_path):
     assert np.isclose(c.camera[15], 4 * math.pi * r * r, rtol=1e-5)
 
 
+@pytest.mark.parametrize("content", [
+    b"PF\n4 2\n-1.0\n" + bytes(4 * 2 * 3 * 4 - 4),          # one float short
+    b"PF\n100000 100000\n-1.0\n" + bytes(48),             # a header that claims 120 GB
+    b"PF\n-4 2\n-1.0\n" + bytes(96),                       # negative width
+    b"PF\n4 2\n0\n" + bytes(96),                           # scale 0 (no byte order)
+    b"P6\n4 2\n255\n" + bytes(24),                         # not a PFM
+])
+def test_malformed_dome_images_are_reported(content, tmp_path):
+    s = scenes.ggx_sphere(level=2, width=16, height=16, spp=1)
+    (tmp_path / "env.pfm").write_bytes(content)
+    with pytest.raises(photon_gpu.PhotonGpuError) as err:
+        _cook(scenes.to_sdl(s), str(tmp_path))
+    assert "cannot read dome image" in str(err.value)
+
+
+def test_little_and_big_endian_dome_images(tmp_path):
+    s = scenes.ggx_sphere(level=2, width=16, height=16, spp=1)
+    for scale, order in ((-1.0, "<f4"), (1.0, ">f4")):
+        (tmp_path / "env.pfm").write_bytes(f"PF\n1 1\n{scale}\n".encode() + np.array([0.25, 0.5, 2.0], order).tobytes())
+        c = _cook(scenes.to_sdl(s), str(tmp_path))
+        env = c.emitters[c.emitters[:, 3] == 1]
+        assert np.array_equal(env[0, :3], np.array([0.25, 0.5, 2.0], np.float32))
+
+
 @pytest.mark.parametrize("snippet, message", [
     ("geometry(sphere) @g = [real radius 1];\nactor(model) @a = [geometry geometry @g] [material material @m];\n"
      "material(matte-opaque) @m = ;", "not supported"),
