@@ -259,6 +259,23 @@ PlyMesh read_ply(const std::string& path)
 	}
 
 	std::vector<char> body((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+	// Every row takes at least a known number of bytes (binary: its scalars and list counts; ASCII:
+	// one character and a separator per value), so element counts the body cannot hold are
+	// rejected before anything is sized by them.
+	long double min_bytes = 0.0L;
+	for(const Element& e : elements)
+	{
+		uint64_t row = 0;
+		for(const Property& p : e.props)
+		{
+			row += ascii ? 2u : type_size(p.is_list ? p.count_type : p.type);
+		}
+		min_bytes += static_cast<long double>(e.count) * static_cast<long double>(row);
+	}
+	if(min_bytes > static_cast<long double>(body.size()) + 1.0L)
+	{
+		throw std::runtime_error("PLY: truncated body (the header's element counts need more bytes than the file holds)");
+	}
 	BodyReader reader(std::move(body), ascii, big);
 
 	PlyMesh mesh;

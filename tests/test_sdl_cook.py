@@ -251,9 +251,16 @@ _PLY_FACE = b"element face 1\nproperty list uchar int vertex_indices\n"
     (b"ply\nformat ascii 1.0\nelement vertex 3\n" + _PLY_XYZ + b"property short q\n" + _PLY_FACE
      .replace(b"int", b"int128") + b"end_header\n", "unknown property type"),
     (b"ply\nformat ascii 1.0\nelement vertex 3\n" + _PLY_XYZ + _PLY_FACE + b"end_header\n0 0 0\n1 0 0\n0 1\n",
+     "PLY: truncated"),
+    (b"ply\nformat ascii 1.0\nelement vertex 3\n" + _PLY_XYZ + _PLY_FACE + b"end_header\n0 0 0\n1 0 0\n0 1 x\n3 0 1 2\n",
      "truncated or malformed ASCII body"),
     (b"ply\nformat binary_little_endian 1.0\nelement vertex 3\n" + _PLY_XYZ + _PLY_FACE + b"end_header\n"
      + np.zeros(9, "<f4").tobytes() + b"\x03" + np.arange(2, dtype="<i4").tobytes(), "truncated binary body"),
+    # element counts far beyond the body: rejected before anything is sized by them
+    (b"ply\nformat binary_little_endian 1.0\nelement vertex 1000000000\n" + _PLY_XYZ + _PLY_FACE
+     + b"end_header\n" + np.zeros(9, "<f4").tobytes(), "truncated body"),
+    (b"ply\nformat ascii 1.0\nelement vertex 3\n" + _PLY_XYZ + _PLY_FACE.replace(b"face 1", b"face 400000000000")
+     + b"end_header\n0 0 0\n1 0 0\n0 1 0\n3 0 1 2\n", "truncated body"),
 ])
 def test_ply_malformed_files_are_reported(content, message, tmp_path):
     (tmp_path / "g0.ply").write_bytes(content)
