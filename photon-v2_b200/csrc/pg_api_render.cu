@@ -306,10 +306,8 @@ int pgpu_scenes_render(const uint64_t* ids, uint32_t n, const uint32_t* spp, uin
 		int device = 0;
 		PG_CUDA_CHECK(cudaGetDevice(&device));
 		const uint32_t workers = std::max(1u, std::min(concurrency, n));
-		cudaEvent_t e0, e1;
-		PG_CUDA_CHECK(cudaEventCreate(&e0));
-		PG_CUDA_CHECK(cudaEventCreate(&e1));
-		PG_CUDA_CHECK(cudaEventRecord(e0, library_stream()));
+		ScopedEvent e0, e1;
+		PG_CUDA_CHECK(cudaEventRecord(e0.get(), library_stream()));
 		// scenes are handed out in order to `workers` host threads, each rendering on its scene's
 		// own stream, so the scenes' kernels overlap on the device
 		std::atomic<uint32_t> next{0};
@@ -351,12 +349,10 @@ int pgpu_scenes_render(const uint64_t* ids, uint32_t n, const uint32_t* spp, uin
 		{
 			t.join();
 		}
-		PG_CUDA_CHECK(cudaEventRecord(e1, library_stream()));
-		PG_CUDA_CHECK(cudaEventSynchronize(e1));
+		PG_CUDA_CHECK(cudaEventRecord(e1.get(), library_stream()));
+		PG_CUDA_CHECK(cudaEventSynchronize(e1.get()));
 		float ms = 0.0f;
-		PG_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-		cudaEventDestroy(e0);
-		cudaEventDestroy(e1);
+		PG_CUDA_CHECK(cudaEventElapsedTime(&ms, e0.get(), e1.get()));
 		for(const auto& e : errors)
 		{
 			if(e)

@@ -111,6 +111,21 @@ private:
 	std::unordered_map<uint64_t, std::shared_ptr<T>> m_items;
 };
 
+// A CUDA event destroyed with its scope, so that a CUDA check that throws between the event's
+// creation and its last use does not leak it.
+class ScopedEvent
+{
+public:
+	ScopedEvent() { PG_CUDA_CHECK(cudaEventCreate(&m_event)); }
+	~ScopedEvent() { cudaEventDestroy(m_event); }
+	ScopedEvent(const ScopedEvent&) = delete;
+	ScopedEvent& operator=(const ScopedEvent&) = delete;
+	cudaEvent_t get() const { return m_event; }
+
+private:
+	cudaEvent_t m_event = nullptr;
+};
+
 // Device buffer with RAII ownership.
 template<typename T>
 class DeviceBuffer

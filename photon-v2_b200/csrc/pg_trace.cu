@@ -594,17 +594,13 @@ int pgpu_trace_closest_device(uint64_t id, const float* d_rays, uint64_t n, void
 	{
 		auto g = get_geometry(id);
 		cudaStream_t s = library_stream();
-		cudaEvent_t e0, e1;
-		PG_CUDA_CHECK(cudaEventCreate(&e0));
-		PG_CUDA_CHECK(cudaEventCreate(&e1));
-		PG_CUDA_CHECK(cudaEventRecord(e0, s));
+		ScopedEvent e0, e1;
+		PG_CUDA_CHECK(cudaEventRecord(e0.get(), s));
 		launch_trace_closest(*g, d_rays, n, d_hits, s);
-		PG_CUDA_CHECK(cudaEventRecord(e1, s));
-		PG_CUDA_CHECK(cudaEventSynchronize(e1));
+		PG_CUDA_CHECK(cudaEventRecord(e1.get(), s));
+		PG_CUDA_CHECK(cudaEventSynchronize(e1.get()));
 		float ms = 0.0f;
-		PG_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-		cudaEventDestroy(e0);
-		cudaEventDestroy(e1);
+		PG_CUDA_CHECK(cudaEventElapsedTime(&ms, e0.get(), e1.get()));
 		check_device_error(*g, s);
 		if(out_ms) { *out_ms = ms; }
 	});
@@ -616,17 +612,13 @@ int pgpu_trace_any_device(uint64_t id, const float* d_rays, uint64_t n, int32_t*
 	{
 		auto g = get_geometry(id);
 		cudaStream_t s = library_stream();
-		cudaEvent_t e0, e1;
-		PG_CUDA_CHECK(cudaEventCreate(&e0));
-		PG_CUDA_CHECK(cudaEventCreate(&e1));
-		PG_CUDA_CHECK(cudaEventRecord(e0, s));
+		ScopedEvent e0, e1;
+		PG_CUDA_CHECK(cudaEventRecord(e0.get(), s));
 		launch_trace_any(*g, d_rays, n, d_occluded, s);
-		PG_CUDA_CHECK(cudaEventRecord(e1, s));
-		PG_CUDA_CHECK(cudaEventSynchronize(e1));
+		PG_CUDA_CHECK(cudaEventRecord(e1.get(), s));
+		PG_CUDA_CHECK(cudaEventSynchronize(e1.get()));
 		float ms = 0.0f;
-		PG_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-		cudaEventDestroy(e0);
-		cudaEventDestroy(e1);
+		PG_CUDA_CHECK(cudaEventElapsedTime(&ms, e0.get(), e1.get()));
 		check_device_error(*g, s);
 		if(out_ms) { *out_ms = ms; }
 	});
