@@ -8,6 +8,7 @@
 #include "../../include/ph_c_core.h"
 #include "../../include/photon_gpu.h"
 
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -28,7 +29,7 @@ struct EngineSlot
 {
 	Engine engine;
 	std::string error_copy;
-	bool region_pending = false;
+	std::atomic<bool> region_pending{false};   // set by phRender, consumed by a polling thread
 };
 
 Registry<EngineSlot>& engines() { static Registry<EngineSlot> r; return r; }
@@ -382,14 +383,13 @@ void phAsyncGetRenderState(PhUInt64 engineId, struct PHRenderState* out_state)
 PhBool phAsyncPollUpdatedFrameRegion(PhUInt64 engineId, PhFrameRegionInfo* out_regionInfo)
 {
 	auto e = engines().get(engineId);
-	if(!e || !out_regionInfo || !e->region_pending)
+	if(!e || !out_regionInfo || !e->region_pending.exchange(false))
 	{
 		return PH_FALSE;
 	}
 	uint32_t w = 0, h = 0;
 	e->engine.get_render_dimension(&w, &h);
 	*out_regionInfo = PhFrameRegionInfo{0, 0, w, h, PH_FRAME_REGION_STATUS_FINISHED};
-	e->region_pending = false;
 	return PH_TRUE;
 }
 
