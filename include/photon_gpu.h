@@ -5,6 +5,11 @@
  * the most recent failure on the calling thread. These entry points sit below the Photon C API
  * (ph_c_core.h, also exported by this library) and expose the hot-path stages one by one so that
  * each can be checked against the reference and measured on its own.
+ *
+ * Devices: an object (geometry, render scene) lives on the device that was current when it was
+ * created, and every later call on it must be made with that device current; otherwise the call
+ * fails with PG_ERR_INVALID_ARGUMENT before any work. Library work runs on one stream per device.
+ * One process may drive several devices this way; the usual layout is one process per GPU.
  */
 #ifndef PHOTON_GPU_H
 #define PHOTON_GPU_H
@@ -82,7 +87,9 @@ PGPU_API int pgpu_trace_any_device(uint64_t id, const float* d_rays, uint64_t n,
  * call; larger n is rejected with PG_ERR_INVALID_ARGUMENT before any work. The array needs no
  * zero-initialisation (every slot a call reads is written earlier in that call).
  * Setup: the first call on a device (with that device current) looks up the array's device
- * address once; a call with n = 0 does only that. Make that first call before beginning any
+ * address once; a call with n = 0 does only that. Like every call on a geometry, it must be made
+ * with the geometry's device current (PG_ERR_INVALID_ARGUMENT otherwise), so that the array, the
+ * stream and the geometry all belong to one device. Make that first call before beginning any
  * stream capture on the device.
  * Calls that overlap in time on the same device (several host threads) race on the one array:
  * the caller serialises them. */
@@ -188,6 +195,24 @@ PGPU_API int pgpu_scene_clear(uint64_t id);
  * library stream around the whole batch). Each id may appear once. */
 PGPU_API int pgpu_scenes_render(const uint64_t* ids, uint32_t n, const uint32_t* spp, uint32_t max_bounces,
                                 uint32_t estimator, uint64_t seed, uint32_t concurrency, float* out_ms);
+/* Light selection of a scene as its kernels use it. Replaces ESPowerFavoring::update / pickEmitter
+ * (Engine/Source/Core/Emitter/Sampler/ESPowerFavoring.cpp:21-59): each emitter's pick
+ * probability, proportional to its approximate flux -- colour energy x area x pi summed over its
+ * triangles for an area light (DiffuseSurfaceEmitter.cpp:55-86, GroupedDiffuseSurfaceEmitter.cpp:
+ * 110-120), luminance x sin(theta) x dome area for the environment. out_pmf [num_emitters] float:
+ * the probability the NEE and MIS weights use; out_alias_pmf [num_emitters] double: the
+ * probability the device alias table realises. Emitters are numbered as at pgpu_scene_create
+ * (the environment last). Any output may be NULL. */
+PGPU_API int pgpu_scene_light_pmf(uint64_t id, float* out_pmf, double* out_alias_pmf, uint32_t* out_num_emitters);
+/* Solid-angle density of direct light samples, computed by the shading kernel's NEE code.
+ * Replaces ESPowerFavoring::calcDirectPdf (ESPowerFavoring.cpp:82-97) over area emitters
+ * (GroupedDiffuseSurfaceEmitter.cpp:80-84, SurfaceEmitter.cpp:37-61): pick probability x
+ * 1 / (triangles of the emitter) x area density converted to solid angle; 0 where the light
+ * triangle's front face does not face the receiving point or the triangle emits nothing.
+ * queries [n][6] float = receiving point (3), point on the light triangle (3); prims [n] = the
+ * light triangle's index in the scene's input order; out_pdf_w [n]. */
+PGPU_API int pgpu_scene_light_pdf(uint64_t id, const float* queries, const uint32_t* prims, uint64_t n,
+                                  float* out_pdf_w);
 /* Kernels the scene's last render launched (all iterations, including the empty ones that end the
  * last CUDA-graph batch). */
 PGPU_API int pgpu_scene_launches(uint64_t id, uint64_t* out_launches);

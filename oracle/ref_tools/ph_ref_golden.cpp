@@ -10,6 +10,22 @@
 //
 // energy <r> <g> <b> <watts>   (see run_energy)
 //
+// lights <groups.f32> <queries.f32> <out.f32>
+//     Light selection and direct-light densities of the reference's power-favouring emitter
+//     sampler (Engine/Source/Core/Emitter/Sampler/ESPowerFavoring.cpp:21-97) over area emitters
+//     made as AAreaLight makes them (Engine/Source/Actor/Light/AAreaLight.cpp:72-85): one
+//     DiffuseSurfaceEmitter for a single triangle, else a GroupedDiffuseSurfaceEmitter, each with a
+//     constant radiance texture.
+//     groups (float32): G, then per group: n, r, g, b, n x 9 vertex coordinates.
+//     queries (float32 x 6 per query): target position (3), group, triangle within the group,
+//        pad; the light point is the triangle's centroid seen along the ray target -> centroid.
+//     out (float32): per group: flux weight (Emitter::calcRadiantFluxApprox, the weight
+//        ESPowerFavoring::update gives it) and pick probability (the sampler's own distribution,
+//        TPwcDistribution1D::pdfDiscrete); then per query: pdfW of ESPowerFavoring::calcDirectPdf
+//        (0 where no pdf), pdfW of the emitter alone (without the pick), 1 if the ray towards the
+//        centroid hit the triangle (else 0 and no densities), and the emission point that hit
+//        produced (3).
+//
 // bsdf  <cases.f32> <out.f32>
 //     Evaluates LambertianReflector, OpaqueMicrofacet (IsoTrowbridgeReitzConstant + Schlick) and
 //     TranslucentMicrofacet (IsoTrowbridgeReitzConstant + exact dielectric Fresnel) through the
@@ -24,6 +40,12 @@
 //        relativeIor, sample_cos, pad, Ng(3), Ns(3) -- the last two are the surface normals the
 //        reference derived from the triangle, which the GPU side must use to compare like for like
 #include "Core/Intersection/PTriangle.h"
+#include "Core/Intersection/PrimitiveMetadata.h"
+#include "Core/Emitter/DiffuseSurfaceEmitter.h"
+#include "Core/Emitter/GroupedDiffuseSurfaceEmitter.h"
+#include "Core/Emitter/Sampler/ESPowerFavoring.h"
+#include "Core/Emitter/Query/DirectEnergyPdfQuery.h"
+#include "Math/Random/TPwcDistribution1D.h"
 #include "Core/Intersection/BVH/TBinaryBvhIntersector.h"
 #include "Core/HitProbe.h"
 #include "Core/Ray.h"
@@ -266,6 +288,133 @@ int run_bsdf(const char* casesPath, const char* outPath)
 	return 0;
 }
 
+// A triangle carrying the metadata that ties it to its emitter, as cooked light primitives do
+// (ESPowerFavoring::calcDirectPdf finds the emitter through the hit primitive's metadata).
+class EmitterTriangle : public PTriangle
+{
+public:
+	EmitterTriangle(const math::Vector3R& a, const math::Vector3R& b, const math::Vector3R& c,
+	                const PrimitiveMetadata* metadata)
+		: PTriangle(a, b, c), m_metadata(metadata)
+	{}
+
+	const PrimitiveMetadata* getMetadata() const override { return m_metadata; }
+
+private:
+	const PrimitiveMetadata* m_metadata;
+};
+
+int run_lights(const char* groupsPath, const char* queriesPath, const char* outPath)
+{
+	const auto g = read_f32(groupsPath);
+	const auto q = read_f32(queriesPath);
+	if(g.empty() || q.size() % 6 != 0)
+	{
+		std::fprintf(stderr, "bad inputs\n");
+		return 1;
+	}
+	const std::size_t numGroups = static_cast<std::size_t>(g[0]);
+	std::vector<std::unique_ptr<PrimitiveMetadata>> metas;
+	std::vector<std::vector<std::unique_ptr<EmitterTriangle>>> tris(numGroups);
+	std::vector<std::vector<math::Vector3R>> centroids(numGroups);
+	std::vector<std::unique_ptr<Emitter>> emitters;
+	std::vector<const Emitter*> emitterPtrs;
+	std::size_t at = 1;
+	for(std::size_t k = 0; k < numGroups; ++k)
+	{
+		const std::size_t n = static_cast<std::size_t>(g.at(at));
+		const math::Spectrum radiance(std::array<real, 3>{g.at(at + 1), g.at(at + 2), g.at(at + 3)});
+		at += 4;
+		metas.push_back(std::make_unique<PrimitiveMetadata>());
+		std::vector<const Primitive*> prims;
+		for(std::size_t i = 0; i < n; ++i, at += 9)
+		{
+			const math::Vector3R va(g.at(at + 0), g.at(at + 1), g.at(at + 2));
+			const math::Vector3R vb(g.at(at + 3), g.at(at + 4), g.at(at + 5));
+			const math::Vector3R vc(g.at(at + 6), g.at(at + 7), g.at(at + 8));
+			tris[k].push_back(std::make_unique<EmitterTriangle>(va, vb, vc, metas.back().get()));
+			centroids[k].push_back(va.add(vb).add(vc).div(3.0_r));
+			prims.push_back(tris[k].back().get());
+		}
+		auto texture = std::make_shared<TConstantTexture<math::Spectrum>>(radiance);
+		if(prims.size() == 1)
+		{
+			emitters.push_back(std::make_unique<DiffuseSurfaceEmitter>(prims[0], texture));
+		}
+		else
+		{
+			emitters.push_back(std::make_unique<GroupedDiffuseSurfaceEmitter>(
+				TSpanView<const Primitive*>(prims.data(), prims.size()), texture));
+		}
+		metas.back()->getSurface().setEmitter(emitters.back().get());
+		emitterPtrs.push_back(emitters.back().get());
+	}
+
+	ESPowerFavoring sampler;
+	sampler.update(TSpanView<const Emitter*>(emitterPtrs.data(), emitterPtrs.size()));
+
+	// the same weights and distribution ESPowerFavoring::update builds (ESPowerFavoring.cpp:41-49)
+	std::vector<real> weights(numGroups);
+	for(std::size_t k = 0; k < numGroups; ++k)
+	{
+		weights[k] = emitterPtrs[k]->calcRadiantFluxApprox();
+	}
+	const math::TPwcDistribution1D<real> distribution(weights);
+
+	std::vector<float> out;
+	for(std::size_t k = 0; k < numGroups; ++k)
+	{
+		out.push_back(weights[k]);
+		out.push_back(distribution.pdfDiscrete(k));
+	}
+	for(std::size_t i = 0; i < q.size() / 6; ++i)
+	{
+		const float* r = &q[6 * i];
+		const math::Vector3R target(r[0], r[1], r[2]);
+		const auto& tri = *tris.at(static_cast<std::size_t>(r[3])).at(static_cast<std::size_t>(r[4]));
+		const math::Vector3R centroid = centroids.at(static_cast<std::size_t>(r[3])).at(static_cast<std::size_t>(r[4]));
+		const math::Vector3R dir = centroid.sub(target);
+		const Ray ray(target, dir.normalize(), 0, dir.length() * 2.0_r);
+		HitProbe probe;
+		float pdfW = 0.0f, emitterPdfW = 0.0f, hit = 0.0f, pos[3] = {0.0f, 0.0f, 0.0f};
+		if(tri.isIntersecting(ray, probe))
+		{
+			hit = 1.0f;
+			const SurfaceHit Xe(ray, probe, SurfaceHitReason(ESurfaceHitReason::IncidentRay));
+			pos[0] = Xe.getPos().x(); pos[1] = Xe.getPos().y(); pos[2] = Xe.getPos().z();
+			DirectEnergyPdfQuery query;
+			query.inputs.set(target, Xe);
+			sampler.calcDirectPdf(query);
+			if(query.outputs)
+			{
+				pdfW = query.outputs.getPdfW();
+			}
+			DirectEnergyPdfQuery alone;
+			alone.inputs.set(target, Xe);
+			emitterPtrs.at(static_cast<std::size_t>(r[3]))->calcDirectPdf(alone);
+			if(alone.outputs)
+			{
+				emitterPdfW = alone.outputs.getPdfW();
+			}
+		}
+		out.push_back(pdfW);
+		out.push_back(emitterPdfW);
+		out.push_back(hit);
+		out.push_back(pos[0]);
+		out.push_back(pos[1]);
+		out.push_back(pos[2]);
+	}
+
+	FILE* f = std::fopen(outPath, "wb");
+	if(!f)
+	{
+		return 1;
+	}
+	std::fwrite(out.data(), sizeof(float), out.size(), f);
+	std::fclose(f);
+	return 0;
+}
+
 }// end anonymous namespace
 
 // energy <r> <g> <b> <watts>: the radiance colour an area light of that colour and power gets,
@@ -293,6 +442,10 @@ int main(int argc, char** argv)
 	{
 		return run_bsdf(argv[2], argv[3]);
 	}
-	std::fprintf(stderr, "usage: %s hits <tris> <rays> <out> | bsdf <cases> <out>\n", argv[0]);
+	if(argc >= 5 && std::string(argv[1]) == "lights")
+	{
+		return run_lights(argv[2], argv[3], argv[4]);
+	}
+	std::fprintf(stderr, "usage: %s hits <tris> <rays> <out> | bsdf <cases> <out> | lights <groups> <queries> <out>\n", argv[0]);
 	return 2;
 }

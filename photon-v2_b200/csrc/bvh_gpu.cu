@@ -669,6 +669,7 @@ std::unique_ptr<Geometry> make_geometry_gpu(const BvhBuildInput& in)
 
 	// 5. collapse, level by level
 	auto g = std::make_unique<Geometry>();
+	g->device = current_device();
 	const uint32_t node_capacity = n + 1;
 	g->nodes.resize(node_capacity);
 	g->tris.resize(n);

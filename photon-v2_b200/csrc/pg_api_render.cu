@@ -94,6 +94,7 @@ void develop_frame(const RenderObject& r, float* out_rgb, uint32_t x, uint32_t y
 	}
 	w = std::min(w, r.width - x);
 	h = std::min(h, r.height - y);
+	std::lock_guard<std::mutex> lock(r.frame_mutex);
 	r.frame.resize(static_cast<std::size_t>(pixels) * 3);
 	cudaStream_t st = library_stream();
 	develop_kernel<<<sm_count() * 4, 256, 0, st>>>(r.film.get(), r.frame.get(), pixels);
@@ -361,6 +362,32 @@ int pgpu_scenes_render(const uint64_t* ids, uint32_t n, const uint32_t* spp, uin
 			}
 		}
 		if(out_ms) { *out_ms = ms; }
+	});
+}
+
+int pgpu_scene_light_pmf(uint64_t id, float* out_pmf, double* out_alias_pmf, uint32_t* out_num_emitters)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		r->scene->light_pmf(out_pmf, out_alias_pmf, out_num_emitters);
+	});
+}
+
+int pgpu_scene_light_pdf(uint64_t id, const float* queries, const uint32_t* prims, uint64_t n, float* out_pdf_w)
+{
+	return guarded([&]
+	{
+		if(n > 0 && (!queries || !prims || !out_pdf_w))
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_light_pdf: null pointer");
+		}
+		if(n > (uint64_t(1) << 31))
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_light_pdf: too many queries in one call");
+		}
+		auto r = get_render(id);
+		r->scene->light_pdf(queries, prims, n, out_pdf_w);
 	});
 }
 

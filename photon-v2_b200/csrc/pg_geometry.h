@@ -14,6 +14,7 @@ struct Geometry
 	DeviceBuffer<uint32_t> error;     // device error flags (PG_DEV_ERR_*)
 	DeviceBuffer<uint32_t> fetch;     // dynamic-fetch cursor of the trace kernels, zeroed per launch
 	BvhBuildStats          stats;
+	int                    device = -1;   // the device current at creation; it holds every buffer above
 };
 
 Registry<Geometry>& geometry_registry();

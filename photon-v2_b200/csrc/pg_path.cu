@@ -117,6 +117,23 @@ __device__ __forceinline__ float pdfa_to_pdfw(float pdf_a, V3 da_to_target, V3 d
 
 __device__ __forceinline__ RGB emitter_radiance(const EmitterRec& e) { return RGB{e.r, e.g, e.b}; }
 
+// Solid-angle density of a direct light sample at xe on light triangle lt (face normal ne) of
+// emitter e, for the receiving point `target`: the power-favouring pick (pmf), the uniform pick
+// among the emitter's triangles (1 / count) and the uniform point on the triangle converted to
+// solid angle (ESPowerFavoring::calcDirectPdf, ESPowerFavoring.cpp:82-97 ->
+// GroupedDiffuseSurfaceEmitter::calcDirectPdf, GroupedDiffuseSurfaceEmitter.cpp:80-84 ->
+// SurfaceEmitter::calcDirectPdfWForSrcPrimitive, SurfaceEmitter.cpp:37-61). 0 where the
+// triangle's front face does not face the target (one-sided emission, canEmit).
+__device__ __forceinline__ float light_triangle_pdf_w(const EmitterRec& e, const TriVerts& lt, V3 ne, V3 xe, V3 target)
+{
+	const V3 emitter_to_target = target - xe;
+	if(!(dot(emitter_to_target, ne) > 0.0f))
+	{
+		return 0.0f;
+	}
+	return pdfa_to_pdfw(1.0f / tri_area(lt), emitter_to_target, ne) * e.rcp_count * e.pmf;
+}
+
 __device__ __forceinline__ uint32_t alias_pick(const float2* alias, uint32_t n, float u)
 {
 	const float scaled = u * static_cast<float>(n);
@@ -652,10 +669,9 @@ shade_kernel(ShadeArgs a)
 				const float lb0 = 1.0f - su, lb1 = su * (1.0f - sv), lb2 = sv * su;
 				const V3 xe = lt.a * lb0 + lt.b * lb1 + lt.c * lb2;
 				const V3 ne = face_normal(lt);
-				const V3 emitter_to_target = pos - xe;
-				if(dot(emitter_to_target, ne) > 0.0f)
+				pdf_w = light_triangle_pdf_w(e, lt, ne, xe, pos);
+				if(pdf_w > 0.0f)
 				{
-					pdf_w = pdfa_to_pdfw(1.0f / tri_area(lt), emitter_to_target, ne) * e.rcp_count * e.pmf;
 					le = emitter_radiance(e);
 					const V3 target_to_emit = xe - pos;
 					if(pdf_w > 0.0f && isfinite(pdf_w) && sidedness_agreed(frame, target_to_emit))
@@ -1290,12 +1306,126 @@ void RenderScene::guide_params(float* out) const
 	PG_CUDA_CHECK(cudaStreamSynchronize(library_stream()));
 }
 
+namespace
+{
+
+// Density of direct light samples (light_triangle_pdf_w, the shading kernel's NEE code) for
+// queries (target xyz, light point xyz) on leaf triangles; 0 for triangles of no emitter.
+__global__ void light_pdf_kernel(DeviceScene s, const float* __restrict__ queries, const uint32_t* __restrict__ leaf,
+                                 uint64_t n, float* __restrict__ out)
+{
+	const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+	if(i >= n)
+	{
+		return;
+	}
+	uint32_t emitter_plus_one = 0;
+	const TriVerts lt = load_tri(s.tris, leaf[i], nullptr, &emitter_plus_one);
+	if(emitter_plus_one == 0u || emitter_plus_one > s.num_emitters)
+	{
+		out[i] = 0.0f;
+		return;
+	}
+	const EmitterRec e = s.emitters[emitter_plus_one - 1u];
+	const float* q = queries + 6 * i;
+	out[i] = light_triangle_pdf_w(e, lt, face_normal(lt), v3(q[3], q[4], q[5]), v3(q[0], q[1], q[2]));
+}
+
+}// end anonymous namespace
+
+void RenderScene::light_pmf(float* out_pmf, double* out_alias_pmf, uint32_t* out_count) const
+{
+	require_same_device(m_geometry->device, "render scene");
+	const uint32_t n = m_dev.num_emitters;
+	if(out_count)
+	{
+		*out_count = n;
+	}
+	if(n == 0)
+	{
+		return;
+	}
+	std::vector<EmitterRec> emitters(n);
+	std::vector<float2> alias(n);
+	cudaStream_t st = library_stream();
+	PG_CUDA_CHECK(cudaMemcpyAsync(emitters.data(), m_emitters.get(), n * sizeof(EmitterRec), cudaMemcpyDeviceToHost, st));
+	PG_CUDA_CHECK(cudaMemcpyAsync(alias.data(), m_alias.get(), n * sizeof(float2), cudaMemcpyDeviceToHost, st));
+	PG_CUDA_CHECK(cudaStreamSynchronize(st));
+	if(out_pmf)
+	{
+		for(uint32_t k = 0; k < n; ++k)
+		{
+			out_pmf[k] = emitters[k].pmf;
+		}
+	}
+	if(out_alias_pmf)
+	{
+		// alias_pick keeps column k with probability x and otherwise takes its alias: column k
+		// gives 1/n x to itself and 1/n (1 - x) to its alias
+		std::vector<double> p(n, 0.0);
+		for(uint32_t k = 0; k < n; ++k)
+		{
+			uint32_t to = 0;
+			std::memcpy(&to, &alias[k].y, sizeof(to));
+			const double keep = std::min(1.0, std::max(0.0, static_cast<double>(alias[k].x)));
+			p[k] += keep / n;
+			if(to < n)
+			{
+				p[to] += (1.0 - keep) / n;
+			}
+		}
+		std::copy(p.begin(), p.end(), out_alias_pmf);
+	}
+}
+
+void RenderScene::light_pdf(const float* queries, const uint32_t* prims, uint64_t n, float* out_pdf_w) const
+{
+	require_same_device(m_geometry->device, "render scene");
+	if(n == 0)
+	{
+		return;
+	}
+	// input triangle index -> leaf slot
+	const std::size_t num_tris = m_geometry->tris.size();
+	std::vector<LeafTri> leaf_tris(num_tris);
+	cudaStream_t st = library_stream();
+	PG_CUDA_CHECK(cudaMemcpyAsync(leaf_tris.data(), m_geometry->tris.get(), m_geometry->tris.bytes(), cudaMemcpyDeviceToHost, st));
+	PG_CUDA_CHECK(cudaStreamSynchronize(st));
+	std::vector<uint32_t> slot_of(num_tris, 0xFFFFFFFFu);
+	for(std::size_t k = 0; k < num_tris; ++k)
+	{
+		if(leaf_tris[k].prim < num_tris)
+		{
+			slot_of[leaf_tris[k].prim] = static_cast<uint32_t>(k);
+		}
+	}
+	std::vector<uint32_t> leaf(n);
+	for(uint64_t i = 0; i < n; ++i)
+	{
+		if(prims[i] >= num_tris || slot_of[prims[i]] == 0xFFFFFFFFu)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "light pdf query " + std::to_string(i) + ": triangle " +
+			            std::to_string(prims[i]) + " is not in the scene (degenerate triangles are dropped)");
+		}
+		leaf[i] = slot_of[prims[i]];
+	}
+	DeviceBuffer<float> d_q(6 * n), d_out(n);
+	DeviceBuffer<uint32_t> d_leaf(n);
+	PG_CUDA_CHECK(cudaMemcpyAsync(d_q.get(), queries, d_q.bytes(), cudaMemcpyHostToDevice, st));
+	PG_CUDA_CHECK(cudaMemcpyAsync(d_leaf.get(), leaf.data(), d_leaf.bytes(), cudaMemcpyHostToDevice, st));
+	light_pdf_kernel<<<static_cast<unsigned>((n + 127) / 128), 128, 0, st>>>(m_dev, d_q.get(), d_leaf.get(), n, d_out.get());
+	PG_CUDA_CHECK(cudaGetLastError());
+	PG_CUDA_CHECK(cudaMemcpyAsync(out_pdf_w, d_out.get(), d_out.bytes(), cudaMemcpyDeviceToHost, st));
+	PG_CUDA_CHECK(cudaStreamSynchronize(st));
+}
+
 // Paths whose radiance a pass of a 4 x 4-filter render keeps (16 B each): larger renders are
 // split into passes of whole samples per pixel.
 constexpr unsigned long long kMaxFilteredPassPaths = 1ull << 27;
 
 float RenderScene::render(const RenderParams& params, double* film_sums)
 {
+	require_same_device(m_geometry->device, "render scene");
 	const unsigned long long wh = static_cast<unsigned long long>(params.width) * params.height;
 	if(params.filter == PG_FILTER_BOX || wh == 0 || wh * params.spp <= kMaxFilteredPassPaths)
 	{

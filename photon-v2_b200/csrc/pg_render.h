@@ -283,6 +283,13 @@ public:
 	// The FP32 network parameters (kNumParams) to the host.
 	void guide_params(float* out) const;
 
+	// Light selection as the kernels see it: each emitter's pick probability (EmitterRec::pmf,
+	// which the NEE and MIS weights use) and the probability the device alias table realises.
+	void light_pmf(float* out_pmf, double* out_alias_pmf, uint32_t* out_count) const;
+	// Direct-light densities of the shading kernel's NEE code: queries [n][6] = receiving point,
+	// point on the light triangle; prims [n] = that triangle's input index.
+	void light_pdf(const float* queries, const uint32_t* prims, uint64_t n, float* out_pdf_w) const;
+
 private:
 	float render_pass(const RenderParams& params, double* film_device);
 	void ensure_capacity(uint32_t capacity);

@@ -3,6 +3,8 @@
 
 #include "pg_render.h"
 
+#include <mutex>
+
 namespace pg
 {
 
@@ -12,6 +14,8 @@ struct RenderObject
 	DeviceBuffer<double> film;      // [h][w][4] sums of filter-weighted radiance and weight (film.cuh)
 	uint32_t filter = PG_FILTER_BOX;
 	mutable DeviceBuffer<float> frame;   // [h][w][3] developed frame (develop_frame)
+	mutable std::mutex frame_mutex;      // one develop at a time: a peek from a polling thread may
+	                                     // overlap a frame readback of the rendering thread
 	uint32_t width = 0, height = 0;
 	uint64_t samples = 0;           // samples per pixel accumulated in the film
 	float last_ms = 0.0f;
@@ -25,7 +29,8 @@ void download_film(const RenderObject& r, double* out_sum);
 
 // Develops the film on the GPU and copies the rectangle [x, x + w) x [y, y + h) of the developed
 // frame into `out_rgb`, a host frame of the film's full size (float [height][width][3]); pixels
-// outside the rectangle are left untouched.
+// outside the rectangle are left untouched. Safe to call from several threads at once (the
+// shared developed-frame buffer is held under the object's frame_mutex).
 void develop_frame(const RenderObject& r, float* out_rgb, uint32_t x, uint32_t y, uint32_t w, uint32_t h);
 
 

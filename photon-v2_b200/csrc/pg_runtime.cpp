@@ -32,20 +32,44 @@ void require_device()
 	}
 }
 
+int current_device()
+{
+	int dev = -1;
+	PG_CUDA_CHECK(cudaGetDevice(&dev));
+	if(dev < 0 || dev >= kMaxDevices)
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, "device index " + std::to_string(dev) + " out of range");
+	}
+	return dev;
+}
+
 cudaStream_t library_stream()
 {
-	static std::once_flag once;
-	static cudaStream_t stream = nullptr;
-	static cudaError_t status = cudaSuccess;
-	std::call_once(once, []
+	static std::mutex mutex;
+	static cudaStream_t streams[kMaxDevices] = {};
+	const int dev = current_device();
+	std::lock_guard<std::mutex> lock(mutex);
+	if(!streams[dev])
 	{
-		status = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
-	});
-	if(status != cudaSuccess)
-	{
-		throw Error(PG_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(status));
+		const cudaError_t status = cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+		if(status != cudaSuccess)
+		{
+			streams[dev] = nullptr;
+			cudaGetLastError();
+			throw Error(PG_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(status));
+		}
 	}
-	return stream;
+	return streams[dev];
+}
+
+void require_same_device(int owner_device, const char* what)
+{
+	const int dev = current_device();
+	if(dev != owner_device)
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, std::string(what) + " lives on device " + std::to_string(owner_device) +
+		            " but device " + std::to_string(dev) + " is current; make its device current first");
+	}
 }
 
 int sm_count()

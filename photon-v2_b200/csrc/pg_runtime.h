@@ -66,8 +66,20 @@ int guarded(Fn&& fn)
 // Fails loudly when no CUDA device is usable: the library has no CPU fallback.
 void require_device();
 
-// The stream all library work is issued on (one per process, created on first use).
+// Devices the library keeps per-device state for (streams, launch shapes, static scratch).
+constexpr int kMaxDevices = 64;
+
+// The current CUDA device (checked against kMaxDevices).
+int current_device();
+
+// The stream library work of the current device is issued on (one per device, created on first
+// use with that device current).
 cudaStream_t library_stream();
+
+// Throws PG_ERR_INVALID_ARGUMENT unless `owner_device` is the current device: objects (geometry,
+// scenes) stay on the device that was current when they were created, and every call on them
+// must be made with that device current.
+void require_same_device(int owner_device, const char* what);
 
 // Thread-safe id -> object table, ids start at 1 (0 is never valid).
 template<typename T>

@@ -7,6 +7,7 @@
 #include "../../include/photon_gpu.h"
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -24,6 +25,7 @@ std::unique_ptr<Geometry> make_geometry(const BvhBuildInput& in)
 {
 	require_device();
 	auto g = std::make_unique<Geometry>();
+	g->device = current_device();
 	WideBvh bvh = build_wide_bvh(in);
 	g->stats = bvh.stats;
 	g->nodes.resize(bvh.nodes.size());
@@ -145,13 +147,26 @@ __global__ void count_kernel(const WideNode* __restrict__ nodes, const LeafTri* 
 	}
 }
 
-// Persistent grid: as many blocks as stay resident on the device at once.
+// Persistent grid: as many blocks as stay resident on the current device at once, computed once
+// per (kernel, device).
 template<class Kernel>
 int persistent_grid(Kernel kernel)
 {
+	static std::mutex mutex;
+	static std::map<std::pair<const void*, int>, int> cache;
+	const int dev = current_device();
+	const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+	std::lock_guard<std::mutex> lock(mutex);
+	const auto it = cache.find(key);
+	if(it != cache.end())
+	{
+		return it->second;
+	}
 	int per_sm = 0;
 	PG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTraceBlock, 0));
-	return std::max(1, per_sm) * sm_count();
+	const int grid = std::max(1, per_sm) * sm_count();
+	cache.emplace(key, grid);
+	return grid;
 }
 
 uint32_t checked_ray_count(uint64_t n)
@@ -170,6 +185,7 @@ std::shared_ptr<Geometry> get_geometry(uint64_t id)
 	{
 		throw Error(PG_ERR_NOT_FOUND, "unknown geometry id " + std::to_string(id));
 	}
+	require_same_device(g->device, ("geometry " + std::to_string(id)).c_str());
 	return g;
 }
 
@@ -360,12 +376,12 @@ void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4*
 {
 	if(count)
 	{
-		static const int grid = persistent_grid(extend_kernel<true>);
+		const int grid = persistent_grid(extend_kernel<true>);
 		extend_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits);
 	}
 	else
 	{
-		static const int grid = persistent_grid(extend_kernel<false>);
+		const int grid = persistent_grid(extend_kernel<false>);
 		extend_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits);
 	}
 	PG_CUDA_CHECK(cudaGetLastError());
@@ -377,13 +393,13 @@ void launch_trace(const DeviceScene& s, RenderCounters* counters, const float4* 
 {
 	if(count)
 	{
-		static const int grid = persistent_grid(trace_kernel<true>);
+		const int grid = persistent_grid(trace_kernel<true>);
 		trace_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
 		                                                 prev.o, prev.d, prev.c, prev.r, rad_cur, film);
 	}
 	else
 	{
-		static const int grid = persistent_grid(trace_kernel<false>);
+		const int grid = persistent_grid(trace_kernel<false>);
 		trace_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
 		                                                  prev.o, prev.d, prev.c, prev.r, rad_cur, film);
 	}
@@ -395,13 +411,13 @@ void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQ
 {
 	if(count)
 	{
-		static const int grid = persistent_grid(shadow_kernel<true>);
+		const int grid = persistent_grid(shadow_kernel<true>);
 		shadow_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, q.t, q.r,
 		                                                  rad_next, film, train_dirw);
 	}
 	else
 	{
-		static const int grid = persistent_grid(shadow_kernel<false>);
+		const int grid = persistent_grid(shadow_kernel<false>);
 		shadow_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, q.t, q.r,
 		                                                   rad_next, film, train_dirw);
 	}
@@ -414,7 +430,7 @@ void launch_trace_closest(const Geometry& g, const float* d_rays, uint64_t n, vo
 	{
 		return;
 	}
-	static const int grid = persistent_grid(trace_closest_kernel);
+	const int grid = persistent_grid(trace_closest_kernel);
 	PG_CUDA_CHECK(cudaMemsetAsync(g.fetch.get(), 0, sizeof(uint32_t), s));
 	trace_closest_kernel<<<grid, kTraceBlock, 0, s>>>(
 		g.nodes.get(), g.tris.get(), reinterpret_cast<const float4*>(d_rays), checked_ray_count(n),
@@ -428,7 +444,7 @@ void launch_trace_any(const Geometry& g, const float* d_rays, uint64_t n, int32_
 	{
 		return;
 	}
-	static const int grid = persistent_grid(trace_any_kernel);
+	const int grid = persistent_grid(trace_any_kernel);
 	PG_CUDA_CHECK(cudaMemsetAsync(g.fetch.get(), 0, sizeof(uint32_t), s));
 	trace_any_kernel<<<grid, kTraceBlock, 0, s>>>(
 		g.nodes.get(), g.tris.get(), reinterpret_cast<const float4*>(d_rays), checked_ray_count(n),

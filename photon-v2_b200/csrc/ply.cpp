@@ -265,6 +265,11 @@ PlyMesh read_ply(const std::string& path)
 	long double min_bytes = 0.0L;
 	for(const Element& e : elements)
 	{
+		if(e.props.empty() && e.count > 0)
+		{
+			// rows of no bytes: the count would drive a loop that reads nothing
+			throw std::runtime_error("PLY: element '" + e.name + "' has rows but no properties");
+		}
 		uint64_t row = 0;
 		for(const Property& p : e.props)
 		{

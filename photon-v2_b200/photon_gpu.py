@@ -62,6 +62,8 @@ PGPU_SIGNATURES = [
     ("pgpu_scene_set_filter", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32]),
     ("pgpu_scene_set_dome_pdf", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32]),
     ("pgpu_scene_launches", ctypes.c_int, [ctypes.c_uint64, _u64p]),
+    ("pgpu_scene_light_pmf", ctypes.c_int, [ctypes.c_uint64, _f32p, _dblp, _u32p]),
+    ("pgpu_scene_light_pdf", ctypes.c_int, [ctypes.c_uint64, _f32p, _u32p, ctypes.c_uint64, _f32p]),
     ("pgpu_scenes_render", ctypes.c_int,
      [_u64p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32, _f32p]),
     ("pgpu_scene_count", ctypes.c_int,
@@ -336,6 +338,29 @@ class RenderScene:
         _check(load().pgpu_scene_profile(self.id, spp, max_bounces, estimator, seed, _ptr(ms, ctypes.c_double)))
         keys = ["prepare_ms", "regen_ms", "extend_ms", "shade_ms", "shadow_ms", "guide_infer_ms", "guide_train_ms"]
         return dict(zip(keys, ms.tolist()))
+
+    def light_pmf(self):
+        """(pmf float32 [E], alias-table pmf float64 [E]) of the scene's emitters (pgpu_scene_light_pmf)."""
+        lib = load()
+        n = ctypes.c_uint32(0)
+        _check(lib.pgpu_scene_light_pmf(self.id, None, None, ctypes.byref(n)))
+        pmf = np.zeros(n.value, np.float32)
+        alias = np.zeros(n.value, np.float64)
+        if n.value:
+            _check(lib.pgpu_scene_light_pmf(self.id, _ptr(pmf, ctypes.c_float), _ptr(alias, ctypes.c_double),
+                                            ctypes.byref(n)))
+        return pmf, alias
+
+    def light_pdf(self, targets: np.ndarray, points: np.ndarray, prims: np.ndarray) -> np.ndarray:
+        """NEE solid-angle densities for receiving points, light points and light-triangle indices
+        (pgpu_scene_light_pdf)."""
+        q = np.ascontiguousarray(np.concatenate([np.asarray(targets, np.float32).reshape(-1, 3),
+                                                 np.asarray(points, np.float32).reshape(-1, 3)], axis=1))
+        pr = np.ascontiguousarray(prims, np.uint32)
+        out = np.zeros(q.shape[0], np.float32)
+        _check(load().pgpu_scene_light_pdf(self.id, _ptr(q, ctypes.c_float), _ptr(pr, ctypes.c_uint32), q.shape[0],
+                                           _ptr(out, ctypes.c_float)))
+        return out
 
     def launches(self) -> int:
         """Kernels launched by the last render (pgpu_scene_launches)."""

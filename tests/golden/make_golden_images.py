@@ -1,6 +1,6 @@
 """Reference renders for the image-parity tests, made by the reference CPU renderer itself.
 
-Run in the build container after building the oracle (``make -f oracle/Makefile.ref -j8``):
+Run in the build container after building the oracle (``make -f oracle/Makefile.ref REF=<reference sources> -j8``):
 
     python tests/golden/make_golden_images.py [workload ...]
 
@@ -9,8 +9,8 @@ With workload names given, only those are re-rendered and the rest of images.npz
 For each workload below the scene is generated by photon-v2_b200/scenes.py, written as SDL, and
 rendered with oracle/_ref/ph_ref_render (phLoadCommands -> phUpdate -> phRender ->
 phAquireFrameRaw). The developed frames go to images.npz (float32 [H, W, 3], row 0 = bottom)
-together with the spp and bounce cap used. Every workload is small (64 x 64) and rendered with
-many samples so that its own noise stays well below the parity bar.
+together with the spp and bounce cap used. Every workload is small (32 x 32 to 128 x 128) and rendered
+with many samples so that its own noise stays well below the parity bar.
 """
 
 import os
@@ -55,6 +55,15 @@ WORKLOADS = {
                                         "empirical"),
     "ggx_sphere_bneept_manual": (lambda spp: scenes.ggx_sphere(level=3, width=64, height=64, spp=spp,
                                                                max_bounces=10), 4096, 10, "manual"),
+    # the benchmarked configurations' geometry at reduced resolution:
+    # the 1M-triangle GGX scene (1,310,726 triangles, 2 quad lights + environment, depth 10) at
+    # 128 x 128 and 65,536 spp -- the converged reference its parity and error are stated against
+    "c2_ggx1m_bneept": (lambda spp: scenes.ggx_sphere(level=8, width=128, height=128, spp=spp,
+                                                      max_bounces=10), 65536, 10),
+    # the slit-light room, full 2M triangles with its dielectric boxes, 32 x 32
+    "slit_room_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10), 65536, 10),
+    # a 40 x 40-block tile of the many-light city (174,802 triangles) with 1,000 lights, depth 12
+    "city_tile_bneept": (lambda spp: scenes.city(64, 64, spp, 12, blocks=40, num_lights=1000), 16384, 12),
 }
 
 
@@ -76,7 +85,7 @@ def render(scene: scenes.Scene, max_bounces: int, threads: int, refine_mode: str
 
 def main() -> None:
     if not os.path.exists(RENDER_TOOL):
-        raise SystemExit(f"{RENDER_TOOL} missing: run `make -f oracle/Makefile.ref -j8` first")
+        raise SystemExit(f"{RENDER_TOOL} missing: run `make -f oracle/Makefile.ref REF=<reference sources> -j8` first")
     threads = os.cpu_count() or 1
     path = os.path.join(HERE, "images.npz")
     only = sys.argv[1:]

@@ -261,6 +261,9 @@ _PLY_FACE = b"element face 1\nproperty list uchar int vertex_indices\n"
      + b"end_header\n" + np.zeros(9, "<f4").tobytes(), "truncated body"),
     (b"ply\nformat ascii 1.0\nelement vertex 3\n" + _PLY_XYZ + _PLY_FACE.replace(b"face 1", b"face 400000000000")
      + b"end_header\n0 0 0\n1 0 0\n0 1 0\n3 0 1 2\n", "truncated body"),
+    # an element with a huge count and no properties: rows of zero bytes would loop without reading
+    (b"ply\nformat ascii 1.0\nelement junk 18446744073709551615\nelement vertex 3\n" + _PLY_XYZ + _PLY_FACE
+     + b"end_header\n0 0 0\n1 0 0\n0 1 0\n3 0 1 2\n", "has rows but no properties"),
 ])
 def test_ply_malformed_files_are_reported(content, message, tmp_path):
     (tmp_path / "g0.ply").write_bytes(content)
