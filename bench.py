@@ -285,6 +285,41 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 4
     }
 
 
+def c2_error(spp: int = 256) -> dict:
+    """The error the benchmarked render carries: the 1M-triangle GGX scene at `spp` through the
+    Photon C API at 128 x 128, against the reference CPU renderer's 65,536-spp render of the same
+    scene (tests/golden/images.npz, made by tests/golden/make_golden_images.py). relMSE falls as
+    1/spp, which gives the spp that reaches 1e-3."""
+    import photon_gpu
+
+    path = os.path.join(ROOT, "tests", "golden", "images.npz")
+    if not os.path.exists(path):
+        return {"unavailable": "tests/golden/images.npz missing"}
+    d = np.load(path)
+    if "c2_ggx1m_bneept" not in d:
+        return {"unavailable": "no 65,536-spp reference render of the scene in images.npz"}
+    ref = d["c2_ggx1m_bneept"]
+    scene = scenes.ggx_sphere(level=8, width=128, height=128, spp=spp, max_bounces=10)
+    with tempfile.TemporaryDirectory() as tmp:
+        p2 = os.path.join(tmp, "scene.p2")
+        with open(p2, "w") as f:
+            f.write(scenes.to_sdl(scene, mesh_format="ply"))
+        scenes.write_meshes(scene, tmp)
+        scenes.write_env(scene, tmp)
+        with photon_gpu.PhotonEngine() as eng:
+            eng.set_working_directory(tmp)
+            assert eng.load_file(p2), eng.errors()
+            eng.set_max_bounces(scene.max_bounces)
+            eng.set_seed(11)
+            eng.update()
+            eng.render()
+            img = eng.frame()
+    err = rel_mse(img, ref)
+    return {"spp": spp, "relmse": err, "spp_for_relmse_1e-3": int(np.ceil(spp * err / 1e-3)),
+            "reference": f"reference CPU renderer, {int(d['c2_ggx1m_bneept__spp'])} spp", "resolution": "128x128",
+            "mean_ratio": (img.mean(axis=(0, 1)) / ref.mean(axis=(0, 1))).tolist(), "eps": 1e-2}
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -380,6 +415,8 @@ def run_ours(args) -> None:
         eng.set_seed(1000003 * rank + 7)
         eng.update()
         update_s = eng.info()["update_seconds"]
+        # launch shapes picked for this scene by the autotuner (untimed calibration renders)
+        tuned = eng.autotune(rebuild=True) if args.autotune else None
 
         for _ in range(args.warmup):
             eng.clear_film()
@@ -440,7 +477,8 @@ def run_ours(args) -> None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
         "config": {"workload": args.workload, "width": scene.width, "height": scene.height, "spp": scene.spp,
                    "max_bounces": scene.max_bounces, "triangles": scene.num_tris, "estimator": "bneept",
-                   "l2": "256 MiB write between timed steps", "parallelism": f"replicas x{world}"},
+                   "l2": "256 MiB write between timed steps", "parallelism": f"replicas x{world}",
+                   "tuned": tuned},
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
                 "path": "phRender + phAquireFrameRaw + phGetFrameRgbData (scene resident after phUpdate)"},
         "gpu_launches": launches,
@@ -455,6 +493,8 @@ def run_ours(args) -> None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as tmp:
             line["cpu_baseline"] = cpu_sample(scene, tmp, target_seconds=args.cpu_seconds)[-1]
+    if rank == 0 and world == 1 and args.workload == "ggx_1m":
+        line["error_vs_65536spp"] = c2_error(scene.spp)
     if rank == 0 and world == 1 and not args.no_guided:
         line["guided_equal_time"] = guided_equal_time()
     if rank == 0:
@@ -498,6 +538,12 @@ def run_flat(args) -> None:
     t0 = time.time()
     rss = [photon_gpu.RenderScene(sc, builder=args.builder) for sc in scene_list]
     build_s = time.time() - t0
+    tuned = None
+    if args.autotune:
+        # launch shapes per scene (untimed calibration renders; the leaf-size rebuild only for
+        # single-scene workloads)
+        tuned = [rs.autotune(sc.spp, max_bounces=sc.max_bounces, rebuild=len(rss) == 1)
+                 for sc, rs in zip(scene_list, rss)]
     paths_per_step = sum(sc.width * sc.height * sc.spp for sc in scene_list)
     l2_flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > 126 MB L2
     seed = 1000003 * rank + 7
@@ -575,7 +621,12 @@ def run_flat(args) -> None:
                    "spp": spps if len(spps) <= 4 else [spps[0], spps[-1]],
                    "max_bounces": scene_list[0].max_bounces, "estimator": "bneept", "bvh": args.builder,
                    "concurrency": args.concurrency if len(scene_list) > 1 else 1,
-                   "l2": "256 MiB write between timed steps", "parallelism": f"replicas x{world}"},
+                   "l2": "256 MiB write between timed steps", "parallelism": f"replicas x{world}",
+                   "tuned": (tuned[0] if tuned and len(tuned) == 1 else
+                             {"scenes": len(tuned), "ms_default": sum(t["ms_default"] for t in tuned),
+                              "ms_tuned": sum(t["ms_tuned"] for t in tuned),
+                              "shapes": sorted({(t["capacity"], t["refill"], t["blocks_per_sm"], t["leaf_tris"])
+                                                for t in tuned})} if tuned else None)},
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
                 "path": "pgpu_scene_render + pgpu_scene_film (frame developed on the GPU, copied to host)"},
         "gpu_launches": launches,
@@ -627,6 +678,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-guided", action="store_true", help="skip the guided-vs-plain equal-time comparison")
     ap.add_argument("--builder", default="sah", choices=["sah", "gpu"], help="BVH builder of flat workloads")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="render with the fixed default launch shapes instead of autotuned ones")
     ap.add_argument("--concurrency", type=int, default=4,
                     help="scenes of a multi-scene workload rendered at once (1: one after another)")
     args = ap.parse_args()

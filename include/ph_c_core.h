@@ -145,6 +145,15 @@ extern PH_API PhUInt64 phGpuGetLaunchCount(PhUInt64 engineId);
 extern PH_API void phGpuProfileRender(PhUInt64 engineId, PhUInt32 mode, PhUInt32 samplesPerPixel,
                                       PhFloat64* out_stats);
 
+/* Picks the launch shapes of the updated scene for the session's samples per pixel, estimator and
+ * bounce cap (pgpu_scene_autotune in photon_gpu.h: path-pool depth, traversal refill threshold,
+ * blocks per SM, and with flags bit 0 the BVH leaf size; bit 1 ignores the cache). cachePath (may
+ * be NULL) keeps choices across sessions. outConfig [4] and outMs [4] as in pgpu_scene_autotune
+ * (either may be NULL). PH_FALSE when no scene is updated or the calibration fails (the error
+ * text goes to phGpuGetErrors). */
+extern PH_API PhBool phGpuAutotune(PhUInt64 engineId, const PhChar* cachePath, PhUInt32 flags,
+                                   PhUInt32* outConfig, PhFloat32* outMs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -188,6 +188,16 @@ PGPU_API int pgpu_scene_set_dome_pdf(uint64_t id, uint32_t mode);
 PGPU_API int pgpu_scene_profile(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator,
                        uint64_t seed, double* out_kernel_ms);
 PGPU_API int pgpu_scene_clear(uint64_t id);
+/* Renders several scenes as ONE wavefront: one pool of paths in flight, one launch of every kernel
+ * per iteration for all the scenes (each queue entry carries its scene), the iterations captured
+ * as CUDA graphs. Scene i renders spp[i] more samples into its film, exactly the paths its own
+ * pgpu_scene_render with the same seed would trace. Replaces the reference's scene-by-scene
+ * EqualSamplingRenderer::doRender (Engine/Source/Core/Renderer/Sampling/
+ * EqualSamplingRenderer.cpp:119-203), one renderer per engine. Every film must use the box filter
+ * and every scene live on the current device; guiding is not applied. The scenes are rendered in
+ * renders of at most 2^31 paths each. *out_ms: device milliseconds of the whole batch. */
+PGPU_API int pgpu_scenes_render_wavefront(const uint64_t* ids, uint32_t n, const uint32_t* spp, uint32_t max_bounces,
+                                          uint32_t estimator, uint64_t seed, float* out_ms);
 /* Renders several scenes at once: scene ids[i] gets spp[i] more samples (numbered after its
  * earlier ones) with the same bounce cap, estimator and seed. Up to `concurrency` host threads
  * render one scene each at a time on the scene's own stream, so small scenes fill the GPU
@@ -213,6 +223,28 @@ PGPU_API int pgpu_scene_light_pmf(uint64_t id, float* out_pmf, double* out_alias
  * light triangle's index in the scene's input order; out_pdf_w [n]. */
 PGPU_API int pgpu_scene_light_pdf(uint64_t id, const float* queries, const uint32_t* prims, uint64_t n,
                                   float* out_pdf_w);
+/* Launch-shape autotuner. No counterpart in the reference, whose EqualSamplingRenderer fixes its
+ * scheduler and tile choice up front (Engine/Source/Core/Renderer/Sampling/
+ * EqualSamplingRenderer.cpp:45-60,94-108); here the knobs are launch shapes. Picks, by coordinate
+ * descent over calibration renders of the scene (spp samples at most, ~16M paths, into a scratch
+ * film; estimator and bounce cap as given), the path-pool depth (queue depth), the traversal
+ * refill threshold, the grid of the grid-stride kernels (blocks per SM) and, with
+ * PG_AUTOTUNE_REBUILD, the BVH leaf size (the tree is rebuilt for each candidate). A candidate
+ * wins only when more than 1 % faster. The choice stays with the scene for later renders.
+ * cache_path (may be NULL): a text file of "fingerprint capacity refill blocks leaf" lines; a scene
+ * whose fingerprint (triangles, resolution, emitters, material kinds, estimator, bounces, filter,
+ * builder) is listed takes that line without calibrating (unless PG_AUTOTUNE_IGNORE_CACHE), and a
+ * new choice is appended. out_config [4] (may be NULL): capacity, refill, blocks per SM, leaf
+ * triangles. out_ms [4] (may be NULL): calibration device ms with the defaults, with the choice,
+ * renders run, 1 if taken from the cache. */
+#define PG_AUTOTUNE_REBUILD 1u
+#define PG_AUTOTUNE_IGNORE_CACHE 2u
+PGPU_API int pgpu_scene_autotune(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator, uint32_t flags,
+                                 const char* cache_path, uint32_t* out_config, float* out_ms);
+/* Sets / reads the launch shapes [4] = capacity (1024..2^24 path slots), refill (1..32 idle
+ * lanes), blocks per SM (1..64), leaf triangles (1..3; a different value rebuilds the BVH). */
+PGPU_API int pgpu_scene_set_launch(uint64_t id, const uint32_t* config);
+PGPU_API int pgpu_scene_get_launch(uint64_t id, uint32_t* out_config);
 /* Kernels the scene's last render launched (all iterations, including the empty ones that end the
  * last CUDA-graph batch). */
 PGPU_API int pgpu_scene_launches(uint64_t id, uint64_t* out_launches);

@@ -62,13 +62,14 @@ struct BinNode
 };
 
 constexpr int kBins = 32;
-constexpr uint32_t kMaxLeafTris = 3;
+constexpr uint32_t kMaxLeafTris = 3;   // the node layout's limit (unary leaf counts of 1..3)
 constexpr std::size_t kParallelThreshold = 1u << 15;
 
 struct BinaryBuilder
 {
 	const Box*            prim_boxes;
 	const float*          centroids;      // [n][3]
+	uint32_t              max_leaf = kMaxLeafTris;
 	std::vector<uint32_t> indices;
 	std::vector<BinNode>  nodes;
 	std::atomic<int32_t>  next_node{0};
@@ -104,7 +105,7 @@ struct BinaryBuilder
 		note_depth(depth);
 
 		const uint32_t n = end - begin;
-		if(n <= kMaxLeafTris)
+		if(n <= max_leaf)
 		{
 			return;
 		}
@@ -524,7 +525,12 @@ WideBvh build_wide_bvh(const BvhBuildInput& in)
 		}
 	}
 
+	if(in.max_leaf_tris < 1 || in.max_leaf_tris > kMaxLeafTris)
+	{
+		throw std::runtime_error("build_wide_bvh: max_leaf_tris must be 1, 2 or 3");
+	}
 	BinaryBuilder bb;
+	bb.max_leaf = in.max_leaf_tris;
 	bb.prim_boxes = boxes.data();
 	bb.centroids = centroids.data();
 	bb.indices.resize(n);

@@ -25,6 +25,9 @@ struct BvhBuildInput
 	// Largest coordinate magnitude any ray origin will have (camera included); used to size the
 	// conservative padding of child boxes so that FP32 slab-test rounding never loses a hit.
 	float           max_origin_abs;
+	// Binned-SAH builder: a node with at most this many triangles becomes a leaf (1..3, the node
+	// layout's limit). Fewer triangles per leaf: more nodes, fewer triangle tests per ray.
+	uint32_t        max_leaf_tris = 3;
 };
 
 struct BvhBuildStats

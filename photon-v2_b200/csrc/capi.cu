@@ -29,7 +29,6 @@ struct EngineSlot
 {
 	Engine engine;
 	std::string error_copy;
-	std::atomic<bool> region_pending{false};   // set by phRender, consumed by a polling thread
 };
 
 Registry<EngineSlot>& engines() { static Registry<EngineSlot> r; return r; }
@@ -121,7 +120,6 @@ void phRender(PhUInt64 engineId)
 	if(auto e = engines().get(engineId))
 	{
 		e->engine.render();
-		e->region_pending = true;
 	}
 }
 
@@ -380,33 +378,65 @@ void phAsyncGetRenderState(PhUInt64 engineId, struct PHRenderState* out_state)
 	}
 }
 
+namespace
+{
+
+PhFrameRegionInfo to_region_info(const Engine::RegionUpdate& r)
+{
+	return PhFrameRegionInfo{r.x, r.y, r.w, r.h,
+	                         r.finished ? PH_FRAME_REGION_STATUS_FINISHED : PH_FRAME_REGION_STATUS_UPDATING};
+}
+
+}// end anonymous namespace
+
 PhBool phAsyncPollUpdatedFrameRegion(PhUInt64 engineId, PhFrameRegionInfo* out_regionInfo)
 {
 	auto e = engines().get(engineId);
-	if(!e || !out_regionInfo || !e->region_pending.exchange(false))
+	if(!e || !out_regionInfo)
 	{
 		return PH_FALSE;
 	}
-	uint32_t w = 0, h = 0;
-	e->engine.get_render_dimension(&w, &h);
-	*out_regionInfo = PhFrameRegionInfo{0, 0, w, h, PH_FRAME_REGION_STATUS_FINISHED};
+	Engine::RegionUpdate r{};
+	if(e->engine.poll_regions(&r, 1) == 0)
+	{
+		return PH_FALSE;
+	}
+	*out_regionInfo = to_region_info(r);
 	return PH_TRUE;
 }
 
 PhSize phAsyncPollUpdatedFrameRegions(PhUInt64 engineId, PhUInt64 /*bufferId*/, PhFrameRegionInfo* out_regionInfos,
                                       PhSize maxRegionInfos)
 {
-	if(maxRegionInfos == 0 || !out_regionInfos)
+	auto e = engines().get(engineId);
+	if(!e || maxRegionInfos == 0 || !out_regionInfos)
 	{
 		return 0;
 	}
-	return phAsyncPollUpdatedFrameRegion(engineId, out_regionInfos) ? 1 : 0;
+	std::vector<Engine::RegionUpdate> regions(std::min<PhSize>(maxRegionInfos, Engine::kMaxQueuedRegions + 1));
+	const std::size_t n = e->engine.poll_regions(regions.data(), regions.size());
+	for(std::size_t i = 0; i < n; ++i)
+	{
+		out_regionInfos[i] = to_region_info(regions[i]);
+	}
+	return n;
 }
 
-PhSize phAsyncPollMergedUpdatedFrameRegions(PhUInt64 engineId, PhUInt64 bufferId, PhSize /*mergeSize*/,
+PhSize phAsyncPollMergedUpdatedFrameRegions(PhUInt64 engineId, PhUInt64 /*bufferId*/, PhSize /*mergeSize*/,
                                             PhFrameRegionInfo* out_regionInfos, PhSize maxRegionInfos)
 {
-	return phAsyncPollUpdatedFrameRegions(engineId, bufferId, out_regionInfos, maxRegionInfos);
+	auto e = engines().get(engineId);
+	if(!e || maxRegionInfos == 0 || !out_regionInfos)
+	{
+		return 0;
+	}
+	Engine::RegionUpdate r{};
+	if(e->engine.poll_merged_regions(&r, 1) == 0)
+	{
+		return 0;
+	}
+	out_regionInfos[0] = to_region_info(r);
+	return 1;
 }
 
 void phAsyncPeekFrame(PhUInt64 engineId, PhUInt64 layerIndex, PhUInt32 xPx, PhUInt32 yPx,
@@ -551,6 +581,40 @@ void phGpuProfileRender(PhUInt64 engineId, PhUInt32 mode, PhUInt32 samplesPerPix
 	catch(const std::exception& ex)
 	{
 		log_error("phGpuProfileRender", ex);
+	}
+}
+
+PhBool phGpuAutotune(PhUInt64 engineId, const PhChar* cachePath, PhUInt32 flags, PhUInt32* outConfig,
+                     PhFloat32* outMs)
+{
+	auto e = engines().get(engineId);
+	if(!e)
+	{
+		return PH_FALSE;
+	}
+	try
+	{
+		const AutotuneResult a = e->engine.autotune(cachePath, flags);
+		if(outConfig)
+		{
+			outConfig[0] = a.config.capacity;
+			outConfig[1] = a.config.refill;
+			outConfig[2] = a.config.blocks_per_sm;
+			outConfig[3] = a.config.leaf_tris;
+		}
+		if(outMs)
+		{
+			outMs[0] = a.ms_default;
+			outMs[1] = a.ms_tuned;
+			outMs[2] = static_cast<float>(a.trials);
+			outMs[3] = a.from_cache ? 1.0f : 0.0f;
+		}
+		return PH_TRUE;
+	}
+	catch(const std::exception& ex)
+	{
+		e->engine.report_error(std::string("autotune failed: ") + ex.what());
+		return PH_FALSE;
 	}
 }
 

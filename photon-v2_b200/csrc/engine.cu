@@ -842,6 +842,25 @@ void Engine::render()
 		m_info = RenderInfo{0.0, 0, 0, 0, m_info.update_seconds, m_info.num_triangles};
 		m_launches = 0;
 		uint32_t done = 0;
+		// progress points: a preview of the finished samples, an UPDATING region, the statistics
+		begin_preview(*m_render);
+		RenderProgress progress;
+		progress.mutex = &m_render->frame_mutex;
+		progress.preview_rgb = m_render->preview.get();
+		progress.published = [&](unsigned long long finished, unsigned long long)
+		{
+			const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+			const double paths = static_cast<double>(wh) * done + static_cast<double>(finished);
+			m_work_done = done + static_cast<uint64_t>(finished / wh);
+			m_elapsed_ms = static_cast<uint64_t>(secs * 1000.0);
+			m_samples_per_second = secs > 0.0 ? static_cast<float>(paths / secs) : 0.0f;
+			push_region(false);
+		};
+		struct PreviewEnd
+		{
+			RenderObject& r;
+			~PreviewEnd() { end_preview(r); }
+		} preview_end{*m_render};
 		while(done < m_spp)
 		{
 			const uint32_t n = std::min(chunk, m_spp - done);
@@ -857,6 +876,7 @@ void Engine::render()
 			p.refine_iters = m_refine.refine_iters;
 			p.seed = m_seed;
 			p.first_sample = m_first_sample + m_render->samples;
+			p.progress = &progress;
 			const float ms = m_render->scene->render(p, m_render->film.get());
 			m_render->samples += n;
 			m_info.device_ms += ms;
@@ -875,6 +895,41 @@ void Engine::render()
 	{
 		record_error(std::string("render failed: ") + e.what());
 	}
+	push_region(true);
+}
+
+void Engine::push_region(bool finished)
+{
+	std::lock_guard<std::mutex> lock(m_region_mutex);
+	if(!finished && m_regions.size() >= kMaxQueuedRegions)
+	{
+		return;
+	}
+	m_regions.push_back(RegionUpdate{0u, 0u, m_width, m_height, finished});
+}
+
+std::size_t Engine::poll_regions(RegionUpdate* out, std::size_t max)
+{
+	std::lock_guard<std::mutex> lock(m_region_mutex);
+	std::size_t n = 0;
+	while(n < max && !m_regions.empty())
+	{
+		out[n++] = m_regions.front();
+		m_regions.pop_front();
+	}
+	return n;
+}
+
+std::size_t Engine::poll_merged_regions(RegionUpdate* out, std::size_t max)
+{
+	std::lock_guard<std::mutex> lock(m_region_mutex);
+	if(max == 0 || m_regions.empty())
+	{
+		return 0;
+	}
+	out[0] = m_regions.back();
+	m_regions.clear();
+	return 1;
 }
 
 void Engine::profile(uint32_t mode, uint32_t spp, double out_stats[14])
@@ -907,6 +962,26 @@ void Engine::profile(uint32_t mode, uint32_t spp, double out_stats[14])
 	out_stats[8] = static_cast<double>(rs.last_shadow_rays());
 	out_stats[9] = static_cast<double>(rs.last_iterations());
 	for(int k = 0; k < 4; ++k) { out_stats[10 + k] = static_cast<double>(rs.last_counts()[k]); }
+}
+
+AutotuneResult Engine::autotune(const char* cache_path, uint32_t flags)
+{
+	if(!m_render)
+	{
+		throw std::runtime_error("autotune: the scene was not updated successfully");
+	}
+	RenderParams p;
+	p.width = m_width;
+	p.height = m_height;
+	p.spp = m_spp;
+	p.max_bounces = m_max_bounces;
+	p.estimator = m_estimator;
+	p.filter = m_render->filter;
+	p.refine_mode = m_refine.refine_mode;
+	p.refine_delta = m_refine.refine_delta;
+	p.refine_iters = m_refine.refine_iters;
+	p.seed = m_seed + 0x632BE59BD9B4E019ull;
+	return m_render->scene->autotune(p, (flags & 1u) != 0u, cache_path, (flags & 2u) != 0u);
 }
 
 void Engine::clear_film()

@@ -8,10 +8,12 @@
 #pragma once
 
 #include "film.cuh"
+#include "pg_render.h"
 #include "sdl.h"
 
 #include <atomic>
 #include <cstdint>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -88,6 +90,24 @@ public:
 	void get_progress(uint64_t* total, uint64_t* done, uint64_t* elapsed_ms) const;
 	void get_statistics(float* percentage, float* samples_per_second) const;
 
+	// A frame region whose developed pixels changed (phAsyncPollUpdatedFrameRegion(s)): while a
+	// render runs, the whole frame is reported UPDATING at every progress point (the film's
+	// estimate over the samples finished so far, which phAsyncPeekFrame returns); when the render
+	// completes, FINISHED. Every sample of a pass covers the whole frame, so regions are the whole
+	// frame. The queue keeps at most kMaxQueuedRegions: further UPDATING regions are dropped,
+	// FINISHED ones always kept (EqualSamplingRenderer::asyncAddUpdatedRegion,
+	// Engine/Source/Core/Renderer/Sampling/EqualSamplingRenderer.cpp:240-254).
+	struct RegionUpdate
+	{
+		uint32_t x, y, w, h;
+		bool finished;
+	};
+	static constexpr std::size_t kMaxQueuedRegions = 1024;
+	// Oldest first; returns the number written.
+	std::size_t poll_regions(RegionUpdate* out, std::size_t max);
+	// Everything queued, merged: at most one region (the frame), FINISHED if the last queued was.
+	std::size_t poll_merged_regions(RegionUpdate* out, std::size_t max);
+
 	// Extensions (ph_c_core.h, "GPU build extensions").
 	void set_max_ray_bounces(uint32_t n) { m_max_bounces = n; }
 	void set_seed(uint64_t seed) { m_seed = seed; }
@@ -106,12 +126,18 @@ public:
 	// Renders into a scratch film with the given render mode and returns the statistics of
 	// phGpuProfileRender.
 	void profile(uint32_t mode, uint32_t spp, double out_stats[14]);
+	// Launch-shape autotuning of the updated scene (RenderScene::autotune) at the session's spp,
+	// estimator and bounce cap.
+	AutotuneResult autotune(const char* cache_path, uint32_t flags);
 	std::string last_error() const;
+	// Adds a message to the errors phGpuGetErrors reports.
+	void report_error(const std::string& msg) { record_error(msg); }
 	void clear_film();
 
 private:
 	void handle(SdlCommand&& cmd);
 	void record_error(const std::string& msg);
+	void push_region(bool finished);
 
 	struct Resource
 	{
@@ -148,6 +174,8 @@ private:
 	std::atomic<float> m_samples_per_second{0.0f};
 	mutable std::mutex m_error_mutex;
 	std::string m_errors;
+	std::mutex m_region_mutex;
+	std::deque<RegionUpdate> m_regions;
 };
 
 bool write_pfm(const std::string& path, const HdrFrame& frame);

@@ -95,15 +95,38 @@ void develop_frame(const RenderObject& r, float* out_rgb, uint32_t x, uint32_t y
 	w = std::min(w, r.width - x);
 	h = std::min(h, r.height - y);
 	std::lock_guard<std::mutex> lock(r.frame_mutex);
-	r.frame.resize(static_cast<std::size_t>(pixels) * 3);
 	cudaStream_t st = library_stream();
-	develop_kernel<<<sm_count() * 4, 256, 0, st>>>(r.film.get(), r.frame.get(), pixels);
-	PG_CUDA_CHECK(cudaGetLastError());
+	const float* src = r.preview.get();
+	if(!r.preview_valid)
+	{
+		r.frame.resize(static_cast<std::size_t>(pixels) * 3);
+		develop_kernel<<<sm_count() * 4, 256, 0, st>>>(r.film.get(), r.frame.get(), pixels);
+		PG_CUDA_CHECK(cudaGetLastError());
+		src = r.frame.get();
+	}
 	const std::size_t pitch = static_cast<std::size_t>(r.width) * 3 * sizeof(float);
 	const std::size_t offset = (static_cast<std::size_t>(y) * r.width + x) * 3;
-	PG_CUDA_CHECK(cudaMemcpy2DAsync(out_rgb + offset, pitch, r.frame.get() + offset, pitch,
+	PG_CUDA_CHECK(cudaMemcpy2DAsync(out_rgb + offset, pitch, src + offset, pitch,
 	                                static_cast<std::size_t>(w) * 3 * sizeof(float), h, cudaMemcpyDeviceToHost, st));
 	PG_CUDA_CHECK(cudaStreamSynchronize(st));
+}
+
+void begin_preview(RenderObject& r)
+{
+	const uint32_t pixels = r.width * r.height;
+	std::lock_guard<std::mutex> lock(r.frame_mutex);
+	r.preview.resize(static_cast<std::size_t>(pixels) * 3);
+	cudaStream_t st = library_stream();
+	develop_kernel<<<sm_count() * 4, 256, 0, st>>>(r.film.get(), r.preview.get(), pixels);
+	PG_CUDA_CHECK(cudaGetLastError());
+	PG_CUDA_CHECK(cudaStreamSynchronize(st));
+	r.preview_valid = true;
+}
+
+void end_preview(RenderObject& r)
+{
+	std::lock_guard<std::mutex> lock(r.frame_mutex);
+	r.preview_valid = false;
 }
 
 void download_film(const RenderObject& r, double* out_sum)
@@ -274,6 +297,67 @@ int pgpu_scene_profile(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t
 	});
 }
 
+int pgpu_scenes_render_wavefront(const uint64_t* ids, uint32_t n, const uint32_t* spp, uint32_t max_bounces,
+                                 uint32_t estimator, uint64_t seed, float* out_ms)
+{
+	return guarded([&]
+	{
+		if(n == 0)
+		{
+			if(out_ms) { *out_ms = 0.0f; }
+			return;
+		}
+		if(!ids || !spp)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scenes_render_wavefront: null ids or spp");
+		}
+		if(estimator > PG_EST_BVPTDL)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scenes_render_wavefront: unknown estimator");
+		}
+		std::vector<std::shared_ptr<RenderObject>> objects;
+		std::vector<const RenderScene*> scenes;
+		std::vector<double*> films;
+		std::vector<uint32_t> counts;
+		std::vector<uint64_t> first;
+		for(uint32_t i = 0; i < n; ++i)
+		{
+			for(uint32_t k = 0; k < i; ++k)
+			{
+				if(ids[k] == ids[i])
+				{
+					throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scenes_render_wavefront: a scene appears twice");
+				}
+			}
+			objects.push_back(get_render(ids[i]));
+			RenderObject& r = *objects.back();
+			if(r.filter != PG_FILTER_BOX)
+			{
+				throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scenes_render_wavefront: every film must use the box filter");
+			}
+			if(spp[i] == 0)
+			{
+				throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scenes_render_wavefront: zero samples");
+			}
+			scenes.push_back(r.scene.get());
+			films.push_back(r.film.get());
+			counts.push_back(spp[i]);
+			first.push_back(r.samples);
+		}
+		RenderParams p;
+		p.max_bounces = max_bounces;
+		p.estimator = estimator;
+		p.seed = seed;
+		// the first scene's pool, stream and graphs run the wavefront of all of them
+		const float ms = objects[0]->scene->render_batch(scenes, films, counts, first, p);
+		for(uint32_t i = 0; i < n; ++i)
+		{
+			objects[i]->samples += spp[i];
+		}
+		if(out_ms) { *out_ms = ms; }
+	});
+}
+
 int pgpu_scenes_render(const uint64_t* ids, uint32_t n, const uint32_t* spp, uint32_t max_bounces,
                        uint32_t estimator, uint64_t seed, uint32_t concurrency, float* out_ms)
 {
@@ -388,6 +472,71 @@ int pgpu_scene_light_pdf(uint64_t id, const float* queries, const uint32_t* prim
 		}
 		auto r = get_render(id);
 		r->scene->light_pdf(queries, prims, n, out_pdf_w);
+	});
+}
+
+int pgpu_scene_autotune(uint64_t id, uint32_t spp, uint32_t max_bounces, uint32_t estimator, uint32_t flags,
+                        const char* cache_path, uint32_t* out_config, float* out_ms)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		if(estimator > PG_EST_BVPTDL || spp == 0)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_autotune: unknown estimator or zero samples");
+		}
+		RenderParams p;
+		p.width = r->width;
+		p.height = r->height;
+		p.spp = spp;
+		p.max_bounces = max_bounces;
+		p.estimator = estimator;
+		p.filter = r->filter;
+		const AutotuneResult a = r->scene->autotune(p, (flags & PG_AUTOTUNE_REBUILD) != 0u, cache_path,
+		                                            (flags & PG_AUTOTUNE_IGNORE_CACHE) != 0u);
+		if(out_config)
+		{
+			out_config[0] = a.config.capacity;
+			out_config[1] = a.config.refill;
+			out_config[2] = a.config.blocks_per_sm;
+			out_config[3] = a.config.leaf_tris;
+		}
+		if(out_ms)
+		{
+			out_ms[0] = a.ms_default;
+			out_ms[1] = a.ms_tuned;
+			out_ms[2] = static_cast<float>(a.trials);
+			out_ms[3] = a.from_cache ? 1.0f : 0.0f;
+		}
+	});
+}
+
+int pgpu_scene_set_launch(uint64_t id, const uint32_t* config)
+{
+	return guarded([&]
+	{
+		if(!config)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_set_launch: null config");
+		}
+		auto r = get_render(id);
+		r->scene->set_launch(LaunchConfig{config[0], config[1], config[2], config[3]});
+	});
+}
+
+int pgpu_scene_get_launch(uint64_t id, uint32_t* out_config)
+{
+	return guarded([&]
+	{
+		if(!out_config)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_get_launch: null config");
+		}
+		const LaunchConfig& c = get_render(id)->scene->launch();
+		out_config[0] = c.capacity;
+		out_config[1] = c.refill;
+		out_config[2] = c.blocks_per_sm;
+		out_config[3] = c.leaf_tris;
 	});
 }
 

@@ -17,7 +17,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <string>
 
 namespace cg = cooperative_groups;
 
@@ -181,6 +183,45 @@ splat_samples_kernel(FilmView film, uint64_t seed, uint64_t first_global, uint32
 	}
 }
 
+// Previews during a render: the continuing paths of the queue the next iteration starts from,
+// counted per pixel.
+__global__ void count_inflight_kernel(const uint32_t* __restrict__ path, const RenderCounters* __restrict__ c,
+                                      uint32_t wh, uint32_t* __restrict__ counts)
+{
+	const uint32_t n = c->n_next;
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		atomicAdd(&counts[path[i] % wh], 1u);
+	}
+}
+
+// The film's estimate over finished samples (HdrRgbFilm::developRegion, HdrRgbFilm.cpp:167-205,
+// on what the finished paths have deposited). The box film's W was raised by this render's spp
+// up front, so the samples of the render that have not finished -- not generated yet (path
+// indices from `generated` on; pixel = index mod wh) or still in flight -- come off it; the
+// 4 x 4 films only hold whole passes, whose W is exact.
+__global__ void develop_preview_kernel(const double* __restrict__ sums, const uint32_t* __restrict__ inflight,
+                                       uint32_t wh, uint32_t spp, unsigned long long generated, int box,
+                                       float* __restrict__ rgb)
+{
+	const unsigned long long full = generated / wh;
+	const uint32_t part = static_cast<uint32_t>(generated % wh);
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wh; i += gridDim.x * blockDim.x)
+	{
+		const double4 s = reinterpret_cast<const double4*>(sums)[i];
+		double w = s.w;
+		if(box)
+		{
+			const unsigned long long gen = full + (i < part ? 1ull : 0ull);
+			w -= static_cast<double>(spp) - static_cast<double>(gen) + static_cast<double>(inflight[i]);
+		}
+		const double rcp = w > 0.0 ? 1.0 / w : 0.0;
+		rgb[3 * static_cast<size_t>(i) + 0] = static_cast<float>(s.x * rcp);
+		rgb[3 * static_cast<size_t>(i) + 1] = static_cast<float>(s.y * rcp);
+		rgb[3 * static_cast<size_t>(i) + 2] = static_cast<float>(s.z * rcp);
+	}
+}
+
 // Box filter: every pixel received spp samples of weight 1.
 __global__ void box_weights_kernel(double* sums, uint32_t num_pixels, double spp)
 {
@@ -194,17 +235,30 @@ __global__ void box_weights_kernel(double* sums, uint32_t num_pixels, double spp
 // 1 + the material type of the hit surface, in the list of that class for this block's residue
 // (kClassLists). Lanes of one class share one atomic. `list_capacity` bounds the slots one list
 // can receive: the slots all blocks of one residue visit in the grid-stride loop.
+// MULTI: the hit triangle belongs to the scene in the top bits of the slot's meta word.
+template<bool MULTI>
 __global__ void __launch_bounds__(kShadeBlock)
-classify_kernel(DeviceScene s, RenderCounters* __restrict__ c, const uint2* __restrict__ hits,
-                uint32_t* __restrict__ order, uint32_t list_capacity)
+classify_kernel(DeviceScene s_single, RenderCounters* __restrict__ c, const uint2* __restrict__ hits,
+                uint32_t* __restrict__ order, uint32_t list_capacity, const uint32_t* __restrict__ meta, BatchView batch)
 {
 	const uint32_t n = c->n_total;
 	const uint32_t residue = blockIdx.x % kClassLists;
 	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		const uint32_t tri = hits[i].x;
-		const uint32_t cls = tri == 0xFFFFFFFFu ? 0u
-		                                        : min(1u + s.materials[__ldg(&s.tris[tri].material)].type, kShadeClasses - 1u);
+		uint32_t cls = 0u;
+		if(tri != 0xFFFFFFFFu)
+		{
+			if constexpr(MULTI)
+			{
+				const DeviceScene& s = batch.scenes[meta[i] >> kMetaSceneShift].scene;
+				cls = min(1u + s.materials[__ldg(&s.tris[tri].material)].type, kShadeClasses - 1u);
+			}
+			else
+			{
+				cls = min(1u + s_single.materials[__ldg(&s_single.tris[tri].material)].type, kShadeClasses - 1u);
+			}
+		}
 		const uint32_t list = cls * kClassLists + residue;
 		const cg::coalesced_group peers = cg::labeled_partition(cg::coalesced_threads(), cls);
 		uint32_t base = 0;
@@ -265,17 +319,48 @@ __global__ void prepare_kernel(RenderCounters* c, uint32_t capacity)
 
 // Camera rays of new paths into the tail of the current queue
 // (PinholeCamera::receiveRay, then BNEEPTEstimator.cpp:63-64: reversed, range [0, max]).
+// MULTI: new paths are numbered across the scenes of `batch` (scene k owns [path_first,
+// path_first + path_count)); each takes its scene's camera, film and sample numbering, and carries
+// its scene in the top bits of its meta word.
+template<bool MULTI>
 __global__ void __launch_bounds__(kShadeBlock)
-regen_kernel(const RenderCounters* __restrict__ c, Camera cam, FilmView film, uint64_t seed,
-             uint64_t first_global, PathBuffers cur)
+regen_kernel(const RenderCounters* __restrict__ c, Camera cam_single, FilmView film_single, uint64_t seed,
+             uint64_t first_global_single, PathBuffers cur, BatchView batch)
 {
 	const uint32_t active = c->n_active;
 	const uint32_t total = c->n_total;
 	const unsigned long long base = c->gen_base;
-	const uint32_t wh = cam.width * cam.height;
 	for(uint32_t i = active + blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
 	{
-		const uint32_t p = static_cast<uint32_t>(base + (i - active));
+		const unsigned long long pb = base + (i - active);
+		uint32_t sid = 0, p;
+		Camera cam;
+		FilmView film;
+		uint64_t first_global;
+		if constexpr(MULTI)
+		{
+			// the last scene whose first path is at or before pb
+			uint32_t lo = 0, hi = batch.count - 1u;
+			while(lo < hi)
+			{
+				const uint32_t mid = (lo + hi + 1u) >> 1;
+				if(batch.scenes[mid].path_first <= pb) { lo = mid; } else { hi = mid - 1u; }
+			}
+			sid = lo;
+			const BatchScene& bs = batch.scenes[sid];
+			p = static_cast<uint32_t>(pb - bs.path_first);
+			cam = bs.scene.cam;
+			film = bs.film;
+			first_global = bs.first_global;
+		}
+		else
+		{
+			p = static_cast<uint32_t>(pb);
+			cam = cam_single;
+			film = film_single;
+			first_global = first_global_single;
+		}
+		const uint32_t wh = cam.width * cam.height;
 		const uint32_t pixel = p % wh;
 		const PathRng rng = make_rng(seed, first_global + p);
 		const float2 raster = raster_position(film, pixel, rng);
@@ -292,7 +377,7 @@ regen_kernel(const RenderCounters* __restrict__ c, Camera cam, FilmView film, ui
 		const V3 d = -recv;
 
 		cur.path[i] = p;
-		cur.meta[i] = 0u;
+		cur.meta[i] = sid << kMetaSceneShift;
 		cur.thr[i] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
 		cur.rad[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 		cur.prev[i] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
@@ -408,18 +493,20 @@ struct ShadeArgs
 	RefineQueue   refine_queue;   // iterative refine mode: requests for refine_kernel
 	const uint32_t* order;        // slots listed per shading class (classify_kernel), or null: slot order
 	uint32_t      order_capacity; // slots per list of `order`
+	BatchView     batch;          // multi-scene renders: scene, film and numbering of every path
 };
 
 __device__ __forceinline__ float4 cur_gf0(const ShadeArgs& a, uint32_t i) { return a.cur.gf0[i]; }
 __device__ __forceinline__ float4 cur_gf1(const ShadeArgs& a, uint32_t i) { return a.cur.gf1[i]; }
 
 // GUIDED instantiates the learned-guiding paths; the plain estimator compiles without them.
-template<bool GUIDED>
+// MULTI: each path shades in the scene of its meta word's top bits (a.batch), into that scene's
+// film, and passes the scene on to its continuation and its NEE record.
+template<bool GUIDED, bool MULTI>
 __global__ void __launch_bounds__(kShadeBlock)
 shade_kernel(ShadeArgs a)
 {
 	const uint32_t total = a.counters->n_total;
-	const DeviceScene& s = a.scene;
 	// work item w -> queue slot: list by list (class-major) through the lists classify_kernel made
 	__shared__ uint32_t list_end[kOrderLists];
 	if(a.order && threadIdx.x == 0)
@@ -449,14 +536,19 @@ shade_kernel(ShadeArgs a)
 		const uint32_t p = a.cur.path[i];
 		const uint32_t meta = a.cur.meta[i];
 		const uint32_t bounce = meta & kMetaBounceMask;
+		const uint32_t sid = MULTI ? meta >> kMetaSceneShift : 0u;
+		const DeviceScene& s = MULTI ? a.batch.scenes[sid].scene : a.scene;
+		const FilmView& film = MULTI ? a.batch.scenes[sid].film : a.film;
+		const uint32_t width_height = MULTI ? a.batch.scenes[sid].width_height : a.width_height;
+		const uint64_t first_global = MULTI ? a.batch.scenes[sid].first_global : a.first_global;
 		const float4 thr4 = ld4(a.cur.thr + i);
 		const float4 rad4 = ld4(a.cur.rad + i);
 		const float4 prev4 = ld4(a.cur.prev + i);
 		const float4 ro = ld4(a.cur.ray_o + i);
 		const float4 rd = ld4(a.cur.ray_d + i);
 		const uint2 hit = a.hits[i];
-		const uint32_t pixel = p % a.width_height;
-		const PathRng rng = make_rng(a.seed, a.first_global + p);
+		const uint32_t pixel = p % width_height;
+		const PathRng rng = make_rng(a.seed, first_global + p);
 
 		const RGB thr_emit = RGB{thr4.x, thr4.y, thr4.z};
 		const float cont = thr4.w;
@@ -526,7 +618,7 @@ shade_kernel(ShadeArgs a)
 					radiance = radiance + le * safe_clamp(thr_emit, 0.0f, kClampMax);
 				}
 			}
-			splat(a.film, pixel, p, radiance);
+			splat(film, pixel, p, radiance);
 			continue;
 		}
 
@@ -544,7 +636,7 @@ shade_kernel(ShadeArgs a)
 		// traceNextSurface rejects hits whose sidedness disagrees (SurfaceTracer.h:126-141).
 		if(!(dot(ng, d) * dot(frame.ns, d) > 0.0f))
 		{
-			splat(a.film, pixel, p, radiance);
+			splat(film, pixel, p, radiance);
 			continue;
 		}
 
@@ -592,7 +684,7 @@ shade_kernel(ShadeArgs a)
 		// ---- does the path continue past this vertex?
 		if((meta & kMetaStopAfter) || bounce >= a.max_bounces)
 		{
-			splat(a.film, pixel, p, radiance);
+			splat(film, pixel, p, radiance);
 			continue;
 		}
 		const RGB throughput = thr_emit * cont;
@@ -807,7 +899,7 @@ shade_kernel(ShadeArgs a)
 				continues = false;
 			}
 			next_meta = (bounce + 1u) | (nee_samplable ? kMetaPrevNee : 0u) | (stop_after ? kMetaStopAfter : 0u) |
-			            (guided && a.guide.train_cap ? kMetaGuideRec : 0u);
+			            (guided && a.guide.train_cap ? kMetaGuideRec : 0u) | (sid << kMetaSceneShift);
 		}
 
 		uint32_t slot = 0;
@@ -842,7 +934,7 @@ shade_kernel(ShadeArgs a)
 		}
 		else
 		{
-			splat(a.film, pixel, p, radiance);
+			splat(film, pixel, p, radiance);
 		}
 
 		if(has_shadow)
@@ -852,11 +944,15 @@ shade_kernel(ShadeArgs a)
 			a.shadow.o[k] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_tmin);
 			a.shadow.d[k] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
 			a.shadow.c[k] = make_float4(sh_c.r, sh_c.g, sh_c.b, __uint_as_float(target));
+			if constexpr(MULTI)
+			{
+				a.shadow.sid[k] = sid;
+			}
 			if(GUIDED && a.shadow.t)
 			{
 				a.shadow.t[k] = make_float2(__uint_as_float(train_row), sh_train);
 			}
-			if(!continues && a.film.filter != PG_FILTER_BOX)
+			if(!continues && film.filter != PG_FILTER_BOX)
 			{
 				a.shadow.r[k] = make_float2(__uint_as_float(p), 0.0f);   // the path, for its sample slot
 			}
@@ -877,9 +973,10 @@ shade_kernel(ShadeArgs a)
 // slot is rewritten with the refined origin, unit direction and range (SurfaceHitRefinery::escape
 // / tryEscape, SurfaceHitRefinery.h:200-360). One-sided escapes come first in the grid-stride
 // order and mutual ones after them, so nearly every warp runs one loop.
+template<bool MULTI>
 __global__ void __launch_bounds__(kShadeBlock)
-refine_kernel(DeviceScene s, const RenderCounters* __restrict__ c, PathBuffers next, ShadowQueue shadow,
-              RefineQueue q, int iters)
+refine_kernel(DeviceScene s_single, const RenderCounters* __restrict__ c, PathBuffers next, ShadowQueue shadow,
+              RefineQueue q, int iters, BatchView batch)
 {
 	const uint32_t n_single = c->n_refine;
 	const uint32_t n = n_single + c->n_refine_mutual;
@@ -892,7 +989,11 @@ refine_kernel(DeviceScene s, const RenderCounters* __restrict__ c, PathBuffers n
 			float4* o = (r & 0x80000000u) ? shadow.o + k : next.ray_o + k;
 			float4* d = (r & 0x80000000u) ? shadow.d + k : next.ray_d + k;
 			const float4 o4 = *o, d4 = *d;
-			const TriVerts tri = load_tri(s.tris, __float_as_uint(o4.w), nullptr, nullptr);
+			// the scene of the ray: its path's (continuation) or its record's (NEE segment)
+			const LeafTri* tris = MULTI ? batch.scenes[(r & 0x80000000u) ? shadow.sid[k]
+			                                                        : next.meta[k] >> kMetaSceneShift].scene.tris
+			                            : s_single.tris;
+			const TriVerts tri = load_tri(tris, __float_as_uint(o4.w), nullptr, nullptr);
 			const EscapeRay e = escape_iterative(xyz(o4), face_normal(tri), tri, xyz(d4), iters);
 			*o = make_float4(e.origin.x, e.origin.y, e.origin.z, e.min_t);
 			*d = make_float4(e.unit_dir.x, e.unit_dir.y, e.unit_dir.z, e.max_distance);
@@ -901,8 +1002,9 @@ refine_kernel(DeviceScene s, const RenderCounters* __restrict__ c, PathBuffers n
 		{
 			const uint32_t k = q.mutual[i - n_single];
 			const float4 o4 = shadow.o[k], d4 = shadow.d[k];
-			const TriVerts tri = load_tri(s.tris, __float_as_uint(o4.w), nullptr, nullptr);
-			const TriVerts tri2 = load_tri(s.tris, __float_as_uint(d4.w), nullptr, nullptr);
+			const LeafTri* tris = MULTI ? batch.scenes[shadow.sid[k]].scene.tris : s_single.tris;
+			const TriVerts tri = load_tri(tris, __float_as_uint(o4.w), nullptr, nullptr);
+			const TriVerts tri2 = load_tri(tris, __float_as_uint(d4.w), nullptr, nullptr);
 			const EscapeRay e = try_escape_iterative(xyz(o4), face_normal(tri), tri, xyz(d4), tri2, iters);
 			if(e.ok)
 			{
@@ -994,6 +1096,12 @@ RenderScene::RenderScene(const SceneDesc& desc, float max_origin_abs)
 	}
 	BvhBuildInput in{desc.tris.data(), desc.tri_material.data(), desc.tri_emitter.data(), n, max_origin_abs};
 	m_geometry = desc.bvh_builder == PG_BVH_GPU_MORTON ? make_geometry_gpu(in) : make_geometry(in);
+	m_max_origin_abs = max_origin_abs;
+	m_bvh_builder = desc.bvh_builder;
+	for(const Material& m : desc.materials)
+	{
+		m_material_types.push_back(m.type);
+	}
 
 	// scene bound, normalising the guiding network's position inputs
 	{
@@ -1182,12 +1290,13 @@ RenderScene::~RenderScene()
 	}
 }
 
-void RenderScene::ensure_capacity(uint32_t capacity)
+void RenderScene::ensure_capacity(uint32_t capacity, uint32_t grid)
 {
-	if(capacity <= m_capacity)
+	if(capacity <= m_capacity && grid == m_order_grid)
 	{
 		return;
 	}
+	capacity = std::max(capacity, m_capacity);
 	for(int b = 0; b < 2; ++b)
 	{
 		m_path[b].resize(capacity);
@@ -1210,12 +1319,12 @@ void RenderScene::ensure_capacity(uint32_t capacity)
 	m_req_mutual.resize(capacity);
 	{
 		// the slots the blocks of one residue visit in classify_kernel's grid-stride loop
-		const uint32_t grid = static_cast<uint32_t>(sm_count()) * 8u;
 		const uint32_t rounds = (capacity + grid * kShadeBlock - 1u) / (grid * kShadeBlock);
 		m_order_list = (grid + kClassLists - 1u) / kClassLists * rounds * kShadeBlock;
 		m_order.resize(static_cast<size_t>(kOrderLists) * m_order_list);
 	}
 	m_capacity = capacity;
+	m_order_grid = grid;
 }
 
 void RenderScene::ensure_guiding(uint32_t capacity)
@@ -1419,6 +1528,320 @@ void RenderScene::light_pdf(const float* queries, const uint32_t* prims, uint64_
 	PG_CUDA_CHECK(cudaStreamSynchronize(st));
 }
 
+void RenderScene::rebuild_bvh(uint32_t max_leaf_tris)
+{
+	require_same_device(m_geometry->device, "render scene");
+	cudaStream_t st = library_stream();
+	const std::size_t n = m_geometry->tris.size();
+	// the resident triangles back in input order
+	std::vector<LeafTri> leaf(n);
+	PG_CUDA_CHECK(cudaMemcpyAsync(leaf.data(), m_geometry->tris.get(), m_geometry->tris.bytes(), cudaMemcpyDeviceToHost, st));
+	PG_CUDA_CHECK(cudaStreamSynchronize(st));
+	std::vector<float> tris(9 * n);
+	std::vector<uint32_t> materials(n), emitters(n);
+	for(const LeafTri& t : leaf)
+	{
+		if(t.prim >= n)
+		{
+			throw Error(PG_ERR_SCENE, "rebuild_bvh: leaf triangle with an out-of-range input index");
+		}
+		float* v = &tris[9 * static_cast<std::size_t>(t.prim)];
+		v[0] = t.v0x; v[1] = t.v0y; v[2] = t.v0z;
+		v[3] = t.v1x; v[4] = t.v1y; v[5] = t.v1z;
+		v[6] = t.v2x; v[7] = t.v2y; v[8] = t.v2z;
+		materials[t.prim] = t.material;
+		emitters[t.prim] = t.emitter_plus_one;
+	}
+	BvhBuildInput in{tris.data(), materials.data(), emitters.data(), n, m_max_origin_abs};
+	in.max_leaf_tris = max_leaf_tris;
+	std::unique_ptr<Geometry> g = m_bvh_builder == PG_BVH_GPU_MORTON ? make_geometry_gpu(in) : make_geometry(in);
+
+	// the emitters' triangle lists in the new leaf order, each sorted by input index as the
+	// constructor sorts them (their offsets and counts do not change)
+	PG_CUDA_CHECK(cudaMemcpyAsync(leaf.data(), g->tris.get(), g->tris.bytes(), cudaMemcpyDeviceToHost, st));
+	PG_CUDA_CHECK(cudaStreamSynchronize(st));
+	std::vector<std::vector<uint32_t>> per_emitter(m_dev.num_emitters);
+	for(uint32_t k = 0; k < leaf.size(); ++k)
+	{
+		const uint32_t e = leaf[k].emitter_plus_one;
+		if(e != 0u && e <= per_emitter.size())
+		{
+			per_emitter[e - 1].push_back(k);
+		}
+	}
+	std::vector<uint32_t> emitter_tris;
+	for(auto& list : per_emitter)
+	{
+		std::sort(list.begin(), list.end(), [&](uint32_t x, uint32_t y) { return leaf[x].prim < leaf[y].prim; });
+		emitter_tris.insert(emitter_tris.end(), list.begin(), list.end());
+	}
+	if(!emitter_tris.empty())
+	{
+		PG_CUDA_CHECK(cudaMemcpyAsync(m_emitter_tris.get(), emitter_tris.data(), emitter_tris.size() * sizeof(uint32_t),
+		                              cudaMemcpyHostToDevice, st));
+		PG_CUDA_CHECK(cudaStreamSynchronize(st));
+	}
+	m_geometry = std::move(g);
+	m_dev.nodes = m_geometry->nodes.get();
+	m_dev.tris = m_geometry->tris.get();
+	m_launch.leaf_tris = max_leaf_tris;
+}
+
+void RenderScene::set_launch(const LaunchConfig& c)
+{
+	if(c.capacity < 1024u || c.capacity > (1u << 24) || c.refill < 1u || c.refill > 32u || c.blocks_per_sm < 1u ||
+	   c.blocks_per_sm > 64u || c.leaf_tris < 1u || c.leaf_tris > 3u)
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, "launch config out of range (capacity 1024..2^24, refill 1..32, "
+		                                     "blocks per SM 1..64, leaf triangles 1..3)");
+	}
+	if(c.leaf_tris != m_launch.leaf_tris)
+	{
+		rebuild_bvh(c.leaf_tris);
+	}
+	m_launch = c;
+}
+
+std::string RenderScene::fingerprint(const RenderParams& base) const
+{
+	uint32_t kinds[8] = {};
+	for(uint32_t t : m_material_types)
+	{
+		++kinds[std::min<uint32_t>(t, 7u)];
+	}
+	std::string key = "tris=" + std::to_string(m_geometry->tris.size()) + ";res=" + std::to_string(base.width) + "x" +
+	                  std::to_string(base.height) + ";emitters=" + std::to_string(m_dev.num_emitters) +
+	                  ";env=" + std::to_string(m_dev.env_emitter >= 0 ? 1 : 0) + ";materials=";
+	for(int k = 0; k < 4; ++k)
+	{
+		key += std::to_string(kinds[k]) + (k < 3 ? "," : "");
+	}
+	key += ";estimator=" + std::to_string(base.estimator) + ";bounces=" + std::to_string(base.max_bounces) +
+	       ";filter=" + std::to_string(base.filter) + ";builder=" + std::to_string(m_bvh_builder);
+	return key;
+}
+
+namespace
+{
+
+bool read_tuning(const char* path, const std::string& key, LaunchConfig* out)
+{
+	std::FILE* f = path ? std::fopen(path, "r") : nullptr;
+	if(!f)
+	{
+		return false;
+	}
+	char line[1024];
+	bool found = false;
+	while(std::fgets(line, sizeof(line), f))
+	{
+		char k[900];
+		LaunchConfig c;
+		if(std::sscanf(line, "%899s %u %u %u %u", k, &c.capacity, &c.refill, &c.blocks_per_sm, &c.leaf_tris) == 5 &&
+		   key == k)
+		{
+			*out = c;   // the last entry of a key wins
+			found = true;
+		}
+	}
+	std::fclose(f);
+	return found;
+}
+
+void append_tuning(const char* path, const std::string& key, const LaunchConfig& c)
+{
+	std::FILE* f = path ? std::fopen(path, "a") : nullptr;
+	if(!f)
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, std::string("autotune: cannot write the cache file ") + path);
+	}
+	std::fprintf(f, "%s %u %u %u %u\n", key.c_str(), c.capacity, c.refill, c.blocks_per_sm, c.leaf_tris);
+	std::fclose(f);
+}
+
+}// end anonymous namespace
+
+AutotuneResult RenderScene::autotune(const RenderParams& base, bool rebuild, const char* cache_path, bool ignore_cache)
+{
+	require_same_device(m_geometry->device, "render scene");
+	AutotuneResult result;
+	const std::string key = fingerprint(base);
+	if(cache_path && !ignore_cache)
+	{
+		LaunchConfig cached;
+		if(read_tuning(cache_path, key, &cached))
+		{
+			set_launch(cached);
+			result.config = m_launch;
+			result.from_cache = true;
+			return result;
+		}
+	}
+
+	// calibration: the scene's own render at a few million paths (whole samples per pixel),
+	// without guiding (its training would run during the calibration renders)
+	const GuideParams guide_before = m_guide_params;
+	m_guide_params.enabled = false;
+	struct RestoreGuide
+	{
+		GuideParams& dst;
+		GuideParams src;
+		~RestoreGuide() { dst = src; }
+	} restore_guide{m_guide_params, guide_before};
+	const unsigned long long wh = static_cast<unsigned long long>(base.width) * base.height;
+	RenderParams p = base;
+	p.mode = PG_RENDER_GRAPH;
+	p.progress = nullptr;
+	p.capacity = 0;
+	p.first_sample = 0;
+	p.spp = static_cast<uint32_t>(std::max<unsigned long long>(1ull, std::min<unsigned long long>(
+		base.spp, (16ull << 20) / std::max<unsigned long long>(1ull, wh))));
+	DeviceBuffer<double> film(static_cast<std::size_t>(wh) * kFilmChannels);
+	PG_CUDA_CHECK(cudaMemsetAsync(film.get(), 0, film.bytes(), m_stream));
+	auto measure = [&](const LaunchConfig& c)
+	{
+		set_launch(c);
+		float best = 0.0f;
+		for(int rep = 0; rep < 3; ++rep)
+		{
+			const float ms = render(p, film.get());   // the first run also warms the graph up
+			if(rep > 0 && (best == 0.0f || ms < best))
+			{
+				best = ms;
+			}
+			++result.trials;
+		}
+		return best;
+	};
+
+	LaunchConfig best = m_launch;
+	float best_ms = measure(best);
+	result.ms_default = best_ms;
+	auto try_values = [&](uint32_t LaunchConfig::*field, std::initializer_list<uint32_t> values)
+	{
+		const uint32_t current = best.*field;
+		for(uint32_t v : values)
+		{
+			if(v == current)
+			{
+				continue;
+			}
+			LaunchConfig c = best;
+			c.*field = v;
+			const float ms = measure(c);
+			if(ms < best_ms * 0.99f)
+			{
+				best = c;
+				best_ms = ms;
+			}
+		}
+	};
+	try_values(&LaunchConfig::capacity, {1u << 19, 1u << 20, 1u << 21, 1u << 22});
+	try_values(&LaunchConfig::refill, {4u, 8u, 12u, 16u});
+	try_values(&LaunchConfig::blocks_per_sm, {4u, 8u, 16u});
+	if(rebuild && m_bvh_builder == PG_BVH_HOST_SAH)
+	{
+		try_values(&LaunchConfig::leaf_tris, {1u, 2u, 3u});
+	}
+	set_launch(best);
+	result.config = best;
+	result.ms_tuned = best_ms;
+	if(cache_path)
+	{
+		append_tuning(cache_path, key, best);
+	}
+	return result;
+}
+
+float RenderScene::render_batch(const std::vector<const RenderScene*>& scenes, const std::vector<double*>& films,
+                                const std::vector<uint32_t>& spp, const std::vector<uint64_t>& first_sample,
+                                const RenderParams& params)
+{
+	require_same_device(m_geometry->device, "render scene");
+	const std::size_t n = scenes.size();
+	if(n == 0 || films.size() != n || spp.size() != n || first_sample.size() != n)
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, "render_batch: scenes, films, spp and first samples differ in number");
+	}
+	for(std::size_t k = 0; k < n; ++k)
+	{
+		if(!scenes[k] || !films[k] || spp[k] == 0)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "render_batch: missing scene or film, or zero samples");
+		}
+		require_same_device(scenes[k]->m_geometry->device, "render_batch scene");
+	}
+	constexpr unsigned long long kMaxPaths = 1ull << 31;
+	float ms = 0.0f;
+	unsigned long long rays = 0, shadow = 0, iterations = 0, launches = 0;
+	std::vector<BatchScene> chunk;
+	unsigned long long acc = 0;
+	auto flush = [&]
+	{
+		if(chunk.empty())
+		{
+			return;
+		}
+		RenderParams p = params;
+		p.width = 1;
+		p.height = 1;
+		p.spp = 1;
+		p.filter = PG_FILTER_BOX;
+		p.first_sample = 0;
+		p.progress = nullptr;
+		ms += render_pass(p, nullptr, &chunk);
+		rays += m_last_rays;
+		shadow += m_last_shadow;
+		iterations += m_last_iterations;
+		launches += m_last_launches + chunk.size() - 1u;   // one box-weight launch per scene part
+		chunk.clear();
+		acc = 0;
+	};
+	for(std::size_t k = 0; k < n; ++k)
+	{
+		const RenderScene& sc = *scenes[k];
+		const unsigned long long wh = static_cast<unsigned long long>(sc.m_dev.cam.width) * sc.m_dev.cam.height;
+		if(wh == 0 || wh > kMaxPaths)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "render_batch: a scene's resolution is empty or too large");
+		}
+		uint64_t sample = first_sample[k];
+		uint32_t remaining = spp[k];
+		while(remaining > 0)
+		{
+			const unsigned long long room = (kMaxPaths - acc) / wh;
+			if(room == 0)
+			{
+				flush();
+				continue;
+			}
+			const uint32_t take = static_cast<uint32_t>(std::min<unsigned long long>(remaining, room));
+			BatchScene b;
+			b.scene = sc.m_dev;
+			b.film = make_film_view(films[k], sc.m_dev.cam.width, sc.m_dev.cam.height, PG_FILTER_BOX);
+			b.path_first = acc;
+			b.path_count = wh * take;
+			b.first_global = sample * wh;
+			b.width_height = static_cast<uint32_t>(wh);
+			b.spp = take;
+			chunk.push_back(b);
+			acc += wh * take;
+			sample += take;
+			remaining -= take;
+			if(chunk.size() == kMaxBatchScenes)
+			{
+				flush();
+			}
+		}
+	}
+	flush();
+	m_last_rays = rays;
+	m_last_shadow = shadow;
+	m_last_iterations = iterations;
+	m_last_launches = launches;
+	return ms;
+}
+
 // Paths whose radiance a pass of a 4 x 4-filter render keeps (16 B each): larger renders are
 // split into passes of whole samples per pixel.
 constexpr unsigned long long kMaxFilteredPassPaths = 1ull << 27;
@@ -1458,32 +1881,45 @@ float RenderScene::render(const RenderParams& params, double* film_sums)
 	return ms;
 }
 
-float RenderScene::render_pass(const RenderParams& params, double* film_sums)
+float RenderScene::render_pass(const RenderParams& params, double* film_sums, const std::vector<BatchScene>* batch)
 {
+	const bool multi = batch != nullptr;
 	if(params.width == 0 || params.height == 0 || params.spp == 0)
 	{
 		throw Error(PG_ERR_INVALID_ARGUMENT, "render: empty image or zero samples");
 	}
-	if(params.width != m_dev.cam.width || params.height != m_dev.cam.height)
+	if(!multi && (params.width != m_dev.cam.width || params.height != m_dev.cam.height))
 	{
 		throw Error(PG_ERR_INVALID_ARGUMENT, "render: resolution differs from the camera's");
 	}
 	const unsigned long long wh = static_cast<unsigned long long>(params.width) * params.height;
-	const unsigned long long total = wh * params.spp;
+	unsigned long long total = wh * params.spp;
+	if(multi)
+	{
+		if(batch->empty() || batch->size() > kMaxBatchScenes || params.progress || params.filter != PG_FILTER_BOX ||
+		   (m_guide_params.enabled && params.estimator == PG_EST_BNEEPT))
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "render: a multi-scene render takes 1..65536 box-filtered scenes, "
+			                                     "without guiding or previews");
+		}
+		total = batch->back().path_first + batch->back().path_count;
+	}
 	if(total > 0xFFFFFFFFull)
 	{
 		throw Error(PG_ERR_INVALID_ARGUMENT, "render: more than 2^32 paths in one call; split the samples");
 	}
-	const uint32_t capacity = static_cast<uint32_t>(std::min<unsigned long long>(params.capacity, total));
-	ensure_capacity(std::max<uint32_t>(capacity, 1024u));
+	const LaunchConfig& lc = m_launch;
+	const uint32_t capacity = static_cast<uint32_t>(std::min<unsigned long long>(params.capacity ? params.capacity
+	                                                                                             : lc.capacity, total));
+	const int sms = sm_count();
+	const int grid = sms * static_cast<int>(lc.blocks_per_sm);   // grid-stride kernels: 128-thread blocks
+	ensure_capacity(std::max<uint32_t>(capacity, 1024u), static_cast<uint32_t>(grid));
+	const int refill = static_cast<int>(lc.refill);
 
 	cudaStream_t st = m_stream;
 	RenderCounters init{};
 	init.total_paths = total;
 	PG_CUDA_CHECK(cudaMemcpyAsync(m_counters.get(), &init, sizeof(init), cudaMemcpyHostToDevice, st));
-
-	const int sms = sm_count();
-	const int grid = sms * 8;   // grid-stride kernels: 8 blocks of 128 threads per SM
 	PathBuffers buf[2];
 	for(int b = 0; b < 2; ++b)
 	{
@@ -1495,6 +1931,25 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums)
 	{
 		sqs[b] = ShadowQueue{m_so[b].get(), m_sd[b].get(), m_sc[b].get()};
 		sqs[b].r = m_sr[b].get();
+	}
+	BatchView bview;
+	if(multi)
+	{
+		for(int b = 0; b < 2; ++b)
+		{
+			if(m_ssid[b].size() < m_capacity)
+			{
+				m_ssid[b].resize(m_capacity);
+			}
+			sqs[b].sid = m_ssid[b].get();
+		}
+		if(m_batch_table.size() < batch->size())
+		{
+			m_batch_table.resize(batch->size());
+		}
+		PG_CUDA_CHECK(cudaMemcpyAsync(m_batch_table.get(), batch->data(), batch->size() * sizeof(BatchScene),
+		                              cudaMemcpyHostToDevice, st));
+		bview = BatchView{m_batch_table.get(), static_cast<uint32_t>(batch->size())};
 	}
 	FilmView film = make_film_view(film_sums, params.width, params.height, params.filter);
 	if(params.filter != PG_FILTER_BOX)
@@ -1558,19 +2013,37 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums)
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[0], st)); }
 		prepare_kernel<<<1, 32, 0, st>>>(m_counters.get(), capacity);
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[1], st)); }
-		regen_kernel<<<grid, kShadeBlock, 0, st>>>(m_counters.get(), m_dev.cam, film, params.seed, first_global, cur);
+		if(multi)
+		{
+			regen_kernel<true><<<grid, kShadeBlock, 0, st>>>(m_counters.get(), m_dev.cam, film, params.seed, first_global,
+			                                                 cur, bview);
+		}
+		else
+		{
+			regen_kernel<false><<<grid, kShadeBlock, 0, st>>>(m_counters.get(), m_dev.cam, film, params.seed, first_global,
+			                                                  cur, bview);
+		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[2], st)); }
 		const ShadowQueue& sq = sqs[merged_shadows ? b : 0];   // this iteration's NEE segments
 		if(merged_shadows)
 		{
-			launch_trace(m_dev, d_counters, cur.ray_o, cur.ray_d, m_hits.get(), sqs[1 - b], cur.rad, film, st,
-			             counting);
-			classify_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, m_hits.get(), m_order.get(), m_order_list);
+			launch_trace(m_dev, d_counters, cur.ray_o, cur.ray_d, m_hits.get(), sqs[1 - b], cur.rad, film, refill, st,
+			             counting, cur.meta, multi ? &bview : nullptr);
+			if(multi)
+			{
+				classify_kernel<true><<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, m_hits.get(), m_order.get(),
+				                                                    m_order_list, cur.meta, bview);
+			}
+			else
+			{
+				classify_kernel<false><<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, m_hits.get(), m_order.get(),
+				                                                     m_order_list, cur.meta, bview);
+			}
 			PG_CUDA_CHECK(cudaGetLastError());
 		}
 		else
 		{
-			launch_extend(m_dev, d_counters, cur.ray_o, cur.ray_d, m_hits.get(), grid, 128, st, counting);
+			launch_extend(m_dev, d_counters, cur.ray_o, cur.ray_d, m_hits.get(), refill, st, counting);
 		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[3], st)); }
 		if(guided)
@@ -1591,25 +2064,38 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums)
 		sa.refine_queue = RefineQueue{m_req_single.get(), m_req_mutual.get()};
 		sa.order = merged_shadows ? m_order.get() : nullptr;
 		sa.order_capacity = m_order_list;
-		if(guided)
+		sa.batch = bview;
+		if(multi)
 		{
-			shade_kernel<true><<<grid, kShadeBlock, 0, st>>>(sa);
+			shade_kernel<false, true><<<grid, kShadeBlock, 0, st>>>(sa);
+		}
+		else if(guided)
+		{
+			shade_kernel<true, false><<<grid, kShadeBlock, 0, st>>>(sa);
 		}
 		else
 		{
-			shade_kernel<false><<<grid, kShadeBlock, 0, st>>>(sa);
+			shade_kernel<false, false><<<grid, kShadeBlock, 0, st>>>(sa);
 		}
 		PG_CUDA_CHECK(cudaGetLastError());
 		if(params.refine_mode == PG_REFINE_ITERATIVE)
 		{
-			refine_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, nxt, sq, sa.refine_queue,
-			                                              static_cast<int>(params.refine_iters));
+			if(multi)
+			{
+				refine_kernel<true><<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, nxt, sq, sa.refine_queue,
+				                                                  static_cast<int>(params.refine_iters), bview);
+			}
+			else
+			{
+				refine_kernel<false><<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, nxt, sq, sa.refine_queue,
+				                                                   static_cast<int>(params.refine_iters), bview);
+			}
 			PG_CUDA_CHECK(cudaGetLastError());
 		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[5], st)); }
 		if(!merged_shadows)
 		{
-			launch_shadow(m_dev, d_counters, sq, nxt.rad, film, grid, 128, st, counting,
+			launch_shadow(m_dev, d_counters, sq, nxt.rad, film, refill, st, counting,
 			              training ? m_tdirw.get() : nullptr);
 		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[6], st)); }
@@ -1633,7 +2119,15 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums)
 	// the box filter's W: spp per pixel, added once (film.cuh)
 	auto add_box_weights = [&]
 	{
-		if(params.filter == PG_FILTER_BOX)
+		if(multi)
+		{
+			for(const BatchScene& b : *batch)
+			{
+				box_weights_kernel<<<sms * 4, 256, 0, st>>>(b.film.sums, b.width_height, static_cast<double>(b.spp));
+				PG_CUDA_CHECK(cudaGetLastError());
+			}
+		}
+		else if(params.filter == PG_FILTER_BOX)
 		{
 			box_weights_kernel<<<sms * 4, 256, 0, st>>>(film_sums, static_cast<uint32_t>(wh), static_cast<double>(params.spp));
 			PG_CUDA_CHECK(cudaGetLastError());
@@ -1654,6 +2148,35 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums)
 		PG_CUDA_CHECK(cudaMallocHost(&m_host_counters, sizeof(RenderCounters)));
 	}
 	RenderCounters* const host_counters = m_host_counters;
+
+	// a preview of the film at a batch boundary (the stream is idle there); see RenderProgress
+	if(params.progress && m_inflight.size() < wh)
+	{
+		m_inflight.resize(wh);
+	}
+	auto publish_preview = [&](const RenderCounters& hc)
+	{
+		RenderProgress& pr = *params.progress;
+		{
+			std::lock_guard<std::mutex> lock(*pr.mutex);
+			const uint32_t pixels = static_cast<uint32_t>(wh);
+			const bool box = params.filter == PG_FILTER_BOX;
+			if(box)
+			{
+				PG_CUDA_CHECK(cudaMemsetAsync(m_inflight.get(), 0, wh * sizeof(uint32_t), st));
+				count_inflight_kernel<<<grid, kShadeBlock, 0, st>>>(buf[0].path, m_counters.get(), pixels, m_inflight.get());
+				PG_CUDA_CHECK(cudaGetLastError());
+			}
+			develop_preview_kernel<<<grid, kShadeBlock, 0, st>>>(film_sums, m_inflight.get(), pixels, params.spp,
+			                                                    hc.next_path, box ? 1 : 0, pr.preview_rgb);
+			PG_CUDA_CHECK(cudaGetLastError());
+			PG_CUDA_CHECK(cudaStreamSynchronize(st));
+		}
+		if(pr.published)
+		{
+			pr.published(hc.next_path - hc.n_next, total);
+		}
+	};
 	cudaEvent_t e0, e1;
 	PG_CUDA_CHECK(cudaEventCreate(&e0));
 	PG_CUDA_CHECK(cudaEventCreate(&e1));
@@ -1673,7 +2196,7 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums)
 		iteration(0, nullptr);
 		iteration(1, nullptr);
 		PG_CUDA_CHECK(cudaStreamEndCapture(st, &graph));
-		const int key = (guided ? 1 : 0) | (training ? 2 : 0);
+		const int key = (guided ? 1 : 0) | (training ? 2 : 0) | (multi ? 4 : 0);
 		bool updated = false;
 		if(m_exec && m_exec_key == key)
 		{
@@ -1713,6 +2236,10 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums)
 			if(host_counters->error)
 			{
 				break;
+			}
+			if(params.progress && !done)
+			{
+				publish_preview(*host_counters);
 			}
 			batch = std::min(batch * 2, 64);
 		}

@@ -20,7 +20,10 @@
 #include "pg_geometry.h"
 
 #include <cstdint>
+#include <functional>
 #include <memory>
+#include <mutex>
+#include <string>
 #include <vector>
 
 namespace pg
@@ -69,6 +72,40 @@ enum RenderMode : uint32_t
 	PG_RENDER_COUNT = 2,    // plain launches, traversal kernels count nodes and triangles
 };
 
+// Progress of a render while it runs (graph mode). At every batch boundary -- the scene's stream
+// idle, every kernel of the batch complete, so the film holds exactly what finished paths put
+// there -- the film's estimate over the samples finished so far is developed into preview_rgb
+// (device memory, [h][w][3] float32, RGB / W with the box film's W counting finished samples
+// only) while `mutex` is held, and then `published` is called with the paths finished so far and
+// the total of the render call. The callback runs on the rendering thread.
+struct RenderProgress
+{
+	std::mutex* mutex = nullptr;
+	float* preview_rgb = nullptr;
+	std::function<void(unsigned long long finished, unsigned long long total)> published;
+};
+
+// Launch shapes of a scene's renders. The defaults were picked by hand on the 1M-triangle GGX
+// scene; RenderScene::autotune picks them per scene from short calibration renders.
+struct LaunchConfig
+{
+	uint32_t capacity = 1u << 21;   // path slots in flight (the wavefront's queue depth)
+	uint32_t refill = 8;            // idle lanes that make a traversal warp fetch new rays
+	uint32_t blocks_per_sm = 8;     // 128-thread blocks per SM of the grid-stride kernels
+	uint32_t leaf_tris = 3;         // triangles per BVH leaf at most (host SAH tree; 1..3)
+};
+
+// What RenderScene::autotune found: the chosen shapes and the calibration render's device
+// milliseconds with the defaults and with the choice.
+struct AutotuneResult
+{
+	LaunchConfig config;
+	float ms_default = 0.0f;
+	float ms_tuned = 0.0f;
+	uint32_t trials = 0;
+	bool from_cache = false;
+};
+
 struct RenderParams
 {
 	uint32_t width = 0, height = 0;
@@ -78,13 +115,14 @@ struct RenderParams
 	uint32_t filter = PG_FILTER_BOX;    // SampleFilterType of the film being rendered into
 	uint64_t seed = 42;
 	uint64_t first_sample = 0;          // sample index offset (resume / replicas)
-	uint32_t capacity = 1u << 21;       // path slots in flight
+	uint32_t capacity = 0;              // path slots in flight (0: the scene's LaunchConfig)
 	uint32_t mode = PG_RENDER_GRAPH;
 	// SurfaceHitRefinery settings (the reference's EngineInitSettings: RefineMode,
 	// SelfIntersectDelta, NumIterativeSurfaceRefinements): 0 manual, 1 empirical, 2 iterative.
 	uint32_t refine_mode = 2;
 	float    refine_delta = 2e-4f;
 	uint32_t refine_iters = 1;
+	RenderProgress* progress = nullptr;  // previews and progress during the render (graph mode only)
 };
 
 // Learned path guiding (BNEEPT only). At Lambertian vertices the direction is drawn from the
@@ -210,6 +248,29 @@ struct ShadowQueue
 	float4* c;          // contribution rgb, target (slot in next buffer, or 0x80000000|pixel)
 	float2* t;          // guided renders: training sample index (bits, or ~0), weight added if unoccluded
 	float2* r;          // filtered films: raster position of the sample a final contribution belongs to
+	uint32_t* sid;      // multi-scene renders: the scene of each record
+};
+
+// One scene of a multi-scene render: its device records, film, and where its paths sit in the
+// render's path numbering (scene k owns batch paths [path_first, path_first + path_count); a
+// path's sample draws use its index within the scene, offset by first_global, so every scene
+// gets the paths its own render would).
+struct BatchScene
+{
+	DeviceScene scene;
+	FilmView    film;
+	unsigned long long path_first;
+	unsigned long long path_count;
+	unsigned long long first_global;
+	uint32_t    width_height;
+	uint32_t    spp;
+};
+
+// The scene table of a multi-scene render (device memory).
+struct BatchView
+{
+	const BatchScene* scenes = nullptr;
+	uint32_t count = 0;
 };
 
 // Device view of the guiding buffers for one render iteration.
@@ -226,22 +287,29 @@ struct GuideArgs
 	float           rcp[3] = {1, 1, 1};
 };
 
+// A multi-scene render (RenderScene::render_batch) keeps each path's scene in the top bits of its
+// meta word; a single-scene render leaves them 0.
+constexpr uint32_t kMetaSceneShift = 16u;
+constexpr uint32_t kMaxBatchScenes = 1u << 16;
 constexpr uint32_t kMetaBounceMask = 0xFFu;
 constexpr uint32_t kMetaPrevNee = 1u << 8;      // the previous vertex used NEE (MIS applies)
 constexpr uint32_t kMetaStopAfter = 1u << 9;    // Russian roulette ended the path after this hit
 constexpr uint32_t kMetaGuideRec = 1u << 10;    // gf0/gf1 hold a guided vertex awaiting its training sample
 constexpr uint32_t kTargetFinal = 0x80000000u;
 
-// Launchers implemented in pg_trace.cu (FMA-enabled traversal kernels).
+// Launchers implemented in pg_trace.cu (FMA-enabled traversal kernels); min_idle is the
+// traversal's refill threshold (LaunchConfig::refill).
 void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4* ray_o,
-                   const float4* ray_d, uint2* hits, int grid, int block, cudaStream_t st, bool count);
+                   const float4* ray_d, uint2* hits, int min_idle, cudaStream_t st, bool count);
 // Closest hits of this iteration's queue and visibility of the previous iteration's shadow
 // queue `prev` in one persistent launch; unoccluded contributions go to rad_cur / the film.
+// With a batch (multi-scene render), `meta` is the current path buffer's meta words and prev.sid
+// the records' scenes.
 void launch_trace(const DeviceScene& s, RenderCounters* counters, const float4* ray_o, const float4* ray_d,
-                  uint2* hits, const ShadowQueue& prev, float4* rad_cur, const FilmView& film, cudaStream_t st,
-                  bool count);
+                  uint2* hits, const ShadowQueue& prev, float4* rad_cur, const FilmView& film, int min_idle,
+                  cudaStream_t st, bool count, const uint32_t* meta = nullptr, const BatchView* batch = nullptr);
 void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
-                   float4* rad_next, const FilmView& film, int grid, int block, cudaStream_t st, bool count,
+                   float4* rad_next, const FilmView& film, int min_idle, cudaStream_t st, bool count,
                    float4* train_dirw = nullptr);
 
 // A scene resident on the GPU together with its render buffers.
@@ -269,6 +337,19 @@ public:
 	// Nodes / triangles visited by closest-hit and any-hit queries in the last counting render.
 	const unsigned long long* last_counts() const { return m_last_counts; }
 
+	// Launch shapes of subsequent renders (leaf_tris differing from the tree's rebuilds it).
+	void set_launch(const LaunchConfig& c);
+	const LaunchConfig& launch() const { return m_launch; }
+	// Picks the launch shapes by coordinate descent over calibration renders of `base` (a few
+	// million paths at its estimator and bounce cap, into a scratch film): path-pool depth,
+	// traversal refill threshold, grid of the grid-stride kernels and, with rebuild, the BVH leaf
+	// size. A candidate replaces the current choice only when it is more than 1 % faster. With a
+	// cache file, a scene of the same fingerprint takes the stored choice without calibrating,
+	// and a new choice is appended to it.
+	AutotuneResult autotune(const RenderParams& base, bool rebuild, const char* cache_path, bool ignore_cache);
+	// Identifies scenes that tune alike: triangles, resolution, emitters, material kinds.
+	std::string fingerprint(const RenderParams& base) const;
+
 	// Learned guiding for subsequent renders; the network is created (He-initialised, fixed seed)
 	// on first use and keeps its training state until reset_guiding().
 	void set_guiding(const GuideParams& g) { m_guide_params = g; }
@@ -290,9 +371,24 @@ public:
 	// point on the light triangle; prims [n] = that triangle's input index.
 	void light_pdf(const float* queries, const uint32_t* prims, uint64_t n, float* out_pdf_w) const;
 
+	// Renders several scenes in one wavefront: one path pool, one launch of every kernel per
+	// iteration for all of them, the iterations captured as graphs. This scene's pool, stream and
+	// graphs run it; every scene listed (this one included or not) must live on this device and
+	// outlive the call. Scene k renders spp[k] more samples into films[k] (box filter, FP64 sums
+	// [h][w][4]) starting at sample first_sample[k]; `params` gives the estimator, bounce cap,
+	// seed and refine settings. The scenes are split into renders of at most 2^31 paths each.
+	// Returns the device milliseconds of all of them.
+	float render_batch(const std::vector<const RenderScene*>& scenes, const std::vector<double*>& films,
+	                   const std::vector<uint32_t>& spp, const std::vector<uint64_t>& first_sample,
+	                   const RenderParams& params);
+	uint32_t width() const { return m_dev.cam.width; }
+	uint32_t height() const { return m_dev.cam.height; }
+
 private:
-	float render_pass(const RenderParams& params, double* film_device);
-	void ensure_capacity(uint32_t capacity);
+	float render_pass(const RenderParams& params, double* film_device, const std::vector<BatchScene>* batch = nullptr);
+	void ensure_capacity(uint32_t capacity, uint32_t grid);
+	// Rebuilds the BVH from the resident triangles with at most max_leaf_tris per leaf.
+	void rebuild_bvh(uint32_t max_leaf_tris);
 	void ensure_guiding(uint32_t capacity);
 
 	std::unique_ptr<Geometry> m_geometry;
@@ -305,6 +401,11 @@ private:
 	DeviceScene               m_dev{};
 
 	uint32_t m_capacity = 0;
+	uint32_t m_order_grid = 0;
+	LaunchConfig m_launch;
+	float m_max_origin_abs = 0.0f;
+	uint32_t m_bvh_builder = 0;
+	std::vector<uint32_t> m_material_types;   // per material (fingerprint)
 	DeviceBuffer<uint32_t> m_path[2], m_meta[2];
 	DeviceBuffer<float4>   m_thr[2], m_rad[2], m_prev[2], m_ro[2], m_rd[2];
 	DeviceBuffer<uint2>    m_hits;
@@ -313,6 +414,9 @@ private:
 	DeviceBuffer<uint32_t> m_req_single, m_req_mutual;
 	DeviceBuffer<uint32_t> m_order;   // shading order: kOrderLists lists of m_order_list slots
 	DeviceBuffer<float4>   m_samples; // 4 x 4 filters: radiance of every path of a pass
+	DeviceBuffer<uint32_t> m_inflight;   // previews: paths in flight per pixel
+	DeviceBuffer<uint32_t> m_ssid[2];    // multi-scene renders: scene of each NEE record
+	DeviceBuffer<BatchScene> m_batch_table;
 	uint32_t m_order_list = 0;
 	DeviceBuffer<RenderCounters> m_counters;
 

@@ -43,7 +43,10 @@ std::unique_ptr<Geometry> make_geometry(const BvhBuildInput& in)
 namespace
 {
 
-constexpr int kTraceBlock = 128;
+constexpr int kTraceBlock = kTraversalBlock;
+// Resident blocks per SM the traversal kernels are compiled for: 8 x 128 threads at 64 registers
+// fill the register file (a larger register budget leaves room for 7 blocks only).
+constexpr int kTraceMinBlocks = 8;
 
 struct HitRecord
 {
@@ -51,7 +54,7 @@ struct HitRecord
 	float    t;
 };
 
-__global__ void __launch_bounds__(kTraceBlock)
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
 trace_closest_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
                      const float4* __restrict__ rays, uint32_t n, uint32_t* __restrict__ next_ray,
                      HitRecord* __restrict__ hits, uint32_t* __restrict__ error)
@@ -67,7 +70,7 @@ trace_closest_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restri
 	}
 }
 
-__global__ void __launch_bounds__(kTraceBlock)
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
 trace_any_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
                  const float4* __restrict__ rays, uint32_t n, uint32_t* __restrict__ next_ray,
                  int32_t* __restrict__ occluded, uint32_t* __restrict__ error)
@@ -204,18 +207,18 @@ void check_device_error(Geometry& g, cudaStream_t s)
 // Closest hit for the render's ray queue; the queue length is read on the device. COUNT adds
 // the visited-node / tested-triangle tallies of the counting render.
 template<bool COUNT>
-__global__ void __launch_bounds__(kTraceBlock)
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
 extend_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
               RenderCounters* __restrict__ counters,
               const float4* __restrict__ ray_o, const float4* __restrict__ ray_d,
-              uint2* __restrict__ hits)
+              uint2* __restrict__ hits, int min_idle)
 {
 	const uint32_t n = counters->n_total;
 	uint32_t err = 0, node_count = 0, tri_count = 0;
 	traverse_persistent<false, COUNT>(nodes, tris, n, &counters->fetch_extend,
 		[&](uint32_t i, float4* a, float4* b) { *a = __ldg(ray_o + i); *b = __ldg(ray_d + i); },
 		[&](uint32_t i, bool hit, uint32_t tri, float t) { hits[i] = make_uint2(hit ? tri : 0xFFFFFFFFu, __float_as_uint(t)); },
-		&err, &node_count, &tri_count);
+		&err, &node_count, &tri_count, 0u, min_idle);
 	if(COUNT)
 	{
 		atomicAdd(&counters->nodes_closest, static_cast<unsigned long long>(node_count));
@@ -278,13 +281,17 @@ __device__ __forceinline__ void add_unoccluded(uint32_t i, const float4* __restr
 // rays, then the visibility of the previous iteration's NEE segments, whose owning paths sit in
 // this iteration's path buffer (their radiance is read by this iteration's shading, after this
 // kernel). A single dynamic-fetch cursor runs over both queues, so the launch has one tail.
-template<bool COUNT>
-__global__ void __launch_bounds__(kTraceBlock)
+// MULTI: the rays belong to the scenes of `batch` (a closest-hit ray's scene in the top bits of its
+// path's meta word, a NEE segment's in its record's sid); each ray walks its own scene's tree and
+// a final contribution goes to its own scene's film.
+template<bool COUNT, bool MULTI>
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
 trace_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
              RenderCounters* __restrict__ counters,
              const float4* __restrict__ ray_o, const float4* __restrict__ ray_d, uint2* __restrict__ hits,
              const float4* __restrict__ so, const float4* __restrict__ sd, const float4* __restrict__ sc,
-             const float2* __restrict__ sr, float4* __restrict__ rad_cur, FilmView film)
+             const float2* __restrict__ sr, float4* __restrict__ rad_cur, FilmView film, int min_idle,
+             const uint32_t* __restrict__ meta, const uint32_t* __restrict__ shadow_sid, BatchView batch)
 {
 	const uint32_t n_closest = counters->n_total;
 	const uint32_t n_shadow = counters->n_shadow_prev;
@@ -292,33 +299,59 @@ trace_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tri
 	{
 		counters->shadow_rays += n_shadow;
 	}
-	uint32_t err = 0, node_count[2] = {0u, 0u}, tri_count[2] = {0u, 0u};
-	traverse_persistent<false, COUNT, true>(nodes, tris, n_closest + n_shadow, &counters->fetch_extend,
-		[&](uint32_t i, float4* a, float4* b)
+	auto scene_of = [&](uint32_t i) -> uint32_t
+	{
+		return i < n_closest ? __ldg(meta + i) >> kMetaSceneShift : __ldg(shadow_sid + (i - n_closest));
+	};
+	auto fetch_ray = [&](uint32_t i, float4* a, float4* b)
+	{
+		if(i < n_closest)
 		{
-			if(i < n_closest)
+			*a = __ldg(ray_o + i);
+			*b = __ldg(ray_d + i);
+		}
+		else
+		{
+			*a = __ldg(so + (i - n_closest));
+			*b = __ldg(sd + (i - n_closest));
+		}
+	};
+	auto finish = [&](uint32_t i, bool hit, uint32_t tri, float t)
+	{
+		if(i < n_closest)
+		{
+			hits[i] = make_uint2(hit ? tri : 0xFFFFFFFFu, __float_as_uint(t));
+		}
+		else if(!hit)
+		{
+			if constexpr(MULTI)
 			{
-				*a = __ldg(ray_o + i);
-				*b = __ldg(ray_d + i);
+				add_unoccluded(i - n_closest, sc, nullptr, sr, rad_cur, batch.scenes[scene_of(i)].film, nullptr);
 			}
 			else
 			{
-				*a = __ldg(so + (i - n_closest));
-				*b = __ldg(sd + (i - n_closest));
-			}
-		},
-		[&](uint32_t i, bool hit, uint32_t tri, float t)
-		{
-			if(i < n_closest)
-			{
-				hits[i] = make_uint2(hit ? tri : 0xFFFFFFFFu, __float_as_uint(t));
-			}
-			else if(!hit)
-			{
 				add_unoccluded(i - n_closest, sc, nullptr, sr, rad_cur, film, nullptr);
 			}
-		},
-		&err, node_count, tri_count, n_closest);
+		}
+	};
+	uint32_t err = 0, node_count[2] = {0u, 0u}, tri_count[2] = {0u, 0u};
+	if constexpr(MULTI)
+	{
+		traverse_persistent<false, COUNT, true, true>(nodes, tris, n_closest + n_shadow, &counters->fetch_extend,
+			[&](uint32_t i, float4* a, float4* b, const WideNode** ln, const LeafTri** lt)
+			{
+				fetch_ray(i, a, b);
+				const DeviceScene& s = batch.scenes[scene_of(i)].scene;
+				*ln = s.nodes;
+				*lt = s.tris;
+			},
+			finish, &err, node_count, tri_count, n_closest, min_idle);
+	}
+	else
+	{
+		traverse_persistent<false, COUNT, true>(nodes, tris, n_closest + n_shadow, &counters->fetch_extend,
+			fetch_ray, finish, &err, node_count, tri_count, n_closest, min_idle);
+	}
 	if(COUNT)
 	{
 		atomicAdd(&counters->nodes_closest, static_cast<unsigned long long>(node_count[0]));
@@ -335,12 +368,12 @@ trace_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tri
 // Visibility of the NEE segments of this iteration (guided training renders, whose training
 // step at the end of the iteration needs them); see add_unoccluded.
 template<bool COUNT>
-__global__ void __launch_bounds__(kTraceBlock)
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
 shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
               RenderCounters* __restrict__ counters,
               const float4* __restrict__ so, const float4* __restrict__ sd, const float4* __restrict__ sc,
               const float2* __restrict__ st, const float2* __restrict__ sr, float4* __restrict__ rad_next,
-              FilmView film, float4* __restrict__ train_dirw)
+              FilmView film, float4* __restrict__ train_dirw, int min_idle)
 {
 	const uint32_t n = counters->n_shadow;
 	if(blockIdx.x == 0 && threadIdx.x == 0)
@@ -357,7 +390,7 @@ shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tr
 				add_unoccluded(i, sc, st, sr, rad_next, film, train_dirw);
 			}
 		},
-		&err, &node_count, &tri_count);
+		&err, &node_count, &tri_count, 0u, min_idle);
 	if(COUNT)
 	{
 		atomicAdd(&counters->nodes_any, static_cast<unsigned long long>(node_count));
@@ -372,54 +405,70 @@ shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tr
 }// end anonymous namespace
 
 void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4* ray_o,
-                   const float4* ray_d, uint2* hits, int, int, cudaStream_t st, bool count)
+                   const float4* ray_d, uint2* hits, int min_idle, cudaStream_t st, bool count)
 {
 	if(count)
 	{
 		const int grid = persistent_grid(extend_kernel<true>);
-		extend_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits);
+		extend_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits, min_idle);
 	}
 	else
 	{
 		const int grid = persistent_grid(extend_kernel<false>);
-		extend_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits);
+		extend_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits, min_idle);
 	}
 	PG_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_trace(const DeviceScene& s, RenderCounters* counters, const float4* ray_o, const float4* ray_d,
-                  uint2* hits, const ShadowQueue& prev, float4* rad_cur, const FilmView& film, cudaStream_t st,
-                  bool count)
+                  uint2* hits, const ShadowQueue& prev, float4* rad_cur, const FilmView& film, int min_idle,
+                  cudaStream_t st, bool count, const uint32_t* meta, const BatchView* batch)
 {
-	if(count)
+	if(batch)
 	{
-		const int grid = persistent_grid(trace_kernel<true>);
-		trace_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
-		                                                 prev.o, prev.d, prev.c, prev.r, rad_cur, film);
+		if(count)
+		{
+			const int grid = persistent_grid(trace_kernel<true, true>);
+			trace_kernel<true, true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
+				prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, meta, prev.sid, *batch);
+		}
+		else
+		{
+			const int grid = persistent_grid(trace_kernel<false, true>);
+			trace_kernel<false, true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
+				prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, meta, prev.sid, *batch);
+		}
+	}
+	else if(count)
+	{
+		const int grid = persistent_grid(trace_kernel<true, false>);
+		trace_kernel<true, false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
+			prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, nullptr, nullptr, BatchView{});
 	}
 	else
 	{
-		const int grid = persistent_grid(trace_kernel<false>);
-		trace_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
-		                                                  prev.o, prev.d, prev.c, prev.r, rad_cur, film);
+		const int grid = persistent_grid(trace_kernel<false, false>);
+		trace_kernel<false, false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
+			prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, nullptr, nullptr, BatchView{});
 	}
 	PG_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
-                   float4* rad_next, const FilmView& film, int, int, cudaStream_t st, bool count, float4* train_dirw)
+                   float4* rad_next, const FilmView& film, int min_idle, cudaStream_t st, bool count,
+                   float4* train_dirw)
 {
 	if(count)
 	{
 		const int grid = persistent_grid(shadow_kernel<true>);
 		shadow_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, q.t, q.r,
-		                                                  rad_next, film, train_dirw);
+		                                                  rad_next, film, train_dirw, min_idle);
 	}
 	else
 	{
 		const int grid = persistent_grid(shadow_kernel<false>);
 		shadow_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, q.t, q.r,
-		                                                   rad_next, film, train_dirw);
+		                                                   rad_next, film, train_dirw, min_idle);
 	}
 	PG_CUDA_CHECK(cudaGetLastError());
 }

@@ -358,46 +358,70 @@ __device__ __forceinline__ bool traverse(
 //
 // Rays differ widely in the work they need (nodes visited, triangles tested), and a warp that
 // traverses 32 rays to completion runs at the pace of its longest ray while finished lanes idle.
-// Here every lane keeps its own traversal state and the warp advances all lanes one step per
-// loop turn (one wide-node intersection, or one triangle test); lanes whose ray has finished are
-// refilled from a global ray counter as soon as kRefillMinIdle of them are idle. The visit order
-// of a single ray is exactly that of traverse() above (same node order, same triangle order,
-// same tie rule), so results are identical; only the scheduling of rays onto lanes changes.
+// Here every lane keeps its own traversal state; lanes whose ray has finished are refilled from a
+// global ray counter as soon as kRefillMinIdle of them are idle.
+//
+// Each loop turn a lane does one wide-node step AND one triangle test. A node step that finds
+// leaf triangles while the lane still has triangles to test parks them in a second slot; the lane
+// then takes no node steps until the first slot drains, so node traversal runs at most one
+// triangle group ahead of the triangle tests. Compared with one step of either kind per turn,
+// where a warp of mixed lanes pays for both code paths and each lane uses one, most lanes now
+// have work in both halves of a turn. Triangles are still tested in the order their groups are
+// found, and nodes are visited in the same front-to-back order, so a ray's answer is that of
+// traverse() above (same tie rule); node culling only sees a best_t that may lag by the parked
+// group, which can cost a few extra node visits.
+//
+// The traversal stack's first kSharedStack entries per thread live in shared memory, the rest
+// (deep trees only) in local memory.
 //
 // Fetch(uint32_t i, float4* origin_tmin, float4* dir_tmax) loads ray i; Finish(uint32_t i,
 // bool hit, uint32_t leaf_tri, float t) consumes its result. n rays are taken from *next_ray,
-// which must be zero when the launch starts. Every lane of the warp must call this function.
+// which must be zero when the launch starts. Every lane of the warp must call this function, in
+// blocks of exactly kTraversalBlock threads.
+//
+// MULTI: rays of several scenes share the launch; fetch has the form Fetch(i, origin_tmin,
+// dir_tmax, const WideNode** nodes, const LeafTri** tris) and names the tree of ray i's scene.
 //
 // MIXED: rays [0, n_closest) are closest-hit queries and rays [n_closest, n) any-hit queries, so
 // one launch serves both queues (each lane switches per ray); counts go to node_count[0] /
-// tri_count[0] for closest-hit rays and [1] for any-hit rays.
+// tri_count[0] for closest-hit rays and [1] for any-hit rays. min_idle: the idle lanes that make
+// a warp fetch new rays (1..32; fewer refills against more idle lanes).
 
 constexpr uint32_t kFullWarp = 0xFFFFFFFFu;
-constexpr int kRefillMinIdle = 8;
+constexpr int kRefillMinIdle = 8;   // the default of min_idle
+constexpr int kTraversalBlock = 128;   // threads per block of every persistent traversal launch
+constexpr int kSharedStack = 8;        // stack entries per thread held in shared memory
 
-template<bool ANY_HIT, bool COUNT, bool MIXED = false, class Fetch, class Finish>
+template<bool ANY_HIT, bool COUNT, bool MIXED = false, bool MULTI = false, class Fetch, class Finish>
 __device__ __forceinline__ void traverse_persistent(
-	const WideNode* __restrict__ nodes,
-	const LeafTri* __restrict__ tris,
+	const WideNode* __restrict__ scene_nodes,
+	const LeafTri* __restrict__ scene_tris,
 	uint32_t n, uint32_t* __restrict__ next_ray,
 	Fetch fetch, Finish finish,
 	uint32_t* out_error, uint32_t* node_count = nullptr, uint32_t* tri_count = nullptr,
-	uint32_t n_closest = 0)
+	uint32_t n_closest = 0, int min_idle = kRefillMinIdle)
 {
-	const uint32_t lane = threadIdx.x & 31u;
+	// [entry][thread]: a lane's entries are 1 KB apart, so lanes at any depths hit distinct banks
+	__shared__ uint2 s_stack[kSharedStack][kTraversalBlock];
+	uint2 l_stack[kTraversalStackSize - kSharedStack];
+
+	const uint32_t tid = threadIdx.x;
+	const uint32_t lane = tid & 31u;
 	const uint32_t lanes_below = (1u << lane) - 1u;
 
-	uint2 stack[kTraversalStackSize];
 	int sp = 0;
 	RayTraits r{};
 	float t_min = 0.0f;
 	float best_t = 0.0f;
 	uint32_t best_tri = 0xFFFFFFFFu, best_prim = 0xFFFFFFFFu;
 	uint32_t child_base = 0, imask = 0, node_hits = 0;
-	uint32_t tri_base = 0, tri_hits = 0;
+	uint32_t tri_base = 0, tri_hits = 0;     // the triangle group under test
+	uint32_t next_base = 0, next_hits = 0;   // a group found while the first was still under test
 	uint32_t ray = 0;
 	bool has_ray = false;
 	bool any_hit = ANY_HIT;   // this lane's query (varies per ray only when MIXED)
+	const WideNode* nodes = scene_nodes;   // this lane's tree (varies per ray only when MULTI)
+	const LeafTri* tris = scene_tris;
 	bool exhausted = false;   // warp-uniform: the counter has passed n
 
 	while(true)
@@ -405,7 +429,7 @@ __device__ __forceinline__ void traverse_persistent(
 		// ---- refill idle lanes (warp-uniform branch)
 		const uint32_t idle = __ballot_sync(kFullWarp, !has_ray);
 		const int num_idle = __popc(idle);
-		if(!exhausted && num_idle >= kRefillMinIdle)
+		if(!exhausted && num_idle >= min_idle)
 		{
 			uint32_t base = 0;
 			if(lane == 0)
@@ -420,7 +444,14 @@ __device__ __forceinline__ void traverse_persistent(
 				if(i < n && i >= base)
 				{
 					float4 a, b;
-					fetch(i, &a, &b);
+					if constexpr(MULTI)
+					{
+						fetch(i, &a, &b, &nodes, &tris);
+					}
+					else
+					{
+						fetch(i, &a, &b);
+					}
 					r = make_ray_traits(a.x, a.y, a.z, b.x, b.y, b.z);
 					t_min = a.w;
 					best_t = b.w;
@@ -431,6 +462,7 @@ __device__ __forceinline__ void traverse_persistent(
 					imask = 1u;
 					node_hits = 1u << r.oct;
 					tri_hits = 0;
+					next_hits = 0;
 					sp = 0;
 					ray = i;
 					has_ray = true;
@@ -447,7 +479,65 @@ __device__ __forceinline__ void traverse_persistent(
 			continue;
 		}
 
-		// ---- one traversal step
+		// ---- one node step, unless a triangle group is already parked
+		if(next_hits == 0u)
+		{
+			if(node_hits == 0u && sp > 0)
+			{
+				--sp;
+				const uint2 e = sp < kSharedStack ? s_stack[sp][tid] : l_stack[sp - kSharedStack];
+				child_base = e.x;
+				imask = e.y >> 8;
+				node_hits = e.y & 0xFFu;
+			}
+			if(node_hits)
+			{
+				const uint32_t key = 31u - __clz(node_hits);
+				node_hits &= ~(1u << key);
+				const uint32_t slot = key ^ r.oct;
+				const uint32_t child = child_base + __popc(imask & ((1u << slot) - 1u));
+				if(node_hits)
+				{
+					if(sp < kTraversalStackSize)
+					{
+						const uint2 e = make_uint2(child_base, (imask << 8) | node_hits);
+						if(sp < kSharedStack)
+						{
+							s_stack[sp][tid] = e;
+						}
+						else
+						{
+							l_stack[sp - kSharedStack] = e;
+						}
+						++sp;
+					}
+					else
+					{
+						*out_error |= PG_DEV_ERR_STACK;
+					}
+				}
+				uint32_t found_base;
+				const uint32_t hits = intersect_children(r, nodes, child, t_min, best_t, &child_base, &found_base, &imask);
+				if(COUNT) { ++node_count[MIXED && any_hit ? 1 : 0]; }
+				node_hits = hits >> 24;
+				const uint32_t found = hits & 0x00FFFFFFu;
+				if(found)
+				{
+					if(tri_hits == 0u)
+					{
+						tri_base = found_base;
+						tri_hits = found;
+					}
+					else
+					{
+						next_base = found_base;
+						next_hits = found;
+					}
+				}
+			}
+		}
+
+		// ---- one triangle test
 		if(tri_hits)
 		{
 			const uint32_t bit = __ffs(tri_hits) - 1u;
@@ -462,6 +552,7 @@ __device__ __forceinline__ void traverse_persistent(
 					best_t = t;
 					best_tri = k;
 					tri_hits = 0;
+					next_hits = 0;
 					node_hits = 0;
 					sp = 0;
 				}
@@ -476,37 +567,11 @@ __device__ __forceinline__ void traverse_persistent(
 					}
 				}
 			}
-		}
-		else
-		{
-			if(node_hits == 0u && sp > 0)
+			if(tri_hits == 0u)
 			{
-				--sp;
-				child_base = stack[sp].x;
-				imask = stack[sp].y >> 8;
-				node_hits = stack[sp].y & 0xFFu;
-			}
-			if(node_hits)
-			{
-				const uint32_t key = 31u - __clz(node_hits);
-				node_hits &= ~(1u << key);
-				const uint32_t slot = key ^ r.oct;
-				const uint32_t child = child_base + __popc(imask & ((1u << slot) - 1u));
-				if(node_hits)
-				{
-					if(sp < kTraversalStackSize)
-					{
-						stack[sp++] = make_uint2(child_base, (imask << 8) | node_hits);
-					}
-					else
-					{
-						*out_error |= PG_DEV_ERR_STACK;
-					}
-				}
-				const uint32_t hits = intersect_children(r, nodes, child, t_min, best_t, &child_base, &tri_base, &imask);
-				if(COUNT) { ++node_count[MIXED && any_hit ? 1 : 0]; }
-				node_hits = hits >> 24;
-				tri_hits = hits & 0x00FFFFFFu;
+				tri_base = next_base;
+				tri_hits = next_hits;
+				next_hits = 0u;
 			}
 		}
 

@@ -63,9 +63,16 @@ PGPU_SIGNATURES = [
     ("pgpu_scene_set_dome_pdf", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32]),
     ("pgpu_scene_launches", ctypes.c_int, [ctypes.c_uint64, _u64p]),
     ("pgpu_scene_light_pmf", ctypes.c_int, [ctypes.c_uint64, _f32p, _dblp, _u32p]),
+    ("pgpu_scene_autotune", ctypes.c_int,
+     [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p, _u32p,
+      _f32p]),
+    ("pgpu_scene_set_launch", ctypes.c_int, [ctypes.c_uint64, _u32p]),
+    ("pgpu_scene_get_launch", ctypes.c_int, [ctypes.c_uint64, _u32p]),
     ("pgpu_scene_light_pdf", ctypes.c_int, [ctypes.c_uint64, _f32p, _u32p, ctypes.c_uint64, _f32p]),
     ("pgpu_scenes_render", ctypes.c_int,
      [_u64p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32, _f32p]),
+    ("pgpu_scenes_render_wavefront", ctypes.c_int,
+     [_u64p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _f32p]),
     ("pgpu_scene_count", ctypes.c_int,
      [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _u64p]),
     ("pgpu_scene_profile", ctypes.c_int,
@@ -279,6 +286,18 @@ def render_scenes(render_scenes, spp, max_bounces=10000, estimator=BNEEPT, seed=
     return ms.value
 
 
+def render_scenes_wavefront(render_scenes, spp, max_bounces=10000, estimator=BNEEPT, seed=42) -> float:
+    """pgpu_scenes_render_wavefront: renders RenderScenes (spp[i] more samples each) as one
+    wavefront -- one path pool and one launch per kernel per iteration for all of them; returns
+    the batch's device ms."""
+    ids = np.array([rs.id for rs in render_scenes], np.uint64)
+    counts = np.array(spp, np.uint32)
+    ms = ctypes.c_float()
+    _check(load().pgpu_scenes_render_wavefront(_ptr(ids, ctypes.c_uint64), len(ids), _ptr(counts, ctypes.c_uint32),
+                                               max_bounces, estimator, seed, ctypes.byref(ms)))
+    return ms.value
+
+
 class RenderScene:
     """A scene resident on the GPU with its FP64 film (pgpu_scene_*)."""
 
@@ -338,6 +357,28 @@ class RenderScene:
         _check(load().pgpu_scene_profile(self.id, spp, max_bounces, estimator, seed, _ptr(ms, ctypes.c_double)))
         keys = ["prepare_ms", "regen_ms", "extend_ms", "shade_ms", "shadow_ms", "guide_infer_ms", "guide_train_ms"]
         return dict(zip(keys, ms.tolist()))
+
+    def autotune(self, spp, max_bounces=10000, estimator=BNEEPT, rebuild=True, cache_path=None,
+                 ignore_cache=False) -> dict:
+        """pgpu_scene_autotune: picks the scene's launch shapes; returns them with the calibration
+        render's device ms under the defaults and under the choice."""
+        cfg = np.zeros(4, np.uint32)
+        ms = np.zeros(4, np.float32)
+        flags = (1 if rebuild else 0) | (2 if ignore_cache else 0)
+        _check(load().pgpu_scene_autotune(self.id, spp, max_bounces, estimator, flags,
+                                          cache_path.encode() if cache_path else None, _ptr(cfg, ctypes.c_uint32),
+                                          _ptr(ms, ctypes.c_float)))
+        return {"capacity": int(cfg[0]), "refill": int(cfg[1]), "blocks_per_sm": int(cfg[2]), "leaf_tris": int(cfg[3]),
+                "ms_default": float(ms[0]), "ms_tuned": float(ms[1]), "trials": int(ms[2]), "from_cache": bool(ms[3])}
+
+    def set_launch(self, capacity=1 << 21, refill=8, blocks_per_sm=8, leaf_tris=3) -> None:
+        cfg = np.array([capacity, refill, blocks_per_sm, leaf_tris], np.uint32)
+        _check(load().pgpu_scene_set_launch(self.id, _ptr(cfg, ctypes.c_uint32)))
+
+    def launch(self) -> dict:
+        cfg = np.zeros(4, np.uint32)
+        _check(load().pgpu_scene_get_launch(self.id, _ptr(cfg, ctypes.c_uint32)))
+        return {"capacity": int(cfg[0]), "refill": int(cfg[1]), "blocks_per_sm": int(cfg[2]), "leaf_tris": int(cfg[3])}
 
     def light_pmf(self):
         """(pmf float32 [E], alias-table pmf float64 [E]) of the scene's emitters (pgpu_scene_light_pmf)."""
@@ -455,6 +496,7 @@ PH_SIGNATURES = [
     ("phGpuGetRenderInfo", None, [ctypes.c_uint64, _dblp, _u64p, _u64p, _u64p, _dblp]),
     ("phGpuGetLaunchCount", ctypes.c_uint64, [ctypes.c_uint64]),
     ("phGpuProfileRender", None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, _dblp]),
+    ("phGpuAutotune", ctypes.c_int, [ctypes.c_uint64, ctypes.c_char_p, ctypes.c_uint32, _u32p, _f32p]),
 ]
 
 
@@ -482,6 +524,17 @@ class CookedScene:
                                  _ptr(self.camera, ctypes.c_float)))
         self.num_materials = nm.value
         self.width, self.height, self.spp, self.estimator, self.sample_filter = (int(x) for x in dims)
+
+
+class FrameRegion(ctypes.Structure):
+    """PhFrameRegionInfo (ph_c_core_types.h)."""
+
+    _fields_ = [("x", ctypes.c_uint32), ("y", ctypes.c_uint32), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32), ("status", ctypes.c_int)]
+
+
+REGION_FINISHED = 1
+REGION_UPDATING = 2
 
 
 class PhotonEngine:
@@ -563,6 +616,18 @@ class PhotonEngine:
     def launch_count(self) -> int:
         return int(load().phGpuGetLaunchCount(self.id))
 
+    def autotune(self, cache_path=None, rebuild=True, ignore_cache=False) -> dict:
+        """phGpuAutotune: launch shapes of the updated scene for the session's spp and estimator."""
+        cfg = np.zeros(4, np.uint32)
+        ms = np.zeros(4, np.float32)
+        flags = (1 if rebuild else 0) | (2 if ignore_cache else 0)
+        ok = load().phGpuAutotune(self.id, cache_path.encode() if cache_path else None, flags,
+                                  _ptr(cfg, ctypes.c_uint32), _ptr(ms, ctypes.c_float))
+        if not ok:
+            raise PhotonGpuError(PG_ERR_SCENE, self.errors())
+        return {"capacity": int(cfg[0]), "refill": int(cfg[1]), "blocks_per_sm": int(cfg[2]), "leaf_tris": int(cfg[3]),
+                "ms_default": float(ms[0]), "ms_tuned": float(ms[1]), "trials": int(ms[2]), "from_cache": bool(ms[3])}
+
     def profile(self, mode: int, spp: int) -> dict:
         """phGpuProfileRender: mode 1 per-kernel timing, mode 2 traversal counting."""
         stats = np.zeros(14, np.float64)
@@ -580,6 +645,46 @@ class PhotonEngine:
         lib.phCreateFrame(ctypes.byref(fid), w, h)
         try:
             lib.phAquireFrameRaw(self.id, 0, fid.value)
+            data = _f32p()
+            lib.phGetFrameRgbData(fid.value, ctypes.byref(data))
+            return np.ctypeslib.as_array(data, shape=(h, w, 3)).copy()
+        finally:
+            lib.phDeleteFrame(fid.value)
+
+    def poll_region(self) -> Optional[Tuple[int, int, int, int, int]]:
+        """phAsyncPollUpdatedFrameRegion: (x, y, width, height, status) or None."""
+        r = FrameRegion()
+        if load().phAsyncPollUpdatedFrameRegion(self.id, ctypes.byref(r)):
+            return (r.x, r.y, r.width, r.height, r.status)
+        return None
+
+    def poll_regions(self, max_regions: int = 64, merged: bool = False):
+        """phAsyncPollUpdatedFrameRegions (or the merged variant): a list of (x, y, w, h, status)."""
+        arr = (FrameRegion * max_regions)()
+        lib = load()
+        if merged:
+            n = lib.phAsyncPollMergedUpdatedFrameRegions(self.id, 0, 1, arr, max_regions)
+        else:
+            n = lib.phAsyncPollUpdatedFrameRegions(self.id, 0, arr, max_regions)
+        return [(r.x, r.y, r.width, r.height, r.status) for r in arr[:n]]
+
+    def progress(self) -> Tuple[int, int, int]:
+        """phAsyncGetRenderProgress: (total work, work done, elapsed ms) in samples per pixel."""
+        class _Progress(ctypes.Structure):
+            _fields_ = [("total", ctypes.c_uint64), ("done", ctypes.c_uint64), ("ms", ctypes.c_uint64)]
+        p = _Progress()
+        load().phAsyncGetRenderProgress(self.id, ctypes.byref(p))
+        return p.total, p.done, p.ms
+
+    def peek(self, x: int = 0, y: int = 0, width: int = 0, height: int = 0) -> np.ndarray:
+        """phAsyncPeekFrameRaw of a rectangle (the whole frame by default) into a new frame:
+        float32 [H, W, 3] of the full frame, pixels outside the rectangle 0."""
+        lib = load()
+        w, h = self.dimension()
+        fid = ctypes.c_uint64()
+        lib.phCreateFrame(ctypes.byref(fid), w, h)
+        try:
+            lib.phAsyncPeekFrameRaw(self.id, 0, x, y, width or w, height or h, fid.value)
             data = _f32p()
             lib.phGetFrameRgbData(fid.value, ctypes.byref(data))
             return np.ctypeslib.as_array(data, shape=(h, w, 3)).copy()

@@ -90,11 +90,71 @@ def render_via_c_api(scene, tmp_path, seed=1, refine_mode="iterative", dome_pdf=
     return img, info
 
 
+# The benchmarked configurations' geometry at reduced resolution (tests/golden/make_golden_images.py):
+# name -> (scene factory, GPU spp, block size of the block relMSE). The meshes reach the GPU as
+# binary PLY files through geometry(ply) (the reference parsed the same triangles as SDL text).
+LARGE_WORKLOADS = {
+    # 1,310,726 triangles, 2 quad lights + environment, GGX in 64 groups, depth 10, 128 x 128
+    "c2_ggx1m_bneept": (lambda spp: scenes.ggx_sphere(level=8, width=128, height=128, spp=spp, max_bounces=10),
+                        65536, 4),
+    # 2,000,042 triangles, light through a 0.05-wide slit, 30 % rough glass boxes, depth 10, 32 x 32
+    "slit_room_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10), 65536, 4),
+    # 174,802 triangles, 1,000 lights of lognormal radiance, GGX roughness 0.02-0.8, depth 12, 64 x 64
+    "city_tile_bneept": (lambda spp: scenes.city(64, 64, spp, 12, blocks=40, num_lights=1000), 16384, 4),
+}
+
+
 def test_golden_images_present():
     d = np.load(IMAGES)
     for name in WORKLOADS:
         assert d[name].shape == (64, 64, 3)
         assert np.all(np.isfinite(d[name])) and d[name].mean() > 0
+    for name, (factory, _, _) in LARGE_WORKLOADS.items():
+        sc = factory(1)
+        assert d[name].shape == (sc.height, sc.width, 3)
+        assert np.all(np.isfinite(d[name])) and d[name].mean() > 0
+
+
+def _block(a, k):
+    h, w, c = a.shape
+    return a.reshape(h // k, k, w // k, k, c).mean(axis=(1, 3))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(LARGE_WORKLOADS))
+def test_benchmarked_geometry_matches_reference(gpu_lib, tmp_path, name):
+    """Image parity on the geometry of the benchmarked configurations: the 1M-triangle GGX scene,
+    the 2M-triangle slit room with its glass, and a 1,000-light city tile, each against a
+    reference render of 16,384-65,536 spp at the same spp on the GPU. Bars: relMSE <= 1e-3 at
+    full resolution and on k x k block means, per-channel means within 1 %."""
+    d = np.load(IMAGES)
+    ref = d[name]
+    factory, spp, k = LARGE_WORKLOADS[name]
+    scene = factory(spp)
+    assert scene.max_bounces == int(d[name + "__bounces"]) and spp == int(d[name + "__spp"])
+    img, _ = render_via_c_api(scene, tmp_path, mesh_format="ply")
+    err = rel_mse(img, ref)
+    err_blocks = rel_mse(_block(img, k), _block(ref, k))
+    means = img.mean(axis=(0, 1)) / ref.mean(axis=(0, 1))
+    print(f"{name}: relMSE {err:.2e}, {k}x{k}-block relMSE {err_blocks:.2e}, mean ratio {means}")
+    assert err <= 1e-3, f"relMSE {err:.3e}"
+    assert err_blocks <= 1e-3, f"block relMSE {err_blocks:.3e}"
+    assert np.all(np.abs(means - 1.0) < 0.01), f"channel means differ: {means}"
+
+
+@pytest.mark.gpu
+def test_c2_error_at_bench_spp(gpu_lib, tmp_path):
+    """The error the benchmarked render carries: the 1M-triangle GGX scene at the bench's 256 spp
+    against the 65,536-spp reference render (at 128 x 128), relMSE as the bench line states it.
+    The error of an n-spp render falls as 1/n, which gives the spp that reaches relMSE 1e-3."""
+    ref = np.load(IMAGES)["c2_ggx1m_bneept"]
+    img, _ = render_via_c_api(scenes.ggx_sphere(level=8, width=128, height=128, spp=256, max_bounces=10), tmp_path,
+                              mesh_format="ply")
+    err = rel_mse(img, ref)
+    print(f"c2 at 256 spp: relMSE {err:.3e} against the 65,536-spp reference; 1e-3 at ~{256 * err / 1e-3:.0f} spp")
+    # Monte Carlo error at 256 spp on this scene: well under 1e-2, and the means agree within 1 %
+    assert err < 1e-2
+    assert np.all(np.abs(img.mean(axis=(0, 1)) / ref.mean(axis=(0, 1)) - 1.0) < 0.01)
 
 
 @pytest.mark.gpu
