@@ -539,7 +539,11 @@ def run_flat(args) -> None:
     rss = [photon_gpu.RenderScene(sc, builder=args.builder) for sc in scene_list]
     build_s = time.time() - t0
     tuned = None
-    if args.autotune:
+    if args.autotune and len(rss) > 1 and args.batch_mode == "wavefront":
+        # launch shapes of the one-wavefront render (untimed calibration wavefronts)
+        tuned = [photon_gpu.autotune_wavefront(rss, [sc.spp for sc in scene_list],
+                                               max_bounces=scene_list[0].max_bounces)]
+    elif args.autotune:
         # launch shapes per scene (untimed calibration renders; the leaf-size rebuild only for
         # single-scene workloads)
         tuned = [rs.autotune(sc.spp, max_bounces=sc.max_bounces, rebuild=len(rss) == 1)
@@ -550,7 +554,18 @@ def run_flat(args) -> None:
 
     def one_pass(read_back: bool = False):
         ms, launches = 0.0, 0
-        if args.concurrency > 1 and len(scene_list) > 1:
+        if args.batch_mode == "wavefront" and len(scene_list) > 1:
+            # every scene in one wavefront: one path pool, one launch per kernel per iteration
+            for rs in rss:
+                rs.clear()
+            ms = photon_gpu.render_scenes_wavefront(rss, [sc.spp for sc in scene_list],
+                                                    max_bounces=scene_list[0].max_bounces, seed=seed)
+            launches = rss[0].launches()
+            if read_back:
+                for rs in rss:
+                    rs.film(with_sums=False)
+            return ms, launches
+        if args.batch_mode == "streams" and args.concurrency > 1 and len(scene_list) > 1:
             # all scenes of the step at once, `concurrency` of them in flight on their own streams;
             # the step's time is the batch's span
             for rs in rss:
@@ -620,7 +635,8 @@ def run_flat(args) -> None:
                    "resolution": sorted({f"{sc.width}x{sc.height}" for sc in scene_list})[:4],
                    "spp": spps if len(spps) <= 4 else [spps[0], spps[-1]],
                    "max_bounces": scene_list[0].max_bounces, "estimator": "bneept", "bvh": args.builder,
-                   "concurrency": args.concurrency if len(scene_list) > 1 else 1,
+                   "batch_mode": args.batch_mode if len(scene_list) > 1 else "single",
+                   "concurrency": args.concurrency if len(scene_list) > 1 and args.batch_mode == "streams" else 1,
                    "l2": "256 MiB write between timed steps", "parallelism": f"replicas x{world}",
                    "tuned": (tuned[0] if tuned and len(tuned) == 1 else
                              {"scenes": len(tuned), "ms_default": sum(t["ms_default"] for t in tuned),
@@ -680,6 +696,9 @@ def main() -> None:
     ap.add_argument("--builder", default="sah", choices=["sah", "gpu"], help="BVH builder of flat workloads")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="render with the fixed default launch shapes instead of autotuned ones")
+    ap.add_argument("--batch-mode", default="wavefront", choices=["wavefront", "streams", "serial"],
+                    help="multi-scene workloads: one wavefront for all scenes, scenes on concurrent streams, "
+                         "or one after another")
     ap.add_argument("--concurrency", type=int, default=4,
                     help="scenes of a multi-scene workload rendered at once (1: one after another)")
     args = ap.parse_args()

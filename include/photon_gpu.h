@@ -112,9 +112,16 @@ PGPU_API int pgpu_guide_forward(const float* params, const float* features, uint
 
 /* Training loss -sum_i w_i log q(d_i | x_i) / sum_i w_i of a batch (features [n][7], unit
  * directions [n][3], weights [n]) and its gradient with respect to all parameters
- * (out_grads[29480]); forward pass on the tensor cores, backward in FP32. */
+ * (out_grads[29480]). Forward and backward passes on the tensor cores (BF16 operands, FP32
+ * accumulation; weight gradients accumulated in tensor memory). */
 PGPU_API int pgpu_guide_gradients(const float* params, const float* features, const float* dirs,
                        const float* weights, uint64_t n, float* out_loss, float* out_grads);
+/* As pgpu_guide_gradients; flags PG_GUIDE_BACKWARD_CUDA_CORES runs the backward pass in FP32 on
+ * the CUDA cores instead (a cross-check of the tensor-core pass). */
+#define PG_GUIDE_BACKWARD_CUDA_CORES 1u
+PGPU_API int pgpu_guide_gradients_ex(const float* params, const float* features, const float* dirs,
+                                     const float* weights, uint64_t n, uint32_t flags, float* out_loss,
+                                     float* out_grads);
 
 /* `steps` Adam steps (learning rate lr) over consecutive batches of `batch` samples of the data
  * set (cycled); params is updated in place, out_losses[steps] (optional) receives each step's loss. */
@@ -198,6 +205,12 @@ PGPU_API int pgpu_scene_clear(uint64_t id);
  * renders of at most 2^31 paths each. *out_ms: device milliseconds of the whole batch. */
 PGPU_API int pgpu_scenes_render_wavefront(const uint64_t* ids, uint32_t n, const uint32_t* spp, uint32_t max_bounces,
                                           uint32_t estimator, uint64_t seed, float* out_ms);
+/* The launch shapes of pgpu_scenes_render_wavefront for these scenes: the autotuner's coordinate
+ * descent (pool depth, refill threshold, blocks per SM) over calibration wavefronts of the batch at
+ * a sixteenth of its samples, into scratch films. The choice is set on the first scene, whose pool
+ * runs the wavefront. out_config [4] and out_ms [4] as in pgpu_scene_autotune. */
+PGPU_API int pgpu_scenes_autotune_wavefront(const uint64_t* ids, uint32_t n, const uint32_t* spp, uint32_t max_bounces,
+                                            uint32_t estimator, uint32_t* out_config, float* out_ms);
 /* Renders several scenes at once: scene ids[i] gets spp[i] more samples (numbered after its
  * earlier ones) with the same bounce cap, estimator and seed. Up to `concurrency` host threads
  * render one scene each at a time on the scene's own stream, so small scenes fill the GPU

@@ -31,10 +31,12 @@ void launch_forward(const unsigned char* d_image, const float* d_features, uint3
 // d_acts: [n][4][64] scratch.
 // With d_n set, at most n samples and the count is read from device memory (graph-safe). With
 // clamp_factor > 0, sample weights are first capped (in place) at clamp_factor x their mean.
+// tensor_cores: the backward pass as BF16 tcgen05 MMAs with FP32 accumulation in tensor memory
+// (default); false: the FP32 CUDA-core backward, kept as a cross-check.
 void launch_gradients(const float* d_params, const unsigned char* d_image, const float* d_features,
                       const float4* d_dirw, uint32_t n, float* d_raw, __nv_bfloat16* d_acts,
                       float* d_grads, float* d_loss, float* d_total, uint32_t* d_error, cudaStream_t s,
-                      const uint32_t* d_n = nullptr, float clamp_factor = 0.0f);
+                      const uint32_t* d_n = nullptr, float clamp_factor = 0.0f, bool tensor_cores = true);
 
 // One Adam step (beta 0.9 / 0.999, eps 1e-8) on the FP32 parameters; zeroes d_grads. The step
 // number t is *d_step + 1, and *d_step is incremented afterwards (graph-safe).

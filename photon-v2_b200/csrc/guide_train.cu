@@ -15,6 +15,7 @@
 #include "guide_mlp.h"
 
 #include "pg_runtime.h"
+#include "tcgen05.cuh"
 #include "../../include/photon_gpu.h"
 
 #include <cuda_bf16.h>
@@ -298,6 +299,358 @@ backward_kernel(const float* __restrict__ params, const float* __restrict__ feat
 	}
 }
 
+// ---------------------------------------------------------------------------------------------
+// Backward pass on the tensor cores (tcgen05, BF16 operands, FP32 accumulators in TMEM).
+//
+// Per 128-sample tile and layer l (4 down to 0), with G_l = d loss / d z_l [128 x out_l] and
+// X_l the layer's input [128 x in_l]:
+//   dW_l += X_l^T G_l      MMA M = 128 (the layer's inputs, padded; one extra row of ones gives
+//                           the bias gradient sum_t G_l[t]), N = out_l, K = 128 samples;
+//   dX_l  = G_l W_l^T      MMA M = 128 samples, N = in_l = 64, K = out_l (layers 4..1);
+//   G_l-1 = dX_l where X_l > 0 (the ReLU that produced X_l).
+// The weight gradients stay in tensor memory across all tiles a CTA processes and reach global
+// memory once per CTA. Operands: G_l as sample rows (K = out_l) for dX, and the transposed
+// X_l^T / G_l^T (K = samples) for dW, written by each thread for its own sample; the transposed
+// buffers' K-chunk stride carries 16 bytes of padding so that the 8 sample groups a warp writes
+// land in different banks.
+
+namespace tcb
+{
+
+using namespace tc;
+
+constexpr int kThreads = 128;
+constexpr uint32_t kLboG = kTile * 16u;                // G rows (samples) x K = outputs: 2048
+constexpr uint32_t kLboXT = kTile * 16u + 16u;         // X^T: 128 rows x K = samples, padded: 2064
+constexpr uint32_t kLboGT = kHidden * 16u + 16u;       // G^T: 64 rows x K = samples, padded: 1040
+constexpr uint32_t kLboW = kHidden * 16u;              // W_l: 64 rows (inputs) x K = outputs: 1024
+
+constexpr int kBwHidden = kHidden * kHidden * 2;       // 8,192
+constexpr int kOffBw = 0;                              // W1, W2, W3, W4 (W4: K = 48)
+constexpr int kOffG = kOffBw + 3 * kBwHidden + kHidden * kOutPad * 2;     // 30,720
+constexpr int kOffXT = kOffG + kTile * kHidden * 2;                       // 47,104
+constexpr int kOffGT = kOffXT + (kTile / 8) * static_cast<int>(kLboXT);   // 80,128
+constexpr int kOffBar = kOffGT + (kTile / 8) * static_cast<int>(kLboGT);  // 96,768
+constexpr int kOffSlot = kOffBar + 8;
+// More than half an SM's shared memory: one CTA per SM, so that each CTA's 512 TMEM columns are free.
+constexpr int kSmemBytes = 120 * 1024;
+static_assert(kOffSlot + 8 <= kSmemBytes && kSmemBytes <= 227 * 1024, "shared memory");
+static_assert(kOffG % 16 == 0 && kOffXT % 16 == 0 && kOffGT % 16 == 0 && kOffBar % 8 == 0, "alignment");
+
+// TMEM columns: the dX accumulator, then the weight gradients of every layer (rows = the layer's
+// inputs, columns = its outputs).
+constexpr uint32_t kColAcc = 0;
+constexpr uint32_t kColW0a = 64;    // inputs 0..127 of layer 0
+constexpr uint32_t kColW0b = 128;   // inputs 128..223 of layer 0, bias in row 96
+// layer l >= 1: 192, 256, 320, 384 (bias in row 64)
+PG_HD constexpr uint32_t col_w(int l) { return l == 0 ? kColW0a : 128u + 64u * static_cast<uint32_t>(l); }
+constexpr uint32_t kTmemColsB = 512;
+
+__device__ __forceinline__ void st_bf16(unsigned char* base, uint32_t off, float v)
+{
+	*reinterpret_cast<__nv_bfloat16*>(base + off) = __float2bfloat16_rn(v);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+backward_tc_kernel(const float* __restrict__ params, const float* __restrict__ features,
+                   const float4* __restrict__ dirw, const float* __restrict__ raw_out,
+                   const __nv_bfloat16* __restrict__ acts, uint32_t n_max, const uint32_t* __restrict__ d_n,
+                   const float* __restrict__ total_weight, float* __restrict__ grads, float* __restrict__ loss,
+                   uint32_t* __restrict__ error)
+{
+	const uint32_t n = d_n ? min(*d_n, n_max) : n_max;
+	const uint32_t num_tiles = (n + kTile - 1) / kTile;
+	if(blockIdx.x >= num_tiles)
+	{
+		return;   // uniform per CTA, before any barrier or tensor-memory use
+	}
+	extern __shared__ __align__(128) unsigned char smem[];
+	const uint32_t tid = threadIdx.x;
+	const uint32_t warp = tid >> 5;
+
+	// W_1..W_4 as B operands of dX: [64 rows = layer inputs][K = layer outputs], BF16 as the
+	// forward pass rounds them
+	for(uint32_t e = tid; e < 3u * kHidden * kHidden + kHidden * kOutPad; e += kThreads)
+	{
+		uint32_t l, i, o, out;
+		if(e < 3u * kHidden * kHidden)
+		{
+			l = 1u + e / (kHidden * kHidden);
+			i = (e % (kHidden * kHidden)) / kHidden;
+			o = e % kHidden;
+			out = kHidden;
+		}
+		else
+		{
+			l = 4u;
+			i = (e - 3u * kHidden * kHidden) / kOutPad;
+			o = (e - 3u * kHidden * kHidden) % kOutPad;
+			out = kOut;
+		}
+		const int w_off[5] = {kOffW0, kOffW1, kOffW2, kOffW3, kOffW4};
+		const float w = o < out ? params[w_off[l] + i * out + o] : 0.0f;
+		st_bf16(smem + kOffBw + (l - 1u) * kBwHidden, core_offset_lbo(i, o, kLboW), w);
+	}
+	const uint32_t bar = smem_u32(smem + kOffBar);
+	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kOffSlot);
+	if(tid == 0)
+	{
+		mbar_init(bar, 1);
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	if(warp == 0)
+	{
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+		             :: "r"(smem_u32(tmem_slot)), "r"(kTmemColsB) : "memory");
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+	}
+	fence_async_smem();
+	fence_before_sync();
+	__syncthreads();
+	fence_after_sync();
+	const uint32_t tmem = *tmem_slot;
+	const uint32_t tmem_row = tmem + ((warp * 32u) << 16);
+
+	unsigned char* gbuf = smem + kOffG;
+	unsigned char* xt = smem + kOffXT;
+	unsigned char* gt = smem + kOffGT;
+	const uint32_t a_g = smem_u32(gbuf), a_xt = smem_u32(xt), a_gt = smem_u32(gt);
+
+	uint32_t phase = 0;
+	bool failed = false;
+	// the staged operands -> one dW chain (and, for layers 4..1, one dX chain), committed and awaited
+	auto run = [&](uint32_t col_w, uint32_t n_out, bool acc_w, int dx_layer) -> bool
+	{
+		fence_async_smem();
+		fence_before_sync();
+		__syncthreads();
+		if(tid == 0)
+		{
+			fence_after_sync();
+			const uint32_t idesc_w = instr_desc(kTile, n_out);
+			for(uint32_t ks = 0; ks < kTile / 16u; ++ks)
+			{
+				const uint64_t ad = smem_desc(a_xt + ks * 2u * kLboXT, kLboXT, 128u);
+				const uint64_t bd = smem_desc(a_gt + ks * 2u * kLboGT, kLboGT, 128u);
+				mma_bf16(tmem + col_w, ad, bd, idesc_w, (acc_w || ks > 0) ? 1u : 0u);
+			}
+			if(dx_layer >= 1)
+			{
+				const uint32_t idesc_x = instr_desc(kTile, kHidden);
+				const uint32_t w_base = smem_u32(smem + kOffBw + (dx_layer - 1) * kBwHidden);
+				for(uint32_t ks = 0; ks < n_out / 16u; ++ks)
+				{
+					const uint64_t ad = smem_desc(a_g + ks * 2u * kLboG, kLboG, 128u);
+					const uint64_t bd = smem_desc(w_base + ks * 2u * kLboW, kLboW, 128u);
+					mma_bf16(tmem + kColAcc, ad, bd, idesc_x, ks > 0 ? 1u : 0u);
+				}
+			}
+			mma_commit(bar);
+		}
+		const bool ok = mbar_wait(bar, phase);
+		if(__syncthreads_or(ok ? 0 : 1))
+		{
+			if(!ok)
+			{
+				mbar_wait(bar, phase);   // bounded: do not free TMEM under running MMAs
+			}
+			return false;
+		}
+		phase ^= 1u;
+		fence_after_sync();
+		return true;
+	};
+
+	bool first = true;
+	for(uint32_t tile = blockIdx.x; tile < num_tiles && !failed; tile += gridDim.x, first = false)
+	{
+		const uint32_t row = tile * kTile + tid;
+		const bool valid = row < n;
+
+		// ---- d loss / d raw outputs (48 columns, the last 8 zero)
+		float g[kHidden];
+		#pragma unroll
+		for(int c = 0; c < kHidden; ++c)
+		{
+			g[c] = 0.0f;
+		}
+		float loss_term = 0.0f;
+		if(valid)
+		{
+			float raw[kOut];
+			#pragma unroll
+			for(int c = 0; c < kOut; ++c)
+			{
+				raw[c] = raw_out[static_cast<size_t>(row) * kOut + c];
+			}
+			const float4 dw = dirw[row];
+			const float scale = -dw.w / fmaxf(*total_weight, 1e-30f);
+			output_gradient(raw, v3(dw.x, dw.y, dw.z), scale, g, &loss_term);
+		}
+		for(int o = 16; o > 0; o >>= 1)
+		{
+			loss_term += __shfl_xor_sync(0xFFFFFFFFu, loss_term, o);
+		}
+		if((tid & 31u) == 0u && loss_term != 0.0f)
+		{
+			atomicAdd(loss, loss_term);
+		}
+
+		// ---- layers 4..1: dW_l and dX_l together
+		for(int l = 4; l >= 1 && !failed; --l)
+		{
+			const uint32_t n_out = l == 4 ? static_cast<uint32_t>(kOutPad) : static_cast<uint32_t>(kHidden);
+			float x[kHidden];
+			const uint4* src = reinterpret_cast<const uint4*>(acts + (static_cast<size_t>(row) * kHiddenLayers + (l - 1)) * kHidden);
+			#pragma unroll
+			for(int c = 0; c < kHidden / 8; ++c)
+			{
+				const uint4 q = valid ? src[c] : make_uint4(0u, 0u, 0u, 0u);
+				const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+				#pragma unroll
+				for(int j = 0; j < 4; ++j)
+				{
+					x[8 * c + 2 * j] = __bfloat162float(__ushort_as_bfloat16(static_cast<unsigned short>(w4[j] & 0xFFFFu)));
+					x[8 * c + 2 * j + 1] = __bfloat162float(__ushort_as_bfloat16(static_cast<unsigned short>(w4[j] >> 16)));
+				}
+			}
+			// X_l^T (+ the ones row) and G_l^T, transposed; G_l as this sample's row
+			#pragma unroll
+			for(int f = 0; f < kHidden; ++f)
+			{
+				st_bf16(xt, core_offset_lbo(static_cast<uint32_t>(f), tid, kLboXT), x[f]);
+			}
+			st_bf16(xt, core_offset_lbo(kHidden, tid, kLboXT), 1.0f);
+			#pragma unroll
+			for(int o = 0; o < kHidden; ++o)
+			{
+				if(o < static_cast<int>(n_out))
+				{
+					st_bf16(gt, core_offset_lbo(static_cast<uint32_t>(o), tid, kLboGT), g[o]);
+				}
+			}
+			#pragma unroll
+			for(int c = 0; c < kHidden / 8; ++c)
+			{
+				if(c * 8 < static_cast<int>(n_out))
+				{
+					uint4 q;
+					q.x = pack_bf16x2(g[8 * c + 0], g[8 * c + 1]);
+					q.y = pack_bf16x2(g[8 * c + 2], g[8 * c + 3]);
+					q.z = pack_bf16x2(g[8 * c + 4], g[8 * c + 5]);
+					q.w = pack_bf16x2(g[8 * c + 6], g[8 * c + 7]);
+					*reinterpret_cast<uint4*>(gbuf + core_offset_lbo(tid, static_cast<uint32_t>(8 * c), kLboG)) = q;
+				}
+			}
+			if(!run(col_w(l), n_out, !first, l))
+			{
+				failed = true;
+				break;
+			}
+			// G_l-1 = dX_l through the ReLU that produced X_l
+			float acc[kHidden];
+			#pragma unroll
+			for(int c = 0; c < 4; ++c)
+			{
+				tmem_ld16(tmem_row + kColAcc + c * 16, acc + c * 16);
+			}
+			tmem_wait_ld();
+			#pragma unroll
+			for(int c = 0; c < kHidden; ++c)
+			{
+				g[c] = x[c] > 0.0f ? acc[c] : 0.0f;
+			}
+			fence_before_sync();
+			__syncthreads();   // every thread's accumulator row is read before the next chain
+		}
+		if(failed)
+		{
+			break;
+		}
+
+		// ---- layer 0: dW_0 in two halves of its 224 one-blob inputs
+		float f7[kInputs];
+		#pragma unroll
+		for(int i = 0; i < kInputs; ++i)
+		{
+			f7[i] = valid ? features[static_cast<size_t>(row) * 8 + i] : 0.0f;
+		}
+		#pragma unroll
+		for(int o = 0; o < kHidden; ++o)
+		{
+			st_bf16(gt, core_offset_lbo(static_cast<uint32_t>(o), tid, kLboGT), g[o]);
+		}
+		for(int half = 0; half < 2; ++half)
+		{
+			const int k0 = half * 128, k1 = half == 0 ? 128 : kIn;
+			for(int k = k0; k < k1; ++k)
+			{
+				st_bf16(xt, core_offset_lbo(static_cast<uint32_t>(k - k0), tid, kLboXT), one_blob(f7[k / kBins], k % kBins));
+			}
+			if(half == 1)
+			{
+				st_bf16(xt, core_offset_lbo(static_cast<uint32_t>(kIn - 128), tid, kLboXT), 1.0f);
+			}
+			if(!run(half == 0 ? kColW0a : kColW0b, kHidden, !first, 0))
+			{
+				failed = true;
+				break;
+			}
+			fence_before_sync();
+			__syncthreads();
+		}
+	}
+
+	if(!failed)
+	{
+		// ---- the CTA's weight gradients to global memory: thread t holds row t of each block
+		auto flush = [&](uint32_t col, uint32_t n_out, int w_off, int b_off, uint32_t rows, uint32_t bias_row,
+		                 uint32_t first_input, uint32_t out_stride)
+		{
+			float v[kHidden];
+			for(uint32_t c = 0; c < n_out; c += 16)
+			{
+				tmem_ld16(tmem_row + col + c, v + c);
+			}
+			tmem_wait_ld();
+			if(tid < rows)
+			{
+				float* dst = grads + w_off + (first_input + tid) * out_stride;
+				for(uint32_t c = 0; c < out_stride; ++c)
+				{
+					if(v[c] != 0.0f) { atomicAdd(dst + c, v[c]); }
+				}
+			}
+			else if(tid == bias_row)
+			{
+				for(uint32_t c = 0; c < out_stride; ++c)
+				{
+					if(v[c] != 0.0f) { atomicAdd(grads + b_off + c, v[c]); }
+				}
+			}
+		};
+		flush(kColW0a, kHidden, kOffW0, kOffB0, 128u, 0xFFFFFFFFu, 0u, kHidden);
+		flush(kColW0b, kHidden, kOffW0, kOffB0, static_cast<uint32_t>(kIn - 128), static_cast<uint32_t>(kIn - 128),
+		      128u, kHidden);
+		flush(col_w(1), kHidden, kOffW1, kOffB1, kHidden, kHidden, 0u, kHidden);
+		flush(col_w(2), kHidden, kOffW2, kOffB2, kHidden, kHidden, 0u, kHidden);
+		flush(col_w(3), kHidden, kOffW3, kOffB3, kHidden, kHidden, 0u, kHidden);
+		flush(col_w(4), kOutPad, kOffW4, kOffB4, kHidden, kHidden, 0u, kOut);
+	}
+	else if(tid == 0)
+	{
+		atomicOr(error, PG_DEV_ERR_GUIDE_WAIT);
+	}
+	fence_before_sync();
+	__syncthreads();
+	if(warp == 0)
+	{
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTmemColsB) : "memory");
+	}
+}
+
+}// end namespace tcb
+
 __global__ void adam_kernel(float* __restrict__ params, float* __restrict__ grads, float* __restrict__ m,
                             float* __restrict__ v, uint32_t count, float lr, float beta1, float beta2,
                             float eps, const uint32_t* __restrict__ step)
@@ -327,7 +680,7 @@ __global__ void step_kernel(uint32_t* step)
 void launch_gradients(const float* d_params, const unsigned char* d_image, const float* d_features,
                       const float4* d_dirw, uint32_t n, float* d_raw, __nv_bfloat16* d_acts,
                       float* d_grads, float* d_loss, float* d_total, uint32_t* d_error, cudaStream_t s,
-                      const uint32_t* d_n, float clamp_factor)
+                      const uint32_t* d_n, float clamp_factor, bool tensor_cores)
 {
 	if(n == 0)
 	{
@@ -345,6 +698,23 @@ void launch_gradients(const float* d_params, const unsigned char* d_image, const
 		PG_CUDA_CHECK(cudaGetLastError());
 	}
 	launch_forward(d_image, d_features, n, d_raw, d_acts, d_error, s, d_n);
+	if(tensor_cores)
+	{
+		static const bool configured_tc = []
+		{
+			PG_CUDA_CHECK(cudaFuncSetAttribute(tcb::backward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			                                   tcb::kSmemBytes));
+			return true;
+		}();
+		(void)configured_tc;
+		// about four tiles per CTA: each CTA adds its weight gradients to global memory once
+		const uint32_t tiles = (n + kTile - 1) / kTile;
+		const uint32_t grid = std::max(1u, std::min(tiles, static_cast<uint32_t>(sm_count()) / 4u));
+		tcb::backward_tc_kernel<<<grid, tcb::kThreads, tcb::kSmemBytes, s>>>(d_params, d_features, d_dirw, d_raw, d_acts,
+		                                                                     n, d_n, d_total, d_grads, d_loss, d_error);
+		PG_CUDA_CHECK(cudaGetLastError());
+		return;
+	}
 	constexpr int smem_bytes = 2 * kBlock * kPitch * sizeof(float);
 	static const bool configured = []
 	{
@@ -395,6 +765,12 @@ extern "C" {
 int pgpu_guide_gradients(const float* params, const float* features, const float* dirs, const float* weights,
                          uint64_t n, float* out_loss, float* out_grads)
 {
+	return pgpu_guide_gradients_ex(params, features, dirs, weights, n, 0u, out_loss, out_grads);
+}
+
+int pgpu_guide_gradients_ex(const float* params, const float* features, const float* dirs, const float* weights,
+                            uint64_t n, uint32_t flags, float* out_loss, float* out_grads)
+{
 	return guarded([&]
 	{
 		if(!params || !out_grads || n == 0 || !features || !dirs || !weights)
@@ -421,7 +797,7 @@ int pgpu_guide_gradients(const float* params, const float* features, const float
 		guide::pack_image(d_params.get(), d_image.get(), s);
 		guide::launch_gradients(d_params.get(), d_image.get(), d_feat.get(), d_dirw.get(), static_cast<uint32_t>(n),
 		                        d_raw.get(), d_acts.get(), d_grads.get(), d_scalars.get(), d_scalars.get() + 1,
-		                        d_err.get(), s);
+		                        d_err.get(), s, nullptr, 0.0f, (flags & PG_GUIDE_BACKWARD_CUDA_CORES) == 0u);
 		float scalars[2] = {0.0f, 0.0f};
 		uint32_t err = 0;
 		PG_CUDA_CHECK(cudaMemcpyAsync(out_grads, d_grads.get(), d_grads.bytes(), cudaMemcpyDeviceToHost, s));

@@ -358,6 +358,49 @@ int pgpu_scenes_render_wavefront(const uint64_t* ids, uint32_t n, const uint32_t
 	});
 }
 
+int pgpu_scenes_autotune_wavefront(const uint64_t* ids, uint32_t n, const uint32_t* spp, uint32_t max_bounces,
+                                   uint32_t estimator, uint32_t* out_config, float* out_ms)
+{
+	return guarded([&]
+	{
+		if(n == 0 || !ids || !spp)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scenes_autotune_wavefront: no scenes");
+		}
+		if(estimator > PG_EST_BVPTDL)
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scenes_autotune_wavefront: unknown estimator");
+		}
+		std::vector<std::shared_ptr<RenderObject>> objects;
+		std::vector<const RenderScene*> scenes;
+		std::vector<uint32_t> counts(spp, spp + n);
+		for(uint32_t i = 0; i < n; ++i)
+		{
+			objects.push_back(get_render(ids[i]));
+			scenes.push_back(objects.back()->scene.get());
+		}
+		RenderParams p;
+		p.max_bounces = max_bounces;
+		p.estimator = estimator;
+		p.seed = 0x2545F4914F6CDD1Dull;
+		const AutotuneResult a = objects[0]->scene->autotune_batch(scenes, counts, p);
+		if(out_config)
+		{
+			out_config[0] = a.config.capacity;
+			out_config[1] = a.config.refill;
+			out_config[2] = a.config.blocks_per_sm;
+			out_config[3] = a.config.leaf_tris;
+		}
+		if(out_ms)
+		{
+			out_ms[0] = a.ms_default;
+			out_ms[1] = a.ms_tuned;
+			out_ms[2] = static_cast<float>(a.trials);
+			out_ms[3] = 0.0f;
+		}
+	});
+}
+
 int pgpu_scenes_render(const uint64_t* ids, uint32_t n, const uint32_t* spp, uint32_t max_bounces,
                        uint32_t estimator, uint64_t seed, uint32_t concurrency, float* out_ms)
 {

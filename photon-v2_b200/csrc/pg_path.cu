@@ -286,7 +286,10 @@ __device__ __forceinline__ uint32_t alloc_slot(uint32_t* counter)
 
 // ---------------------------------------------------------------------------------------------
 
-__global__ void prepare_kernel(RenderCounters* c, uint32_t capacity)
+// parity: the iteration's place in the ping-pong pair. Training samples are made in odd
+// iterations and trained on at the end of the following even one, so the count of samples is
+// reset only when an odd iteration starts.
+__global__ void prepare_kernel(RenderCounters* c, uint32_t capacity, uint32_t parity)
 {
 	if(threadIdx.x != 0 || blockIdx.x != 0)
 	{
@@ -307,7 +310,10 @@ __global__ void prepare_kernel(RenderCounters* c, uint32_t capacity)
 	c->fetch_shadow = 0;
 	c->guided_total += c->n_guided;
 	c->n_guided = 0;
-	c->n_train = 0;
+	if(parity)
+	{
+		c->n_train = 0;
+	}
 	c->n_refine = 0;
 	c->n_refine_mutual = 0;
 	for(uint32_t k = 0; k < kOrderLists; ++k)
@@ -899,7 +905,7 @@ shade_kernel(ShadeArgs a)
 				continues = false;
 			}
 			next_meta = (bounce + 1u) | (nee_samplable ? kMetaPrevNee : 0u) | (stop_after ? kMetaStopAfter : 0u) |
-			            (guided && a.guide.train_cap ? kMetaGuideRec : 0u) | (sid << kMetaSceneShift);
+			            (guided && a.guide.mark ? kMetaGuideRec : 0u) | (sid << kMetaSceneShift);
 		}
 
 		uint32_t slot = 0;
@@ -1714,6 +1720,17 @@ AutotuneResult RenderScene::autotune(const RenderParams& base, bool rebuild, con
 		return best;
 	};
 
+	descend(result, measure, rebuild && m_bvh_builder == PG_BVH_HOST_SAH);
+	if(cache_path)
+	{
+		append_tuning(cache_path, key, result.config);
+	}
+	return result;
+}
+
+void RenderScene::descend(AutotuneResult& result, const std::function<float(const LaunchConfig&)>& measure,
+                          bool leaf_size)
+{
 	LaunchConfig best = m_launch;
 	float best_ms = measure(best);
 	result.ms_default = best_ms;
@@ -1739,17 +1756,51 @@ AutotuneResult RenderScene::autotune(const RenderParams& base, bool rebuild, con
 	try_values(&LaunchConfig::capacity, {1u << 19, 1u << 20, 1u << 21, 1u << 22});
 	try_values(&LaunchConfig::refill, {4u, 8u, 12u, 16u});
 	try_values(&LaunchConfig::blocks_per_sm, {4u, 8u, 16u});
-	if(rebuild && m_bvh_builder == PG_BVH_HOST_SAH)
+	if(leaf_size)
 	{
 		try_values(&LaunchConfig::leaf_tris, {1u, 2u, 3u});
 	}
 	set_launch(best);
 	result.config = best;
 	result.ms_tuned = best_ms;
-	if(cache_path)
+}
+
+AutotuneResult RenderScene::autotune_batch(const std::vector<const RenderScene*>& scenes, const std::vector<uint32_t>& spp,
+                                           const RenderParams& params)
+{
+	// calibration: the batch at a sixteenth of its samples (at least one per scene), into scratch films
+	std::vector<DeviceBuffer<double>> films;
+	std::vector<double*> film_ptrs;
+	std::vector<uint32_t> counts;
+	std::vector<uint64_t> first(scenes.size(), 0);
+	for(std::size_t k = 0; k < scenes.size(); ++k)
 	{
-		append_tuning(cache_path, key, best);
+		if(!scenes[k])
+		{
+			throw Error(PG_ERR_INVALID_ARGUMENT, "autotune_batch: missing scene");
+		}
+		films.emplace_back(static_cast<std::size_t>(scenes[k]->width()) * scenes[k]->height() * kFilmChannels);
+		PG_CUDA_CHECK(cudaMemsetAsync(films.back().get(), 0, films.back().bytes(), m_stream));
+		film_ptrs.push_back(films.back().get());
+		counts.push_back(std::max<uint32_t>(1u, spp.at(k) / 16u));
 	}
+	AutotuneResult result;
+	auto measure = [&](const LaunchConfig& c)
+	{
+		set_launch(c);
+		float best = 0.0f;
+		for(int rep = 0; rep < 3; ++rep)
+		{
+			const float ms = render_batch(scenes, film_ptrs, counts, first, params);
+			if(rep > 0 && (best == 0.0f || ms < best))
+			{
+				best = ms;
+			}
+			++result.trials;
+		}
+		return best;
+	};
+	descend(result, measure, false);
 	return result;
 }
 
@@ -1981,7 +2032,7 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		}
 		if(training)
 		{
-			sqs[0].t = m_st.get();
+			sqs[1].t = m_st.get();   // NEE records of the odd iterations, which make the training samples
 		}
 		gargs.map = m_gmap.get();
 		gargs.feat = m_gfeat.get();
@@ -2000,10 +2051,18 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 	}
 	RenderCounters* const d_counters = m_counters.get();
 	// The NEE segments made by an iteration's shading are traced by the next iteration's
-	// trace_kernel together with its closest-hit rays (one launch, one tail). Training renders
-	// keep a separate any-hit launch at the end of the iteration instead: the training step that
-	// ends the iteration needs the unoccluded NEE of its own samples.
-	const bool merged_shadows = !training;
+	// trace_kernel together with its closest-hit rays (one launch, one tail). Training follows
+	// the same rhythm: an even iteration marks its guided vertices, the odd one after it makes
+	// their training samples (the radiance found at the next vertex plus its NEE, whose segments
+	// the following even iteration's trace resolves), and that even iteration ends with one Adam
+	// step on them -- one step per pair of iterations.
+	GuideArgs gargs_of[2] = {gargs, gargs};
+	if(training)
+	{
+		gargs_of[0].train_cap = 0u;
+		gargs_of[0].mark = 1u;
+		gargs_of[1].mark = 0u;
+	}
 
 	// The five launches of one iteration; `ev` (optional) brackets each with events.
 	auto iteration = [&](int b, cudaEvent_t* ev)
@@ -2011,7 +2070,7 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		const PathBuffers& cur = buf[b];
 		const PathBuffers& nxt = buf[1 - b];
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[0], st)); }
-		prepare_kernel<<<1, 32, 0, st>>>(m_counters.get(), capacity);
+		prepare_kernel<<<1, 32, 0, st>>>(m_counters.get(), capacity, static_cast<uint32_t>(b));
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[1], st)); }
 		if(multi)
 		{
@@ -2024,32 +2083,28 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 			                                                  cur, bview);
 		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[2], st)); }
-		const ShadowQueue& sq = sqs[merged_shadows ? b : 0];   // this iteration's NEE segments
-		if(merged_shadows)
+		const ShadowQueue& sq = sqs[b];   // this iteration's NEE segments
+		// closest hits of this iteration and the previous iteration's NEE segments (whose training
+		// samples, in an even iteration of a training render, gain their unoccluded NEE here)
+		launch_trace(m_dev, d_counters, cur.ray_o, cur.ray_d, m_hits.get(), sqs[1 - b], cur.rad, film, refill, st,
+		             counting, cur.meta, multi ? &bview : nullptr, sqs[1 - b].t ? m_tdirw.get() : nullptr);
+		if(multi)
 		{
-			launch_trace(m_dev, d_counters, cur.ray_o, cur.ray_d, m_hits.get(), sqs[1 - b], cur.rad, film, refill, st,
-			             counting, cur.meta, multi ? &bview : nullptr);
-			if(multi)
-			{
-				classify_kernel<true><<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, m_hits.get(), m_order.get(),
-				                                                    m_order_list, cur.meta, bview);
-			}
-			else
-			{
-				classify_kernel<false><<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, m_hits.get(), m_order.get(),
-				                                                     m_order_list, cur.meta, bview);
-			}
-			PG_CUDA_CHECK(cudaGetLastError());
+			classify_kernel<true><<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, m_hits.get(), m_order.get(),
+			                                                    m_order_list, cur.meta, bview);
 		}
 		else
 		{
-			launch_extend(m_dev, d_counters, cur.ray_o, cur.ray_d, m_hits.get(), refill, st, counting);
+			classify_kernel<false><<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, m_hits.get(), m_order.get(),
+			                                                     m_order_list, cur.meta, bview);
 		}
+		PG_CUDA_CHECK(cudaGetLastError());
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[3], st)); }
+		const GuideArgs& gargs_b = gargs_of[b];
 		if(guided)
 		{
 			// network inputs of this iteration's guidable vertices, then the tensor-core forward pass
-			guide_query_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, cur, m_hits.get(), gargs, max_bounces);
+			guide_query_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, cur, m_hits.get(), gargs_b, max_bounces);
 			PG_CUDA_CHECK(cudaGetLastError());
 			guide::launch_forward(m_gimage.get(), m_gfeat.get(), capacity, nullptr, nullptr, m_gerr.get(), st,
 			                      &d_counters->n_guided, m_graw.get());
@@ -2057,12 +2112,12 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[4], st)); }
 		ShadeArgs sa{m_dev, cur, nxt, m_hits.get(), sq, m_counters.get(), film, params.seed, first_global,
 		             max_bounces, params.estimator, static_cast<uint32_t>(wh)};
-		sa.guide = gargs;
+		sa.guide = gargs_b;
 		sa.refine.mode = params.refine_mode;
 		sa.refine.delta = params.refine_delta;
 		sa.refine.iters = static_cast<int>(params.refine_iters);
 		sa.refine_queue = RefineQueue{m_req_single.get(), m_req_mutual.get()};
-		sa.order = merged_shadows ? m_order.get() : nullptr;
+		sa.order = m_order.get();
 		sa.order_capacity = m_order_list;
 		sa.batch = bview;
 		if(multi)
@@ -2093,15 +2148,11 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 			PG_CUDA_CHECK(cudaGetLastError());
 		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[5], st)); }
-		if(!merged_shadows)
-		{
-			launch_shadow(m_dev, d_counters, sq, nxt.rad, film, refill, st, counting,
-			              training ? m_tdirw.get() : nullptr);
-		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[6], st)); }
-		if(training)
+		if(training && b == 0)
 		{
-			// one Adam step on this iteration's samples; the new weights serve the next iteration
+			// one Adam step on the samples of the previous (odd) iteration, complete now that this
+			// iteration's trace has added their NEE; the new weights serve the next iterations
 			PG_CUDA_CHECK(cudaMemsetAsync(m_gscalars.get(), 0, sizeof(float), st));
 			guide::launch_gradients(m_gparams.get(), m_gimage.get(), m_tfeat.get(), m_tdirw.get(), train_cap,
 			                        m_traw.get(), reinterpret_cast<__nv_bfloat16*>(m_tacts.get()), m_ggrads.get(),
@@ -2232,7 +2283,7 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 			PG_CUDA_CHECK(cudaMemcpyAsync(host_counters, m_counters.get(), sizeof(RenderCounters), cudaMemcpyDeviceToHost, st));
 			PG_CUDA_CHECK(cudaStreamSynchronize(st));
 			done = host_counters->next_path >= host_counters->total_paths && host_counters->n_next == 0 &&
-			       (!merged_shadows || host_counters->n_shadow == 0);
+			       host_counters->n_shadow == 0;
 			if(host_counters->error)
 			{
 				break;
@@ -2276,7 +2327,7 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 				}
 			}
 			done = host_counters->next_path >= host_counters->total_paths && host_counters->n_next == 0 &&
-			       (!merged_shadows || host_counters->n_shadow == 0);
+			       host_counters->n_shadow == 0;
 			if(host_counters->error)
 			{
 				break;
@@ -2303,9 +2354,10 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		// step, repack, loss
 		const unsigned long long per_iteration = 5ull +
 		                                         (params.refine_mode == PG_REFINE_ITERATIVE ? 1ull : 0ull) +
-		                                         (guided ? 2ull : 0ull) +
-		                                         (training ? (m_guide_params.clamp > 0.0f ? 8ull : 6ull) : 0ull);
-		m_last_launches = iterations * per_iteration + 1ull;   // + the film's box-weight or splat launch
+		                                         (guided ? 2ull : 0ull);
+		const unsigned long long per_step = training ? (m_guide_params.clamp > 0.0f ? 8ull : 6ull) : 0ull;
+		// + one training step per even iteration, + the film's box-weight or splat launch
+		m_last_launches = iterations * per_iteration + (iterations + 1ull) / 2ull * per_step + 1ull;
 	}
 	m_last_counts[0] = final_counters.nodes_closest;
 	m_last_counts[1] = final_counters.tris_closest;

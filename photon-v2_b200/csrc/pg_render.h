@@ -282,6 +282,7 @@ struct GuideArgs
 	float*          train_feat = nullptr; // [batch][8]: features 0-6, |cos| / pdf
 	float4*         train_dirw = nullptr; // [batch]: direction, weight
 	uint32_t        train_cap = 0;        // 0: no training samples recorded
+	uint32_t        mark = 0;             // 1: guided vertices await their training sample at the next vertex
 	float           alpha = 0.0f;         // 0: guiding off
 	float           lo[3] = {0, 0, 0};    // scene bound, for the position features
 	float           rcp[3] = {1, 1, 1};
@@ -304,10 +305,12 @@ void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4*
 // Closest hits of this iteration's queue and visibility of the previous iteration's shadow
 // queue `prev` in one persistent launch; unoccluded contributions go to rad_cur / the film.
 // With a batch (multi-scene render), `meta` is the current path buffer's meta words and prev.sid
-// the records' scenes.
+// the records' scenes. With train_dirw (guided training renders), an unoccluded record whose
+// prev.t names a training sample adds its weight to that sample.
 void launch_trace(const DeviceScene& s, RenderCounters* counters, const float4* ray_o, const float4* ray_d,
                   uint2* hits, const ShadowQueue& prev, float4* rad_cur, const FilmView& film, int min_idle,
-                  cudaStream_t st, bool count, const uint32_t* meta = nullptr, const BatchView* batch = nullptr);
+                  cudaStream_t st, bool count, const uint32_t* meta = nullptr, const BatchView* batch = nullptr,
+                  float4* train_dirw = nullptr);
 void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
                    float4* rad_next, const FilmView& film, int min_idle, cudaStream_t st, bool count,
                    float4* train_dirw = nullptr);
@@ -347,6 +350,10 @@ public:
 	// cache file, a scene of the same fingerprint takes the stored choice without calibrating,
 	// and a new choice is appended to it.
 	AutotuneResult autotune(const RenderParams& base, bool rebuild, const char* cache_path, bool ignore_cache);
+	// The launch shapes of render_batch on this scene's pool for the given batch (calibrated at a
+	// sixteenth of its samples; leaf sizes stay as they are).
+	AutotuneResult autotune_batch(const std::vector<const RenderScene*>& scenes, const std::vector<uint32_t>& spp,
+	                              const RenderParams& params);
 	// Identifies scenes that tune alike: triangles, resolution, emitters, material kinds.
 	std::string fingerprint(const RenderParams& base) const;
 
@@ -387,6 +394,10 @@ public:
 private:
 	float render_pass(const RenderParams& params, double* film_device, const std::vector<BatchScene>* batch = nullptr);
 	void ensure_capacity(uint32_t capacity, uint32_t grid);
+	// Coordinate descent over the launch shapes (pool depth, refill threshold, blocks per SM, and
+	// optionally leaf size), `measure` giving a candidate's calibration milliseconds; the winner is
+	// set on this scene.
+	void descend(AutotuneResult& result, const std::function<float(const LaunchConfig&)>& measure, bool leaf_size);
 	// Rebuilds the BVH from the resident triangles with at most max_leaf_tris per leaf.
 	void rebuild_bvh(uint32_t max_leaf_tris);
 	void ensure_guiding(uint32_t capacity);

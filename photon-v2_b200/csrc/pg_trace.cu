@@ -291,7 +291,8 @@ trace_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tri
              const float4* __restrict__ ray_o, const float4* __restrict__ ray_d, uint2* __restrict__ hits,
              const float4* __restrict__ so, const float4* __restrict__ sd, const float4* __restrict__ sc,
              const float2* __restrict__ sr, float4* __restrict__ rad_cur, FilmView film, int min_idle,
-             const uint32_t* __restrict__ meta, const uint32_t* __restrict__ shadow_sid, BatchView batch)
+             const uint32_t* __restrict__ meta, const uint32_t* __restrict__ shadow_sid, BatchView batch,
+             const float2* __restrict__ st, float4* __restrict__ train_dirw)
 {
 	const uint32_t n_closest = counters->n_total;
 	const uint32_t n_shadow = counters->n_shadow_prev;
@@ -330,7 +331,7 @@ trace_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tri
 			}
 			else
 			{
-				add_unoccluded(i - n_closest, sc, nullptr, sr, rad_cur, film, nullptr);
+				add_unoccluded(i - n_closest, sc, st, sr, rad_cur, film, train_dirw);
 			}
 		}
 	};
@@ -422,7 +423,7 @@ void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4*
 
 void launch_trace(const DeviceScene& s, RenderCounters* counters, const float4* ray_o, const float4* ray_d,
                   uint2* hits, const ShadowQueue& prev, float4* rad_cur, const FilmView& film, int min_idle,
-                  cudaStream_t st, bool count, const uint32_t* meta, const BatchView* batch)
+                  cudaStream_t st, bool count, const uint32_t* meta, const BatchView* batch, float4* train_dirw)
 {
 	if(batch)
 	{
@@ -430,26 +431,28 @@ void launch_trace(const DeviceScene& s, RenderCounters* counters, const float4* 
 		{
 			const int grid = persistent_grid(trace_kernel<true, true>);
 			trace_kernel<true, true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
-				prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, meta, prev.sid, *batch);
+				prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, meta, prev.sid, *batch, nullptr, nullptr);
 		}
 		else
 		{
 			const int grid = persistent_grid(trace_kernel<false, true>);
 			trace_kernel<false, true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
-				prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, meta, prev.sid, *batch);
+				prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, meta, prev.sid, *batch, nullptr, nullptr);
 		}
 	}
 	else if(count)
 	{
 		const int grid = persistent_grid(trace_kernel<true, false>);
 		trace_kernel<true, false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
-			prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, nullptr, nullptr, BatchView{});
+			prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, nullptr, nullptr, BatchView{},
+			train_dirw ? prev.t : nullptr, train_dirw);
 	}
 	else
 	{
 		const int grid = persistent_grid(trace_kernel<false, false>);
 		trace_kernel<false, false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
-			prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, nullptr, nullptr, BatchView{});
+			prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, nullptr, nullptr, BatchView{},
+			train_dirw ? prev.t : nullptr, train_dirw);
 	}
 	PG_CUDA_CHECK(cudaGetLastError());
 }

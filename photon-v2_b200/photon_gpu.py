@@ -46,6 +46,8 @@ PGPU_SIGNATURES = [
     ("pgpu_bsdf_eval", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
     ("pgpu_guide_forward", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
     ("pgpu_guide_gradients", ctypes.c_int, [_f32p, _f32p, _f32p, _f32p, ctypes.c_uint64, _f32p, _f32p]),
+    ("pgpu_guide_gradients_ex", ctypes.c_int,
+     [_f32p, _f32p, _f32p, _f32p, ctypes.c_uint64, ctypes.c_uint32, _f32p, _f32p]),
     ("pgpu_guide_train", ctypes.c_int,
      [_f32p, _f32p, _f32p, _f32p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _f32p]),
     ("pgpu_scene_create", ctypes.c_int,
@@ -73,6 +75,8 @@ PGPU_SIGNATURES = [
      [_u64p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32, _f32p]),
     ("pgpu_scenes_render_wavefront", ctypes.c_int,
      [_u64p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _f32p]),
+    ("pgpu_scenes_autotune_wavefront", ctypes.c_int,
+     [_u64p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, _u32p, _f32p]),
     ("pgpu_scene_count", ctypes.c_int,
      [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _u64p]),
     ("pgpu_scene_profile", ctypes.c_int,
@@ -215,16 +219,18 @@ def guide_forward(params: np.ndarray, features: np.ndarray) -> np.ndarray:
     return out
 
 
-def guide_gradients(params, features, dirs, weights):
-    """(loss, gradient [29480]) of the guiding loss on one batch (GPU)."""
+def guide_gradients(params, features, dirs, weights, cuda_cores: bool = False):
+    """(loss, gradient [29480]) of the guiding loss on one batch (GPU): backward pass on the tensor
+    cores, or with cuda_cores in FP32 on the CUDA cores."""
     p = np.ascontiguousarray(params, np.float32).reshape(-1)
     f = np.ascontiguousarray(features, np.float32).reshape(-1, 7)
     d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
     w = np.ascontiguousarray(weights, np.float32).reshape(-1)
     g = np.empty_like(p)
     loss = ctypes.c_float()
-    _check(load().pgpu_guide_gradients(_ptr(p, ctypes.c_float), _ptr(f, ctypes.c_float), _ptr(d, ctypes.c_float),
-                                       _ptr(w, ctypes.c_float), f.shape[0], ctypes.byref(loss), _ptr(g, ctypes.c_float)))
+    _check(load().pgpu_guide_gradients_ex(_ptr(p, ctypes.c_float), _ptr(f, ctypes.c_float), _ptr(d, ctypes.c_float),
+                                          _ptr(w, ctypes.c_float), f.shape[0], 1 if cuda_cores else 0,
+                                          ctypes.byref(loss), _ptr(g, ctypes.c_float)))
     return loss.value, g
 
 
@@ -296,6 +302,19 @@ def render_scenes_wavefront(render_scenes, spp, max_bounces=10000, estimator=BNE
     _check(load().pgpu_scenes_render_wavefront(_ptr(ids, ctypes.c_uint64), len(ids), _ptr(counts, ctypes.c_uint32),
                                                max_bounces, estimator, seed, ctypes.byref(ms)))
     return ms.value
+
+
+def autotune_wavefront(render_scenes, spp, max_bounces=10000, estimator=BNEEPT) -> dict:
+    """pgpu_scenes_autotune_wavefront: launch shapes of the one-wavefront render of these scenes."""
+    ids = np.array([rs.id for rs in render_scenes], np.uint64)
+    counts = np.array(spp, np.uint32)
+    cfg = np.zeros(4, np.uint32)
+    ms = np.zeros(4, np.float32)
+    _check(load().pgpu_scenes_autotune_wavefront(_ptr(ids, ctypes.c_uint64), len(ids), _ptr(counts, ctypes.c_uint32),
+                                                 max_bounces, estimator, _ptr(cfg, ctypes.c_uint32),
+                                                 _ptr(ms, ctypes.c_float)))
+    return {"capacity": int(cfg[0]), "refill": int(cfg[1]), "blocks_per_sm": int(cfg[2]), "leaf_tris": int(cfg[3]),
+            "ms_default": float(ms[0]), "ms_tuned": float(ms[1]), "trials": int(ms[2])}
 
 
 class RenderScene:

@@ -78,3 +78,33 @@ def test_wavefront_rejects_filtered_films_and_duplicates(gpu_lib):
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.gpu
+def test_wavefront_autotune(gpu_lib):
+    """The wavefront's launch shapes tuned on calibration wavefronts; the tuned batch still renders
+    every scene's own paths."""
+    import photon_gpu
+
+    sc = _scenes()[:3]
+    rss = [photon_gpu.RenderScene(s) for s in sc]
+    try:
+        t = photon_gpu.autotune_wavefront(rss, [s.spp for s in sc], max_bounces=10)
+        print(f"wavefront autotune: {t}")
+        assert t["trials"] > 0 and t["ms_tuned"] <= t["ms_default"]
+        assert rss[0].launch()["capacity"] == t["capacity"]
+        solo = []
+        for s, rs in zip(sc, rss):
+            rs.clear()
+        photon_gpu.render_scenes_wavefront(rss, [s.spp for s in sc], max_bounces=10, seed=5)
+        tuned = [rs.film()[1] for rs in rss]
+        for s, rs in zip(sc, rss):
+            rs.clear()
+            rs.render(s.spp, max_bounces=10, seed=5)
+            solo.append(rs.film()[1])
+        for a, b in zip(tuned, solo):
+            assert np.array_equal(a[..., 3], b[..., 3])
+            assert _rel(a[..., :3], b[..., :3]) < 1e-12
+    finally:
+        for rs in rss:
+            rs.close()
