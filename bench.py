@@ -201,16 +201,27 @@ def roofline_of(kernel_ms: dict, rays: float, shadow_rays: float, iterations: fl
         alg_bytes, kname = (32 + 8 + 80 + 48 + 112 + 48) * rays, "shade"
     achieved = alg_bytes / (kernel_ms[dominant] / 1e3) / 1e9
     traffic = None
+    l2 = None
     prof_path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(prof_path):
         with open(prof_path) as f:
             rec = json.load(f).get(dominant) or {}
+        entries = (shadow_rays if dominant == "shadow_ms" else
+                   rays + shadow_rays if dominant == "extend_ms" and merged else rays) / max(1, iterations)
         if rec.get("dram_bytes_per_entry"):
-            entries = (shadow_rays if dominant == "shadow_ms" else
-                       rays + shadow_rays if dominant == "extend_ms" and merged else rays) / max(1, iterations)
             traffic = rec["dram_bytes_per_entry"] * entries
+        if rec.get("l2_bytes_per_entry"):
+            # the L2 side of the same kernel: bytes the SMs moved through L2 per launch (ncu
+            # lts__t_bytes scaled by queue entries) over the kernel's measured time here, and
+            # the L2 throughput fraction ncu reported for that launch
+            l2_bytes = rec["l2_bytes_per_entry"] * entries
+            launch_s = kernel_ms[dominant] / 1e3 / max(1, iterations)
+            l2 = {"bytes_per_launch": l2_bytes, "achieved_gbs": l2_bytes / launch_s / 1e9,
+                  "ncu_lts_throughput_pct": rec.get("lts_throughput_pct"),
+                  "ncu_issue_active_pct": rec.get("issue_active_pct"),
+                  "ncu_threads_per_instruction": rec.get("thread_inst_per_inst")}
     return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peaks["hbm_gbs"],
-            "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+            "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "l2": l2,
             "algorithmic_bytes_per_launch": alg_bytes / max(1, iterations),
             "peak_source": peaks["source"],
             "model": {"bytes_per_closest_ray": bytes_closest, "nodes_per_closest_ray": nodes_per_ray,
@@ -223,71 +234,64 @@ def rel_mse(x: np.ndarray, ref: np.ndarray, eps: float = 1e-2) -> float:
     return float(np.mean((x.astype(np.float64) - ref) ** 2 / (ref.astype(np.float64) ** 2 + eps)))
 
 
-def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 4096, plain_spp: int = 64,
-                      warmup_renders: int = 4, trials: int = 6) -> dict:
-    """Equal-time comparison of guided and plain GPU BNEEPT on the slit-light room (2M triangles).
+def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 65536, probe_spp: int = 64,
+                      target: float = 1e-3, warmup_renders: int = 8, warmup_spp: int = 32) -> dict:
+    """Guided vs plain GPU BNEEPT on the slit-light room (2M triangles), as time to reach a relMSE
+    target against a 65,536-spp plain render of the same scene.
 
-    A plain render of `plain_spp` samples sets the time budget; the guided renderer, after
-    `warmup_renders` training renders of plain_spp / 2 samples, renders as many samples as fit in
-    the same device time (its per-sample cost measured on a calibration render). Both are scored by
-    relMSE against a `ref_spp` plain render, averaged over `trials` independent renders of each
-    (single renders of this scene are dominated by rare bright paths). `relmse_ratio` < 1 means
-    guiding wins at equal time; the ratio also estimates (time for guided to reach the plain
-    error) / (plain time). `guided_frozen` repeats the guided renders with training switched off
-    after the warm-up (inference only), at its own equal-time sample count."""
+    relMSE of an unbiased n-spp render falls as 1/n, so each method is rendered once at a probe
+    count, its relMSE gives the count that reaches `target`, and it is rendered again at that
+    count: time_to_target = its device time x (its relMSE / target). Guided renders start from a
+    network trained by `warmup_renders` renders (training time reported apart) and keep training;
+    `guided_frozen` renders with the trained network and no further training. A ratio below 1
+    means guiding reaches the target sooner; the north star's target is a ratio of at most 0.5.
+    """
     import photon_gpu
 
     scene = scenes.slit_room(res, res, 1, 10, num_boxes=num_boxes)
+
+    def to_target(rs, seed):
+        rs.clear()
+        rs.render(probe_spp, max_bounces=10, seed=seed)
+        e_probe = rel_mse(rs.film()[0], ref)
+        spp = int(min(16384, max(probe_spp, np.ceil(probe_spp * e_probe / target))))
+        rs.clear()
+        r = rs.render(spp, max_bounces=10, seed=seed + 1)
+        e = rel_mse(rs.film()[0], ref)
+        return {"spp": spp, "ms": r["ms"], "relmse": e, "probe_relmse": e_probe,
+                "ms_to_target": r["ms"] * e / target}
+
     with photon_gpu.RenderScene(scene) as rs:
+        t0 = time.time()
         rs.render(ref_spp, max_bounces=10, seed=1)
         ref = rs.film()[0]
-        e_plain, plain_ms = [], []
-        for t in range(trials):
-            rs.clear()
-            plain_ms.append(rs.render(plain_spp, max_bounces=10, seed=2 + 1000 * t)["ms"])
-            e_plain.append(rel_mse(rs.film()[0], ref))
+        ref_s = time.time() - t0
+        plain = to_target(rs, 100)
         rs.set_guiding(True, True, 0.5, 3e-3, 16384)
+        train_ms = 0.0
         for k in range(warmup_renders):
             rs.clear()
-            calib = rs.render(max(1, plain_spp // 2), max_bounces=10, seed=100 + k)
-        ms_per_spp = calib["ms"] / max(1, plain_spp // 2)
-        guided_spp = max(1, int(statistics.median(plain_ms) / ms_per_spp))
-        e_guided, guided_ms = [], []
-        for t in range(trials):
-            rs.clear()
-            guided_ms.append(rs.render(guided_spp, max_bounces=10, seed=3 + 1000 * t)["ms"])
-            e_guided.append(rel_mse(rs.film()[0], ref))
+            train_ms += rs.render(warmup_spp, max_bounces=10, seed=200 + k)["ms"]
+        guided = to_target(rs, 300)
         info = rs.guide_info()
-        # the same network frozen (inference only, no training step): its own equal-time spp
         rs.set_guiding(True, False, 0.5, 3e-3, 16384)
-        rs.clear()
-        calib = rs.render(max(1, plain_spp // 2), max_bounces=10, seed=200)
-        frozen_spp = max(1, int(statistics.median(plain_ms) / (calib["ms"] / max(1, plain_spp // 2))))
-        e_frozen, frozen_ms = [], []
-        for t in range(trials):
-            rs.clear()
-            frozen_ms.append(rs.render(frozen_spp, max_bounces=10, seed=4 + 1000 * t)["ms"])
-            e_frozen.append(rel_mse(rs.film()[0], ref))
-    mp, mg, mf = float(np.mean(e_plain)), float(np.mean(e_guided)), float(np.mean(e_frozen))
+        frozen = to_target(rs, 400)
+    ratio = guided["ms_to_target"] / plain["ms_to_target"]
     return {
-        "workload": f"slit_room {res}x{res}, {scene.num_tris} triangles, depth 10",
+        "workload": f"slit_room {res}x{res}, {scene.num_tris} triangles, depth 10 (the C4 room at reduced resolution)",
         "width": res, "height": res, "triangles": scene.num_tris, "max_bounces": 10,
-        "reference_spp": ref_spp, "trials": trials,
-        "plain": {"spp": plain_spp, "ms": statistics.median(plain_ms), "relmse": mp,
-                  "relmse_trials": e_plain},
-        "guided": {"spp": guided_spp, "ms": statistics.median(guided_ms), "relmse": mg,
-                   "relmse_trials": e_guided, "warmup_spp": warmup_renders * max(1, plain_spp // 2),
-                   "train_loss": info["loss"]},
-        "relmse_ratio": mg / mp if mp > 0 else None,
-        "guided_frozen": {"spp": frozen_spp, "ms": statistics.median(frozen_ms), "relmse": mf,
-                          "relmse_trials": e_frozen, "note": "the trained network without further training steps"},
-        "relmse_ratio_frozen": mf / mp if mp > 0 else None,
+        "reference_spp": ref_spp, "reference_s": ref_s, "target_relmse": target, "relmse_eps": 1e-2,
+        "plain": plain, "guided": guided, "guided_frozen": frozen,
+        "training": {"renders": warmup_renders, "spp": warmup_spp, "ms": train_ms, "final_loss": info["loss"]},
+        "time_ratio": ratio,
+        "time_ratio_with_training": (guided["ms_to_target"] + train_ms) / plain["ms_to_target"],
+        "time_ratio_frozen": frozen["ms_to_target"] / plain["ms_to_target"],
     }
 
 
 def c2_error(spp: int = 256) -> dict:
     """The error the benchmarked render carries: the 1M-triangle GGX scene at `spp` through the
-    Photon C API at 128 x 128, against the reference CPU renderer's 65,536-spp render of the same
+    Photon C API at 64 x 64, against the reference CPU renderer's 65,536-spp render of the same
     scene (tests/golden/images.npz, made by tests/golden/make_golden_images.py). relMSE falls as
     1/spp, which gives the spp that reaches 1e-3."""
     import photon_gpu
@@ -299,7 +303,7 @@ def c2_error(spp: int = 256) -> dict:
     if "c2_ggx1m_bneept" not in d:
         return {"unavailable": "no 65,536-spp reference render of the scene in images.npz"}
     ref = d["c2_ggx1m_bneept"]
-    scene = scenes.ggx_sphere(level=8, width=128, height=128, spp=spp, max_bounces=10)
+    scene = scenes.ggx_sphere(level=8, width=64, height=64, spp=spp, max_bounces=10)
     with tempfile.TemporaryDirectory() as tmp:
         p2 = os.path.join(tmp, "scene.p2")
         with open(p2, "w") as f:
@@ -316,7 +320,7 @@ def c2_error(spp: int = 256) -> dict:
             img = eng.frame()
     err = rel_mse(img, ref)
     return {"spp": spp, "relmse": err, "spp_for_relmse_1e-3": int(np.ceil(spp * err / 1e-3)),
-            "reference": f"reference CPU renderer, {int(d['c2_ggx1m_bneept__spp'])} spp", "resolution": "128x128",
+            "reference": f"reference CPU renderer, {int(d['c2_ggx1m_bneept__spp'])} spp", "resolution": "64x64",
             "mean_ratio": (img.mean(axis=(0, 1)) / ref.mean(axis=(0, 1))).tolist(), "eps": 1e-2}
 
 
@@ -495,6 +499,8 @@ def run_ours(args) -> None:
             line["cpu_baseline"] = cpu_sample(scene, tmp, target_seconds=args.cpu_seconds)[-1]
     if rank == 0 and world == 1 and args.workload == "ggx_1m":
         line["error_vs_65536spp"] = c2_error(scene.spp)
+        if not args.no_other_workloads:
+            line["other_workloads"] = other_workloads()
     if rank == 0 and world == 1 and not args.no_guided:
         line["guided_equal_time"] = guided_equal_time()
     if rank == 0:
@@ -660,6 +666,57 @@ def run_flat(args) -> None:
         print(json.dumps(line))
 
 
+def other_workloads(steps: int = 2, scale: int = 8) -> dict:
+    """The other benchmarked configurations measured in the same run, each at 1/scale of its
+    samples per pixel (at least 8): the batched 64 scenes as one wavefront, the slit-light room
+    rendered plain, and the many-light city. Device-timed Mpaths/s over `steps` renders after one
+    warm-up render (launch shapes autotuned first, untimed)."""
+    import torch
+
+    import photon_gpu
+
+    out = {}
+    l2_flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    for name in ("batched", "slit_room", "city"):
+        t0 = time.time()
+        scene_list = FLAT_WORKLOADS[name]()
+        for sc in scene_list:
+            sc.spp = max(8, sc.spp // scale)
+        rss = [photon_gpu.RenderScene(sc) for sc in scene_list]
+        setup_s = time.time() - t0
+        spp = [sc.spp for sc in scene_list]
+        bounces = scene_list[0].max_bounces
+        if len(rss) > 1:
+            tuned = photon_gpu.autotune_wavefront(rss, spp, max_bounces=bounces)
+            render = lambda: photon_gpu.render_scenes_wavefront(rss, spp, max_bounces=bounces, seed=7)
+        else:
+            tuned = rss[0].autotune(spp[0], max_bounces=bounces, rebuild=True)
+            render = lambda: rss[0].render(spp[0], max_bounces=bounces, seed=7)["ms"]
+        paths = sum(sc.width * sc.height * sc.spp for sc in scene_list)
+        for rs in rss:
+            rs.clear()
+        render()
+        ms = 0.0
+        for _ in range(steps):
+            l2_flush.fill_(1.0)
+            torch.cuda.synchronize()
+            for rs in rss:
+                rs.clear()
+            ms += render()
+        out[name] = {"value": paths * steps / (ms / 1e3) / 1e6, "unit": "Mpaths/s", "steps": steps,
+                     "paths_per_step": paths, "ms_per_step": ms / steps, "scenes": len(scene_list),
+                     "triangles": int(sum(sc.num_tris for sc in scene_list)),
+                     "spp": sorted(set(spp)) if len(set(spp)) <= 2 else [min(spp), max(spp)],
+                     "spp_scale": f"1/{scale} of the configuration's spp (at least 8)",
+                     "mode": "one wavefront" if len(rss) > 1 else "single scene",
+                     "tuned": {k: tuned[k] for k in ("capacity", "refill", "blocks_per_sm", "leaf_tris",
+                                                     "ms_default", "ms_tuned")},
+                     "setup_s": setup_s}
+        for rs in rss:
+            rs.close()
+    return out
+
+
 def cpu_sample_many(scene_list, target_seconds: float, paths_per_core_s: float = EST_CPU_PATHS_PER_CORE_S) -> dict:
     """CPU baseline of a multi-scene or very large workload: the oracle port (binary scene file;
     SDL text of tens of millions of triangles is impractical to parse) on the first scenes, each
@@ -694,6 +751,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-guided", action="store_true", help="skip the guided-vs-plain equal-time comparison")
     ap.add_argument("--builder", default="sah", choices=["sah", "gpu"], help="BVH builder of flat workloads")
+    ap.add_argument("--no-other-workloads", action="store_true",
+                    help="skip the reduced-spp measurement of the batched, slit-room and city workloads")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="render with the fixed default launch shapes instead of autotuned ones")
     ap.add_argument("--batch-mode", default="wavefront", choices=["wavefront", "streams", "serial"],

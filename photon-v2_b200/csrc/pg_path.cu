@@ -1896,16 +1896,20 @@ float RenderScene::render_batch(const std::vector<const RenderScene*>& scenes, c
 // Paths whose radiance a pass of a 4 x 4-filter render keeps (16 B each): larger renders are
 // split into passes of whole samples per pixel.
 constexpr unsigned long long kMaxFilteredPassPaths = 1ull << 27;
+constexpr unsigned long long kMaxBoxPassPaths = 1ull << 31;
 
 float RenderScene::render(const RenderParams& params, double* film_sums)
 {
 	require_same_device(m_geometry->device, "render scene");
 	const unsigned long long wh = static_cast<unsigned long long>(params.width) * params.height;
-	if(params.filter == PG_FILTER_BOX || wh == 0 || wh * params.spp <= kMaxFilteredPassPaths)
+	// passes of whole samples per pixel: 4 x 4 films keep every path's radiance for the pass; a
+	// box film's pass only has to stay within the path numbering of one pass (2^31 paths)
+	const unsigned long long max_pass = params.filter == PG_FILTER_BOX ? kMaxBoxPassPaths : kMaxFilteredPassPaths;
+	if(wh == 0 || wh * params.spp <= max_pass)
 	{
 		return render_pass(params, film_sums);
 	}
-	const uint32_t pass_spp = static_cast<uint32_t>(std::max<unsigned long long>(1ull, kMaxFilteredPassPaths / wh));
+	const uint32_t pass_spp = static_cast<uint32_t>(std::max<unsigned long long>(1ull, max_pass / wh));
 	float ms = 0.0f;
 	unsigned long long rays = 0, shadow = 0, iterations = 0, launches = 0, counts[4] = {0, 0, 0, 0};
 	double kernel_ms[7] = {0, 0, 0, 0, 0, 0, 0};

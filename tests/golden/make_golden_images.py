@@ -57,8 +57,8 @@ WORKLOADS = {
                                                                max_bounces=10), 4096, 10, "manual"),
     # the benchmarked configurations' geometry at reduced resolution:
     # the 1M-triangle GGX scene (1,310,726 triangles, 2 quad lights + environment, depth 10) at
-    # 128 x 128 and 65,536 spp -- the converged reference its parity and error are stated against
-    "c2_ggx1m_bneept": (lambda spp: scenes.ggx_sphere(level=8, width=128, height=128, spp=spp,
+    # 64 x 64 and 65,536 spp -- the converged reference its parity and error are stated against
+    "c2_ggx1m_bneept": (lambda spp: scenes.ggx_sphere(level=8, width=64, height=64, spp=spp,
                                                       max_bounces=10), 65536, 10),
     # the slit-light room, full 2M triangles with its dielectric boxes, 32 x 32
     "slit_room_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10), 65536, 10),

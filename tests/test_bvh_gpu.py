@@ -141,3 +141,24 @@ def test_render_with_gpu_built_tree_matches_reference(gpu_lib):
     err = float(np.mean((block(img) - block(ref)) ** 2 / (block(ref) ** 2 + 1e-2)))
     means = img.mean(axis=(0, 1)) / ref.mean(axis=(0, 1))
     assert err <= 1e-3 and np.all(np.abs(means - 1) < 0.01), (err, means)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("builder", ["sah", "gpu"])
+def test_city_traversal_stays_within_the_stack(gpu_lib, builder):
+    """The many-light city at full size (21,599,374 triangles, 10,000 lights): both builders keep
+    the 8-wide tree shallower than the 64-entry traversal stack (the builders refuse deeper trees),
+    and a render of the scene, whose traversal kernels raise a device flag on any stack overflow,
+    completes (an overflow ends the render with PG_ERR_STACK_OVERFLOW)."""
+    import photon_gpu
+
+    sc = scenes.city(96, 54, 4, 12)
+    with photon_gpu.RenderScene(sc, builder=builder) as rs:
+        rs.render(4, max_bounces=12, seed=3)
+        rgb = rs.film(with_sums=False)[0]
+    assert np.all(np.isfinite(rgb)) and rgb.mean() > 0
+    tris = np.concatenate([g.tris for g in sc.groups])
+    with photon_gpu.Geometry(tris, builder=builder) as g:
+        depth = g.stats()["max_depth"]
+    print(f"city ({builder}): {tris.shape[0]} triangles, wide-tree depth {depth}")
+    assert depth < 64

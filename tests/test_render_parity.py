@@ -94,8 +94,8 @@ def render_via_c_api(scene, tmp_path, seed=1, refine_mode="iterative", dome_pdf=
 # name -> (scene factory, GPU spp, block size of the block relMSE). The meshes reach the GPU as
 # binary PLY files through geometry(ply) (the reference parsed the same triangles as SDL text).
 LARGE_WORKLOADS = {
-    # 1,310,726 triangles, 2 quad lights + environment, GGX in 64 groups, depth 10, 128 x 128
-    "c2_ggx1m_bneept": (lambda spp: scenes.ggx_sphere(level=8, width=128, height=128, spp=spp, max_bounces=10),
+    # 1,310,726 triangles, 2 quad lights + environment, GGX in 64 groups, depth 10, 64 x 64
+    "c2_ggx1m_bneept": (lambda spp: scenes.ggx_sphere(level=8, width=64, height=64, spp=spp, max_bounces=10),
                         65536, 4),
     # 2,000,042 triangles, light through a 0.05-wide slit, 30 % rough glass boxes, depth 10, 32 x 32
     "slit_room_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10), 65536, 4),
@@ -145,10 +145,10 @@ def test_benchmarked_geometry_matches_reference(gpu_lib, tmp_path, name):
 @pytest.mark.gpu
 def test_c2_error_at_bench_spp(gpu_lib, tmp_path):
     """The error the benchmarked render carries: the 1M-triangle GGX scene at the bench's 256 spp
-    against the 65,536-spp reference render (at 128 x 128), relMSE as the bench line states it.
+    against the 65,536-spp reference render (at 64 x 64), relMSE as the bench line states it.
     The error of an n-spp render falls as 1/n, which gives the spp that reaches relMSE 1e-3."""
     ref = np.load(IMAGES)["c2_ggx1m_bneept"]
-    img, _ = render_via_c_api(scenes.ggx_sphere(level=8, width=128, height=128, spp=256, max_bounces=10), tmp_path,
+    img, _ = render_via_c_api(scenes.ggx_sphere(level=8, width=64, height=64, spp=256, max_bounces=10), tmp_path,
                               mesh_format="ply")
     err = rel_mse(img, ref)
     print(f"c2 at 256 spp: relMSE {err:.3e} against the 65,536-spp reference; 1e-3 at ~{256 * err / 1e-3:.0f} spp")
