@@ -298,11 +298,8 @@ constexpr uint32_t kMetaStopAfter = 1u << 9;    // Russian roulette ended the pa
 constexpr uint32_t kMetaGuideRec = 1u << 10;    // gf0/gf1 hold a guided vertex awaiting its training sample
 constexpr uint32_t kTargetFinal = 0x80000000u;
 
-// Launchers implemented in pg_trace.cu (FMA-enabled traversal kernels); min_idle is the
-// traversal's refill threshold (LaunchConfig::refill).
-void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4* ray_o,
-                   const float4* ray_d, uint2* hits, int min_idle, cudaStream_t st, bool count);
-// Closest hits of this iteration's queue and visibility of the previous iteration's shadow
+// Launcher implemented in pg_trace.cu (FMA-enabled traversal kernels); min_idle is the
+// traversal's refill threshold (LaunchConfig::refill). Closest hits of this iteration's queue and visibility of the previous iteration's shadow
 // queue `prev` in one persistent launch; unoccluded contributions go to rad_cur / the film.
 // With a batch (multi-scene render), `meta` is the current path buffer's meta words and prev.sid
 // the records' scenes. With train_dirw (guided training renders), an unoccluded record whose
@@ -311,9 +308,6 @@ void launch_trace(const DeviceScene& s, RenderCounters* counters, const float4* 
                   uint2* hits, const ShadowQueue& prev, float4* rad_cur, const FilmView& film, int min_idle,
                   cudaStream_t st, bool count, const uint32_t* meta = nullptr, const BatchView* batch = nullptr,
                   float4* train_dirw = nullptr);
-void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
-                   float4* rad_next, const FilmView& film, int min_idle, cudaStream_t st, bool count,
-                   float4* train_dirw = nullptr);
 
 // A scene resident on the GPU together with its render buffers.
 class RenderScene

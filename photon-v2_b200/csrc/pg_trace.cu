@@ -204,32 +204,6 @@ void check_device_error(Geometry& g, cudaStream_t s)
 	}
 }
 
-// Closest hit for the render's ray queue; the queue length is read on the device. COUNT adds
-// the visited-node / tested-triangle tallies of the counting render.
-template<bool COUNT>
-__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
-extend_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
-              RenderCounters* __restrict__ counters,
-              const float4* __restrict__ ray_o, const float4* __restrict__ ray_d,
-              uint2* __restrict__ hits, int min_idle)
-{
-	const uint32_t n = counters->n_total;
-	uint32_t err = 0, node_count = 0, tri_count = 0;
-	traverse_persistent<false, COUNT>(nodes, tris, n, &counters->fetch_extend,
-		[&](uint32_t i, float4* a, float4* b) { *a = __ldg(ray_o + i); *b = __ldg(ray_d + i); },
-		[&](uint32_t i, bool hit, uint32_t tri, float t) { hits[i] = make_uint2(hit ? tri : 0xFFFFFFFFu, __float_as_uint(t)); },
-		&err, &node_count, &tri_count, 0u, min_idle);
-	if(COUNT)
-	{
-		atomicAdd(&counters->nodes_closest, static_cast<unsigned long long>(node_count));
-		atomicAdd(&counters->tris_closest, static_cast<unsigned long long>(tri_count));
-	}
-	if(err)
-	{
-		atomicOr(&counters->error, err);
-	}
-}
-
 // An unoccluded NEE contribution (shadow record i): to the owning path's radiance (slot in the
 // path buffer the record was made for) or, for paths that ended at that vertex, straight to the
 // FP64 film; guided renders also credit the training sample the record belongs to.
@@ -366,60 +340,7 @@ trace_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tri
 	}
 }
 
-// Visibility of the NEE segments of this iteration (guided training renders, whose training
-// step at the end of the iteration needs them); see add_unoccluded.
-template<bool COUNT>
-__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
-shadow_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tris,
-              RenderCounters* __restrict__ counters,
-              const float4* __restrict__ so, const float4* __restrict__ sd, const float4* __restrict__ sc,
-              const float2* __restrict__ st, const float2* __restrict__ sr, float4* __restrict__ rad_next,
-              FilmView film, float4* __restrict__ train_dirw, int min_idle)
-{
-	const uint32_t n = counters->n_shadow;
-	if(blockIdx.x == 0 && threadIdx.x == 0)
-	{
-		counters->shadow_rays += n;
-	}
-	uint32_t err = 0, node_count = 0, tri_count = 0;
-	traverse_persistent<true, COUNT>(nodes, tris, n, &counters->fetch_shadow,
-		[&](uint32_t i, float4* a, float4* b) { *a = __ldg(so + i); *b = __ldg(sd + i); },
-		[&](uint32_t i, bool occluded, uint32_t, float)
-		{
-			if(!occluded)
-			{
-				add_unoccluded(i, sc, st, sr, rad_next, film, train_dirw);
-			}
-		},
-		&err, &node_count, &tri_count, 0u, min_idle);
-	if(COUNT)
-	{
-		atomicAdd(&counters->nodes_any, static_cast<unsigned long long>(node_count));
-		atomicAdd(&counters->tris_any, static_cast<unsigned long long>(tri_count));
-	}
-	if(err)
-	{
-		atomicOr(&counters->error, err);
-	}
-}
-
 }// end anonymous namespace
-
-void launch_extend(const DeviceScene& s, RenderCounters* counters, const float4* ray_o,
-                   const float4* ray_d, uint2* hits, int min_idle, cudaStream_t st, bool count)
-{
-	if(count)
-	{
-		const int grid = persistent_grid(extend_kernel<true>);
-		extend_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits, min_idle);
-	}
-	else
-	{
-		const int grid = persistent_grid(extend_kernel<false>);
-		extend_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits, min_idle);
-	}
-	PG_CUDA_CHECK(cudaGetLastError());
-}
 
 void launch_trace(const DeviceScene& s, RenderCounters* counters, const float4* ray_o, const float4* ray_d,
                   uint2* hits, const ShadowQueue& prev, float4* rad_cur, const FilmView& film, int min_idle,
@@ -453,25 +374,6 @@ void launch_trace(const DeviceScene& s, RenderCounters* counters, const float4* 
 		trace_kernel<false, false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, ray_o, ray_d, hits,
 			prev.o, prev.d, prev.c, prev.r, rad_cur, film, min_idle, nullptr, nullptr, BatchView{},
 			train_dirw ? prev.t : nullptr, train_dirw);
-	}
-	PG_CUDA_CHECK(cudaGetLastError());
-}
-
-void launch_shadow(const DeviceScene& s, RenderCounters* counters, const ShadowQueue& q,
-                   float4* rad_next, const FilmView& film, int min_idle, cudaStream_t st, bool count,
-                   float4* train_dirw)
-{
-	if(count)
-	{
-		const int grid = persistent_grid(shadow_kernel<true>);
-		shadow_kernel<true><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, q.t, q.r,
-		                                                  rad_next, film, train_dirw, min_idle);
-	}
-	else
-	{
-		const int grid = persistent_grid(shadow_kernel<false>);
-		shadow_kernel<false><<<grid, kTraceBlock, 0, st>>>(s.nodes, s.tris, counters, q.o, q.d, q.c, q.t, q.r,
-		                                                   rad_next, film, train_dirw, min_idle);
 	}
 	PG_CUDA_CHECK(cudaGetLastError());
 }
