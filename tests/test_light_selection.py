@@ -16,9 +16,11 @@ classes answer:
 
 Bars: the GPU pick probability equals flux / sum(flux) within 1e-6 relative and the reference's
 realised pmf within 2e-7 absolute; the device alias table realises the GPU pmf within 1e-6
-relative; the NEE density equals the reference emitter density x flux / sum(flux) within 1e-5
-relative, the reference's own pdf within 1e-5 relative wherever its pmf is not rounded (relative
-CDF error below 1e-6), and is exactly 0 wherever the reference's is (back-facing light points).
+relative; the NEE density equals the reference emitter density x flux / sum(flux) within
+1e-5 + 3e-7 / cos relative (cos: the cosine at the light point, whose float32 error of a few ulps
+of 1 both sides share, so grazing light points carry it amplified), the reference's own pdf within
+the same bar wherever its pmf is not rounded (relative CDF error below 1e-6), and is exactly 0
+wherever the reference's is (back-facing light points).
 """
 
 import os
@@ -97,10 +99,20 @@ def test_gpu_nee_densities_match_reference(gpu_lib, count):
     ref_zero = d["emitter_pdf_w"] == 0
     assert np.all(pdf[ref_zero] == 0.0), "density where the reference's light point does not face the target"
     has = ~ref_zero
+    # The density divides by the cosine at the light point; both sides compute that cosine in
+    # float32 to a few ulps of 1, so at grazing light points its relative error grows as 1 / cos.
+    tri = d["tris"][d["prim"]].astype(np.float64)
+    nrm = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    to_target = d["targets"].astype(np.float64) - d["point"]
+    cos = np.abs((nrm * to_target).sum(1)) / np.linalg.norm(to_target, axis=1)
+    tol = 1e-5 + 3e-7 / np.maximum(cos, 1e-12)
     want = d["emitter_pdf_w"][has] * ideal[owner[has]]
     rel = np.abs(pdf[has] - want) / want
-    print(f"{count} emitters: {has.sum()} densities, max rel error {rel.max():.2e}")
-    assert rel.max() <= 1e-5
+    print(f"{count} emitters: {has.sum()} densities, max rel error {rel.max():.2e}, "
+          f"max error / bar {np.max(rel / tol[has]):.2f}, smallest cosine {cos[has].min():.1e}")
+    assert np.all(rel <= tol[has])
     # against the reference's own density where its pmf is not visibly rounded
     exact = has & (np.abs(d["pmf"][owner] - ideal[owner]) <= 1e-6 * ideal[owner])
-    np.testing.assert_allclose(pdf[exact], d["pdf_w"][exact], rtol=1e-5)
+    rel_ref = np.abs(pdf[exact] - d["pdf_w"][exact]) / d["pdf_w"][exact]
+    assert np.all(rel_ref <= tol[exact])
