@@ -707,9 +707,11 @@ void launch_gradients(const float* d_params, const unsigned char* d_image, const
 			return true;
 		}();
 		(void)configured_tc;
-		// about four tiles per CTA: each CTA adds its weight gradients to global memory once
+		// one CTA per SM: a batch of up to one tile per SM runs in one round of tiles; larger
+		// batches keep their weight gradients in TMEM across each CTA's tiles, and every CTA adds
+		// them to global memory once
 		const uint32_t tiles = (n + kTile - 1) / kTile;
-		const uint32_t grid = std::max(1u, std::min(tiles, static_cast<uint32_t>(sm_count()) / 4u));
+		const uint32_t grid = std::max(1u, std::min(tiles, static_cast<uint32_t>(sm_count())));
 		tcb::backward_tc_kernel<<<grid, tcb::kThreads, tcb::kSmemBytes, s>>>(d_params, d_features, d_dirw, d_raw, d_acts,
 		                                                                     n, d_n, d_total, d_grads, d_loss, d_error);
 		PG_CUDA_CHECK(cudaGetLastError());

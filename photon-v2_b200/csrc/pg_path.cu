@@ -708,6 +708,8 @@ shade_kernel(ShadeArgs a)
 		const bool defer_refine = a.refine.mode == PG_REFINE_ITERATIVE;
 		RGB sh_c{};
 		float sh_train = 0.0f;   // unweighted direct-light estimate (luminance) for the training sample
+		uint32_t nee_row = 0xFFFFFFFFu;   // this vertex's NEE direction as a training sample of its own
+		float nee_w = 0.0f;
 		const uint32_t grow = GUIDED ? a.guide.map[i] : 0xFFFFFFFFu;
 		const bool guided = GUIDED && grow != 0xFFFFFFFFu;
 		const float* graw = guided ? a.guide.raw + static_cast<size_t>(grow) * guide::kMixFloats : nullptr;
@@ -816,6 +818,30 @@ shade_kernel(ShadeArgs a)
 					if(GUIDED && train_row != 0xFFFFFFFFu)
 					{
 						sh_train = luminance(le * (f * (fabsf(dot(frame.ns, l)) / pdf_w))) * train_wfac;
+					}
+					if(GUIDED && guided && a.guide.train_cap)
+					{
+						// The light sample is a direction with known incident radiance and density:
+						// an importance-weighted sample of the incident-light distribution the network
+						// learns (weight lum(Le) |cos| / pdf, credited only if the segment turns out
+						// unoccluded). Light seen through a narrow opening is found far more often this
+						// way than by directions the BSDF or the network sampled.
+						const float wn = luminance(le) * fabsf(dot(frame.ns, l)) / pdf_w;
+						if(wn > 0.0f && isfinite(wn))
+						{
+							const uint32_t k2 = alloc_slot(&a.counters->n_train);
+							if(k2 < a.guide.train_cap)
+							{
+								const float4* fr = reinterpret_cast<const float4*>(a.guide.feat + static_cast<size_t>(grow) * 8);
+								float4* dst = reinterpret_cast<float4*>(a.guide.train_feat + static_cast<size_t>(k2) * 8);
+								const float4 f1 = fr[1];
+								dst[0] = fr[0];
+								dst[1] = make_float4(f1.x, f1.y, f1.z, 0.0f);
+								a.guide.train_dirw[k2] = make_float4(l.x, l.y, l.z, 0.0f);
+								nee_row = k2;
+								nee_w = wn;
+							}
+						}
 					}
 					const float mis = pdf_w * pdf_w / (pdf_w * pdf_w + pdf_bsdf * pdf_bsdf);
 					RGB w = f * fabsf(dot(frame.ns, l));
@@ -956,7 +982,7 @@ shade_kernel(ShadeArgs a)
 			}
 			if(GUIDED && a.shadow.t)
 			{
-				a.shadow.t[k] = make_float2(__uint_as_float(train_row), sh_train);
+				a.shadow.t[k] = make_float4(__uint_as_float(train_row), sh_train, __uint_as_float(nee_row), nee_w);
 			}
 			if(!continues && film.filter != PG_FILTER_BOX)
 			{
@@ -1026,6 +1052,7 @@ refine_kernel(DeviceScene s_single, const RenderCounters* __restrict__ c, PathBu
 				if(shadow.t)
 				{
 					shadow.t[k].y = 0.0f;
+					shadow.t[k].w = 0.0f;
 				}
 				shadow.o[k] = make_float4(o4.x, o4.y, o4.z, 0.0f);
 				shadow.d[k] = make_float4(0.0f, 0.0f, 1.0f, 0.0f);

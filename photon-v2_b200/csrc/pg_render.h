@@ -246,7 +246,8 @@ struct ShadowQueue
 	float4* o;          // origin, tmin
 	float4* d;          // direction, tmax
 	float4* c;          // contribution rgb, target (slot in next buffer, or 0x80000000|pixel)
-	float2* t;          // guided renders: training sample index (bits, or ~0), weight added if unoccluded
+	float4* t;          // guided renders: two training samples (index bits, or ~0; weight added if unoccluded):
+	                    // the previous vertex's sample, and this vertex's own NEE-direction sample
 	float2* r;          // filtered films: raster position of the sample a final contribution belongs to
 	uint32_t* sid;      // multi-scene renders: the scene of each record
 };
@@ -431,7 +432,7 @@ private:
 	bool m_guide_ready = false;
 	float m_bound_lo[3] = {0, 0, 0}, m_bound_rcp[3] = {1, 1, 1};
 	DeviceBuffer<float4>   m_gf0[2], m_gf1[2];
-	DeviceBuffer<float2>   m_st;
+	DeviceBuffer<float4>   m_st;
 	DeviceBuffer<uint32_t> m_gmap;
 	DeviceBuffer<float>    m_gfeat, m_graw;
 	DeviceBuffer<float>    m_tfeat, m_traw;

@@ -208,17 +208,21 @@ void check_device_error(Geometry& g, cudaStream_t s)
 // path buffer the record was made for) or, for paths that ended at that vertex, straight to the
 // FP64 film; guided renders also credit the training sample the record belongs to.
 __device__ __forceinline__ void add_unoccluded(uint32_t i, const float4* __restrict__ sc,
-                                               const float2* __restrict__ st, const float2* __restrict__ sr,
+                                               const float4* __restrict__ st, const float2* __restrict__ sr,
                                                float4* __restrict__ rad_target, const FilmView& film,
                                                float4* __restrict__ train_dirw)
 {
 	if(train_dirw)
 	{
-		const float2 tr = __ldg(st + i);
-		const uint32_t row = __float_as_uint(tr.x);
+		const float4 tr = __ldg(st + i);
+		const uint32_t row = __float_as_uint(tr.x), nee_row = __float_as_uint(tr.z);
 		if(row != 0xFFFFFFFFu && tr.y != 0.0f)
 		{
 			atomicAdd(&train_dirw[row].w, tr.y);
+		}
+		if(nee_row != 0xFFFFFFFFu && tr.w != 0.0f)
+		{
+			atomicAdd(&train_dirw[nee_row].w, tr.w);
 		}
 	}
 	const float4 c = __ldg(sc + i);
@@ -266,7 +270,7 @@ trace_kernel(const WideNode* __restrict__ nodes, const LeafTri* __restrict__ tri
              const float4* __restrict__ so, const float4* __restrict__ sd, const float4* __restrict__ sc,
              const float2* __restrict__ sr, float4* __restrict__ rad_cur, FilmView film, int min_idle,
              const uint32_t* __restrict__ meta, const uint32_t* __restrict__ shadow_sid, BatchView batch,
-             const float2* __restrict__ st, float4* __restrict__ train_dirw)
+             const float4* __restrict__ st, float4* __restrict__ train_dirw)
 {
 	const uint32_t n_closest = counters->n_total;
 	const uint32_t n_shadow = counters->n_shadow_prev;
