@@ -239,50 +239,67 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 6
     """Guided vs plain GPU BNEEPT on the slit-light room (2M triangles), as time to reach a relMSE
     target against a 65,536-spp plain render of the same scene.
 
-    relMSE of an unbiased n-spp render falls as 1/n, so each method is rendered once at a probe
+    relMSE of an unbiased n-spp render falls as c/n, so each method is rendered once at a probe
     count, its relMSE gives the count that reaches `target`, and it is rendered again at that
-    count: time_to_target = its device time x (its relMSE / target). Guided renders start from a
-    network trained by `warmup_renders` renders (training time reported apart) and keep training;
-    `guided_frozen` renders with the trained network and no further training. A ratio below 1
-    means guiding reaches the target sooner; the north star's target is a ratio of at most 0.5.
+    count: time_to_target = its device time x (its relMSE / target). The reference render is itself
+    noisy: against it, an n-spp render measures c/n + c_plain/ref_spp, where the second term (the
+    reference's own error, estimated from the plain renders) is the same for every method and is
+    subtracted before the extrapolation. Guided renders start from a network trained by
+    `warmup_renders` renders (training time reported apart) and keep training; `guided_frozen`
+    renders with the trained network and no further training. A ratio below 1 means guiding
+    reaches the target sooner; the north star's target is a ratio of at most 0.5.
     """
     import photon_gpu
 
     scene = scenes.slit_room(res, res, 1, 10, num_boxes=num_boxes)
+    floor = {"relmse": 0.0}
 
-    def to_target(rs, seed):
+    def to_target(rs, seed, plain=False):
         rs.clear()
         rs.render(probe_spp, max_bounces=10, seed=seed)
         e_probe = rel_mse(rs.film()[0], ref)
-        spp = int(min(16384, max(probe_spp, np.ceil(probe_spp * e_probe / target))))
+        if plain:
+            # e = c/n + c/ref_spp for the plain estimator against its own reference
+            floor["relmse"] = e_probe / (1.0 / probe_spp + 1.0 / ref_spp) / ref_spp
+        c_probe = max(e_probe - floor["relmse"], 1e-12) * probe_spp
+        spp = int(min(65536, max(probe_spp, np.ceil(c_probe / target))))
         rs.clear()
         r = rs.render(spp, max_bounces=10, seed=seed + 1)
         e = rel_mse(rs.film()[0], ref)
-        return {"spp": spp, "ms": r["ms"], "relmse": e, "probe_relmse": e_probe,
-                "ms_to_target": r["ms"] * e / target}
+        if plain:
+            floor["relmse"] = e / (1.0 / spp + 1.0 / ref_spp) / ref_spp
+        e_own = max(e - floor["relmse"], 1e-12)
+        return {"spp": spp, "ms": r["ms"], "relmse_vs_reference": e, "relmse": e_own, "probe_relmse": e_probe,
+                "ms_to_target": r["ms"] * e_own / target}
 
     with photon_gpu.RenderScene(scene) as rs:
         t0 = time.time()
         rs.render(ref_spp, max_bounces=10, seed=1)
         ref = rs.film()[0]
         ref_s = time.time() - t0
-        plain = to_target(rs, 100)
+        plain = to_target(rs, 100, plain=True)
         rs.set_guiding(True, True, 0.5, 3e-3, 16384)
         train_ms = 0.0
         for k in range(warmup_renders):
             rs.clear()
             train_ms += rs.render(warmup_spp, max_bounces=10, seed=200 + k)["ms"]
         guided = to_target(rs, 300)
+        prof_guided = rs.profile(probe_spp, max_bounces=10, seed=310)
         info = rs.guide_info()
         rs.set_guiding(True, False, 0.5, 3e-3, 16384)
         frozen = to_target(rs, 400)
+        rs.set_guiding(False, False, 0.5, 3e-3, 16384)
+        prof_plain = rs.profile(probe_spp, max_bounces=10, seed=110)
     ratio = guided["ms_to_target"] / plain["ms_to_target"]
     return {
-        "workload": f"slit_room {res}x{res}, {scene.num_tris} triangles, depth 10 (the C4 room at reduced resolution)",
+        "workload": f"slit_room {res}x{res}, {scene.num_tris} triangles, depth 10",
         "width": res, "height": res, "triangles": scene.num_tris, "max_bounces": 10,
         "reference_spp": ref_spp, "reference_s": ref_s, "target_relmse": target, "relmse_eps": 1e-2,
+        "reference_noise_relmse": floor["relmse"],
         "plain": plain, "guided": guided, "guided_frozen": frozen,
         "training": {"renders": warmup_renders, "spp": warmup_spp, "ms": train_ms, "final_loss": info["loss"]},
+        # per-kernel device ms of one probe-spp render each (extend_ms: the merged trace launch)
+        "cost_breakdown_ms": {"plain": prof_plain, "guided": prof_guided},
         "time_ratio": ratio,
         "time_ratio_with_training": (guided["ms_to_target"] + train_ms) / plain["ms_to_target"],
         "time_ratio_frozen": frozen["ms_to_target"] / plain["ms_to_target"],
