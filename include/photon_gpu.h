@@ -109,6 +109,10 @@ PGPU_API int pgpu_trace_counts(uint64_t id, const float* rays, uint64_t n, int a
  * W3, b3, W4[64][40], b4 (W[in][out]). The forward pass runs on the tensor cores (tcgen05, BF16
  * operands, FP32 accumulation). features: host [n][7]; out_raw: host [n][40]. */
 PGPU_API int pgpu_guide_forward(const float* params, const float* features, uint64_t n, float* out_raw);
+/* The same forward pass, returning the decoded mixtures the renderer samples: host [n][48], per
+ * lobe (weight, mean x, y, z, concentration kappa, weight x kappa / (2 pi (1 - exp(-2 kappa)))),
+ * weights the softmax of the logits, means normalised, kappa = exp(raw) clamped to [1e-2, 5e3]. */
+PGPU_API int pgpu_guide_mixture(const float* params, const float* features, uint64_t n, float* out_mix);
 
 /* Training loss -sum_i w_i log q(d_i | x_i) / sum_i w_i of a batch (features [n][7], unit
  * directions [n][3], weights [n]) and its gradient with respect to all parameters

@@ -1,13 +1,19 @@
 // Guiding network on the 5th-generation tensor cores: fused forward pass of the whole MLP with
 // tcgen05.mma (BF16 operands in shared memory, FP32 accumulators in tensor memory).
 //
-// One CTA of 128 threads per SM walks 128-row tiles of queries. Per tile:
-//   1. every thread one-blob encodes its query row into the A operand buffer (BF16, 224 columns);
+// Two CTAs of 256 threads per SM walk 128-row tiles of queries; each row is owned by two threads
+// (part 0: threads 0-127, part 1: threads 128-255, thread t and t + 128 on row t), so that the
+// per-row work between the MMAs is split in two and each SM has 16 warps to hide its latency.
+// Per tile:
+//   1. the two threads of a row one-blob encode its inputs (alternating inputs) into the A
+//      operand buffer (BF16, 224 columns, fed to the MMAs in two K halves);
 //   2. per layer, one elected thread issues the K/16 MMAs (M = 128, N = 64 or 48, K = 16 each)
 //      into tensor memory and commits them to an mbarrier;
-//   3. after the barrier completes, thread t reads row t of the accumulator (tcgen05.ld, TMEM lane
-//      t), adds the bias, applies ReLU, rounds to BF16 and writes the row as the next layer's A
-//      operand (or, after the last layer, the 40 raw outputs to global memory).
+//   3. after the barrier completes, each thread reads its half of its row of the accumulator
+//      (tcgen05.ld from the TMEM lane of the row: warps w and w + 4 share lanes 32 (w % 4) ...),
+//      adds the bias, applies ReLU, rounds to BF16 and writes it as the next layer's A operand;
+//      after the last layer each thread decodes 4 of the row's 8 lobes (the softmax's maximum and
+//      sum are exchanged through shared memory) or writes its 20 raw outputs.
 // All weights (BF16, 59 KB) stay resident in shared memory for the kernel's lifetime.
 //
 // Operand layout: K-major, no swizzle. A core matrix is 8 rows x 16 bytes (8 BF16 along K); for a
@@ -37,8 +43,11 @@ namespace
 
 using namespace tc;
 
-constexpr int kThreads = 128;
+constexpr int kThreads = 256;                 // two threads per tile row
+constexpr int kParts = kThreads / kTile;
 constexpr uint32_t kTmemCols = 128;   // power of two >= 64 accumulator columns
+static_assert(kParts == 2 && kHidden == 64 && kLobes == 8 && kOut == 40 && kOutPad == 48,
+              "the column split below assumes two parts, 64 hidden units and 8 lobes");
 
 // ---- shared-memory image of the weights (also the device-side packed format)
 constexpr int kW0Bytes = kHidden * kIn * 2;         // 28,672
@@ -63,7 +72,8 @@ constexpr int kActHBytes = kTile * kHidden * 2;     // 16,384: hidden pong
 constexpr int kOffSmemImage = 0;
 constexpr int kOffSmemActIn = (kImageBytes + 1023) / 1024 * 1024;
 constexpr int kOffSmemActH = kOffSmemActIn + kActInBytes;
-constexpr int kOffSmemBar = kOffSmemActH + kActHBytes;         // 8-byte aligned
+constexpr int kOffSmemXch = kOffSmemActH + kActHBytes;         // [part][row] float2: softmax max, sum
+constexpr int kOffSmemBar = kOffSmemXch + kParts * kTile * 8;  // 8-byte aligned
 constexpr int kOffSmemTmem = kOffSmemBar + 8;
 constexpr int kSmemBytes = kOffSmemTmem + 8;
 static_assert(kImageBytes % 16 == 0 && kOffSmemActH % 16 == 0 && kOffSmemBar % 8 == 0, "alignment");
@@ -97,6 +107,8 @@ mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restr
 	extern __shared__ __align__(128) unsigned char smem[];
 	const uint32_t tid = threadIdx.x;
 	const uint32_t warp = tid >> 5;
+	const uint32_t r = tid & (kTile - 1);   // the tile row this thread works on
+	const uint32_t part = tid / kTile;      // which half of the row's columns / lobes
 
 	// weights + biases into shared memory
 	{
@@ -124,11 +136,12 @@ mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restr
 	__syncthreads();
 	fence_after_sync();
 	const uint32_t tmem = *tmem_slot;
-	const uint32_t tmem_row = tmem + ((warp * 32u) << 16);   // this warp's 32 lanes, column 0
+	const uint32_t tmem_row = tmem + (((warp & 3u) * 32u) << 16);   // this warp's 32 lanes, column 0
 
 	const float* bias = reinterpret_cast<const float*>(smem + kOffImgBias);
 	unsigned char* act_in = smem + kOffSmemActIn;
 	unsigned char* act_h = smem + kOffSmemActH;
+	float2* xch = reinterpret_cast<float2*>(smem + kOffSmemXch);
 	const uint32_t w_addr[5] = {smem_u32(smem + kOffImgW0), smem_u32(smem + kOffImgW1), smem_u32(smem + kOffImgW2),
 	                            smem_u32(smem + kOffImgW3), smem_u32(smem + kOffImgW4)};
 
@@ -137,7 +150,7 @@ mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restr
 	const uint32_t num_tiles = (n + kTile - 1) / kTile;
 	for(uint32_t tile = blockIdx.x; tile < num_tiles && !failed; tile += gridDim.x)
 	{
-		const uint32_t row = tile * kTile + tid;
+		const uint32_t row = tile * kTile + r;
 		const bool valid = row < n;
 
 		float f[kInputs];
@@ -181,12 +194,13 @@ mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restr
 			return true;
 		};
 
-		// 1. input layer in two K halves: one-blob encode, then accumulate into TMEM
+		// 1. input layer in two K halves: one-blob encode (the row's two threads take alternate
+		//    inputs), then accumulate into TMEM
 		bool tile_ok = true;
 		for(int half = 0; half < 2 && tile_ok; ++half)
 		{
 			const int i0 = half == 0 ? 0 : 4, i1 = half == 0 ? 4 : kInputs;
-			for(int i = i0; i < i1; ++i)
+			for(int i = i0 + static_cast<int>(part); i < i1; i += kParts)
 			{
 				#pragma unroll
 				for(int c = 0; c < kBins / 8; ++c)
@@ -197,7 +211,7 @@ mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restr
 					{
 						v[j] = valid ? fast_blob(f[i], c * 8 + j) : 0.0f;
 					}
-					store_row8(act_in, tid, static_cast<uint32_t>((i - i0) * kBins + c * 8), v);
+					store_row8(act_in, r, static_cast<uint32_t>((i - i0) * kBins + c * 8), v);
 				}
 			}
 			fence_async_smem();
@@ -229,70 +243,99 @@ mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restr
 				}
 			}
 
-			float acc[64];
-			#pragma unroll
-			for(int c = 0; c < 4; ++c)
-			{
-				if(c * 16 < static_cast<int>(n_dim))
-				{
-					tmem_ld16(tmem_row + c * 16, acc + c * 16);
-				}
-			}
-			tmem_wait_ld();
-
 			if(!last)
 			{
-				const float* b = bias + layer * kHidden;
+				// hidden units [32 part, 32 part + 32) of the row
+				const uint32_t c0 = part * 32u;
+				float acc[32];
+				tmem_ld16(tmem_row + c0, acc);
+				tmem_ld16(tmem_row + c0 + 16u, acc + 16);
+				tmem_wait_ld();
+				const float* b = bias + layer * kHidden + c0;
 				#pragma unroll
-				for(int j = 0; j < kHidden; ++j)
+				for(int j = 0; j < 32; ++j)
 				{
 					acc[j] = fmaxf(acc[j] + b[j], 0.0f);
 				}
 				#pragma unroll
-				for(int c = 0; c < kHidden / 8; ++c)
+				for(int c = 0; c < 4; ++c)
 				{
-					store_row8(o_buf, tid, c * 8, acc + c * 8);
+					store_row8(o_buf, r, c0 + c * 8, acc + c * 8);
 				}
 				if(out_acts && valid)
 				{
-					uint4* dst = reinterpret_cast<uint4*>(out_acts + (static_cast<size_t>(row) * kHiddenLayers + layer) * kHidden);
+					uint4* dst = reinterpret_cast<uint4*>(out_acts + (static_cast<size_t>(row) * kHiddenLayers + layer) * kHidden + c0);
 					#pragma unroll
-					for(int c = 0; c < kHidden / 8; ++c)
+					for(int c = 0; c < 4; ++c)
 					{
 						dst[c] = make_uint4(pack_bf16x2(acc[c * 8 + 0], acc[c * 8 + 1]), pack_bf16x2(acc[c * 8 + 2], acc[c * 8 + 3]),
 						                    pack_bf16x2(acc[c * 8 + 4], acc[c * 8 + 5]), pack_bf16x2(acc[c * 8 + 6], acc[c * 8 + 7]));
 					}
 				}
 			}
-			else if(valid)
+			else
 			{
-				const float* b = bias + kHiddenLayers * kHidden;
+				// lobes [4 part, 4 part + 4): raw outputs [20 part, 20 part + 20), inside the
+				// loaded accumulator columns [16 part, 16 part + 32)
+				float acc[32];
+				tmem_ld16(tmem_row + part * 16u, acc);
+				tmem_ld16(tmem_row + part * 16u + 16u, acc + 16);
+				tmem_wait_ld();
+				const float* b = bias + kHiddenLayers * kHidden + part * 20u;
+				float raw[20];
 				#pragma unroll
-				for(int j = 0; j < kOut; ++j)
+				for(int q = 0; q < 20; ++q)
 				{
-					acc[j] += b[j];
+					raw[q] = (part ? acc[q + 4] : acc[q]) + b[q];
 				}
-				if(out_raw)
+				if(out_raw && valid)
 				{
-					float4* dst = reinterpret_cast<float4*>(out_raw + static_cast<size_t>(row) * kOut);
+					float4* dst = reinterpret_cast<float4*>(out_raw + static_cast<size_t>(row) * kOut + part * 20u);
 					#pragma unroll
-					for(int c = 0; c < kOut / 4; ++c)
+					for(int c = 0; c < 5; ++c)
 					{
-						dst[c] = make_float4(acc[4 * c + 0], acc[4 * c + 1], acc[4 * c + 2], acc[4 * c + 3]);
+						dst[c] = make_float4(raw[4 * c + 0], raw[4 * c + 1], raw[4 * c + 2], raw[4 * c + 3]);
 					}
 				}
-				if(out_mix)
+				if(out_mix)   // a kernel argument: the same for every thread, so the barriers are safe
 				{
-					const Mixture m = decode(acc);
-					float2* dst = reinterpret_cast<float2*>(out_mix + static_cast<size_t>(row) * kMixFloats);
+					// the mixture of decode(): softmax weights over all 8 lobes, unit means, clamped
+					// concentrations, and each lobe's weight x vMF normalisation
+					float mx = raw[0];
 					#pragma unroll
-					for(int j = 0; j < kLobes; ++j)
+					for(int j = 1; j < 4; ++j)
 					{
-						const float k = m.kappa[j];
-						const float c = m.w[j] * k / (2.0f * kPi * (1.0f - expf(-2.0f * k)));
-						dst[3 * j + 0] = make_float2(m.w[j], m.mu[j].x);
-						dst[3 * j + 1] = make_float2(m.mu[j].y, m.mu[j].z);
-						dst[3 * j + 2] = make_float2(k, c);
+						mx = fmaxf(mx, raw[5 * j]);
+					}
+					xch[part * kTile + r].x = mx;
+					__syncthreads();
+					mx = fmaxf(xch[r].x, xch[kTile + r].x);
+					float e[4], sum = 0.0f;
+					#pragma unroll
+					for(int j = 0; j < 4; ++j)
+					{
+						e[j] = expf(raw[5 * j] - mx);
+						sum += e[j];
+					}
+					xch[part * kTile + r].y = sum;
+					__syncthreads();
+					sum = xch[r].y + xch[kTile + r].y;
+					if(valid)
+					{
+						float2* dst = reinterpret_cast<float2*>(out_mix + static_cast<size_t>(row) * kMixFloats) + 12u * part;
+						#pragma unroll
+						for(int j = 0; j < 4; ++j)
+						{
+							const float w = e[j] / sum;
+							V3 d = v3(raw[5 * j + 1], raw[5 * j + 2], raw[5 * j + 3]);
+							const float l2 = dot(d, d);
+							const V3 mu = l2 > 1e-20f ? d * (1.0f / sqrtf(l2)) : v3(0.0f, 0.0f, 1.0f);
+							const float k = fminf(fmaxf(expf(raw[5 * j + 4]), kMinKappa), kMaxKappa);
+							const float c = w * k / (2.0f * kPi * (1.0f - expf(-2.0f * k)));
+							dst[3 * j + 0] = make_float2(w, mu.x);
+							dst[3 * j + 1] = make_float2(mu.y, mu.z);
+							dst[3 * j + 2] = make_float2(k, c);
+						}
 					}
 				}
 			}
@@ -399,50 +442,88 @@ void launch_forward(const unsigned char* d_image, const float* d_features, uint3
 
 using namespace pg;
 
+namespace
+{
+
+// Host entry of the forward pass: copies the parameters and queries in, runs the tensor-core
+// kernel, and copies back the raw outputs [n][40] and / or the decoded mixtures [n][48].
+void forward_on_host(const char* what, const float* params, const float* features, uint64_t n, float* out_raw,
+                     float* out_mix)
+{
+	if(!params || (n > 0 && (!features || (!out_raw && !out_mix))))
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, std::string(what) + ": null pointer");
+	}
+	if(n > (1u << 30))
+	{
+		throw Error(PG_ERR_INVALID_ARGUMENT, std::string(what) + ": too many queries");
+	}
+	require_device();
+	if(n == 0)
+	{
+		return;
+	}
+	cudaStream_t s = library_stream();
+	DeviceBuffer<float> d_params(guide::kNumParams);
+	DeviceBuffer<unsigned char> d_image(guide::image_bytes());
+	DeviceBuffer<float> d_feat(n * 8);
+	DeviceBuffer<float> d_raw(out_raw ? n * guide::kOut : 0);
+	DeviceBuffer<float> d_mix(out_mix ? n * guide::kMixFloats : 0);
+	DeviceBuffer<uint32_t> d_err(1);
+	PG_CUDA_CHECK(cudaMemsetAsync(d_err.get(), 0, sizeof(uint32_t), s));
+	PG_CUDA_CHECK(cudaMemcpyAsync(d_params.get(), params, d_params.bytes(), cudaMemcpyHostToDevice, s));
+	// features: host [n][7] -> device [n][8]
+	std::vector<float> feat(n * 8, 0.0f);
+	for(uint64_t i = 0; i < n; ++i)
+	{
+		std::memcpy(&feat[i * 8], features + i * guide::kInputs, sizeof(float) * guide::kInputs);
+	}
+	PG_CUDA_CHECK(cudaMemcpyAsync(d_feat.get(), feat.data(), d_feat.bytes(), cudaMemcpyHostToDevice, s));
+	guide::pack_image(d_params.get(), d_image.get(), s);
+	guide::launch_forward(d_image.get(), d_feat.get(), static_cast<uint32_t>(n), out_raw ? d_raw.get() : nullptr,
+	                      nullptr, d_err.get(), s, nullptr, out_mix ? d_mix.get() : nullptr);
+	uint32_t err = 0;
+	if(out_raw)
+	{
+		PG_CUDA_CHECK(cudaMemcpyAsync(out_raw, d_raw.get(), d_raw.bytes(), cudaMemcpyDeviceToHost, s));
+	}
+	if(out_mix)
+	{
+		PG_CUDA_CHECK(cudaMemcpyAsync(out_mix, d_mix.get(), d_mix.bytes(), cudaMemcpyDeviceToHost, s));
+	}
+	PG_CUDA_CHECK(cudaMemcpyAsync(&err, d_err.get(), sizeof(err), cudaMemcpyDeviceToHost, s));
+	PG_CUDA_CHECK(cudaStreamSynchronize(s));
+	if(err)
+	{
+		throw Error(PG_ERR_CUDA, "guiding network: tensor-core wait timed out");
+	}
+}
+
+}// end anonymous namespace
+
 extern "C" {
 
 int pgpu_guide_forward(const float* params, const float* features, uint64_t n, float* out_raw)
 {
 	return guarded([&]
 	{
-		if(!params || (n > 0 && (!features || !out_raw)))
+		if(n > 0 && !out_raw)
 		{
 			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_guide_forward: null pointer");
 		}
-		if(n > (1u << 30))
+		forward_on_host("pgpu_guide_forward", params, features, n, out_raw, nullptr);
+	});
+}
+
+int pgpu_guide_mixture(const float* params, const float* features, uint64_t n, float* out_mix)
+{
+	return guarded([&]
+	{
+		if(n > 0 && !out_mix)
 		{
-			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_guide_forward: too many queries");
+			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_guide_mixture: null pointer");
 		}
-		require_device();
-		if(n == 0)
-		{
-			return;
-		}
-		cudaStream_t s = library_stream();
-		DeviceBuffer<float> d_params(guide::kNumParams);
-		DeviceBuffer<unsigned char> d_image(guide::image_bytes());
-		DeviceBuffer<float> d_feat(n * 8);
-		DeviceBuffer<float> d_out(n * guide::kOut);
-		DeviceBuffer<uint32_t> d_err(1);
-		PG_CUDA_CHECK(cudaMemsetAsync(d_err.get(), 0, sizeof(uint32_t), s));
-		PG_CUDA_CHECK(cudaMemcpyAsync(d_params.get(), params, d_params.bytes(), cudaMemcpyHostToDevice, s));
-		// features: host [n][7] -> device [n][8]
-		std::vector<float> feat(n * 8, 0.0f);
-		for(uint64_t i = 0; i < n; ++i)
-		{
-			std::memcpy(&feat[i * 8], features + i * guide::kInputs, sizeof(float) * guide::kInputs);
-		}
-		PG_CUDA_CHECK(cudaMemcpyAsync(d_feat.get(), feat.data(), d_feat.bytes(), cudaMemcpyHostToDevice, s));
-		guide::pack_image(d_params.get(), d_image.get(), s);
-		guide::launch_forward(d_image.get(), d_feat.get(), static_cast<uint32_t>(n), d_out.get(), nullptr, d_err.get(), s);
-		uint32_t err = 0;
-		PG_CUDA_CHECK(cudaMemcpyAsync(out_raw, d_out.get(), d_out.bytes(), cudaMemcpyDeviceToHost, s));
-		PG_CUDA_CHECK(cudaMemcpyAsync(&err, d_err.get(), sizeof(err), cudaMemcpyDeviceToHost, s));
-		PG_CUDA_CHECK(cudaStreamSynchronize(s));
-		if(err)
-		{
-			throw Error(PG_ERR_CUDA, "guiding network: tensor-core wait timed out");
-		}
+		forward_on_host("pgpu_guide_mixture", params, features, n, nullptr, out_mix);
 	});
 }
 

@@ -232,11 +232,9 @@ __device__ __forceinline__ uint32_t intersect_children(
 #pragma unroll
 		for(int j = 0; j < 4; ++j)
 		{
+			// Branch-free: every slot is tested (an empty slot, m = 0, contributes no bits), so the
+			// lanes of a warp stay converged through the eight tests whatever their nodes hold.
 			const uint32_t m = byte_of(meta[half], j);
-			if(m == 0u)
-			{
-				continue;
-			}
 			const float tnx = fmaf(static_cast<float>(byte_of(nearx, j)), scx, bx);
 			const float tny = fmaf(static_cast<float>(byte_of(neary, j)), scy, by);
 			const float tnz = fmaf(static_cast<float>(byte_of(nearz, j)), scz, bz);
@@ -245,19 +243,10 @@ __device__ __forceinline__ uint32_t intersect_children(
 			const float tfz = fmaf(static_cast<float>(byte_of(farz, j)), scz, bz);
 			const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, t_min));
 			const float tf = fminf(fminf(tfx, tfy), fminf(tfz, t_max));
-			if(tn <= tf)
-			{
-				const int s = half * 4 + j;
-				if((imask >> s) & 1u)
-				{
-					hits |= 1u << (24u + (static_cast<uint32_t>(s) ^ r.oct));
-				}
-				else
-				{
-					const uint32_t unary = m >> 5;
-					hits |= unary << (m & 31u);
-				}
-			}
+			const int s = half * 4 + j;
+			const uint32_t bits = ((imask >> s) & 1u) ? 1u << (24u + (static_cast<uint32_t>(s) ^ r.oct))
+			                                          : (m >> 5) << (m & 31u);
+			hits |= (tn <= tf && m != 0u) ? bits : 0u;
 		}
 	}
 	return hits;

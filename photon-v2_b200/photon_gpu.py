@@ -45,6 +45,7 @@ PGPU_SIGNATURES = [
      [ctypes.c_uint64, _f32p, ctypes.c_uint64, ctypes.c_int, _dblp, _dblp]),
     ("pgpu_bsdf_eval", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
     ("pgpu_guide_forward", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
+    ("pgpu_guide_mixture", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
     ("pgpu_guide_gradients", ctypes.c_int, [_f32p, _f32p, _f32p, _f32p, ctypes.c_uint64, _f32p, _f32p]),
     ("pgpu_guide_gradients_ex", ctypes.c_int,
      [_f32p, _f32p, _f32p, _f32p, ctypes.c_uint64, ctypes.c_uint32, _f32p, _f32p]),
@@ -215,6 +216,17 @@ def guide_forward(params: np.ndarray, features: np.ndarray) -> np.ndarray:
     f = np.ascontiguousarray(features, np.float32).reshape(-1, 7)
     out = np.empty((f.shape[0], 40), np.float32)
     _check(load().pgpu_guide_forward(_ptr(p, ctypes.c_float), _ptr(f, ctypes.c_float), f.shape[0],
+                                     _ptr(out, ctypes.c_float)))
+    return out
+
+
+def guide_mixture(params: np.ndarray, features: np.ndarray) -> np.ndarray:
+    """Decoded mixtures [n, 8, 6] of the guiding network for features [n, 7]: per lobe (weight,
+    mean xyz, kappa, weight x vMF normalisation), as the renderer samples them."""
+    p = np.ascontiguousarray(params, np.float32).reshape(-1)
+    f = np.ascontiguousarray(features, np.float32).reshape(-1, 7)
+    out = np.empty((f.shape[0], 8, 6), np.float32)
+    _check(load().pgpu_guide_mixture(_ptr(p, ctypes.c_float), _ptr(f, ctypes.c_float), f.shape[0],
                                      _ptr(out, ctypes.c_float)))
     return out
 

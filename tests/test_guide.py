@@ -73,6 +73,28 @@ def test_tensor_core_forward_matches_oracle(gpu_lib, n):
     assert err.mean() <= 0.002 * rms, (err.mean(), rms)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 200, 4099])
+def test_decoded_mixture_matches_oracle_decode(gpu_lib, n):
+    """The mixtures the forward kernel decodes for the renderer (the two threads of a row each
+    decode 4 lobes, exchanging the softmax's maximum and sum) against the oracle's decode of the
+    kernel's own raw outputs."""
+    import photon_gpu
+
+    params = ref.init_params(11, out_scale=1.0)
+    f, _, _ = _batch(n, 12)
+    raw = photon_gpu.guide_forward(params, f)
+    mix = photon_gpu.guide_mixture(params, f)
+    w, mu, kappa = ref.decode(raw)
+    norm = w * kappa / (2 * np.pi * (1 - np.exp(-2 * kappa)))
+    assert np.all(np.isfinite(mix))
+    np.testing.assert_allclose(mix[:, :, 0], w, rtol=2e-6, atol=1e-7)
+    np.testing.assert_allclose(mix[:, :, 1:4], mu, rtol=0, atol=1e-6)
+    np.testing.assert_allclose(mix[:, :, 4], kappa, rtol=2e-6)
+    np.testing.assert_allclose(mix[:, :, 5], norm, rtol=1e-5)
+    assert np.allclose(mix[:, :, 0].sum(axis=1), 1.0, atol=2e-6)
+
+
 def _sample_vmf(mu, kappa, rng):
     """Directions around unit mu [n, 3] with concentration kappa (Wood / Jakob method)."""
     n = mu.shape[0]
