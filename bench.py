@@ -235,7 +235,8 @@ def rel_mse(x: np.ndarray, ref: np.ndarray, eps: float = 1e-2) -> float:
 
 
 def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 65536, probe_spp: int = 64,
-                      target: float = 1e-3, warmup_renders: int = 8, warmup_spp: int = 32) -> dict:
+                      target: float = 1e-3, warmup_renders: int = 8, warmup_spp: int = 32,
+                      alpha: float = 0.5) -> dict:
     """Guided vs plain GPU BNEEPT on the slit-light room (2M triangles), as time to reach a relMSE
     target against a 65,536-spp plain render of the same scene.
 
@@ -246,8 +247,9 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 6
     reference's own error, estimated from the plain renders) is the same for every method and is
     subtracted before the extrapolation. Guided renders start from a network trained by
     `warmup_renders` renders (training time reported apart) and keep training; `guided_frozen`
-    renders with the trained network and no further training. A ratio below 1 means guiding
-    reaches the target sooner; the north star's target is a ratio of at most 0.5.
+    renders with the trained network and no further training. alpha: the probability of sampling
+    the learned mixture at a guided vertex. A ratio below 1 means guiding reaches the target
+    sooner; the north star's target is a ratio of at most 0.5.
     """
     import photon_gpu
 
@@ -278,7 +280,7 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 6
         ref = rs.film()[0]
         ref_s = time.time() - t0
         plain = to_target(rs, 100, plain=True)
-        rs.set_guiding(True, True, 0.5, 3e-3, 16384)
+        rs.set_guiding(True, True, alpha, 3e-3, 16384)
         train_ms = 0.0
         for k in range(warmup_renders):
             rs.clear()
@@ -286,16 +288,16 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 6
         guided = to_target(rs, 300)
         prof_guided = rs.profile(probe_spp, max_bounces=10, seed=310)
         info = rs.guide_info()
-        rs.set_guiding(True, False, 0.5, 3e-3, 16384)
+        rs.set_guiding(True, False, alpha, 3e-3, 16384)
         frozen = to_target(rs, 400)
-        rs.set_guiding(False, False, 0.5, 3e-3, 16384)
+        rs.set_guiding(False, False, alpha, 3e-3, 16384)
         prof_plain = rs.profile(probe_spp, max_bounces=10, seed=110)
     ratio = guided["ms_to_target"] / plain["ms_to_target"]
     return {
         "workload": f"slit_room {res}x{res}, {scene.num_tris} triangles, depth 10",
         "width": res, "height": res, "triangles": scene.num_tris, "max_bounces": 10,
         "reference_spp": ref_spp, "reference_s": ref_s, "target_relmse": target, "relmse_eps": 1e-2,
-        "reference_noise_relmse": floor["relmse"],
+        "reference_noise_relmse": floor["relmse"], "alpha": alpha,
         "plain": plain, "guided": guided, "guided_frozen": frozen,
         "training": {"renders": warmup_renders, "spp": warmup_spp, "ms": train_ms, "final_loss": info["loss"]},
         # per-kernel device ms of one probe-spp render each (extend_ms: the merged trace launch)
