@@ -286,10 +286,9 @@ __device__ __forceinline__ uint32_t alloc_slot(uint32_t* counter)
 
 // ---------------------------------------------------------------------------------------------
 
-// parity: the iteration's place in the ping-pong pair. Training samples are made in odd
-// iterations and trained on at the end of the following even one, so the count of samples is
-// reset only when an odd iteration starts.
-__global__ void prepare_kernel(RenderCounters* c, uint32_t capacity, uint32_t parity)
+// new_samples: this iteration starts a training period's samples (position 1 of the four-iteration
+// period), so their count is reset; the samples of a period are trained on at its last iteration.
+__global__ void prepare_kernel(RenderCounters* c, uint32_t capacity, uint32_t new_samples)
 {
 	if(threadIdx.x != 0 || blockIdx.x != 0)
 	{
@@ -310,7 +309,7 @@ __global__ void prepare_kernel(RenderCounters* c, uint32_t capacity, uint32_t pa
 	c->fetch_shadow = 0;
 	c->guided_total += c->n_guided;
 	c->n_guided = 0;
-	if(parity)
+	if(new_samples)
 	{
 		c->n_train = 0;
 	}
@@ -588,6 +587,33 @@ shade_kernel(ShadeArgs a)
 				a.guide.train_dirw[k] = make_float4(d.x, d.y, d.z, 0.0f);
 			}
 		}
+		// The training record this path's contributions are credited to: the one made here, or one
+		// made at an earlier vertex and still open. An open record collects what the path gathers
+		// after its next vertex (emission found later, NEE further on) divided by the path
+		// throughput at that vertex, i.e. the radiance that arrived along the sampled direction
+		// after more bounces, such as light reaching a matte surface through glass.
+		uint32_t rec_row = GUIDED ? train_row : 0xFFFFFFFFu;
+		float rec_scale = 0.0f;   // the record's |cos| / pdf over the throughput at its next vertex
+		const bool rec_new = GUIDED && train_row != 0xFFFFFFFFu;
+		if(GUIDED && !rec_new && (meta & kMetaGuideOpen) && a.guide.open)
+		{
+			const float4 g0 = cur_gf0(a, i);
+			rec_row = __float_as_uint(g0.x);
+			rec_scale = g0.y;
+		}
+		const float lum_before = GUIDED ? luminance(radiance) : 0.0f;
+		// emission this vertex added to the path, credited to an open record
+		auto credit_open = [&]
+		{
+			if(GUIDED && rec_row != 0xFFFFFFFFu && !rec_new)
+			{
+				const float added = luminance(radiance) - lum_before;
+				if(added > 0.0f && isfinite(added))
+				{
+					a.guide.train_dirw[rec_row].w += added * rec_scale;
+				}
+			}
+		};
 
 		// ---- miss: environment (the dome primitive is hit after every triangle missed)
 		if(hit.x == 0xFFFFFFFFu)
@@ -624,6 +650,7 @@ shade_kernel(ShadeArgs a)
 					radiance = radiance + le * safe_clamp(thr_emit, 0.0f, kClampMax);
 				}
 			}
+			credit_open();
 			splat(film, pixel, p, radiance);
 			continue;
 		}
@@ -685,6 +712,7 @@ shade_kernel(ShadeArgs a)
 			{
 				radiance = radiance + le * safe_clamp(thr_emit, 0.0f, kClampMax);
 			}
+			credit_open();
 		}
 
 		// ---- does the path continue past this vertex?
@@ -694,6 +722,10 @@ shade_kernel(ShadeArgs a)
 			continue;
 		}
 		const RGB throughput = thr_emit * cont;
+		if(rec_new)
+		{
+			rec_scale = train_wfac / fmaxf(luminance(throughput), 1e-20f);
+		}
 		const Material mat = s.materials[mat_index];
 		const V3 v = -d;
 
@@ -707,7 +739,6 @@ shade_kernel(ShadeArgs a)
 		// all execute the same loop; this kernel leaves the hit point, its triangle and the target.
 		const bool defer_refine = a.refine.mode == PG_REFINE_ITERATIVE;
 		RGB sh_c{};
-		float sh_train = 0.0f;   // unweighted direct-light estimate (luminance) for the training sample
 		uint32_t nee_row = 0xFFFFFFFFu;   // this vertex's NEE direction as a training sample of its own
 		float nee_w = 0.0f;
 		const uint32_t grow = GUIDED ? a.guide.map[i] : 0xFFFFFFFFu;
@@ -814,10 +845,6 @@ shade_kernel(ShadeArgs a)
 					{
 						// the direction-sampling technique at a guided vertex is the one-sample mixture
 						pdf_bsdf = alpha * guide_pdf(graw, l) + (1.0f - alpha) * pdf_bsdf;
-					}
-					if(GUIDED && train_row != 0xFFFFFFFFu)
-					{
-						sh_train = luminance(le * (f * (fabsf(dot(frame.ns, l)) / pdf_w))) * train_wfac;
 					}
 					if(GUIDED && guided && a.guide.train_cap)
 					{
@@ -930,8 +957,10 @@ shade_kernel(ShadeArgs a)
 				// throughput, so a killed BVPT path ends here
 				continues = false;
 			}
+			const bool new_rec = guided && a.guide.mark;
+			const bool keep_rec = GUIDED && !new_rec && rec_row != 0xFFFFFFFFu && a.guide.keep;
 			next_meta = (bounce + 1u) | (nee_samplable ? kMetaPrevNee : 0u) | (stop_after ? kMetaStopAfter : 0u) |
-			            (guided && a.guide.mark ? kMetaGuideRec : 0u) | (sid << kMetaSceneShift);
+			            (new_rec ? kMetaGuideRec : 0u) | (keep_rec ? kMetaGuideOpen : 0u) | (sid << kMetaSceneShift);
 		}
 
 		uint32_t slot = 0;
@@ -963,6 +992,10 @@ shade_kernel(ShadeArgs a)
 				a.next.gf0[slot] = fr[0];
 				a.next.gf1[slot] = make_float4(f1.x, f1.y, f1.z, bs.cos / guided_pdf);
 			}
+			else if(GUIDED && (next_meta & kMetaGuideOpen))
+			{
+				a.next.gf0[slot] = make_float4(__uint_as_float(rec_row), rec_scale, 0.0f, 0.0f);
+			}
 		}
 		else
 		{
@@ -982,7 +1015,12 @@ shade_kernel(ShadeArgs a)
 			}
 			if(GUIDED && a.shadow.t)
 			{
-				a.shadow.t[k] = make_float4(__uint_as_float(train_row), sh_train, __uint_as_float(nee_row), nee_w);
+				// credited when the next iteration's trace finds the segment unoccluded, if that
+				// trace comes before the training step
+				const bool credit = rec_row != 0xFFFFFFFFu && a.guide.nee_credit;
+				a.shadow.t[k] = make_float4(__uint_as_float(credit ? rec_row : 0xFFFFFFFFu),
+				                            credit ? luminance(sh_c) * rec_scale : 0.0f,
+				                            __uint_as_float(nee_row), nee_w);
 			}
 			if(!continues && film.filter != PG_FILTER_BOX)
 			{
@@ -1370,7 +1408,8 @@ void RenderScene::ensure_guiding(uint32_t capacity)
 			m_gf0[b].resize(capacity);
 			m_gf1[b].resize(capacity);
 		}
-		m_st.resize(capacity);
+		m_st[0].resize(capacity);
+		m_st[1].resize(capacity);
 		m_gmap.resize(capacity);
 		m_gfeat.resize(static_cast<std::size_t>(capacity) * 8);
 		m_graw.resize(static_cast<std::size_t>(capacity) * guide::kMixFloats);
@@ -2063,7 +2102,9 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		}
 		if(training)
 		{
-			sqs[1].t = m_st.get();   // NEE records of the odd iterations, which make the training samples
+			// NEE records name the training samples their unoccluded contribution is credited to
+			sqs[0].t = m_st[0].get();
+			sqs[1].t = m_st[1].get();
 		}
 		gargs.map = m_gmap.get();
 		gargs.feat = m_gfeat.get();
@@ -2082,26 +2123,40 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 	}
 	RenderCounters* const d_counters = m_counters.get();
 	// The NEE segments made by an iteration's shading are traced by the next iteration's
-	// trace_kernel together with its closest-hit rays (one launch, one tail). Training follows
-	// the same rhythm: an even iteration marks its guided vertices, the odd one after it makes
-	// their training samples (the radiance found at the next vertex plus its NEE, whose segments
-	// the following even iteration's trace resolves), and that even iteration ends with one Adam
-	// step on them -- one step per pair of iterations.
-	GuideArgs gargs_of[2] = {gargs, gargs};
+	// trace_kernel together with its closest-hit rays (one launch, one tail). Training runs in
+	// periods of four iterations (position q = iteration mod 4):
+	//   q = 0  guided vertices are marked;
+	//   q = 1  the next vertex makes their training samples (the emission found there, and its
+	//          NEE) and opens them; NEE-direction samples of this iteration's guided vertices;
+	//   q = 2  open samples collect the emission and NEE their paths gather (NEE-direction samples
+	//          again);
+	//   q = 3  open samples collect the emission found; the iteration ends with one Adam step.
+	// The trace of q = 2 and q = 3 resolves the NEE of q = 1 and q = 2, so every credit lands
+	// before the step. Without training the period is two iterations (the two path buffers).
+	const int period = training ? 4 : 2;
+	GuideArgs gargs_of[4] = {gargs, gargs, gargs, gargs};
 	if(training)
 	{
-		gargs_of[0].train_cap = 0u;
-		gargs_of[0].mark = 1u;
-		gargs_of[1].mark = 0u;
+		for(int q = 0; q < 4; ++q)
+		{
+			gargs_of[q].mark = q == 0 ? 1u : 0u;
+			gargs_of[q].train_cap = (q == 1 || q == 2) ? train_cap : 0u;
+			gargs_of[q].open = q >= 1 ? 1u : 0u;
+			gargs_of[q].keep = (q == 1 || q == 2) ? 1u : 0u;
+			gargs_of[q].nee_credit = (q == 1 || q == 2) ? 1u : 0u;
+		}
 	}
 
-	// The five launches of one iteration; `ev` (optional) brackets each with events.
-	auto iteration = [&](int b, cudaEvent_t* ev)
+	// The launches of one iteration at position q of the period (path buffer q & 1); `ev`
+	// (optional) brackets each with events.
+	auto iteration = [&](int q, cudaEvent_t* ev)
 	{
+		const int b = q & 1;
 		const PathBuffers& cur = buf[b];
 		const PathBuffers& nxt = buf[1 - b];
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[0], st)); }
-		prepare_kernel<<<1, 32, 0, st>>>(m_counters.get(), capacity, static_cast<uint32_t>(b));
+		// the training samples of a period start at q = 1
+		prepare_kernel<<<1, 32, 0, st>>>(m_counters.get(), capacity, q == 1 ? 1u : 0u);
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[1], st)); }
 		if(multi)
 		{
@@ -2131,7 +2186,7 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		}
 		PG_CUDA_CHECK(cudaGetLastError());
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[3], st)); }
-		const GuideArgs& gargs_b = gargs_of[b];
+		const GuideArgs& gargs_b = gargs_of[q];
 		if(guided)
 		{
 			// network inputs of this iteration's guidable vertices, then the tensor-core forward pass
@@ -2180,10 +2235,10 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[5], st)); }
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[6], st)); }
-		if(training && b == 0)
+		if(training && q == 3)
 		{
-			// one Adam step on the samples of the previous (odd) iteration, complete now that this
-			// iteration's trace has added their NEE; the new weights serve the next iterations
+			// one Adam step on the period's samples, complete now; the new weights serve the
+			// next period
 			PG_CUDA_CHECK(cudaMemsetAsync(m_gscalars.get(), 0, sizeof(float), st));
 			guide::launch_gradients(m_gparams.get(), m_gimage.get(), m_tfeat.get(), m_tdirw.get(), train_cap,
 			                        m_traw.get(), reinterpret_cast<__nv_bfloat16*>(m_tacts.get()), m_ggrads.get(),
@@ -2269,14 +2324,16 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 
 	if(params.mode == PG_RENDER_GRAPH)
 	{
-		// One graph = two iterations (ping -> pong -> ping). The launch sequence only depends on
-		// whether guiding and training run, so the executable graph of the previous render is
-		// updated with this render's kernel arguments and instantiated again only when its
-		// topology changed.
+		// One graph = one period: two iterations (ping -> pong -> ping), four when training. The
+		// launch sequence only depends on whether guiding and training run, so the executable
+		// graph of the previous render is updated with this render's kernel arguments and
+		// instantiated again only when its topology changed.
 		cudaGraph_t graph;
 		PG_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-		iteration(0, nullptr);
-		iteration(1, nullptr);
+		for(int q = 0; q < period; ++q)
+		{
+			iteration(q, nullptr);
+		}
 		PG_CUDA_CHECK(cudaStreamEndCapture(st, &graph));
 		const int key = (guided ? 1 : 0) | (training ? 2 : 0) | (multi ? 4 : 0);
 		bool updated = false;
@@ -2310,7 +2367,7 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 			{
 				PG_CUDA_CHECK(cudaGraphLaunch(exec, st));
 			}
-			iterations += 2ull * batch;
+			iterations += static_cast<unsigned long long>(period) * batch;
 			PG_CUDA_CHECK(cudaMemcpyAsync(host_counters, m_counters.get(), sizeof(RenderCounters), cudaMemcpyDeviceToHost, st));
 			PG_CUDA_CHECK(cudaStreamSynchronize(st));
 			done = host_counters->next_path >= host_counters->total_paths && host_counters->n_next == 0 &&
@@ -2338,11 +2395,9 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		for(cudaEvent_t& e : ev) { PG_CUDA_CHECK(cudaEventCreate(&e)); }
 		PG_CUDA_CHECK(cudaEventRecord(e0, st));
 		add_box_weights();
-		int b = 0;
 		while(!done && iterations < max_iterations)
 		{
-			iteration(b, timing ? ev : nullptr);
-			b = 1 - b;
+			iteration(static_cast<int>(iterations % static_cast<unsigned long long>(period)), timing ? ev : nullptr);
 			++iterations;
 			PG_CUDA_CHECK(cudaMemcpyAsync(host_counters, m_counters.get(), sizeof(RenderCounters), cudaMemcpyDeviceToHost, st));
 			PG_CUDA_CHECK(cudaStreamSynchronize(st));
@@ -2387,8 +2442,8 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		                                         (params.refine_mode == PG_REFINE_ITERATIVE ? 1ull : 0ull) +
 		                                         (guided ? 2ull : 0ull);
 		const unsigned long long per_step = training ? (m_guide_params.clamp > 0.0f ? 8ull : 6ull) : 0ull;
-		// + one training step per even iteration, + the film's box-weight or splat launch
-		m_last_launches = iterations * per_iteration + (iterations + 1ull) / 2ull * per_step + 1ull;
+		// + one training step per period of four iterations, + the film's box-weight or splat launch
+		m_last_launches = iterations * per_iteration + iterations / 4ull * per_step + 1ull;
 	}
 	m_last_counts[0] = final_counters.nodes_closest;
 	m_last_counts[1] = final_counters.tris_closest;

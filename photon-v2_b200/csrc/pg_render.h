@@ -284,6 +284,9 @@ struct GuideArgs
 	float4*         train_dirw = nullptr; // [batch]: direction, weight
 	uint32_t        train_cap = 0;        // 0: no training samples recorded
 	uint32_t        mark = 0;             // 1: guided vertices await their training sample at the next vertex
+	uint32_t        open = 0;             // 1: open training records collect this iteration's emission
+	uint32_t        keep = 0;             // 1: open records stay open into the next iteration
+	uint32_t        nee_credit = 0;       // 1: this iteration's NEE records credit training samples
 	float           alpha = 0.0f;         // 0: guiding off
 	float           lo[3] = {0, 0, 0};    // scene bound, for the position features
 	float           rcp[3] = {1, 1, 1};
@@ -297,6 +300,7 @@ constexpr uint32_t kMetaBounceMask = 0xFFu;
 constexpr uint32_t kMetaPrevNee = 1u << 8;      // the previous vertex used NEE (MIS applies)
 constexpr uint32_t kMetaStopAfter = 1u << 9;    // Russian roulette ended the path after this hit
 constexpr uint32_t kMetaGuideRec = 1u << 10;    // gf0/gf1 hold a guided vertex awaiting its training sample
+constexpr uint32_t kMetaGuideOpen = 1u << 11;   // gf0 holds an open training record (row, weight scale)
 constexpr uint32_t kTargetFinal = 0x80000000u;
 
 // Launcher implemented in pg_trace.cu (FMA-enabled traversal kernels); min_idle is the
@@ -432,7 +436,7 @@ private:
 	bool m_guide_ready = false;
 	float m_bound_lo[3] = {0, 0, 0}, m_bound_rcp[3] = {1, 1, 1};
 	DeviceBuffer<float4>   m_gf0[2], m_gf1[2];
-	DeviceBuffer<float4>   m_st;
+	DeviceBuffer<float4>   m_st[2];
 	DeviceBuffer<uint32_t> m_gmap;
 	DeviceBuffer<float>    m_gfeat, m_graw;
 	DeviceBuffer<float>    m_tfeat, m_traw;
