@@ -178,7 +178,9 @@ mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restr
 				}
 				mma_commit(bar);
 			}
-			const bool ok = mbar_wait(bar, phase);
+			// one thread polls the barrier; the others wait at the block barrier, which issues no
+			// instructions while the MMAs run
+			const bool ok = tid == 0 ? mbar_wait(bar, phase) : true;
 			if(__syncthreads_or(ok ? 0 : 1))
 			{
 				// the tensor cores did not report back: one more bounded wait for this phase so

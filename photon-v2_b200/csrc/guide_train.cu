@@ -447,7 +447,9 @@ backward_tc_kernel(const float* __restrict__ params, const float* __restrict__ f
 			}
 			mma_commit(bar);
 		}
-		const bool ok = mbar_wait(bar, phase);
+		// one thread polls the barrier; the others wait at the block barrier, which issues no
+		// instructions while the MMAs run
+		const bool ok = tid == 0 ? mbar_wait(bar, phase) : true;
 		if(__syncthreads_or(ok ? 0 : 1))
 		{
 			if(!ok)
