@@ -323,12 +323,14 @@ def city(width: int = 1920, height: int = 1080, spp: int = 1024, max_bounces: in
 
 
 def slit_room(width: int = 1024, height: int = 1024, spp: int = 64, max_bounces: int = 10,
-              num_boxes: int = 166_667, seed: int = 3, estimator: str = "bneept") -> Scene:
+              num_boxes: int = 166_667, seed: int = 3, estimator: str = "bneept",
+              glass_fraction: float = 0.3) -> Scene:
     """Learned-guiding workload: a 10 x 10 x 4 room filled with seeded random furniture boxes
     (12 triangles each; 166,667 boxes = 2M triangles), lit only by a 1 x 1 quad light behind a
     dividing wall that has a single 0.05-wide vertical slit. 70 % of the boxes are Lambertian,
     30 % rough GGX glass (IOR 1.5, roughness 0.1). Almost all light enters the room through the
-    slit, so BSDF sampling rarely finds it: the case path guiding is for."""
+    slit, so BSDF sampling rarely finds it: the case path guiding is for. glass_fraction 0 makes
+    every box Lambertian (the same boxes: the random draws do not change)."""
     rng = np.random.default_rng(seed)
     # room shell, faces pointing inwards
     shell = boxes_axis_aligned(np.array([[0.0, 0.0, 0.0]]), np.array([[10.0, 4.0, 10.0]]))[:, [0, 2, 1]]
@@ -343,13 +345,15 @@ def slit_room(width: int = 1024, height: int = 1024, spp: int = 64, max_bounces:
     k = int(num_boxes)
     largest = float(np.clip(0.25 * (2000.0 / max(k, 1)) ** (1.0 / 3.0), 0.04, 0.25))
     size = rng.uniform(0.08 * largest, largest, (k, 3)) * np.array([1.0, 1.6, 1.0])
-    lo = np.stack([rng.uniform(0.1, 7.8, k), np.where(rng.random(k) < 0.6, 0.0, rng.uniform(0.0, 3.5, k)),
+    # boxes "on the floor" stand 1 mm above it: a box bottom in the floor's plane would make the
+    # closest hit of a ray inside a glass box an arbitrary pick between two coplanar triangles
+    lo = np.stack([rng.uniform(0.1, 7.8, k), np.where(rng.random(k) < 0.6, 1e-3, rng.uniform(0.0, 3.5, k)),
                    rng.uniform(0.1, 9.9, k)], 1)
     near_camera = (lo[:, 0] < 1.6) & (lo[:, 2] < 1.6)
     lo[near_camera, 0] += 1.6
     hi = np.minimum(lo + size, np.array([7.9, 3.95, 9.95]))
     boxes = boxes_axis_aligned(lo, hi).reshape(k, 12, 3, 3)
-    glass = rng.random(k) < 0.3
+    glass = rng.random(k) < glass_fraction
     groups = [
         MeshGroup(np.concatenate([shell, wall]).astype(np.float32), Material("matte", albedo=(0.7, 0.7, 0.7))),
         MeshGroup(boxes[~glass].reshape(-1, 3, 3), Material("matte", albedo=(0.6, 0.55, 0.5))),

@@ -62,6 +62,11 @@ WORKLOADS = {
                                                       max_bounces=10), 65536, 10),
     # the slit-light room, full 2M triangles with its dielectric boxes, 32 x 32
     "slit_room_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10), 65536, 10),
+    # the same room with every box Lambertian, and with glass at depth 2: light through the slit
+    # without the caustics of the glass boxes, whose rare, very bright paths make the full room's
+    # image mean converge slowly
+    "slit_room_matte_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10, glass_fraction=0.0), 16384, 10),
+    "slit_room_depth2_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 2), 262144, 2),
     # a 40 x 40-block tile of the many-light city (174,802 triangles) with 1,000 lights, depth 12
     "city_tile_bneept": (lambda spp: scenes.city(64, 64, spp, 12, blocks=40, num_lights=1000), 16384, 12),
 }

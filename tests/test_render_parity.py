@@ -99,6 +99,9 @@ LARGE_WORKLOADS = {
                         65536, 1e-3),
     # 2,000,042 triangles, light through a 0.05-wide slit, 30 % rough glass boxes, depth 10, 32 x 32
     "slit_room_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10), 65536, None),
+    # the same room with every box Lambertian (no caustics), and with its glass at depth 2
+    "slit_room_matte_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10, glass_fraction=0.0), 16384, None),
+    "slit_room_depth2_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 2), 262144, None),
     # 174,802 triangles, 1,000 lights of lognormal radiance, GGX roughness 0.02-0.8, depth 12, 64 x 64
     "city_tile_bneept": (lambda spp: scenes.city(64, 64, spp, 12, blocks=40, num_lights=1000), 16384, None),
 }
@@ -120,6 +123,21 @@ def _block(a, k):
     return a.reshape(h // k, k, w // k, k, c).mean(axis=(1, 3))
 
 
+def _mean_spread(scene, spp, seeds=8):
+    """Relative standard deviation, per channel, of the image mean of spp-sample renders over
+    seeds: the noise of a reference render's mean, measured on the GPU."""
+    import photon_gpu
+
+    with photon_gpu.RenderScene(scene) as rs:
+        means = []
+        for k in range(seeds):
+            rs.clear()
+            rs.render(spp, max_bounces=scene.max_bounces, seed=500 + k)
+            means.append(rs.film(with_sums=False)[0].mean(axis=(0, 1)))
+    m = np.asarray(means, np.float64)
+    return m.std(axis=0, ddof=1) / m.mean(axis=0)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(LARGE_WORKLOADS))
 def test_benchmarked_geometry_matches_reference(gpu_lib, tmp_path, name):
@@ -128,10 +146,15 @@ def test_benchmarked_geometry_matches_reference(gpu_lib, tmp_path, name):
     renders of 16,384-65,536 spp. The GPU side renders 4 x the reference's samples, so the
     difference is mostly the reference's own noise. A systematic difference (bias) survives
     averaging, noise does not: relMSE of 8 x 8-block means <= 1e-3 (64 x less noise) and
-    per-channel means within 1 %. Where the reference render is converged enough (the 1M-triangle
-    scene) relMSE <= 1e-3 holds at full resolution too; in the slit room and the city, light found
-    through a 5 cm slit or from 1,000 small lights on near-mirror GGX leaves a 16K-65K-spp
-    reference with per-pixel noise above that (its full-resolution relMSE is printed)."""
+    per-channel means within 1 %, or within 4 standard deviations of the difference where the
+    image mean itself is that noisy: the spread of the mean over 8 GPU renders at the reference's
+    spp gives the reference's (sigma) and the GPU image's (sigma / 2). That is the case in the slit
+    room with its glass, where rare paths through glass boxes lit through the slit carry most of
+    the error (sigma ~2 % at 65,536 spp); its glass-free and depth-2 variants hold the 1 % bar.
+    Where the reference render is converged enough (the 1M-triangle scene) relMSE <= 1e-3 holds
+    at full resolution too; in the slit room and the city, light found through a 5 cm slit or
+    from 1,000 small lights on near-mirror GGX leaves a 16K-65K-spp reference with per-pixel
+    noise above that (its full-resolution relMSE is printed)."""
     d = np.load(IMAGES)
     ref = d[name]
     factory, spp, full_bar = LARGE_WORKLOADS[name]
@@ -142,9 +165,12 @@ def test_benchmarked_geometry_matches_reference(gpu_lib, tmp_path, name):
     err = rel_mse(img, ref)
     err_blocks = rel_mse(_block(img, 8), _block(ref, 8))
     means = img.mean(axis=(0, 1)) / ref.mean(axis=(0, 1))
-    print(f"{name}: relMSE {err:.2e}, 8x8-block relMSE {err_blocks:.2e}, mean ratio {means}")
+    sigma = _mean_spread(factory(1), spp)
+    bar = np.maximum(0.01, 4.0 * sigma * np.sqrt(1.0 + 1.0 / 4.0))
+    print(f"{name}: relMSE {err:.2e}, 8x8-block relMSE {err_blocks:.2e}, mean ratio {means}, "
+          f"relative sigma of a {spp}-spp mean {sigma}, bar {bar}")
     assert err_blocks <= 1e-3, f"block relMSE {err_blocks:.3e}"
-    assert np.all(np.abs(means - 1.0) < 0.01), f"channel means differ: {means}"
+    assert np.all(np.abs(means - 1.0) < bar), f"channel means differ: {means} (bar {bar})"
     if full_bar is not None:
         assert err <= full_bar, f"relMSE {err:.3e}"
 
