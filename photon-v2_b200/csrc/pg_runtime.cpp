@@ -62,14 +62,18 @@ cudaStream_t library_stream()
 	return streams[dev];
 }
 
-void require_same_device(int owner_device, const char* what)
+void check_same_device(int owner_device, int current, const char* what)
 {
-	const int dev = current_device();
-	if(dev != owner_device)
+	if(current != owner_device)
 	{
 		throw Error(PG_ERR_INVALID_ARGUMENT, std::string(what) + " lives on device " + std::to_string(owner_device) +
-		            " but device " + std::to_string(dev) + " is current; make its device current first");
+		            " but device " + std::to_string(current) + " is current; make its device current first");
 	}
+}
+
+void require_same_device(int owner_device, const char* what)
+{
+	check_same_device(owner_device, current_device(), what);
 }
 
 int sm_count()

@@ -80,6 +80,8 @@ cudaStream_t library_stream();
 // scenes) stay on the device that was current when they were created, and every call on them
 // must be made with that device current.
 void require_same_device(int owner_device, const char* what);
+// The comparison itself, for a given current device.
+void check_same_device(int owner_device, int current, const char* what);
 
 // Thread-safe id -> object table, ids start at 1 (0 is never valid).
 template<typename T>
