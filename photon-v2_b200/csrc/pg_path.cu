@@ -29,6 +29,11 @@ namespace
 {
 
 constexpr int kShadeBlock = 128;
+// Iterations per training period of a guided render that trains (even: the path buffers alternate).
+// Periods of 6 and 8 iterations measured the same equal-time ratio on the slit room within the
+// run-to-run spread, with fewer training steps.
+constexpr int kTrainPeriod = 4;
+static_assert(kTrainPeriod >= 4 && kTrainPeriod % 2 == 0, "training period");
 constexpr float kClampMax = 1e9f;
 
 // ---------------------------------------------------------------------------------------------
@@ -2124,26 +2129,28 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 	RenderCounters* const d_counters = m_counters.get();
 	// The NEE segments made by an iteration's shading are traced by the next iteration's
 	// trace_kernel together with its closest-hit rays (one launch, one tail). Training runs in
-	// periods of four iterations (position q = iteration mod 4):
-	//   q = 0  guided vertices are marked;
-	//   q = 1  the next vertex makes their training samples (the emission found there, and its
-	//          NEE) and opens them; NEE-direction samples of this iteration's guided vertices;
-	//   q = 2  open samples collect the emission and NEE their paths gather (NEE-direction samples
-	//          again);
-	//   q = 3  open samples collect the emission found; the iteration ends with one Adam step.
-	// The trace of q = 2 and q = 3 resolves the NEE of q = 1 and q = 2, so every credit lands
-	// before the step. Without training the period is two iterations (the two path buffers).
-	const int period = training ? 4 : 2;
-	GuideArgs gargs_of[4] = {gargs, gargs, gargs, gargs};
-	if(training)
+	// periods of P = kTrainPeriod iterations (position q = iteration mod P):
+	//   q = 0        guided vertices are marked;
+	//   q = 1        the next vertex makes their training samples (the emission found there, and
+	//                its NEE) and opens them;
+	//   1 <= q < P-1 open samples collect the emission and NEE their paths gather; guided vertices
+	//                also record their NEE directions as samples;
+	//   q = P-1      open samples collect the emission found; the iteration ends with one Adam step.
+	// The trace of q = 2 ... P-1 resolves the NEE of q = 1 ... P-2, so every credit lands before
+	// the step. Without training the period is two iterations (the two path buffers).
+	const int period = training ? kTrainPeriod : 2;
+	GuideArgs gargs_of[kTrainPeriod];
+	for(int q = 0; q < kTrainPeriod; ++q)
 	{
-		for(int q = 0; q < 4; ++q)
+		gargs_of[q] = gargs;
+		if(training)
 		{
+			const bool mid = q >= 1 && q <= kTrainPeriod - 2;
 			gargs_of[q].mark = q == 0 ? 1u : 0u;
-			gargs_of[q].train_cap = (q == 1 || q == 2) ? train_cap : 0u;
+			gargs_of[q].train_cap = mid ? train_cap : 0u;
 			gargs_of[q].open = q >= 1 ? 1u : 0u;
-			gargs_of[q].keep = (q == 1 || q == 2) ? 1u : 0u;
-			gargs_of[q].nee_credit = (q == 1 || q == 2) ? 1u : 0u;
+			gargs_of[q].keep = mid ? 1u : 0u;
+			gargs_of[q].nee_credit = mid ? 1u : 0u;
 		}
 	}
 
@@ -2235,7 +2242,7 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[5], st)); }
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[6], st)); }
-		if(training && q == 3)
+		if(training && q == kTrainPeriod - 1)
 		{
 			// one Adam step on the period's samples, complete now; the new weights serve the
 			// next period
@@ -2442,8 +2449,8 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		                                         (params.refine_mode == PG_REFINE_ITERATIVE ? 1ull : 0ull) +
 		                                         (guided ? 2ull : 0ull);
 		const unsigned long long per_step = training ? (m_guide_params.clamp > 0.0f ? 8ull : 6ull) : 0ull;
-		// + one training step per period of four iterations, + the film's box-weight or splat launch
-		m_last_launches = iterations * per_iteration + iterations / 4ull * per_step + 1ull;
+		// + one training step per training period, + the film's box-weight or splat launch
+		m_last_launches = iterations * per_iteration + iterations / kTrainPeriod * per_step + 1ull;
 	}
 	m_last_counts[0] = final_counters.nodes_closest;
 	m_last_counts[1] = final_counters.tris_closest;
