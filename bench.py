@@ -249,7 +249,7 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 6
     `warmup_renders` renders (training time reported apart) and keep training; `guided_frozen`
     renders with the trained network and no further training. alpha: the probability of sampling
     the learned mixture at a guided vertex. A ratio below 1 means guiding reaches the target
-    sooner; the north star's target is a ratio of at most 0.5.
+    sooner; the target is a ratio of at most 0.5.
     """
     import photon_gpu
 
