@@ -2177,8 +2177,8 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		}
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[2], st)); }
 		const ShadowQueue& sq = sqs[b];   // this iteration's NEE segments
-		// closest hits of this iteration and the previous iteration's NEE segments (whose training
-		// samples, in an even iteration of a training render, gain their unoccluded NEE here)
+		// closest hits of this iteration and the previous iteration's NEE segments (whose
+		// unoccluded contributions, in a training render, are also credited to training samples)
 		launch_trace(m_dev, d_counters, cur.ray_o, cur.ray_d, m_hits.get(), sqs[1 - b], cur.rad, film, refill, st,
 		             counting, cur.meta, multi ? &bview : nullptr, sqs[1 - b].t ? m_tdirw.get() : nullptr);
 		if(multi)
