@@ -61,7 +61,7 @@ WORKLOADS = {
     "c2_ggx1m_bneept": (lambda spp: scenes.ggx_sphere(level=8, width=64, height=64, spp=spp,
                                                       max_bounces=10), 65536, 10),
     # the slit-light room, full 2M triangles with its dielectric boxes, 32 x 32
-    "slit_room_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10), 65536, 10),
+    "slit_room_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10), 262144, 10),
     # the same room with every box Lambertian, and with glass at depth 2: light through the slit
     # without the caustics of the glass boxes, whose rare, very bright paths make the full room's
     # image mean converge slowly

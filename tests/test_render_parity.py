@@ -98,7 +98,7 @@ LARGE_WORKLOADS = {
     "c2_ggx1m_bneept": (lambda spp: scenes.ggx_sphere(level=8, width=64, height=64, spp=spp, max_bounces=10),
                         65536, 1e-3),
     # 2,000,042 triangles, light through a 0.05-wide slit, 30 % rough glass boxes, depth 10, 32 x 32
-    "slit_room_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10), 65536, None),
+    "slit_room_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10), 262144, None),
     # the same room with every box Lambertian (no caustics), and with its glass at depth 2
     "slit_room_matte_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 10, glass_fraction=0.0), 16384, None),
     "slit_room_depth2_bneept": (lambda spp: scenes.slit_room(32, 32, spp, 2), 262144, None),
