@@ -141,8 +141,24 @@ PG_HD float mixture_pdf(const Mixture& m, V3 w)
 	return p;
 }
 
-// Samples one lobe by u0, then a direction from it (W. Jakob, "Numerically stable sampling of
-// the von Mises Fisher distribution on S2", 2012) from (u1, u2).
+// A direction from one vMF lobe (mean n, concentration k) by (u1, u2) (W. Jakob, "Numerically
+// stable sampling of the von Mises Fisher distribution on S2", 2012).
+PG_HD V3 vmf_sample(V3 n, float k, float u1, float u2)
+{
+	const float w = 1.0f + logf(fmaxf(u1 + (1.0f - u1) * expf(-2.0f * k), 1e-30f)) / k;
+	const float s = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+	const float phi = 2.0f * kPi * u2;
+	const V3 local = v3(s * cosf(phi), s * sinf(phi), w);
+	// orthonormal basis around mu (Duff et al. 2017)
+	const float sign = n.z >= 0.0f ? 1.0f : -1.0f;
+	const float a = -1.0f / (sign + n.z);
+	const float b = n.x * n.y * a;
+	const V3 t = v3(1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x);
+	const V3 bt = v3(b, sign + n.y * n.y * a, -n.y);
+	return normalize(t * local.x + bt * local.y + n * local.z);
+}
+
+// Samples one lobe by u0, then a direction from it by (u1, u2).
 PG_HD V3 mixture_sample(const Mixture& m, float u0, float u1, float u2)
 {
 	int j = 0;
@@ -152,19 +168,7 @@ PG_HD V3 mixture_sample(const Mixture& m, float u0, float u1, float u2)
 		++j;
 		acc += m.w[j];
 	}
-	const float k = m.kappa[j];
-	const float w = 1.0f + logf(fmaxf(u1 + (1.0f - u1) * expf(-2.0f * k), 1e-30f)) / k;
-	const float s = sqrtf(fmaxf(0.0f, 1.0f - w * w));
-	const float phi = 2.0f * kPi * u2;
-	const V3 local = v3(s * cosf(phi), s * sinf(phi), w);
-	// orthonormal basis around mu (Duff et al. 2017)
-	const V3 n = m.mu[j];
-	const float sign = n.z >= 0.0f ? 1.0f : -1.0f;
-	const float a = -1.0f / (sign + n.z);
-	const float b = n.x * n.y * a;
-	const V3 t = v3(1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x);
-	const V3 bt = v3(b, sign + n.y * n.y * a, -n.y);
-	return normalize(t * local.x + bt * local.y + n * local.z);
+	return vmf_sample(m.mu[j], m.kappa[j], u1, u2);
 }
 
 }// end namespace guide

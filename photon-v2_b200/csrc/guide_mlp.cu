@@ -92,12 +92,6 @@ __device__ __forceinline__ void store_row8(unsigned char* buf, uint32_t r, uint3
 
 // ---- the fused forward kernel
 
-__device__ __forceinline__ float fast_blob(float s, int bin)
-{
-	const float z = (s - (static_cast<float>(bin) + 0.5f) * (1.0f / kBins)) * kBins;
-	return __expf(-0.5f * z * z);
-}
-
 __global__ void __launch_bounds__(kThreads, 2)
 mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restrict__ features,
                    uint32_t n_max, const uint32_t* __restrict__ d_n, float* __restrict__ out_raw,
@@ -204,14 +198,33 @@ mlp_forward_kernel(const unsigned char* __restrict__ image, const float* __restr
 			const int i0 = half == 0 ? 0 : 4, i1 = half == 0 ? 4 : kInputs;
 			for(int i = i0 + static_cast<int>(part); i < i1; i += kParts)
 			{
+				// the input by selects, so that f stays in registers (a run-time index would put
+				// it in local memory)
+				float fi = f[0];
+				#pragma unroll
+				for(int q = 1; q < kInputs; ++q)
+				{
+					fi = i == q ? f[q] : fi;
+				}
+				// Its 32 bins g_b = exp(-z_b^2 / 2), z_b = 32 fi - (b + 1/2). Per 8-bin chunk one
+				// exponential gives g at the chunk's first bin and one the ratio to the next bin,
+				// g_{b+1} / g_b = exp(z_b - 1/2), which shrinks by e^-1 per bin: two multiplies per
+				// further bin. Where the chunk's first bin underflows to 0, every bin of the chunk
+				// is below 1e-8.
+				const float s32 = fi * static_cast<float>(kBins) - 0.5f;
 				#pragma unroll
 				for(int c = 0; c < kBins / 8; ++c)
 				{
+					const float z0 = s32 - static_cast<float>(c * 8);
+					float g = __expf(-0.5f * z0 * z0);
+					float ratio = __expf(z0 - 0.5f);
 					float v[8];
 					#pragma unroll
 					for(int j = 0; j < 8; ++j)
 					{
-						v[j] = valid ? fast_blob(f[i], c * 8 + j) : 0.0f;
+						v[j] = valid ? g : 0.0f;
+						g *= ratio;
+						ratio *= 0.36787944117144233f;   // e^-1
 					}
 					store_row8(act_in, r, static_cast<uint32_t>((i - i0) * kBins + c * 8), v);
 				}

@@ -582,12 +582,20 @@ backward_tc_kernel(const float* __restrict__ params, const float* __restrict__ f
 		{
 			st_bf16(gt, core_offset_lbo(static_cast<uint32_t>(o), tid, kLboGT), g[o]);
 		}
+		// unrolled over the inputs so that f7 stays in registers (indexed at run time it went to
+		// local memory)
+		#pragma unroll
 		for(int half = 0; half < 2; ++half)
 		{
-			const int k0 = half * 128, k1 = half == 0 ? 128 : kIn;
-			for(int k = k0; k < k1; ++k)
+			const int k0 = half * 128;
+			#pragma unroll
+			for(int i = half * 4; i < (half == 0 ? 4 : kInputs); ++i)
 			{
-				st_bf16(xt, core_offset_lbo(static_cast<uint32_t>(k - k0), tid, kLboXT), one_blob(f7[k / kBins], k % kBins));
+				#pragma unroll 8
+				for(int b = 0; b < kBins; ++b)
+				{
+					st_bf16(xt, core_offset_lbo(static_cast<uint32_t>(i * kBins + b - k0), tid, kLboXT), one_blob(f7[i], b));
+				}
 			}
 			if(half == 1)
 			{

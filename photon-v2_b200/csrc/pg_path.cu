@@ -416,17 +416,18 @@ __device__ __noinline__ float guide_pdf(const float* __restrict__ mix, V3 w)
 
 __device__ __noinline__ V3 guide_sample(const float* __restrict__ mix, float u0, float u1, float u2)
 {
+	// the lobe as guide::mixture_sample picks it (the first whose running weight sum exceeds u0),
+	// then only that lobe's mean and concentration are loaded: no local copy of the mixture
 	const float2* q = reinterpret_cast<const float2*>(mix);
-	guide::Mixture m;
-	#pragma unroll
-	for(int j = 0; j < guide::kLobes; ++j)
+	int j = 0;
+	float acc = __ldg(q).x;
+	while(j < guide::kLobes - 1 && u0 >= acc)
 	{
-		const float2 a = __ldg(q + 3 * j), b = __ldg(q + 3 * j + 1), c = __ldg(q + 3 * j + 2);
-		m.w[j] = a.x;
-		m.mu[j] = v3(a.y, b.x, b.y);
-		m.kappa[j] = c.x;
+		++j;
+		acc += __ldg(q + 3 * j).x;
 	}
-	return guide::mixture_sample(m, u0, u1, u2);
+	const float2 a = __ldg(q + 3 * j), b = __ldg(q + 3 * j + 1), c = __ldg(q + 3 * j + 2);
+	return guide::vmf_sample(v3(a.y, b.x, b.y), c.x, u1, u2);
 }
 
 __device__ __forceinline__ bool guidable(const Material& m)
