@@ -236,7 +236,7 @@ def rel_mse(x: np.ndarray, ref: np.ndarray, eps: float = 1e-2) -> float:
 
 def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 65536, probe_spp: int = 64,
                       target: float = 1e-3, warmup_renders: int = 8, warmup_spp: int = 32,
-                      alpha: float = 0.5) -> dict:
+                      alpha: float = 0.5, depth: int = 1) -> dict:
     """Guided vs plain GPU BNEEPT on the slit-light room (2M triangles), as time to reach a relMSE
     target against a 65,536-spp plain render of the same scene.
 
@@ -248,7 +248,8 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 6
     subtracted before the extrapolation. Guided renders start from a network trained by
     `warmup_renders` renders (training time reported apart) and keep training; `guided_frozen`
     renders with the trained network and no further training. alpha: the probability of sampling
-    the learned mixture at a guided vertex. A ratio below 1 means guiding reaches the target
+    the learned mixture at a guided vertex; depth: the vertices guided, the first `depth` of each
+    path (0: all). A ratio below 1 means guiding reaches the target
     sooner; the target is a ratio of at most 0.5.
     """
     import photon_gpu
@@ -281,6 +282,7 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 6
         ref_s = time.time() - t0
         plain = to_target(rs, 100, plain=True)
         rs.set_guiding(True, True, alpha, 3e-3, 16384)
+        rs.set_guiding_depth(depth)
         train_ms = 0.0
         for k in range(warmup_renders):
             rs.clear()
@@ -297,7 +299,7 @@ def guided_equal_time(num_boxes: int = 166_667, res: int = 256, ref_spp: int = 6
         "workload": f"slit_room {res}x{res}, {scene.num_tris} triangles, depth 10",
         "width": res, "height": res, "triangles": scene.num_tris, "max_bounces": 10,
         "reference_spp": ref_spp, "reference_s": ref_s, "target_relmse": target, "relmse_eps": 1e-2,
-        "reference_noise_relmse": floor["relmse"], "alpha": alpha,
+        "reference_noise_relmse": floor["relmse"], "alpha": alpha, "guided_depth": depth,
         "plain": plain, "guided": guided, "guided_frozen": frozen,
         "training": {"renders": warmup_renders, "spp": warmup_spp, "ms": train_ms, "final_loss": info["loss"]},
         # per-kernel device ms of one probe-spp render each (extend_ms: the merged trace launch)

@@ -272,12 +272,15 @@ PGPU_API int pgpu_scene_count(uint64_t id, uint32_t spp, uint32_t max_bounces, u
                               uint64_t seed, uint64_t* out_counts);
 
 /* Learned path guiding for the scene's subsequent BNEEPT renders (no reference counterpart). At
- * Lambertian vertices the next direction comes from the network's vMF mixture with probability
- * alpha, else from the BSDF, weighted by the one-sample MIS density, so renders stay unbiased;
- * NEE's MIS uses the same density. With train != 0 every render iteration records up to `batch`
- * (vertex, direction, incident radiance) samples and takes one Adam step (learning rate lr).
- * The network persists across renders until pgpu_scene_guide_reset. */
+ * guided Lambertian vertices the next direction comes from the network's vMF mixture with
+ * probability alpha, else from the BSDF, weighted by the one-sample MIS density, so renders stay
+ * unbiased; NEE's MIS uses the same density. With train != 0 every period of four render
+ * iterations records up to `batch` (vertex, direction, incident radiance) samples and takes one
+ * Adam step (learning rate lr). The network persists across renders until pgpu_scene_guide_reset. */
 PGPU_API int pgpu_scene_set_guiding(uint64_t id, int enabled, int train, float alpha, float lr, uint32_t batch);
+/* Which vertices are guided: the first `depth` of every path (default 1, the surfaces the camera
+ * sees; 0 = every vertex). Kept across pgpu_scene_set_guiding calls. */
+PGPU_API int pgpu_scene_set_guiding_depth(uint64_t id, uint32_t depth);
 PGPU_API int pgpu_scene_guide_reset(uint64_t id);
 /* Last render's mean training loss, guided vertices, per-kernel milliseconds of a profiled render
  * (prepare, regen, extend, shade, shadow, guide inference, guide training; 7 doubles) and the FP32

@@ -688,12 +688,23 @@ int pgpu_scene_set_guiding(uint64_t id, int enabled, int train, float alpha, flo
 			throw Error(PG_ERR_INVALID_ARGUMENT, "pgpu_scene_set_guiding: alpha must lie in (0, 1), lr > 0, "
 			                                     "0 < batch <= 2^22");
 		}
-		GuideParams g;
+		GuideParams g = r->scene->guiding();
 		g.enabled = enabled != 0;
 		g.train = train != 0;
 		g.alpha = alpha;
 		g.lr = lr;
 		g.batch = batch;
+		r->scene->set_guiding(g);
+	});
+}
+
+int pgpu_scene_set_guiding_depth(uint64_t id, uint32_t depth)
+{
+	return guarded([&]
+	{
+		auto r = get_render(id);
+		GuideParams g = r->scene->guiding();
+		g.depth = depth;
 		r->scene->set_guiding(g);
 	});
 }

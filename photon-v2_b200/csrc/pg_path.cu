@@ -73,6 +73,7 @@ enum : uint32_t
 	DIM_BSDF_0 = 6, DIM_BSDF_1 = 7, DIM_BSDF_2 = 8,
 	DIM_RR = 9,
 	DIM_GUIDE_SEL = 10, DIM_GUIDE_0 = 11, DIM_GUIDE_1 = 12, DIM_GUIDE_2 = 13,
+	DIM_TRAIN_KEEP = 14,
 };
 
 // Relative luminance of linear sRGB (CIE Y), used by Russian roulette
@@ -291,9 +292,12 @@ __device__ __forceinline__ uint32_t alloc_slot(uint32_t* counter)
 
 // ---------------------------------------------------------------------------------------------
 
-// new_samples: this iteration starts a training period's samples (position 1 of the four-iteration
-// period), so their count is reset; the samples of a period are trained on at its last iteration.
-__global__ void prepare_kernel(RenderCounters* c, uint32_t capacity, uint32_t new_samples)
+// Training periods (guided renders that train): at position 0 the count of marked vertices starts
+// afresh; at position 1 the count of samples does, and the share of marked vertices that record a
+// sample is set so that they fill record_budget rows on average. Every marked vertex is kept with
+// the same probability, whatever the material its path reaches next (taking the first rows
+// handed out would favour the classes the shading kernel processes first).
+__global__ void prepare_kernel(RenderCounters* c, uint32_t capacity, uint32_t period_pos, uint32_t record_budget)
 {
 	if(threadIdx.x != 0 || blockIdx.x != 0)
 	{
@@ -314,8 +318,14 @@ __global__ void prepare_kernel(RenderCounters* c, uint32_t capacity, uint32_t ne
 	c->fetch_shadow = 0;
 	c->guided_total += c->n_guided;
 	c->n_guided = 0;
-	if(new_samples)
+	if(period_pos == 0u)
 	{
+		c->n_marked = 0;
+	}
+	if(period_pos == 1u)
+	{
+		c->rec_keep = c->n_marked > record_budget ? static_cast<float>(record_budget) / static_cast<float>(c->n_marked)
+		                                          : 1.0f;
 		c->n_train = 0;
 	}
 	c->n_refine = 0;
@@ -578,7 +588,9 @@ shade_kernel(ShadeArgs a)
 		//      (added by the shadow kernel)
 		uint32_t train_row = 0xFFFFFFFFu;
 		float train_wfac = 0.0f;
-		if(GUIDED && (meta & kMetaGuideRec) && a.guide.train_cap)
+		// (a miss without an environment brings no light: its sample would weigh 0)
+		if(GUIDED && (meta & kMetaGuideRec) && a.guide.train_cap && (hit.x != 0xFFFFFFFFu || s.env_emitter >= 0) &&
+		   rng.u01(bounce, DIM_TRAIN_KEEP) < a.counters->rec_keep)
 		{
 			const uint32_t k = alloc_slot(&a.counters->n_train);
 			if(k < a.guide.train_cap)
@@ -964,6 +976,10 @@ shade_kernel(ShadeArgs a)
 				continues = false;
 			}
 			const bool new_rec = guided && a.guide.mark;
+			if(GUIDED && new_rec)
+			{
+				alloc_slot(&a.counters->n_marked);   // counted: sets the next iteration's keep share
+			}
 			const bool keep_rec = GUIDED && !new_rec && rec_row != 0xFFFFFFFFu && a.guide.keep;
 			next_meta = (bounce + 1u) | (nee_samplable ? kMetaPrevNee : 0u) | (stop_after ? kMetaStopAfter : 0u) |
 			            (new_rec ? kMetaGuideRec : 0u) | (keep_rec ? kMetaGuideOpen : 0u) | (sid << kMetaSceneShift);
@@ -2164,7 +2180,8 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		const PathBuffers& nxt = buf[1 - b];
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[0], st)); }
 		// the training samples of a period start at q = 1
-		prepare_kernel<<<1, 32, 0, st>>>(m_counters.get(), capacity, q == 1 ? 1u : 0u);
+		prepare_kernel<<<1, 32, 0, st>>>(m_counters.get(), capacity, training ? static_cast<uint32_t>(q) : 2u,
+		                                 train_cap / 4u * 3u);
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[1], st)); }
 		if(multi)
 		{
@@ -2198,7 +2215,9 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		if(guided)
 		{
 			// network inputs of this iteration's guidable vertices, then the tensor-core forward pass
-			guide_query_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, cur, m_hits.get(), gargs_b, max_bounces);
+			guide_query_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, cur, m_hits.get(), gargs_b,
+			                                                 m_guide_params.depth == 0u || m_guide_params.depth > max_bounces
+			                                                     ? max_bounces : m_guide_params.depth);
 			PG_CUDA_CHECK(cudaGetLastError());
 			guide::launch_forward(m_gimage.get(), m_gfeat.get(), capacity, nullptr, nullptr, m_gerr.get(), st,
 			                      &d_counters->n_guided, m_graw.get());

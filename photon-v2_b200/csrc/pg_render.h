@@ -138,6 +138,7 @@ struct GuideParams
 	float    lr = 1e-2f;
 	uint32_t batch = 16384;
 	float    clamp = 10.0f;     // training weights capped at clamp x the batch mean (0 = off)
+	uint32_t depth = 1;         // vertices guided: the first `depth` of each path (0 = every vertex)
 };
 
 // Host-side scene description handed to the renderer.
@@ -214,6 +215,8 @@ struct alignas(16) RenderCounters
 	uint32_t n_class[kOrderLists];   // closest-hit results per shading-class list (classify_kernel)
 	uint32_t n_refine;       // surface-refinery requests this iteration: one-sided escapes
 	uint32_t n_refine_mutual;// and escapes towards a light-triangle point
+	uint32_t n_marked;       // guided vertices marked for training samples in this training period
+	float    rec_keep;       // probability that a marked vertex's sample is recorded (fits the batch)
 };
 
 // Surface-refinery requests of one iteration (iterative refine mode). The shading kernel leaves

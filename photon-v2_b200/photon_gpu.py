@@ -84,6 +84,7 @@ PGPU_SIGNATURES = [
      [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _dblp]),
     ("pgpu_scene_set_guiding", ctypes.c_int,
      [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_uint32]),
+    ("pgpu_scene_set_guiding_depth", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32]),
     ("pgpu_scene_guide_reset", ctypes.c_int, [ctypes.c_uint64]),
     ("pgpu_scene_guide_info", ctypes.c_int, [ctypes.c_uint64, _f32p, _u64p, _dblp, _f32p]),
     ("pgpu_sdl_cook", ctypes.c_int,
@@ -449,6 +450,10 @@ class RenderScene:
 
     def set_guiding(self, enabled=True, train=True, alpha=0.5, lr=1e-2, batch=16384):
         _check(load().pgpu_scene_set_guiding(self.id, int(enabled), int(train), alpha, lr, batch))
+
+    def set_guiding_depth(self, depth: int) -> None:
+        """Guide the first `depth` vertices of every path (default 1; 0 = every vertex)."""
+        _check(load().pgpu_scene_set_guiding_depth(self.id, depth))
 
     def guide_reset(self):
         _check(load().pgpu_scene_guide_reset(self.id))

@@ -19,7 +19,9 @@ def _rel_mse(x, ref, eps=1e-2):
 
 
 @pytest.mark.gpu
-def test_guided_render_is_unbiased(gpu_lib):
+@pytest.mark.parametrize("depth", [1, 0])
+def test_guided_render_is_unbiased(gpu_lib, depth):
+    """depth 1 guides the surfaces the camera sees (the default), 0 every vertex."""
     import photon_gpu
 
     scene = scenes.cornell(32, 32, 1, 8)
@@ -28,6 +30,7 @@ def test_guided_render_is_unbiased(gpu_lib):
         plain = rs.film()[0]
         rs.clear()
         rs.set_guiding(True, True, 0.5, 3e-3, 16384)
+        rs.set_guiding_depth(depth)
         rs.render(8192, max_bounces=8, seed=5)
         guided = rs.film()[0]
         info = rs.guide_info()
