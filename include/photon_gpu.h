@@ -143,6 +143,18 @@ PGPU_API int pgpu_guide_train(float* params, const float* features, const float*
  *      pdfAppliedBsdfCos(3), relativeIor, cos, 0. Strict sidedness, radiance transport. */
 PGPU_API int pgpu_bsdf_eval(const float* cases, const float* normals, uint64_t n, float* out);
 
+/* Film splat of given samples through the device filter and deposit functions the renderer uses,
+ * for checking the film against the reference's HdrRgbFilm::addRgbSample
+ * (Engine/Source/Core/Filmic/HdrRgbFilm.cpp:82-123) and its sample filters
+ * (Engine/Source/Core/Filmic/SampleFilter.cpp:12-59). filter: 1 gaussian, 2 Mitchell-Netravali,
+ * 3 Blackman-Harris (the 4 x 4 filters; the box filter's samples go to their own pixel without a
+ * weight and are not splatted). samples: float32 [n][5] = raster x, raster y (pixel (i, j) covers
+ * [i, i + 1) x [j, j + 1)), r, g, b; n at most 2^26. out_sums: float64 [height][width][4] =
+ * filter-weighted R, G, B sums and the weight sum W of every pixel (developed value = RGB / W),
+ * starting from zero. The film has 1 to 2^24 pixels. */
+PGPU_API int pgpu_film_splat(uint32_t filter, uint32_t width, uint32_t height, const float* samples, uint64_t n,
+                       double* out_sums);
+
 /* ---------------------------------------------------------------------------------------------
  * Render scenes: the full BNEEPT / BVPT / BVPTDL estimators on the GPU.
  *

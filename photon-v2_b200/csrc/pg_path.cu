@@ -1129,18 +1129,34 @@ refine_kernel(DeviceScene s_single, const RenderCounters* __restrict__ c, PathBu
 namespace
 {
 
+// Alias table (Vose) over non-negative weights; out_pmf[i] = weights[i] / sum. Weights that sum to
+// zero give the uniform pmf, as the reference's piecewise-constant distribution falls back to a
+// linear CDF then (Math/Random/TPwcDistribution1D.ipp:53-74); a non-finite sum is treated the same
+// way, so that the table stays valid. Every column of a uniform table keeps itself.
 void build_alias(const std::vector<double>& weights, std::vector<float2>& out_alias, std::vector<double>& out_pmf)
 {
 	const std::size_t n = weights.size();
-	out_alias.assign(n, make_float2(1.0f, 0.0f));
+	out_alias.resize(n);
+	for(std::size_t i = 0; i < n; ++i)
+	{
+		const uint32_t self = static_cast<uint32_t>(i);
+		float fself;
+		std::memcpy(&fself, &self, 4);
+		out_alias[i] = make_float2(1.0f, fself);
+	}
 	out_pmf.assign(n, 0.0);
 	double sum = 0.0;
 	for(double w : weights)
 	{
 		sum += w;
 	}
-	if(n == 0 || !(sum > 0.0))
+	if(n == 0)
 	{
+		return;
+	}
+	if(!(sum > 0.0) || !std::isfinite(sum))
+	{
+		out_pmf.assign(n, 1.0 / static_cast<double>(n));
 		return;
 	}
 	std::vector<double> scaled(n);

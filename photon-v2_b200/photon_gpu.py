@@ -44,6 +44,8 @@ PGPU_SIGNATURES = [
     ("pgpu_trace_counts", ctypes.c_int,
      [ctypes.c_uint64, _f32p, ctypes.c_uint64, ctypes.c_int, _dblp, _dblp]),
     ("pgpu_bsdf_eval", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
+    ("pgpu_film_splat", ctypes.c_int,
+     [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _f32p, ctypes.c_uint64, _dblp]),
     ("pgpu_guide_forward", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
     ("pgpu_guide_mixture", ctypes.c_int, [_f32p, _f32p, ctypes.c_uint64, _f32p]),
     ("pgpu_guide_gradients", ctypes.c_int, [_f32p, _f32p, _f32p, _f32p, ctypes.c_uint64, _f32p, _f32p]),
@@ -209,6 +211,19 @@ def bsdf_eval(cases: np.ndarray, normals: np.ndarray) -> np.ndarray:
     _check(load().pgpu_bsdf_eval(_ptr(c, ctypes.c_float), _ptr(nrm, ctypes.c_float), c.shape[0],
                                  _ptr(out, ctypes.c_float)))
     return out
+
+
+FILM_FILTERS = {"gaussian": 1, "mitchell-netravali": 2, "blackman-harris": 3}
+
+
+def film_splat(sample_filter: str, width: int, height: int, samples: np.ndarray) -> np.ndarray:
+    """(R, G, B, W) sums float64 [height, width, 4] of samples [n, 5] = raster x, raster y, r, g, b
+    splatted through one of the 4 x 4 filters on the GPU."""
+    smp = np.ascontiguousarray(samples, np.float32).reshape(-1, 5)
+    sums = np.empty((height, width, 4), np.float64)
+    _check(load().pgpu_film_splat(FILM_FILTERS[sample_filter], width, height, _ptr(smp, ctypes.c_float), smp.shape[0],
+                                  _ptr(sums, ctypes.c_double)))
+    return sums
 
 
 def guide_forward(params: np.ndarray, features: np.ndarray) -> np.ndarray:

@@ -116,3 +116,47 @@ def test_gpu_nee_densities_match_reference(gpu_lib, count):
     exact = has & (np.abs(d["pmf"][owner] - ideal[owner]) <= 1e-6 * ideal[owner])
     rel_ref = np.abs(pdf[exact] - d["pdf_w"][exact]) / d["pdf_w"][exact]
     assert np.all(rel_ref <= tol[exact])
+
+
+def _quad_lights(radiances):
+    """Equal unit quads in a row, each its own area emitter of grey radiance r (so that their
+    fluxes stand in the ratio of the radiances)."""
+    groups = []
+    for k, r in enumerate(radiances):
+        x = 3.0 * k
+        quad = np.array([[[x, 0, 0], [x + 1, 0, 0], [x + 1, 1, 0]],
+                         [[x, 0, 0], [x + 1, 1, 0], [x, 1, 0]]], np.float32)
+        groups.append(scenes.MeshGroup(quad, scenes.BLACK, radiance=(float(r), float(r), float(r))))
+    return scenes.Scene("quad lights", 8, 8, 1, 2, cam_pos=(0.0, 0.0, -20.0), cam_dir=(0.0, 0.0, 1.0),
+                        cam_up=(0.0, 1.0, 0.0), fov_deg=40.0, groups=groups)
+
+
+@pytest.mark.gpu
+def test_gpu_pick_never_takes_zero_power_emitters(gpu_lib):
+    """The reference's PiecewiseConstantDistribution1DTest.ContinuousSampleInRange
+    (Engine/EngineTest/Source/Math/Random/distribution_test.cpp:21-44): of the weights
+    {0, 0, 1, 0, 2, 3, 0}, entries 0, 1, 3 and 6 are never sampled. As light selection: their pick
+    probability and the probability the device alias table realises for them are exactly 0, and
+    the others take 1/6, 2/6 and 3/6 (1e-6 relative)."""
+    import photon_gpu
+
+    weights = np.array([0, 0, 1, 0, 2, 3, 0], np.float64)
+    with photon_gpu.RenderScene(_quad_lights(weights)) as rs:
+        pmf, alias_pmf = rs.light_pmf()
+    zero = weights == 0
+    assert np.all(pmf[zero] == 0.0) and np.all(alias_pmf[zero] == 0.0)
+    np.testing.assert_allclose(pmf[~zero], weights[~zero] / 6.0, rtol=1e-6)
+    np.testing.assert_allclose(alias_pmf[~zero], weights[~zero] / 6.0, rtol=1e-6)
+
+
+@pytest.mark.gpu
+def test_gpu_pick_of_all_zero_powers_is_uniform(gpu_lib):
+    """The reference's PiecewiseConstantDistribution1DTest.CornerCases (distribution_test.cpp:
+    80-92): weights that are all zero give the uniform distribution, 1/3 each for three; the same
+    for three emitters of zero radiance (the device table realises it exactly)."""
+    import photon_gpu
+
+    with photon_gpu.RenderScene(_quad_lights([0.0, 0.0, 0.0])) as rs:
+        pmf, alias_pmf = rs.light_pmf()
+    np.testing.assert_allclose(pmf, 1.0 / 3.0, rtol=1e-7)
+    assert np.all(alias_pmf == 1.0 / 3.0)
