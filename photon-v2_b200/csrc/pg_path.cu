@@ -237,15 +237,30 @@ __global__ void box_weights_kernel(double* sums, uint32_t num_pixels, double spp
 	}
 }
 
+// Surfaces where a guided render samples the learned mixture: non-black matte.
+__device__ __forceinline__ bool guidable(const Material& m)
+{
+	return m.type == PG_MAT_MATTE && (m.cr > 0.0f || m.cg > 0.0f || m.cb > 0.0f);
+}
+
+// Whether guide_query_kernel gives the queue entry a network row: a hit on a guidable surface at
+// a vertex below the guiding depth, on a path that continues after it.
+__device__ __forceinline__ bool guided_vertex(const Material& m, uint32_t meta, uint32_t guide_depth)
+{
+	return !(meta & kMetaStopAfter) && (meta & kMetaBounceMask) < guide_depth && guidable(m);
+}
+
 // Lists every slot of the current queue under its shading class (kShadeClasses): 0 for a miss,
-// 1 + the material type of the hit surface, in the list of that class for this block's residue
-// (kClassLists). Lanes of one class share one atomic. `list_capacity` bounds the slots one list
-// can receive: the slots all blocks of one residue visit in the grid-stride loop.
+// 1 + the material type of the hit surface, or kGuidedClass for a vertex a guided render guides
+// (guide_depth > 0: the vertices below that bounce), in the list of that class for this block's
+// residue (kClassLists). Lanes of one class share one atomic. `list_capacity` bounds the slots one
+// list can receive: the slots all blocks of one residue visit in the grid-stride loop.
 // MULTI: the hit triangle belongs to the scene in the top bits of the slot's meta word.
 template<bool MULTI>
 __global__ void __launch_bounds__(kShadeBlock)
 classify_kernel(DeviceScene s_single, RenderCounters* __restrict__ c, const uint2* __restrict__ hits,
-                uint32_t* __restrict__ order, uint32_t list_capacity, const uint32_t* __restrict__ meta, BatchView batch)
+                uint32_t* __restrict__ order, uint32_t list_capacity, const uint32_t* __restrict__ meta, BatchView batch,
+                uint32_t guide_depth)
 {
 	const uint32_t n = c->n_total;
 	const uint32_t residue = blockIdx.x % kClassLists;
@@ -258,11 +273,13 @@ classify_kernel(DeviceScene s_single, RenderCounters* __restrict__ c, const uint
 			if constexpr(MULTI)
 			{
 				const DeviceScene& s = batch.scenes[meta[i] >> kMetaSceneShift].scene;
-				cls = min(1u + s.materials[__ldg(&s.tris[tri].material)].type, kShadeClasses - 1u);
+				cls = min(1u + s.materials[__ldg(&s.tris[tri].material)].type, kGuidedClass - 1u);
 			}
 			else
 			{
-				cls = min(1u + s_single.materials[__ldg(&s_single.tris[tri].material)].type, kShadeClasses - 1u);
+				const Material& m = s_single.materials[__ldg(&s_single.tris[tri].material)];
+				cls = guide_depth > 0u && guided_vertex(m, meta[i], guide_depth) ? kGuidedClass
+				                                                                 : min(1u + m.type, kGuidedClass - 1u);
 			}
 		}
 		const uint32_t list = cls * kClassLists + residue;
@@ -440,11 +457,6 @@ __device__ __noinline__ V3 guide_sample(const float* __restrict__ mix, float u0,
 	return guide::vmf_sample(v3(a.y, b.x, b.y), c.x, u1, u2);
 }
 
-__device__ __forceinline__ bool guidable(const Material& m)
-{
-	return m.type == PG_MAT_MATTE && (m.cr > 0.0f || m.cg > 0.0f || m.cb > 0.0f);
-}
-
 // Network inputs for every queue entry that will be shaded at a guidable vertex; entries are
 // compacted into rows (map: entry -> row).
 __global__ void __launch_bounds__(kShadeBlock)
@@ -457,10 +469,10 @@ guide_query_kernel(DeviceScene s, RenderCounters* __restrict__ c, PathBuffers cu
 		const uint2 hit = hits[i];
 		const uint32_t meta = cur.meta[i];
 		uint32_t row = 0xFFFFFFFFu;
-		if(hit.x != 0xFFFFFFFFu && !(meta & kMetaStopAfter) && (meta & kMetaBounceMask) < max_bounces)
+		if(hit.x != 0xFFFFFFFFu)
 		{
 			const LeafTri& lt = s.tris[hit.x];
-			if(guidable(s.materials[lt.material]))
+			if(guided_vertex(s.materials[lt.material], meta, max_bounces))
 			{
 				const float4 o = cur.ray_o[i];
 				const float4 d4 = cur.ray_d[i];
@@ -2126,6 +2138,10 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 
 	// learned guiding (BNEEPT only)
 	const bool guided = m_guide_params.enabled && params.estimator == PG_EST_BNEEPT;
+	// the vertices a guided render guides: those below this bounce (0: none)
+	const uint32_t guide_depth = !guided ? 0u
+	                             : (m_guide_params.depth == 0u || m_guide_params.depth > max_bounces ? max_bounces
+	                                                                                                : m_guide_params.depth);
 	const bool training = guided && m_guide_params.train;
 	GuideArgs gargs;
 	uint32_t train_cap = 0;
@@ -2218,12 +2234,12 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		if(multi)
 		{
 			classify_kernel<true><<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, m_hits.get(), m_order.get(),
-			                                                    m_order_list, cur.meta, bview);
+			                                                    m_order_list, cur.meta, bview, 0u);
 		}
 		else
 		{
 			classify_kernel<false><<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, m_hits.get(), m_order.get(),
-			                                                     m_order_list, cur.meta, bview);
+			                                                     m_order_list, cur.meta, bview, guide_depth);
 		}
 		PG_CUDA_CHECK(cudaGetLastError());
 		if(ev) { PG_CUDA_CHECK(cudaEventRecord(ev[3], st)); }
@@ -2231,9 +2247,7 @@ float RenderScene::render_pass(const RenderParams& params, double* film_sums, co
 		if(guided)
 		{
 			// network inputs of this iteration's guidable vertices, then the tensor-core forward pass
-			guide_query_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, cur, m_hits.get(), gargs_b,
-			                                                 m_guide_params.depth == 0u || m_guide_params.depth > max_bounces
-			                                                     ? max_bounces : m_guide_params.depth);
+			guide_query_kernel<<<grid, kShadeBlock, 0, st>>>(m_dev, d_counters, cur, m_hits.get(), gargs_b, guide_depth);
 			PG_CUDA_CHECK(cudaGetLastError());
 			guide::launch_forward(m_gimage.get(), m_gfeat.get(), capacity, nullptr, nullptr, m_gerr.get(), st,
 			                      &d_counters->n_guided, m_graw.get());

@@ -182,11 +182,14 @@ struct DeviceScene
 };
 
 // Shading classes of a closest-hit result: 0 = miss, then 1 + the hit surface's material type
-// (matte, conductor, dielectric, absorber). classify_kernel lists the queue slots of each class
-// so that the shading kernel's warps mostly run one material's code. Each class has kClassLists
-// lists, one per residue of the block index, so that the list counters' atomics spread over
-// kOrderLists addresses instead of queuing on five.
-constexpr uint32_t kShadeClasses = 5;
+// (matte, conductor, dielectric, absorber), and last the matte vertices that a guided render
+// guides (kGuidedClass), whose shading also evaluates and samples the learned mixture: kept apart,
+// they fill whole warps instead of making every matte warp wait on its guided lanes.
+// classify_kernel lists the queue slots of each class so that the shading kernel's warps mostly
+// run one code path. Each class has kClassLists lists, one per residue of the block index, so that
+// the list counters' atomics spread over kOrderLists addresses instead of queuing on six.
+constexpr uint32_t kShadeClasses = 6;
+constexpr uint32_t kGuidedClass = kShadeClasses - 1u;
 constexpr uint32_t kClassLists = 16;
 constexpr uint32_t kOrderLists = kShadeClasses * kClassLists;
 
