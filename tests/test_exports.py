@@ -135,3 +135,42 @@ def test_frames_load_and_save_pfm_without_a_device(tmp_path):
         assert lib.phLoadFrame(fid.value, str(tmp_path / "missing.pfm").encode()) == 0
     finally:
         lib.phDeleteFrame(fid.value)
+
+
+@pytest.mark.parametrize("filt, width, height, n, null_samples, message", [
+    (0, 4, 4, 1, False, "not one of the 4 x 4 filters"),        # box: its samples are not splatted
+    (7, 4, 4, 1, False, "not one of the 4 x 4 filters"),
+    (1, 0, 4, 1, False, "1 to 2^24 pixels"),
+    (1, 4097, 4097, 1, False, "1 to 2^24 pixels"),
+    (1, 4, 4, (1 << 26) + 1, False, "more than 2^26 samples"),
+    (1, 4, 4, 3, True, "null pointer"),
+])
+def test_film_splat_rejects_bad_input_before_device_work(filt, width, height, n, null_samples, message):
+    """pgpu_film_splat checks its filter, film size, sample count and pointers on the host, so these
+    calls fail with status 1 and the reason also on a machine without a GPU."""
+    import ctypes
+
+    import numpy as np
+
+    lib = photon_gpu.load()
+    smp = np.zeros((1, 5), np.float32)   # never read: every case is rejected first
+    sums = np.zeros(4, np.float64)
+    p_smp = None if null_samples else smp.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    status = lib.pgpu_film_splat(filt, width, height, p_smp, n, sums.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    assert status == 1
+    assert message in lib.pgpu_last_error().decode()
+
+
+def test_noalloc_rejects_oversized_batches_before_device_work():
+    """pgpu_trace_closest_noalloc refuses more rays than its static staging holds (65,536) before it
+    looks at the geometry or the device."""
+    import ctypes
+
+    import numpy as np
+
+    lib = photon_gpu.load()
+    rays = np.zeros((1, 8), np.float32)   # never read: the count is rejected first
+    status = lib.pgpu_trace_closest_noalloc(0, rays.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), 65537,
+                                            None, None, None)
+    assert status == 1
+    assert "exceed the static scratch capacity" in lib.pgpu_last_error().decode()
